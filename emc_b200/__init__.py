@@ -1,0 +1,278 @@
+"""emc_b200 -- B200 EMC engine (expand -> maximize -> compress).
+
+Python host wrapper over libemc_b200.so (C ABI in include/emc_b200.h and the
+reference-compatible include/emc.h).  The compute path is the CUDA library;
+importing this module never falls back to a CPU implementation: if the
+library is missing, ``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libemc_b200.so")
+
+GAUSS, POISSON = 0, 1
+NEAREST, TRILINEAR = 0, 1
+FP32, MIXED = 0, 1
+_NAMES = {
+    "gauss": GAUSS, "poisson": POISSON, "nearest": NEAREST, "trilinear": TRILINEAR,
+    "fp32": FP32, "mixed": MIXED,
+}
+BUF_MODEL, BUF_WEIGHT, BUF_SCALING, BUF_RESP, BUF_SLICES, BUF_TOTALRESP = range(6)
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
+          4: "device wait timed out", 5: "call out of order", 6: "data out of exact range",
+          7: "unsupported"}
+
+
+class EmcError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [("side", C.c_int32), ("likelihood", C.c_int32), ("interp", C.c_int32),
+                ("precision", C.c_int32), ("n_patterns", C.c_int64), ("n_rotations", C.c_int64),
+                ("sigma", C.c_float), ("poisson_floor", C.c_float), ("device", C.c_int32),
+                ("flags", C.c_int32)]
+
+
+class IterStats(C.Structure):
+    _fields_ = [("sum_plogp", C.c_double), ("total_loglik", C.c_double),
+                ("model_max", C.c_double), ("total_resp", C.c_double)]
+
+
+class SynthConfig(C.Structure):
+    _fields_ = [("side", C.c_int32), ("n_scatterers", C.c_int32), ("object_radius", C.c_double),
+                ("n_patterns", C.c_int64), ("mean_photons", C.c_double),
+                ("scale_sigma", C.c_double), ("beamstop_radius", C.c_double),
+                ("seed", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.isfile(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m emc_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P, I64 = C.c_void_p, C.c_int64
+        for name, args, res in [
+            ("emc_create", [P, P], C.c_int), ("emc_destroy", [P], C.c_int),
+            ("emc_set_geometry", [P, P, P, P, P], C.c_int), ("emc_set_rotations", [P, P, P], C.c_int),
+            ("emc_set_patterns", [P, P], C.c_int), ("emc_set_model", [P, P], C.c_int),
+            ("emc_set_scaling", [P, P], C.c_int), ("emc_iterate", [P, P], C.c_int),
+            ("emc_expand", [P], C.c_int), ("emc_maximize", [P], C.c_int),
+            ("emc_compress", [P], C.c_int), ("emc_synchronize", [P], C.c_int),
+            ("emc_get_model", [P, P], C.c_int), ("emc_get_scaling", [P, P], C.c_int),
+            ("emc_get_buffer", [P, C.c_int, P, C.c_size_t], C.c_int),
+            ("emc_device_buffer", [P, C.c_int, P, P], C.c_int),
+            ("emc_stream", [P], P), ("emc_active_pixels", [P], I64),
+            ("emc_last_error", [P], C.c_char_p), ("emc_status_string", [C.c_int], C.c_char_p),
+            ("emc_n_to_samples", [C.c_int], I64),
+            ("emc_generate_rotations", [C.c_int, C.c_int, P, P], I64),
+            ("emc_detector_coordinates", [C.c_int, C.c_double, C.c_double, C.c_double, P, P, P], None),
+            ("emc_synthesize", [P, P, P, P, P, P, P, P, P], C.c_int),
+            ("emc_random_model", [C.c_int, C.c_uint64, P], None),
+            ("emc_legacy_last_status", [], C.c_int),
+            ("emc_set_profiling", [P, C.c_int], C.c_int), ("emc_stage_times", [P, P], C.c_int),
+            ("emc_launch_count", [P], I64),
+        ]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _check(status, ctx=None):
+    if status != 0:
+        msg = lib().emc_last_error(ctx)
+        raise EmcError(status, msg.decode() if msg else "")
+
+
+# ------------------------------------------------------------ generators --
+
+def generate_rotations(n: int, halve: bool = True):
+    """600-cell rotation sampling (emc.c:49-363); halved to one of each +-q."""
+    L = lib()
+    R = L.emc_generate_rotations(n, int(halve), None, None)
+    q = np.zeros((R, 4), np.float32)
+    w = np.zeros(R, np.float32)
+    got = L.emc_generate_rotations(n, int(halve), _ptr(q), _ptr(w))
+    if got < 0:
+        raise RuntimeError("rotation sampling failed")
+    return q[:got], w[:got]
+
+
+def detector_coordinates(side, wavelength, pixel_size, detector_distance):
+    """Pixel coordinates with Ewald curvature (emc.c:365-393), [y*side+x]."""
+    x, y, z = (np.zeros(side * side, np.float32) for _ in range(3))
+    lib().emc_detector_coordinates(side, wavelength, pixel_size, detector_distance, _ptr(x), _ptr(y),
+                                   _ptr(z))
+    return x, y, z
+
+
+def random_model(side, seed=0):
+    m = np.zeros(side ** 3, np.float32)
+    lib().emc_random_model(side, seed, _ptr(m))
+    return m
+
+
+def synthesize(side, n_patterns, x, y, z, mean_photons=1000.0, scale_sigma=0.3,
+               beamstop_radius=0.0, n_scatterers=40, object_radius=0.3, seed=0):
+    """Seeded synthetic dataset: returns dict(model, counts, mask, rotations, scales)."""
+    sc = SynthConfig(side, n_scatterers, object_radius, n_patterns, mean_photons, scale_sigma,
+                     beamstop_radius, seed)
+    npix = side * side
+    model = np.zeros(side ** 3, np.float32)
+    counts = np.zeros((n_patterns, npix), np.float32)
+    mask = np.zeros(npix, np.int32)
+    rot = np.zeros((n_patterns, 4), np.float32)
+    scales = np.zeros(n_patterns, np.float32)
+    x, y, z = (np.ascontiguousarray(a, np.float32) for a in (x, y, z))
+    _check(lib().emc_synthesize(C.byref(sc), _ptr(x), _ptr(y), _ptr(z), _ptr(model), _ptr(counts),
+                                _ptr(mask), _ptr(rot), _ptr(scales)))
+    return dict(model=model, counts=counts, mask=mask, rotations=rot, scales=scales)
+
+
+# --------------------------------------------------------------- context --
+
+class Context:
+    """One EMC dataset resident on a GPU (include/emc_b200.h)."""
+
+    def __init__(self, side, n_patterns, n_rotations, likelihood="gauss", interp="nearest",
+                 precision="fp32", sigma=0.4, poisson_floor=1e-10, device=0):
+        cfg = Config(side, _NAMES[likelihood], _NAMES[interp], _NAMES[precision], n_patterns,
+                     n_rotations, sigma, poisson_floor, device, 0)
+        h = C.c_void_p()
+        st = lib().emc_create(C.byref(cfg), C.byref(h))
+        _check(st, None)
+        self._h = h
+        self.side, self.N, self.R = side, n_patterns, n_rotations
+        self.M = side ** 3
+        self.config = cfg
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().emc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, st):
+        _check(st, self._h)
+
+    @staticmethod
+    def _f32(a):
+        return np.ascontiguousarray(a, np.float32)
+
+    def set_geometry(self, x, y, z, mask):
+        x, y, z = (self._f32(a) for a in (x, y, z))
+        m = np.ascontiguousarray(mask, np.int32)
+        self._c(lib().emc_set_geometry(self._h, _ptr(x), _ptr(y), _ptr(z), _ptr(m)))
+
+    def set_rotations(self, q, w):
+        q, w = self._f32(q), self._f32(w)
+        assert q.shape == (self.R, 4) and w.shape == (self.R,)
+        self._c(lib().emc_set_rotations(self._h, _ptr(q), _ptr(w)))
+
+    def set_patterns(self, counts):
+        k = self._f32(counts)
+        assert k.size == self.N * self.side * self.side
+        self._c(lib().emc_set_patterns(self._h, _ptr(k)))
+
+    def set_model(self, model):
+        m = self._f32(model)
+        assert m.size == self.M
+        self._c(lib().emc_set_model(self._h, _ptr(m)))
+
+    def set_scaling(self, s):
+        s = self._f32(s)
+        assert s.size == self.N
+        self._c(lib().emc_set_scaling(self._h, _ptr(s)))
+
+    def iterate(self, stats=True):
+        if not stats:
+            self._c(lib().emc_iterate(self._h, None))
+            return None
+        st = IterStats()
+        self._c(lib().emc_iterate(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in IterStats._fields_}
+
+    def expand(self):
+        self._c(lib().emc_expand(self._h))
+
+    def maximize(self):
+        self._c(lib().emc_maximize(self._h))
+
+    def compress(self):
+        self._c(lib().emc_compress(self._h))
+
+    def synchronize(self):
+        self._c(lib().emc_synchronize(self._h))
+
+    @property
+    def active_pixels(self):
+        return int(lib().emc_active_pixels(self._h))
+
+    @property
+    def stream(self):
+        return lib().emc_stream(self._h)
+
+    def get_model(self):
+        m = np.zeros(self.M, np.float32)
+        self._c(lib().emc_get_model(self._h, _ptr(m)))
+        return m
+
+    def get_scaling(self):
+        s = np.zeros(self.N, np.float32)
+        self._c(lib().emc_get_scaling(self._h, _ptr(s)))
+        return s
+
+    def get_buffer(self, which):
+        shapes = {BUF_MODEL: (self.M,), BUF_WEIGHT: (self.M,), BUF_SCALING: (self.N,),
+                  BUF_RESP: (self.R, self.N), BUF_SLICES: (self.R, self.active_pixels),
+                  BUF_TOTALRESP: (self.R,)}
+        out = np.zeros(shapes[which], np.float32)
+        self._c(lib().emc_get_buffer(self._h, which, _ptr(out), out.nbytes))
+        return out
+
+    def set_profiling(self, on=True):
+        self._c(lib().emc_set_profiling(self._h, int(on)))
+
+    def stage_times(self):
+        """ms of [expand, maximize contraction, responsibility pass, compress, normalise]."""
+        ms = np.zeros(5, np.float32)
+        self._c(lib().emc_stage_times(self._h, _ptr(ms)))
+        return ms
+
+    @property
+    def launch_count(self):
+        return int(lib().emc_launch_count(self._h))
+
+    def device_buffer(self, which):
+        p, n = C.c_void_p(), C.c_size_t()
+        self._c(lib().emc_device_buffer(self._h, which, C.byref(p), C.byref(n)))
+        return p.value, n.value

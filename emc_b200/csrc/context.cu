@@ -1,0 +1,719 @@
+// Context API (include/emc_b200.h): one dataset resident in HBM, iterated
+// in the order of the reference's main loop (emc.c:989-1084).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/emc_b200.h"
+#include "kernels.cuh"
+#include "tc.cuh"
+
+using namespace emc;
+
+namespace {
+
+constexpr int64_t kRespChunk = 2048;  // rotations per block row of the responsibility sweeps
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+__global__ void gather_cols_kernel(const float* src, int64_t rows, int64_t ld, const int32_t* pix,
+                                   int64_t npa, float* dst) {
+  const int64_t r = blockIdx.y;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < npa;
+       j += (int64_t)gridDim.x * blockDim.x)
+    dst[r * npa + j] = src[r * ld + pix[j]];
+}
+
+__global__ void split_sum_kernel(const __half* hi, const __half* lo, int64_t R, int64_t ld,
+                                 int64_t npa, float* out) {
+  const int64_t r = blockIdx.y;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < npa;
+       j += (int64_t)gridDim.x * blockDim.x)
+    out[r * npa + j] = __half2float(hi[r * ld + j]) + __half2float(lo[r * ld + j]);
+}
+
+}  // namespace
+
+struct emc_context {
+  emc_config cfg{};
+  std::string err;
+  cudaStream_t st = nullptr;
+  int num_sms = 148;
+  int64_t N = 0, R = 0, npix = 0, M = 0, npa = 0;
+  bool mixed = false, gauss = true;
+  bool have_geom = false, have_rot = false, have_pat = false, have_model = false;
+  int stage = 0;  // 0 ready to expand, 1 expanded, 2 maximized
+  std::vector<void*> allocs;
+
+  // geometry (compact active pixels)
+  int32_t* d_pix = nullptr;
+  int32_t* d_ins = nullptr;
+  float *d_cx = nullptr, *d_cy = nullptr, *d_cz = nullptr;
+  // rotations
+  float *d_quat = nullptr, *d_rotw = nullptr;
+  // patterns
+  float* d_K = nullptr;  // [N][npa] FP32 (FP32 path)
+  double *d_patsq = nullptr, *d_patsum = nullptr;
+  // model state
+  float *d_model = nullptr, *d_weight = nullptr, *d_scaling = nullptr, *d_scaling_prev = nullptr;
+  float* d_T = nullptr;
+  double* d_rowstat = nullptr;
+  double* d_scratch = nullptr;  // reductions
+  double* d_stats = nullptr;    // [0] mean [1] max [2] plogp [3] loglik
+  // FP32 path
+  float* d_S = nullptr;   // [R][npa]
+  float* d_LL = nullptr;  // [R][N]
+  double* d_den = nullptr;
+  double* d_lse32 = nullptr;
+  double* d_plogp_part = nullptr;
+  // mixed path
+  int64_t Npad = 0, Ppad = 0, Rpad = 0, nrt = 0;
+  __half *d_Kh = nullptr, *d_Kt = nullptr, *d_Bhi = nullptr, *d_Blo = nullptr;
+  __half *d_Phi = nullptr, *d_Plo = nullptr;
+  float* d_Y = nullptr;
+  float2* d_part = nullptr;
+  double *d_lse = nullptr, *d_den2 = nullptr, *d_plogp2 = nullptr;
+  float* d_Tpart = nullptr;
+  float* d_export = nullptr;
+  CUtensorMap tmKh, tmKt, tmBhi, tmBlo, tmPhi, tmPlo;
+  TcStatus* d_status = nullptr;
+  // profiling: events at stage boundaries, kernel launch count
+  // Two event sets alternate between iterations, so the times of iteration
+  // i-1 can be read while iteration i is still queued.
+  bool prof = false;
+  cudaEvent_t ev[2][6] = {{nullptr}};
+  int cur = 0;
+  int64_t prof_iters = 0;
+  int64_t launches = 0;
+  void mark(int i) {
+    if (!prof) return;
+    if (i == 0) {
+      cur ^= 1;
+      ++prof_iters;
+    }
+    cudaEventRecord(ev[cur][i], st);
+  }
+
+  emc_status fail(emc_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    err = buf;
+    return s;
+  }
+  emc_status cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return EMC_OK;
+    return fail(e == cudaErrorMemoryAllocation ? EMC_ERR_OOM : EMC_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+  }
+  template <class T>
+  emc_status alloc(T** p, size_t count, bool zero = false) {
+    void* q = nullptr;
+    const size_t bytes = count * sizeof(T) ? count * sizeof(T) : 16;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return cuda(e, "cudaMalloc");
+    allocs.push_back(q);
+    if (zero) {
+      e = cudaMemsetAsync(q, 0, bytes, st);
+      if (e != cudaSuccess) return cuda(e, "cudaMemset");
+    }
+    *p = static_cast<T*>(q);
+    return EMC_OK;
+  }
+  void release(void* p) {
+    for (auto& a : allocs)
+      if (a == p) {
+        cudaFree(a);
+        a = nullptr;
+      }
+  }
+};
+
+#define TRY(x)                              \
+  do {                                      \
+    emc_status _s = (x);                    \
+    if (_s != EMC_OK) return _s;            \
+  } while (0)
+#define CK(ctx, x) TRY((ctx)->cuda((x), #x))
+
+static thread_local std::string g_create_err;
+
+extern "C" {
+
+const char* emc_status_string(emc_status s) {
+  switch (s) {
+    case EMC_OK: return "ok";
+    case EMC_ERR_ARG: return "invalid argument";
+    case EMC_ERR_CUDA: return "CUDA error";
+    case EMC_ERR_OOM: return "out of device memory";
+    case EMC_ERR_TIMEOUT: return "device wait timed out";
+    case EMC_ERR_STATE: return "call out of order";
+    case EMC_ERR_RANGE: return "data outside the exact range of the selected precision";
+    case EMC_ERR_UNSUPPORTED: return "unsupported";
+  }
+  return "unknown status";
+}
+
+const char* emc_last_error(const emc_context* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_err.c_str();
+}
+
+emc_status emc_create(const emc_config* cfg, emc_context** out) {
+  if (!cfg || !out) return EMC_ERR_ARG;
+  *out = nullptr;
+  if (cfg->side < 2 || cfg->side > 1024 || cfg->n_patterns < 1 || cfg->n_rotations < 1 ||
+      (cfg->likelihood != EMC_LL_GAUSS && cfg->likelihood != EMC_LL_POISSON) ||
+      (cfg->interp != EMC_INTERP_NEAREST && cfg->interp != EMC_INTERP_TRILINEAR) ||
+      (cfg->precision != EMC_PREC_FP32 && cfg->precision != EMC_PREC_MIXED) ||
+      (cfg->likelihood == EMC_LL_GAUSS && !(cfg->sigma > 0)) ||
+      (cfg->likelihood == EMC_LL_POISSON && !(cfg->poisson_floor > 0))) {
+    g_create_err = "emc_create: invalid configuration";
+    return EMC_ERR_ARG;
+  }
+  emc_context* c = new emc_context();
+  c->cfg = *cfg;
+  c->N = cfg->n_patterns;
+  c->R = cfg->n_rotations;
+  c->npix = (int64_t)cfg->side * cfg->side;
+  c->M = c->npix * cfg->side;
+  c->mixed = cfg->precision == EMC_PREC_MIXED;
+  c->gauss = cfg->likelihood == EMC_LL_GAUSS;
+  auto bail = [&](emc_status s) {
+    g_create_err = c->err;
+    emc_destroy(c);
+    return s;
+  };
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e != cudaSuccess) return bail(c->cuda(e, "cudaSetDevice"));
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, cfg->device);
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, cfg->device);
+  if (c->mixed && major != 10) {
+    c->fail(EMC_ERR_UNSUPPORTED, "mixed precision needs an sm_100 device (found sm_%d)", major * 10);
+    return bail(EMC_ERR_UNSUPPORTED);
+  }
+  e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(c->cuda(e, "cudaStreamCreate"));
+  emc_status s;
+  if ((s = c->alloc(&c->d_model, c->M, true)) || (s = c->alloc(&c->d_weight, c->M, true)) ||
+      (s = c->alloc(&c->d_scaling, c->N)) || (s = c->alloc(&c->d_scaling_prev, c->N)) ||
+      (s = c->alloc(&c->d_quat, 4 * c->R)) || (s = c->alloc(&c->d_rotw, c->R)) ||
+      (s = c->alloc(&c->d_T, c->R, true)) || (s = c->alloc(&c->d_rowstat, c->R, true)) ||
+      (s = c->alloc(&c->d_scratch, 4096)) || (s = c->alloc(&c->d_stats, 16, true)) ||
+      (s = c->alloc(&c->d_patsq, c->N, true)) || (s = c->alloc(&c->d_patsum, c->N, true)) ||
+      (s = c->alloc(&c->d_status, 1, true)))
+    return bail(s);
+  if ((s = c->cuda(launch_fill(c->d_scaling, c->N, 1.0f, c->st), "fill")) != EMC_OK) return bail(s);
+  *out = c;
+  return EMC_OK;
+}
+
+emc_status emc_destroy(emc_context* ctx) {
+  if (!ctx) return EMC_OK;
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  for (void* p : ctx->allocs)
+    if (p) cudaFree(p);
+  for (auto& set : ctx->ev)
+    for (auto& e : set)
+      if (e) cudaEventDestroy(e);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx;
+  return EMC_OK;
+}
+
+void* emc_stream(emc_context* ctx) { return ctx ? (void*)ctx->st : nullptr; }
+int64_t emc_launch_count(const emc_context* ctx) { return ctx ? ctx->launches : 0; }
+
+emc_status emc_set_profiling(emc_context* c, int on) {
+  if (!c) return EMC_ERR_ARG;
+  if (on && !c->ev[0][0])
+    for (auto& set : c->ev)
+      for (auto& e : set) CK(c, cudaEventCreate(&e));
+  c->prof = on != 0;
+  c->prof_iters = 0;
+  return EMC_OK;
+}
+
+emc_status emc_stage_times(emc_context* c, float* ms) {
+  // times of the previous profiled iteration when there is one (the newest
+  // may still be running), else of the newest
+  if (!c || !ms) return EMC_ERR_ARG;
+  if (!c->ev[0][0] || c->prof_iters == 0) return c->fail(EMC_ERR_STATE, "nothing profiled");
+  const int set = c->prof_iters >= 2 ? (c->cur ^ 1) : c->cur;
+  CK(c, cudaEventSynchronize(c->ev[set][5]));
+  for (int i = 0; i < 5; ++i)
+    CK(c, cudaEventElapsedTime(&ms[i], c->ev[set][i], c->ev[set][i + 1]));
+  return EMC_OK;
+}
+int64_t emc_active_pixels(const emc_context* ctx) { return ctx ? ctx->npa : 0; }
+
+static emc_status alloc_work(emc_context* c) {
+  // called once geometry is known (npa fixes every pixel dimension)
+  const int64_t R = c->R, N = c->N, npa = c->npa;
+  if (!c->mixed) {
+    TRY(c->alloc(&c->d_S, R * npa));
+    TRY(c->alloc(&c->d_LL, R * N));
+    TRY(c->alloc(&c->d_K, N * npa));
+    TRY(c->alloc(&c->d_den, ((R + 127) / 128) * N));
+    TRY(c->alloc(&c->d_plogp_part, (N + 31) / 32 + 1));
+    TRY(c->alloc(&c->d_lse32, N));
+    return EMC_OK;
+  }
+  c->Npad = round_up(N, 128);
+  c->Ppad = round_up(npa, 256);
+  c->Rpad = round_up(R, 256);
+  c->nrt = c->Rpad / 256;
+  const int64_t nchunk = (R + kRespChunk - 1) / kRespChunk;
+  TRY(c->alloc(&c->d_Kh, c->Npad * c->Ppad, true));
+  TRY(c->alloc(&c->d_Kt, c->Ppad * c->Npad, true));
+  TRY(c->alloc(&c->d_Bhi, c->Rpad * c->Ppad, true));
+  TRY(c->alloc(&c->d_Blo, c->Rpad * c->Ppad, true));
+  TRY(c->alloc(&c->d_Phi, c->Rpad * c->Npad, true));
+  TRY(c->alloc(&c->d_Plo, c->Rpad * c->Npad, true));
+  TRY(c->alloc(&c->d_Y, R * c->Npad));
+  TRY(c->alloc(&c->d_part, c->nrt * N));
+  TRY(c->alloc(&c->d_lse, N));
+  TRY(c->alloc(&c->d_den2, nchunk * N));
+  TRY(c->alloc(&c->d_plogp2, nchunk * N));
+  TRY(c->alloc(&c->d_Tpart, (c->Npad / 64) * R));
+  bool ok = tc_encode_2d(&c->tmKh, c->d_Kh, c->Ppad, c->Npad, 128) &&
+            tc_encode_2d(&c->tmBhi, c->d_Bhi, c->Ppad, c->Rpad, 256) &&
+            tc_encode_2d(&c->tmBlo, c->d_Blo, c->Ppad, c->Rpad, 256) &&
+            tc_encode_2d(&c->tmPhi, c->d_Phi, c->Npad, c->Rpad, 128) &&
+            tc_encode_2d(&c->tmPlo, c->d_Plo, c->Npad, c->Rpad, 128) &&
+            tc_encode_2d(&c->tmKt, c->d_Kt, c->Npad, c->Ppad, 256);
+  if (!ok) return c->fail(EMC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  return EMC_OK;
+}
+
+emc_status emc_set_geometry(emc_context* c, const float* x, const float* y, const float* z,
+                            const int32_t* mask) {
+  if (!c || !x || !y || !z || !mask) return EMC_ERR_ARG;
+  if (c->have_geom) return c->fail(EMC_ERR_STATE, "geometry is already set");
+  std::vector<int32_t> pix, ins;
+  std::vector<float> cx, cy, cz;
+  for (int64_t i = 0; i < c->npix; ++i)
+    if (mask[i] != 0) {  // emc_cuda.cu:120: pixels with mask != 0 enter the likelihood
+      pix.push_back((int32_t)i);
+      ins.push_back(mask[i] == 1 ? 1 : 0);  // emc_atomic.cu:30: only mask == 1 is inserted
+      cx.push_back(x[i]);
+      cy.push_back(y[i]);
+      cz.push_back(z[i]);
+    }
+  if (pix.empty()) return c->fail(EMC_ERR_ARG, "mask has no active pixel");
+  c->npa = (int64_t)pix.size();
+  TRY(c->alloc(&c->d_pix, c->npa));
+  TRY(c->alloc(&c->d_ins, c->npa));
+  TRY(c->alloc(&c->d_cx, c->npa));
+  TRY(c->alloc(&c->d_cy, c->npa));
+  TRY(c->alloc(&c->d_cz, c->npa));
+  CK(c, cudaMemcpyAsync(c->d_pix, pix.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_ins, ins.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_cx, cx.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_cy, cy.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_cz, cz.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
+  TRY(alloc_work(c));
+  CK(c, cudaStreamSynchronize(c->st));
+  c->have_geom = true;
+  return EMC_OK;
+}
+
+emc_status emc_set_rotations(emc_context* c, const float* q, const float* w) {
+  if (!c || !q || !w) return EMC_ERR_ARG;
+  CK(c, cudaMemcpyAsync(c->d_quat, q, sizeof(float) * 4 * c->R, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_rotw, w, sizeof(float) * c->R, cudaMemcpyHostToDevice, c->st));
+  c->have_rot = true;
+  return EMC_OK;
+}
+
+emc_status emc_set_patterns(emc_context* c, const float* counts) {
+  if (!c || !counts) return EMC_ERR_ARG;
+  if (!c->have_geom) return c->fail(EMC_ERR_STATE, "set the geometry before the patterns");
+  const int64_t N = c->N, npa = c->npa;
+  // full images to the device, then gathered to the active pixels there
+  float* full = nullptr;
+  CK(c, cudaMallocAsync((void**)&full, sizeof(float) * N * c->npix, c->st));
+  float* compact = c->d_K;
+  emc_status s = EMC_OK;
+  if (c->mixed && (s = c->cuda(cudaMallocAsync((void**)&compact, sizeof(float) * N * npa, c->st),
+                               "cudaMallocAsync")) != EMC_OK) {
+    cudaFreeAsync(full, c->st);
+    return s;
+  }
+  cudaError_t e = cudaMemcpyAsync(full, counts, sizeof(float) * N * c->npix,
+                                  cudaMemcpyHostToDevice, c->st);
+  if (e == cudaSuccess) {
+    for (int64_t r0 = 0; r0 < N && e == cudaSuccess; r0 += 65535) {
+      const int64_t rows = N - r0 < 65535 ? N - r0 : 65535;
+      gather_cols_kernel<<<dim3(8, (unsigned)rows), 256, 0, c->st>>>(full + r0 * c->npix, rows,
+                                                                      c->npix, c->d_pix, npa,
+                                                                      compact + r0 * npa);
+      e = cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) e = launch_pattern_stats(compact, nullptr, N, npa, npa, 1, c->d_patsq, c->st);
+  if (e == cudaSuccess) e = launch_pattern_stats(compact, nullptr, N, npa, npa, 0, c->d_patsum, c->st);
+  int bad = 0;
+  if (e == cudaSuccess && c->mixed) {
+    int* d_bad = reinterpret_cast<int*>(c->d_scratch);
+    e = cudaMemsetAsync(d_bad, 0, sizeof(int), c->st);
+    if (e == cudaSuccess)
+      e = launch_pack_patterns(compact, N, npa, c->Npad, c->Ppad, c->d_Kh, c->d_Kt, d_bad, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+  }
+  cudaFreeAsync(full, c->st);
+  if (c->mixed) cudaFreeAsync(compact, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return c->cuda(e, "emc_set_patterns");
+  if (bad)
+    return c->fail(EMC_ERR_RANGE,
+                   "%d counts are not integers in [0, 2048]; the mixed path needs them exact in FP16",
+                   bad);
+  c->have_pat = true;
+  return EMC_OK;
+}
+
+emc_status emc_set_model(emc_context* c, const float* model) {
+  if (!c || !model) return EMC_ERR_ARG;
+  CK(c, cudaMemcpyAsync(c->d_model, model, sizeof(float) * c->M, cudaMemcpyHostToDevice, c->st));
+  c->have_model = true;
+  c->stage = 0;
+  return EMC_OK;
+}
+
+emc_status emc_set_scaling(emc_context* c, const float* scaling) {
+  if (!c || !scaling) return EMC_ERR_ARG;
+  CK(c, cudaMemcpyAsync(c->d_scaling, scaling, sizeof(float) * c->N, cudaMemcpyHostToDevice, c->st));
+  return EMC_OK;
+}
+
+static double gauss_inv(const emc_context* c) {
+  return 1.0 / (2.0 * (double)c->npa * (double)c->cfg.sigma * (double)c->cfg.sigma);
+}
+
+emc_status emc_expand(emc_context* c) {
+  if (!c) return EMC_ERR_ARG;
+  if (!c->have_geom || !c->have_rot || !c->have_pat || !c->have_model)
+    return c->fail(EMC_ERR_STATE, "geometry, rotations, patterns and model must be set first");
+  if (c->stage != 0) return c->fail(EMC_ERR_STATE, "expand called out of order");
+  ExpandArgs a{};
+  a.model = c->d_model;
+  a.quat = c->d_quat;
+  a.cx = c->d_cx;
+  a.cy = c->d_cy;
+  a.cz = c->d_cz;
+  a.R = c->R;
+  a.npix = c->npa;
+  a.side = c->cfg.side;
+  a.interp = c->cfg.interp;
+  a.floor_ = c->cfg.poisson_floor;
+  a.rowstat = c->d_rowstat;
+  if (!c->mixed) {
+    a.ld = c->npa;
+    a.out = c->gauss ? EXP_F32 : EXP_LOG_F32;
+    a.stat = c->gauss ? STAT_NONE : STAT_SUM;
+    a.out_f32 = c->d_S;
+  } else {
+    a.ld = c->Ppad;
+    a.out = EXP_F16_SPLIT;
+    a.log_split = c->gauss ? 0 : 1;
+    a.stat = c->gauss ? STAT_SUMSQ : STAT_SUM;
+    a.out_hi = c->d_Bhi;
+    a.out_lo = c->d_Blo;
+  }
+  c->mark(0);
+  CK(c, launch_expand(a, c->st));
+  c->launches += 1;
+  c->mark(1);
+  c->stage = 1;
+  return EMC_OK;
+}
+
+emc_status emc_maximize(emc_context* c) {
+  if (!c) return EMC_ERR_ARG;
+  if (c->stage != 1) return c->fail(EMC_ERR_STATE, "maximize called before expand");
+  const int64_t R = c->R, N = c->N;
+  CK(c, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * N,
+                        cudaMemcpyDeviceToDevice, c->st));
+  if (!c->mixed) {
+    LLArgs l{};
+    l.A = c->d_S;
+    l.K = c->d_K;
+    l.scaling = c->d_scaling;
+    l.rowstat = c->d_rowstat;
+    l.R = R;
+    l.N = N;
+    l.npa = c->npa;
+    l.ldA = c->npa;
+    l.ldK = c->npa;
+    l.ldLL = N;
+    l.gauss_inv = gauss_inv(c);
+    l.poisson = c->gauss ? 0 : 1;
+    l.LL = c->d_LL;
+    CK(c, launch_ll_fp32(l, c->st));
+    c->mark(2);
+    int nparts = 0;
+    CK(c, launch_softmax_fp32(c->d_LL, R, N, c->d_plogp_part, &nparts, c->st));
+    CK(c, launch_sum_f64(c->d_plogp_part, nparts, c->d_stats + 2, c->st));
+    int64_t nden = 0;
+    if (c->gauss) {
+      CrossArgs x{};
+      x.S = c->d_S;
+      x.K = c->d_K;
+      x.P = c->d_LL;
+      x.R = R;
+      x.N = N;
+      x.npa = c->npa;
+      x.ldS = c->npa;
+      x.ldK = c->npa;
+      x.den_part = c->d_den;
+      CK(c, launch_scaling_cross(x, c->st));
+      nden = (R + 127) / 128;
+    } else {
+      CK(c, launch_scaling_rowweighted(c->d_LL, c->d_rowstat, R, N, c->d_den, &nden, c->st));
+    }
+    CK(c, launch_scaling_finish(c->gauss ? c->d_patsq : c->d_patsum, c->d_den, nden, N,
+                                c->d_scaling, c->st));
+    CK(c, launch_row_sums(c->d_LL, R, N, c->d_T, c->st));
+    c->launches += 7;
+  } else {
+    MaxEpiArgs e{};
+    e.N = N;
+    e.R = R;
+    e.ldY = c->Npad;
+    e.poisson = c->gauss ? 0 : 1;
+    e.scaling = c->d_scaling_prev;
+    e.rowstat = c->d_rowstat;
+    e.patstat = c->d_patsq;
+    e.gauss_inv = gauss_inv(c);
+    e.Y = c->d_Y;
+    e.part = c->d_part;
+    CK(c, launch_maximize_tc(c->tmKh, c->tmBhi, c->tmBlo, c->Npad, c->Rpad, c->Ppad, e,
+                             c->d_status, c->num_sms, c->st));
+    c->mark(2);
+    RespArgs a{};
+    a.N = N;
+    a.R = R;
+    a.ldY = c->Npad;
+    a.ldP = c->Npad;
+    a.nparts = c->nrt;
+    a.poisson = e.poisson;
+    a.Y = c->d_Y;
+    a.part = c->d_part;
+    a.scaling = c->d_scaling_prev;
+    a.rowstat = c->d_rowstat;
+    a.patstat = c->d_patsq;
+    a.patsum = c->d_patsum;
+    a.gauss_inv = e.gauss_inv;
+    a.lse = c->d_lse;
+    a.den_part = c->d_den2;
+    a.plogp_part = c->d_plogp2;
+    a.new_scaling = c->d_scaling;
+    a.c0 = 1.0f;
+    a.Phi = c->d_Phi;
+    a.Plo = c->d_Plo;
+    a.Tpart = c->d_Tpart;
+    a.T = c->d_T;
+    a.P32 = nullptr;
+    CK(c, launch_resp_pass(a, kRespChunk, c->st));
+    CK(c, launch_sum_f64(c->d_plogp2, N, c->d_stats + 2, c->st));
+    CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
+    c->launches += 9;
+  }
+  c->mark(3);
+  c->stage = 2;
+  return EMC_OK;
+}
+
+emc_status emc_compress(emc_context* c) {
+  if (!c) return EMC_ERR_ARG;
+  if (c->stage != 2) return c->fail(EMC_ERR_STATE, "compress called before maximize");
+  // emc.c:1025-1026 reset, then emc_cuda.cu:292-362 insert, :414-433 normalise
+  CK(c, cudaMemsetAsync(c->d_model, 0, sizeof(float) * c->M, c->st));
+  CK(c, cudaMemsetAsync(c->d_weight, 0, sizeof(float) * c->M, c->st));
+  if (!c->mixed) {
+    CompressArgs a{};
+    a.P = c->d_LL;
+    a.K = c->d_K;
+    a.scaling = c->d_scaling;
+    a.T = c->d_T;
+    a.R = c->R;
+    a.N = c->N;
+    a.npa = c->npa;
+    a.ldK = c->npa;
+    a.ldU = c->npa;
+    a.U = c->d_S;  // the averaged slices replace the expanded ones (emc_atomic.cu:96)
+    CK(c, launch_compress_fp32(a, c->st));
+    InsertArgs in{};
+    in.U = c->d_S;
+    in.T = c->d_T;
+    in.rotw = c->d_rotw;
+    in.quat = c->d_quat;
+    in.cx = c->d_cx;
+    in.cy = c->d_cy;
+    in.cz = c->d_cz;
+    in.ins = c->d_ins;
+    in.R = c->R;
+    in.npix = c->npa;
+    in.ldU = c->npa;
+    in.side = c->cfg.side;
+    in.interp = c->cfg.interp;
+    in.model = c->d_model;
+    in.weight = c->d_weight;
+    CK(c, launch_insert(in, c->st));
+    c->launches += 2;
+  } else {
+    CmpEpiArgs e{};
+    e.R = c->R;
+    e.npa = c->npa;
+    e.side = c->cfg.side;
+    e.interp = c->cfg.interp;
+    e.inv_c0 = 1.0f;
+    e.quat = c->d_quat;
+    e.rotw = c->d_rotw;
+    e.T = c->d_T;
+    e.cx = c->d_cx;
+    e.cy = c->d_cy;
+    e.cz = c->d_cz;
+    e.ins = c->d_ins;
+    e.model = c->d_model;
+    e.weight = c->d_weight;
+    CK(c, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
+                             c->d_status, c->num_sms, c->st));
+    c->launches += 1;
+  }
+  c->mark(4);
+  CK(c, launch_normalize_model(c->d_model, c->d_weight, c->M, c->mixed ? 1 : 0, c->d_scratch,
+                               c->d_stats, c->st));
+  c->launches += 4;
+  c->mark(5);
+  c->stage = 0;
+  return EMC_OK;
+}
+
+static emc_status check_status(emc_context* c) {
+  TcStatus h{};
+  CK(c, cudaMemcpyAsync(&h, c->d_status, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  if (h.code != 0) {
+    cudaMemsetAsync(c->d_status, 0, sizeof(TcStatus), c->st);
+    cudaStreamSynchronize(c->st);
+    return c->fail(EMC_ERR_TIMEOUT, "tensor-core kernel wait %d timed out in block %d", h.where,
+                   h.block);
+  }
+  return EMC_OK;
+}
+
+emc_status emc_synchronize(emc_context* c) {
+  if (!c) return EMC_ERR_ARG;
+  return check_status(c);
+}
+
+emc_status emc_iterate(emc_context* c, emc_iter_stats* stats) {
+  TRY(emc_expand(c));
+  TRY(emc_maximize(c));
+  TRY(emc_compress(c));
+  if (stats) {
+    TRY(check_status(c));
+    double h[4] = {0, 0, 0, 0};
+    CK(c, cudaMemcpy(h, c->d_stats, sizeof(h), cudaMemcpyDeviceToHost));
+    double T = 0;
+    std::vector<float> t(c->R);
+    CK(c, cudaMemcpy(t.data(), c->d_T, sizeof(float) * c->R, cudaMemcpyDeviceToHost));
+    for (float v : t) T += v;
+    stats->model_max = h[1];
+    stats->sum_plogp = h[2];
+    stats->total_loglik = c->mixed ? h[3] : 0.0;
+    stats->total_resp = T;
+  }
+  return EMC_OK;
+}
+
+emc_status emc_get_model(emc_context* c, float* model) {
+  return emc_get_buffer(c, EMC_BUF_MODEL, model, sizeof(float) * (c ? c->M : 0));
+}
+
+emc_status emc_get_scaling(emc_context* c, float* scaling) {
+  return emc_get_buffer(c, EMC_BUF_SCALING, scaling, sizeof(float) * (c ? c->N : 0));
+}
+
+emc_status emc_device_buffer(emc_context* c, emc_buffer which, void** dptr, size_t* bytes) {
+  if (!c || !dptr) return EMC_ERR_ARG;
+  void* p = nullptr;
+  size_t n = 0;
+  switch (which) {
+    case EMC_BUF_MODEL: p = c->d_model; n = sizeof(float) * c->M; break;
+    case EMC_BUF_WEIGHT: p = c->d_weight; n = sizeof(float) * c->M; break;
+    case EMC_BUF_SCALING: p = c->d_scaling; n = sizeof(float) * c->N; break;
+    case EMC_BUF_TOTALRESP: p = c->d_T; n = sizeof(float) * c->R; break;
+    case EMC_BUF_RESP:
+      if (c->mixed) return c->fail(EMC_ERR_UNSUPPORTED, "mixed path keeps no FP32 responsibility matrix");
+      p = c->d_LL; n = sizeof(float) * c->R * c->N; break;
+    case EMC_BUF_SLICES:
+      if (c->mixed) return c->fail(EMC_ERR_UNSUPPORTED, "mixed path keeps FP16 hi/lo slices");
+      p = c->d_S; n = sizeof(float) * c->R * c->npa; break;
+    default: return EMC_ERR_ARG;
+  }
+  *dptr = p;
+  if (bytes) *bytes = n;
+  return EMC_OK;
+}
+
+emc_status emc_get_buffer(emc_context* c, emc_buffer which, void* host, size_t bytes) {
+  if (!c || !host) return EMC_ERR_ARG;
+  TRY(check_status(c));
+  if (c->mixed && (which == EMC_BUF_RESP || which == EMC_BUF_SLICES)) {
+    const size_t n = which == EMC_BUF_RESP ? (size_t)(c->R * c->N) : (size_t)(c->R * c->npa);
+    if (bytes != n * sizeof(float)) return c->fail(EMC_ERR_ARG, "buffer size mismatch");
+    if (which == EMC_BUF_RESP && c->stage != 2 && c->stage != 0)
+      return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+    float* tmp = nullptr;
+    CK(c, cudaMalloc(&tmp, n * sizeof(float)));
+    cudaError_t e;
+    if (which == EMC_BUF_RESP) {
+      RespArgs a{};
+      a.N = c->N;
+      a.R = c->R;
+      a.ldY = c->Npad;
+      a.poisson = c->gauss ? 0 : 1;
+      a.Y = c->d_Y;
+      a.scaling = c->d_scaling_prev;
+      a.rowstat = c->d_rowstat;
+      a.patstat = c->d_patsq;
+      a.gauss_inv = gauss_inv(c);
+      a.lse = c->d_lse;
+      e = launch_resp_export(a, tmp, c->st);
+    } else {
+      split_sum_kernel<<<dim3(8, (unsigned)(c->R < 65535 ? c->R : 65535)), 256, 0, c->st>>>(
+          c->d_Bhi, c->d_Blo, c->R, c->Ppad, c->npa, tmp);
+      e = cudaGetLastError();
+      for (int64_t r0 = 65535; r0 < c->R && e == cudaSuccess; r0 += 65535) {
+        const int64_t rows = c->R - r0 < 65535 ? c->R - r0 : 65535;
+        split_sum_kernel<<<dim3(8, (unsigned)rows), 256, 0, c->st>>>(
+            c->d_Bhi + r0 * c->Ppad, c->d_Blo + r0 * c->Ppad, rows, c->Ppad, c->npa,
+            tmp + r0 * c->npa);
+        e = cudaGetLastError();
+      }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(tmp);
+    return c->cuda(e, "emc_get_buffer");
+  }
+  void* p = nullptr;
+  size_t n = 0;
+  TRY(emc_device_buffer(c, which, &p, &n));
+  if (bytes != n) return c->fail(EMC_ERR_ARG, "buffer size mismatch (%zu != %zu)", bytes, n);
+  CK(c, cudaMemcpyAsync(host, p, n, cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  return EMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,632 @@
+// FP32 CUDA-core kernels: expand, the likelihood / scaling / slice-average
+// contractions as register-tiled FP32 kernels, softmax, insertion and model
+// normalisation.  This is the plain-FP32 path of the engine and the engine
+// behind the reference-compatible API in legacy.cu.
+#include <cfloat>
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "voxel.h"
+
+namespace emc {
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sum of one double per thread over the block (blockDim.x multiple of 32).
+__device__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < nw; ++i) s += red[i];
+  return s;  // valid on thread 0
+}
+
+__device__ float block_max(float v, float* red) {
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  float s = -FLT_MAX;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < nw; ++i) s = fmaxf(s, red[i]);
+  return s;
+}
+
+// ------------------------------------------------------------------ expand --
+// One block per rotation; threads stride over pixels.  emc_cuda.cu:51-111 for
+// the nearest mode (exclusive lower bound), trilinear otherwise.
+__global__ void __launch_bounds__(kBlock) expand_kernel(const ExpandArgs a) {
+  __shared__ double red[32];
+  const int64_t r = blockIdx.x;
+  float m[9];
+  emc_voxel::rotation_matrix(a.quat + 4 * r, m);
+  double stat = 0.0;
+  for (int64_t i = threadIdx.x; i < a.ld; i += blockDim.x) {
+    float w = 0.0f;
+    const bool real = i < a.npix;
+    if (real) {
+      float u[3];
+      emc_voxel::position(m, a.side, a.cx[i], a.cy[i], a.cz[i], u);
+      if (a.interp == 0) {
+        int64_t v;
+        if (emc_voxel::nearest(u, a.side, 1, &v)) w = __ldg(a.model + v);
+      } else {
+        int64_t v[8];
+        float ww[8];
+        const int n = emc_voxel::trilinear(u, a.side, v, ww);
+        for (int c = 0; c < n; ++c) w = fmaf(ww[c], __ldg(a.model + v[c]), w);
+      }
+      if (a.stat != STAT_NONE && (!a.stat_mask || a.stat_mask[i] != 0))
+        stat += a.stat == STAT_SUMSQ ? (double)w * w : (double)w;
+    }
+    const int64_t o = r * a.ld + i;
+    if (a.out == EXP_F32) {
+      a.out_f32[o] = w;
+    } else if (a.out == EXP_LOG_F32) {
+      a.out_f32[o] = real ? logf(fmaxf(w, a.floor_)) : 0.0f;
+    } else {
+      const float x = real ? (a.log_split ? logf(fmaxf(w, a.floor_)) : w) : 0.0f;
+      const __half hi = __float2half_rn(x);
+      a.out_hi[o] = hi;
+      a.out_lo[o] = __float2half_rn(x - __half2float(hi));
+    }
+  }
+  if (a.rowstat) {
+    const double s = block_sum(stat, red);
+    if (threadIdx.x == 0) a.rowstat[r] = s;
+  }
+}
+
+// ------------------------------------------------------- tiled contraction --
+// C-tile of 128 rows x 64 columns per block, K-steps of 32, 256 threads with
+// an 8x4 register tile each.  Op supplies the operand loads, the per-element
+// update and the epilogue.
+constexpr int TM = 128, TN = 64, TK = 32;
+
+template <class Op>
+__global__ void __launch_bounds__(kBlock) tile_kernel(const Op op) {
+  __shared__ __align__(16) float As[TK][TM + 4];
+  __shared__ __align__(16) float Bs[TK][TN + 4];
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+  const int64_t m0 = (int64_t)blockIdx.y * TM;
+  const int64_t n0 = (int64_t)blockIdx.x * TN;
+  using Acc = typename Op::Acc;
+  Acc acc[8][4];
+  float tacc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      acc[i][j] = 0;
+      tacc[i][j] = 0.0f;
+    }
+  float ra[16], rb[8];
+  auto load = [&](int64_t k0) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) ra[i] = op.a(m0 + (t >> 5) + 8 * i, k0 + (t & 31));
+    if constexpr (Op::kBKMajor) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) rb[i] = op.b(n0 + (t >> 5) + 8 * i, k0 + (t & 31));
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) rb[i] = op.b(n0 + (t & 63), k0 + (t >> 6) + 4 * i);
+    }
+  };
+  auto stash = [&]() {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) As[t & 31][(t >> 5) + 8 * i] = ra[i];
+    if constexpr (Op::kBKMajor) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) Bs[t & 31][(t >> 5) + 8 * i] = rb[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) Bs[(t >> 6) + 4 * i][t & 63] = rb[i];
+    }
+  };
+  const int64_t K = op.ksize();
+  load(0);
+  for (int64_t k0 = 0; k0 < K; k0 += TK) {
+    __syncthreads();
+    stash();
+    __syncthreads();
+    if (k0 + TK < K) load(k0 + TK);
+#pragma unroll 8
+    for (int kk = 0; kk < TK; ++kk) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[kk][ty * 8]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[kk][ty * 8 + 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[kk][tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[4] = {b0.x, b0.y, b0.z, b0.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) tacc[i][j] = Op::inner(tacc[i][j], av[i], bv[j]);
+    }
+    // fold each 32-step partial into the (possibly FP64) running sum
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        acc[i][j] += (Acc)tacc[i][j];
+        tacc[i][j] = 0.0f;
+      }
+  }
+  __syncthreads();  // the epilogue may reuse As
+  op.epilogue(acc, m0 + ty * 8, n0 + tx * 4, (float*)&As[0][0]);
+}
+
+__device__ __forceinline__ int64_t col_of(const int32_t* pix, int64_t j) { return pix ? pix[j] : j; }
+
+// Likelihood: rows = rotations, columns = patterns, reduction over pixels.
+struct OpLL {
+  using Acc = double;
+  static constexpr bool kBKMajor = true;
+  LLArgs p;
+  __device__ int64_t ksize() const { return p.npa; }
+  __device__ float a(int64_t r, int64_t j) const {
+    return (r < p.R && j < p.npa) ? __ldg(p.A + r * p.ldA + col_of(p.pix, j)) : 0.0f;
+  }
+  __device__ float b(int64_t n, int64_t j) const {
+    if (n >= p.N || j >= p.npa) return 0.0f;
+    const float k = __ldg(p.K + n * p.ldK + col_of(p.pix, j));
+    return p.poisson ? k : k / __ldg(p.scaling + n);  // gaussian: image / scaling (emc_cuda.cu:121)
+  }
+  static __device__ __forceinline__ float inner(float acc, float a, float b);
+  __device__ void epilogue(double (&acc)[8][4], int64_t r0, int64_t n0, float*) const {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int64_t r = r0 + i;
+      if (r >= p.R) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t n = n0 + j;
+        if (n >= p.N) continue;
+        const double v = p.poisson ? acc[i][j] - (double)p.scaling[n] * p.rowstat[r]
+                                   : -acc[i][j] * p.gauss_inv;
+        p.LL[r * p.ldLL + n] = (float)v;
+      }
+    }
+  }
+};
+struct OpLLGauss : OpLL {
+  static __device__ __forceinline__ float inner(float acc, float a, float b) {
+    const float d = a - b;
+    return fmaf(d, d, acc);
+  }
+};
+struct OpLLPoisson : OpLL {
+  static __device__ __forceinline__ float inner(float acc, float a, float b) { return fmaf(a, b, acc); }
+};
+
+// Gaussian scaling denominator: sum_r P_rp sum_j S_rj K_pj, reduced over the
+// tile's rows in the epilogue.
+struct OpCross {
+  using Acc = float;
+  static constexpr bool kBKMajor = true;
+  CrossArgs p;
+  __device__ int64_t ksize() const { return p.npa; }
+  __device__ float a(int64_t r, int64_t j) const {
+    return (r < p.R && j < p.npa) ? __ldg(p.S + r * p.ldS + col_of(p.pix, j)) : 0.0f;
+  }
+  __device__ float b(int64_t n, int64_t j) const {
+    return (n < p.N && j < p.npa) ? __ldg(p.K + n * p.ldK + col_of(p.pix, j)) : 0.0f;
+  }
+  static __device__ __forceinline__ float inner(float acc, float a, float b) { return fmaf(a, b, acc); }
+  __device__ void epilogue(float (&acc)[8][4], int64_t r0, int64_t n0, float* smem) const {
+    double* red = reinterpret_cast<double*>(smem);  // [16][64]
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t n = n0 + j;
+      double s = 0;
+      if (n < p.N)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int64_t r = r0 + i;
+          if (r < p.R) s += (double)__ldg(p.P + r * p.N + n) * acc[i][j];
+        }
+      red[ty * 64 + tx * 4 + j] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      const int64_t n = (int64_t)blockIdx.x * TN + threadIdx.x;
+      double s = 0;
+      for (int k = 0; k < 16; ++k) s += red[k * 64 + threadIdx.x];
+      if (n < p.N) p.den_part[(int64_t)blockIdx.y * p.N + n] = s;
+    }
+  }
+};
+
+// Slice average: rows = rotations, columns = pixels, reduction over patterns.
+struct OpCompress {
+  using Acc = float;
+  static constexpr bool kBKMajor = false;
+  CompressArgs p;
+  __device__ int64_t ksize() const { return p.N; }
+  __device__ float a(int64_t r, int64_t k) const {
+    return (r < p.R && k < p.N) ? __ldg(p.P + r * p.N + k) : 0.0f;
+  }
+  __device__ float b(int64_t j, int64_t k) const {
+    return (j < p.npa && k < p.N) ? __ldg(p.K + k * p.ldK + col_of(p.pix, j)) / __ldg(p.scaling + k)
+                                  : 0.0f;
+  }
+  static __device__ __forceinline__ float inner(float acc, float a, float b) { return fmaf(a, b, acc); }
+  __device__ void epilogue(float (&acc)[8][4], int64_t r0, int64_t j0, float*) const {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int64_t r = r0 + i;
+      if (r >= p.R) continue;
+      const float T = p.T[r];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t jj = j0 + j;
+        if (jj >= p.npa) continue;
+        // emc_atomic.cu:105-111: divide by the slice's total responsibility
+        p.U[r * p.ldU + col_of(p.pix, jj)] = T > 1e-10f ? acc[i][j] / T : acc[i][j];
+      }
+    }
+  }
+};
+
+// ----------------------------------------------------------------- softmax --
+// 32 patterns per block (lane == pattern), 8 warps share the rotations.
+__global__ void __launch_bounds__(kBlock) softmax_kernel(float* X, int64_t R, int64_t N,
+                                                         double* plogp_part) {
+  __shared__ float smax[8][32];
+  __shared__ float ssum[8][32];
+  __shared__ double sred[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t p = (int64_t)blockIdx.x * 32 + lane;
+  const bool ok = p < N;
+  float mx = -FLT_MAX;
+  if (ok)
+    for (int64_t r = w; r < R; r += 8) mx = fmaxf(mx, X[r * N + p]);
+  smax[w][lane] = mx;
+  __syncthreads();
+  mx = smax[0][lane];
+  for (int k = 1; k < 8; ++k) mx = fmaxf(mx, smax[k][lane]);
+  float s = 0.0f;
+  if (ok)
+    for (int64_t r = w; r < R; r += 8) {
+      const float d = X[r * N + p] - mx;
+      if (d > -1.0e10f) s += expf(d);  // emc_cuda.cu:463-468
+    }
+  ssum[w][lane] = s;
+  __syncthreads();
+  s = 0.0f;
+  for (int k = 0; k < 8; ++k) s += ssum[k][lane];
+  const float inv = 1.0f / s;
+  double pl = 0.0;
+  if (ok)
+    for (int64_t r = w; r < R; r += 8) {
+      const float d = X[r * N + p] - mx;
+      const float P = d > -1.0e10f ? expf(d) * inv : 0.0f;
+      X[r * N + p] = P;
+      if (P > 0.0f) pl += (double)P * log((double)P);
+    }
+  sred[w][lane] = pl;
+  __syncthreads();
+  if (w == 0) {
+    double t = 0;
+    for (int k = 0; k < 8; ++k) t += sred[k][lane];
+    t = warp_sum(t);
+    if (lane == 0 && plogp_part) plogp_part[blockIdx.x] = t;
+  }
+}
+
+__global__ void xlogx_partial(const float* x, int64_t n, double* part) {
+  __shared__ double red[32];
+  double s = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float v = x[i];
+    if (v > 0.0f) s += (double)v * log((double)v);
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void sum_f64_kernel(const double* x, int64_t n, double* out) {
+  __shared__ double red[32];
+  double s = 0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += x[i];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// --------------------------------------------------------------- scaling --
+// den_part[blockIdx.y][p] = sum_{r in chunk} P_rp w_r; lane == pattern.
+__global__ void __launch_bounds__(kBlock) rowweighted_kernel(const float* P, const double* wr,
+                                                             int64_t R, int64_t N, int64_t rchunk,
+                                                             double* part) {
+  __shared__ double red[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t p = (int64_t)blockIdx.x * 32 + lane;
+  const int64_t r0 = (int64_t)blockIdx.y * rchunk, r1 = min(R, r0 + rchunk);
+  double s = 0;
+  if (p < N)
+    for (int64_t r = r0 + w; r < r1; r += 8) s += (double)P[r * N + p] * wr[r];
+  red[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && p < N) {
+    double t = 0;
+    for (int k = 0; k < 8; ++k) t += red[k][lane];
+    part[(int64_t)blockIdx.y * N + p] = t;
+  }
+}
+
+__global__ void scaling_finish_kernel(const double* num, const double* part, int64_t nparts,
+                                      int64_t N, float* scaling) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  double d = 0;
+  for (int64_t k = 0; k < nparts; ++k) d += part[k * N + p];
+  // emc_cuda.cu:226; a pattern without photons or weight keeps its scale
+  if (num[p] > 0.0 && d > 0.0) scaling[p] = (float)(num[p] / d);
+}
+
+__global__ void pattern_stats_kernel(const float* K, const int32_t* pix, int64_t N, int64_t npa,
+                                     int64_t ldK, int squares, double* num) {
+  const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= N) return;
+  double s = 0;
+  for (int64_t j = lane; j < npa; j += 32) {
+    const double k = K[p * ldK + col_of(pix, j)];
+    s += squares ? k * k : k;
+  }
+  s = warp_sum(s);
+  if (lane == 0) num[p] = s;
+}
+
+__global__ void row_sums_kernel(const float* P, int64_t R, int64_t N, float* T) {
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= R) return;
+  double s = 0;
+  for (int64_t p = lane; p < N; p += 32) s += P[r * N + p];
+  s = warp_sum(s);
+  if (lane == 0) T[r] = (float)s;
+}
+
+// ----------------------------------------------------------------- insert --
+// One block per rotation (emc_atomic.cu:115-133 + :17-73).
+__global__ void __launch_bounds__(kBlock) insert_kernel(const InsertArgs a) {
+  const int64_t r = blockIdx.x;
+  const float T = a.T[r];
+  if (!(T > 1e-10f)) return;
+  const float w = a.rotw[r] * T;
+  float m[9];
+  emc_voxel::rotation_matrix(a.quat + 4 * r, m);
+  for (int64_t i = threadIdx.x; i < a.npix; i += blockDim.x) {
+    if (a.ins[i] != 1) continue;
+    float u[3];
+    emc_voxel::position(m, a.side, a.cx[i], a.cy[i], a.cz[i], u);
+    const float s = a.U[r * a.ldU + i];
+    if (a.interp == 0) {
+      int64_t v;
+      if (!emc_voxel::nearest(u, a.side, 0, &v)) continue;
+      atomicAdd(a.model + v, w * s);
+      atomicAdd(a.weight + v, w);
+    } else {
+      int64_t v[8];
+      float ww[8];
+      const int n = emc_voxel::trilinear(u, a.side, v, ww);
+      for (int c = 0; c < n; ++c) {
+        atomicAdd(a.model + v[c], ww[c] * w * s);
+        atomicAdd(a.weight + v[c], ww[c] * w);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------- normalise --
+__global__ void divide_kernel(float* model, const float* weight, int64_t M, int fp64,
+                              double* part) {
+  __shared__ double red[32];
+  double s = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float wv = weight[i];
+    float v;
+    if (wv > 0.0f)  // emc_cuda.cu:416-420
+      v = fp64 ? (float)((double)model[i] / (double)wv) : model[i] / wv;
+    else
+      v = 0.0f;
+    model[i] = v;
+    s += v;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void scale_max_kernel(float* model, int64_t M, const double* sum, int fp64,
+                                 double* stats, double* part) {
+  __shared__ float red[32];
+  const double mean = *sum / (double)M;
+  const float f = (float)(1.0 / mean);
+  float mx = 0.0f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float v = model[i];
+    if (mean != 0.0) v = fp64 ? (float)((double)v / mean) : v * f;
+    model[i] = v;
+    mx = fmaxf(mx, v);
+  }
+  mx = block_max(mx, red);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = mx;
+    if (blockIdx.x == 0) stats[0] = mean;
+  }
+}
+
+__global__ void max_partial_kernel(const float* x, int64_t n, double* part) {
+  __shared__ float red[32];
+  float mx = -FLT_MAX;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    mx = fmaxf(mx, x[i]);
+  mx = block_max(mx, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = mx;
+}
+
+__global__ void max_f64_kernel(const double* x, int64_t n, double* out) {
+  __shared__ float red[32];
+  float mx = -FLT_MAX;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) mx = fmaxf(mx, (float)x[i]);
+  mx = block_max(mx, red);
+  if (threadIdx.x == 0) *out = mx;
+}
+
+__global__ void fill_kernel(float* x, int64_t n, float v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+constexpr int kReduceBlocks = 592;  // 4 x 148 SMs; partial arrays hold this many values
+
+inline int grid_for(int64_t n) {
+  const int64_t b = (n + kBlock - 1) / kBlock;
+  return (int)(b < kReduceBlocks ? (b > 0 ? b : 1) : kReduceBlocks);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers --
+
+cudaError_t launch_expand(const ExpandArgs& a, cudaStream_t st) {
+  if (a.R <= 0) return cudaSuccess;
+  expand_kernel<<<(unsigned)a.R, kBlock, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ll_fp32(const LLArgs& a, cudaStream_t st) {
+  if (a.R <= 0 || a.N <= 0) return cudaSuccess;
+  dim3 grid((unsigned)((a.N + TN - 1) / TN), (unsigned)((a.R + TM - 1) / TM));
+  if (a.poisson) {
+    OpLLPoisson op;
+    op.p = a;
+    tile_kernel<<<grid, kBlock, 0, st>>>(op);
+  } else {
+    OpLLGauss op;
+    op.p = a;
+    tile_kernel<<<grid, kBlock, 0, st>>>(op);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_softmax_fp32(float* X, int64_t R, int64_t N, double* plogp_part, int* nparts,
+                                cudaStream_t st) {
+  const int64_t nb = (N + 31) / 32;
+  if (nparts) *nparts = (int)nb;
+  softmax_kernel<<<(unsigned)nb, kBlock, 0, st>>>(X, R, N, plogp_part);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xlogx_sum(const float* x, int64_t n, double* out, double* scratch,
+                             cudaStream_t st) {
+  const int g = grid_for(n);
+  xlogx_partial<<<g, kBlock, 0, st>>>(x, n, scratch);
+  sum_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scaling_cross(const CrossArgs& a, cudaStream_t st) {
+  dim3 grid((unsigned)((a.N + TN - 1) / TN), (unsigned)((a.R + TM - 1) / TM));
+  OpCross op;
+  op.p = a;
+  tile_kernel<<<grid, kBlock, 0, st>>>(op);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scaling_rowweighted(const float* P, const double* w, int64_t R, int64_t N,
+                                       double* den_part, int64_t* nparts, cudaStream_t st) {
+  const int64_t rchunk = 1024;
+  const int64_t nc = (R + rchunk - 1) / rchunk;
+  *nparts = nc;
+  dim3 grid((unsigned)((N + 31) / 32), (unsigned)nc);
+  rowweighted_kernel<<<grid, kBlock, 0, st>>>(P, w, R, N, rchunk, den_part);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scaling_finish(const double* num, const double* den_part, int64_t nparts,
+                                  int64_t N, float* scaling, cudaStream_t st) {
+  scaling_finish_kernel<<<(unsigned)((N + kBlock - 1) / kBlock), kBlock, 0, st>>>(num, den_part,
+                                                                                 nparts, N, scaling);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pattern_stats(const float* K, const int32_t* pix, int64_t N, int64_t npa,
+                                 int64_t ldK, int squares, double* num, cudaStream_t st) {
+  pattern_stats_kernel<<<(unsigned)((N + 7) / 8), kBlock, 0, st>>>(K, pix, N, npa, ldK, squares, num);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_row_sums(const float* P, int64_t R, int64_t N, float* T, cudaStream_t st) {
+  row_sums_kernel<<<(unsigned)((R + 7) / 8), kBlock, 0, st>>>(P, R, N, T);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compress_fp32(const CompressArgs& a, cudaStream_t st) {
+  dim3 grid((unsigned)((a.npa + TN - 1) / TN), (unsigned)((a.R + TM - 1) / TM));
+  OpCompress op;
+  op.p = a;
+  tile_kernel<<<grid, kBlock, 0, st>>>(op);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_insert(const InsertArgs& a, cudaStream_t st) {
+  if (a.R <= 0) return cudaSuccess;
+  insert_kernel<<<(unsigned)a.R, kBlock, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normalize_model(float* model, const float* weight, int64_t M, int fp64,
+                                   double* scratch, double* stats, cudaStream_t st) {
+  // scratch: kReduceBlocks + 2 doubles; stats[0] = mean, stats[1] = max
+  const int g = grid_for(M);
+  divide_kernel<<<g, kBlock, 0, st>>>(model, weight, M, fp64, scratch);
+  sum_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, scratch + kReduceBlocks);
+  scale_max_kernel<<<g, kBlock, 0, st>>>(model, M, scratch + kReduceBlocks, fp64, stats, scratch);
+  max_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, stats + 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_model_max(const float* model, int64_t M, double* scratch, double* out,
+                             cudaStream_t st) {
+  const int g = grid_for(M);
+  max_partial_kernel<<<g, kBlock, 0, st>>>(model, M, scratch);
+  max_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill(float* x, int64_t n, float v, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  fill_kernel<<<grid_for(n), kBlock, 0, st>>>(x, n, v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sum_f64(const double* x, int64_t n, double* out, cudaStream_t st) {
+  sum_f64_kernel<<<1, kBlock, 0, st>>>(x, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace emc

@@ -1,0 +1,94 @@
+// Mixed-precision (tcgen05) path: launch interface.
+#pragma once
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace emc {
+
+// Device-side status of the tensor-core kernels: code != 0 when a bounded
+// wait gave up (the kernel then drained its copies, freed TMEM and returned).
+struct TcStatus {
+  int code;
+  int where;
+  int block;
+  int pad;
+};
+enum { TC_OK = 0, TC_TIMEOUT = 1 };
+
+bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
+                  uint32_t box_rows);
+
+// Maximize contraction: acc[p][r] = sum_j K[p][j] (B_hi[r][j] + B_lo[r][j]),
+// 128 patterns x 256 rotations per tile.  Epilogue writes Y[r][p] (LL for
+// poisson, the cross term C for gaussian) and per-pattern partial
+// (max, sum exp) of LL over the tile's rotations.
+struct MaxEpiArgs {
+  int64_t N, R, ldY;
+  int poisson;
+  const float* scaling;    // [N] current phi
+  const double* rowstat;   // [R] poisson: sum W_r; gaussian: sum S_r^2
+  const double* patstat;   // [N] gaussian: sum K_p^2
+  double gauss_inv;        // 1 / (2 cnt sigma^2)
+  float* Y;                // [R][ldY]
+  float2* part;            // [ceil(R/256)][N] (max, sum exp(LL - max))
+};
+cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
+                               const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
+                               int64_t Kpad, const MaxEpiArgs& e, TcStatus* status,
+                               int num_sms, cudaStream_t st);
+
+// Compress contraction: acc[r][j] = sum_p (P'_hi + P'_lo)[r][p] Kt[j][p],
+// 128 rotations x 256 pixels per tile, inserted in the epilogue.
+struct CmpEpiArgs {
+  int64_t R, npa;
+  int side, interp;
+  float inv_c0;            // undo the global scale of P'
+  const float* quat;       // [R][4]
+  const float* rotw;       // [R]
+  const float* T;          // [R]
+  const float* cx;         // [npa] active-pixel coordinates
+  const float* cy;
+  const float* cz;
+  const int32_t* ins;      // [npa] insert flag (mask == 1)
+  float* model;
+  float* weight;
+};
+cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
+                               const CUtensorMap& tmKt, int64_t Rpad, int64_t Ppad,
+                               int64_t Npad, const CmpEpiArgs& e, TcStatus* status, int num_sms,
+                               cudaStream_t st);
+
+// Responsibility pass of the mixed path.
+struct RespArgs {
+  int64_t N, R, ldY, ldP, nparts;  // nparts = number of 256-rotation tiles
+  int poisson;
+  const float* Y;
+  const float2* part;
+  const float* scaling;    // phi used for LL
+  const double* rowstat;
+  const double* patstat;   // gaussian: sum K^2 (also the scaling numerator)
+  const double* patsum;    // poisson: sum K (scaling numerator)
+  double gauss_inv;
+  double* lse;             // [N]
+  double* den_part;        // [nchunk][N]
+  double* plogp_part;      // [nchunk][N]
+  float* new_scaling;      // [N]
+  float c0;                // global scale of P'
+  __half* Phi;             // [Rpad][ldP]
+  __half* Plo;
+  float* Tpart;            // [ceil(N/64)][R]
+  float* T;                // [R]
+  float* P32;              // optional [R][N] FP32 responsibilities
+};
+cudaError_t launch_resp_pass(RespArgs& a, int64_t rchunk, cudaStream_t st);
+// FP32 responsibilities [R][N] from Y and lse (readback / tests).
+cudaError_t launch_resp_export(const RespArgs& a, float* P, cudaStream_t st);
+// Builds the FP16 pattern operands: Kh[Npad][Ppad] and Kt[Ppad][Npad] from
+// compact FP32 counts [N][npa]; bad[0] counts entries that are not integers in [0, 2048].
+cudaError_t launch_pack_patterns(const float* K, int64_t N, int64_t npa, int64_t Npad,
+                                 int64_t Ppad, __half* Kh, __half* Kt, int* bad,
+                                 cudaStream_t st);
+
+}  // namespace emc

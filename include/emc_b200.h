@@ -1,0 +1,155 @@
+/*
+ * emc_b200.h -- context API of the B200 EMC engine (libemc_b200.so).
+ *
+ * One context holds one dataset resident in HBM: detector geometry and mask,
+ * rotation table, photon-count patterns, model, weight grid and per-pattern
+ * scaling.  emc_iterate() runs one expand -> maximize -> compress iteration
+ * in the order of the reference's main loop (emc.c:989-1084) on the
+ * context's CUDA stream.
+ *
+ * Compared to the reference's API (include/emc.h) it adds: status codes on
+ * every call, 64-bit sizes, a poisson likelihood and trilinear interpolation
+ * next to the reference's gaussian / nearest-voxel ones, and a mixed-precision
+ * tensor-core path (tcgen05, FP16 hi+lo operands, FP32 accumulation, FP64
+ * log-sum-exp and normalisation).  All pointers are host pointers unless a
+ * function says otherwise.
+ */
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  EMC_OK = 0,
+  EMC_ERR_ARG = 1,      /* invalid argument or size */
+  EMC_ERR_CUDA = 2,     /* CUDA runtime error (emc_last_error has the text) */
+  EMC_ERR_OOM = 3,      /* device allocation failed */
+  EMC_ERR_TIMEOUT = 4,  /* a bounded device-side wait gave up (kernel returned early) */
+  EMC_ERR_STATE = 5,    /* call out of order (e.g. iterate before set_patterns) */
+  EMC_ERR_RANGE = 6,    /* data outside what the selected precision represents exactly */
+  EMC_ERR_UNSUPPORTED = 7
+} emc_status;
+
+enum { EMC_LL_GAUSS = 0, EMC_LL_POISSON = 1 };
+enum { EMC_INTERP_NEAREST = 0, EMC_INTERP_TRILINEAR = 1 };
+enum { EMC_PREC_FP32 = 0, EMC_PREC_MIXED = 1 };
+
+typedef struct {
+  int32_t side;         /* detector side in pixels == model side in voxels */
+  int32_t likelihood;   /* EMC_LL_* */
+  int32_t interp;       /* EMC_INTERP_* */
+  int32_t precision;    /* EMC_PREC_* */
+  int64_t n_patterns;
+  int64_t n_rotations;
+  float sigma;          /* gaussian width (reference emc.c:734 uses 0.4) */
+  float poisson_floor;  /* lower bound of W inside log W (poisson) */
+  int32_t device;       /* CUDA device ordinal */
+  int32_t flags;        /* reserved, 0 */
+} emc_config;
+
+typedef struct {
+  double sum_plogp;     /* sum P log P: the value emc.c:1018 logs as "likelihood" */
+  double total_loglik;  /* sum_p logsumexp_r LL_rp, FP64 */
+  double model_max;     /* after normalisation */
+  double total_resp;    /* sum_r T_r (== number of patterns) */
+} emc_iter_stats;
+
+typedef struct emc_context emc_context;
+
+/* Buffers readable with emc_get_buffer (host copy) / emc_device_buffer. */
+typedef enum {
+  EMC_BUF_MODEL = 0,    /* float [side^3] */
+  EMC_BUF_WEIGHT = 1,   /* float [side^3] weight grid of the last compress */
+  EMC_BUF_SCALING = 2,  /* float [N] */
+  EMC_BUF_RESP = 3,     /* float [R][N] responsibilities after maximize */
+  EMC_BUF_SLICES = 4,   /* float [R][Pa] expanded slices (FP32 path), Pa = active pixels */
+  EMC_BUF_TOTALRESP = 5 /* float [R] T_r */
+} emc_buffer;
+
+const char *emc_status_string(emc_status s);
+/* Text of the last error on this context (or of the last failed emc_create). */
+const char *emc_last_error(const emc_context *ctx);
+
+emc_status emc_create(const emc_config *cfg, emc_context **out);
+emc_status emc_destroy(emc_context *ctx);
+
+/* Pixel coordinates (emc.c:365-393 layout, [y*side+x]) and mask.  Pixels with
+ * mask != 0 enter the likelihood and scaling; mask == 1 pixels are inserted
+ * (emc_cuda.cu:120, emc_atomic.cu:30). */
+emc_status emc_set_geometry(emc_context *ctx, const float *x, const float *y, const float *z,
+                            const int32_t *mask);
+/* Unit quaternions [R][4] and rotation weights [R]. */
+emc_status emc_set_rotations(emc_context *ctx, const float *quaternions, const float *weights);
+/* Photon counts [N][side*side] (non-negative; the mixed path needs integers <= 2048). */
+emc_status emc_set_patterns(emc_context *ctx, const float *counts);
+emc_status emc_set_model(emc_context *ctx, const float *model);
+emc_status emc_set_scaling(emc_context *ctx, const float *scaling);
+
+/* One iteration.  stats may be NULL; with stats the call waits for the
+ * iteration, without it the work is only enqueued on the context stream. */
+emc_status emc_iterate(emc_context *ctx, emc_iter_stats *stats);
+/* Stage-by-stage form of emc_iterate (the three calls in order == one iteration). */
+emc_status emc_expand(emc_context *ctx);
+emc_status emc_maximize(emc_context *ctx);
+emc_status emc_compress(emc_context *ctx);
+
+emc_status emc_synchronize(emc_context *ctx);
+emc_status emc_get_model(emc_context *ctx, float *model);
+emc_status emc_get_scaling(emc_context *ctx, float *scaling);
+emc_status emc_get_buffer(emc_context *ctx, emc_buffer which, void *host, size_t bytes);
+/* Device pointer of a buffer (valid until emc_destroy). */
+emc_status emc_device_buffer(emc_context *ctx, emc_buffer which, void **dptr, size_t *bytes);
+/* Per-stage device timing.  With profiling on, every iteration records CUDA
+ * events around its stages.  emc_stage_times returns milliseconds of
+ * [expand, maximize contraction, responsibility pass (softmax + scaling),
+ * compress contraction + insertion, normalisation] of the previous profiled
+ * iteration (of the only one after the first), waiting for it if needed, so
+ * it can be called after each emc_iterate without draining the stream. */
+emc_status emc_set_profiling(emc_context *ctx, int on);
+emc_status emc_stage_times(emc_context *ctx, float ms[5]);
+/* Number of kernels this context has launched since creation. */
+int64_t emc_launch_count(const emc_context *ctx);
+/* cudaStream_t the context enqueues on. */
+void *emc_stream(emc_context *ctx);
+/* Number of active (mask != 0) pixels. */
+int64_t emc_active_pixels(const emc_context *ctx);
+
+/* ---- host-side input generators (reference host code, C++ here) ---- */
+
+int64_t emc_n_to_samples(int n); /* emc.c:43 */
+/* 600-cell rotation sampling of emc.c:49-363.  halve != 0 keeps one quaternion
+ * of each +-q pair (both give the same slice) and renormalises the weights.
+ * Returns R, or -1 on failure; quaternions/weights may be NULL to query R. */
+int64_t emc_generate_rotations(int n, int halve, float *quaternions, float *weights);
+/* emc.c:365-393, arrays [y*side+x]. */
+void emc_detector_coordinates(int side, double wavelength, double pixel_size,
+                              double detector_distance, float *x, float *y, float *z);
+
+typedef struct {
+  int32_t side;
+  int32_t n_scatterers;      /* point scatterers of unit strength */
+  double object_radius;      /* sphere radius as a fraction of the box side */
+  int64_t n_patterns;
+  double mean_photons;       /* mean photons per pattern */
+  double scale_sigma;        /* lognormal sigma of the per-pattern scale */
+  double beamstop_radius;    /* pixels; mask = 0 within this radius */
+  uint64_t seed;
+} emc_synth_config;
+
+/* Synthetic dataset: |F|^2 of point scatterers on a side^3 grid (model, may be
+ * NULL), counts [N][side^2] drawn as Poisson(slice at a uniform random
+ * rotation x mean_photons/sum(slice) x lognormal scale), mask [side^2],
+ * true_rotations [N][4] and true_scales [N] (either may be NULL).
+ * Coordinates x,y,z come from emc_detector_coordinates. */
+emc_status emc_synthesize(const emc_synth_config *sc, const float *x, const float *y,
+                          const float *z, float *true_model, float *counts, int32_t *mask,
+                          float *true_rotations, float *true_scales);
+/* Uniform [0,1) initial model (emc.c:893-898 with a counter-based generator). */
+void emc_random_model(int side, uint64_t seed, float *model);
+
+#ifdef __cplusplus
+}
+#endif
