@@ -17,8 +17,6 @@ using namespace emc;
 
 namespace {
 
-constexpr int64_t kRespChunk = 2048;  // rotations per block row of the responsibility sweeps
-
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 __global__ void gather_cols_kernel(const float* src, int64_t rows, int64_t ld, const int32_t* pix,
@@ -76,10 +74,8 @@ struct emc_context {
   __half *d_Kh = nullptr, *d_Kt = nullptr, *d_Bhi = nullptr, *d_Blo = nullptr;
   __half *d_Phi = nullptr, *d_Plo = nullptr;
   float* d_Y = nullptr;
-  float2* d_part = nullptr;
-  double *d_lse = nullptr, *d_den2 = nullptr, *d_plogp2 = nullptr;
-  float* d_Tpart = nullptr;
-  float* d_export = nullptr;
+  float4* d_part = nullptr;
+  double *d_lse = nullptr, *d_plogp = nullptr;
   CUtensorMap tmKh, tmKt, tmBhi, tmBlo, tmPhi, tmPlo;
   TcStatus* d_status = nullptr;
   // profiling: events at stage boundaries, kernel launch count
@@ -270,7 +266,6 @@ static emc_status alloc_work(emc_context* c) {
   c->Ppad = round_up(npa, 256);
   c->Rpad = round_up(R, 256);
   c->nrt = c->Rpad / 256;
-  const int64_t nchunk = (R + kRespChunk - 1) / kRespChunk;
   TRY(c->alloc(&c->d_Kh, c->Npad * c->Ppad, true));
   TRY(c->alloc(&c->d_Kt, c->Ppad * c->Npad, true));
   TRY(c->alloc(&c->d_Bhi, c->Rpad * c->Ppad, true));
@@ -280,9 +275,7 @@ static emc_status alloc_work(emc_context* c) {
   TRY(c->alloc(&c->d_Y, R * c->Npad));
   TRY(c->alloc(&c->d_part, c->nrt * N));
   TRY(c->alloc(&c->d_lse, N));
-  TRY(c->alloc(&c->d_den2, nchunk * N));
-  TRY(c->alloc(&c->d_plogp2, nchunk * N));
-  TRY(c->alloc(&c->d_Tpart, (c->Npad / 64) * R));
+  TRY(c->alloc(&c->d_plogp, N));
   bool ok = tc_encode_2d(&c->tmKh, c->d_Kh, c->Ppad, c->Npad, 128) &&
             tc_encode_2d(&c->tmBhi, c->d_Bhi, c->Ppad, c->Rpad, 256) &&
             tc_encode_2d(&c->tmBlo, c->d_Blo, c->Ppad, c->Rpad, 256) &&
@@ -460,8 +453,9 @@ emc_status emc_maximize(emc_context* c) {
     CK(c, launch_ll_fp32(l, c->st));
     c->mark(2);
     int nparts = 0;
-    CK(c, launch_softmax_fp32(c->d_LL, R, N, c->d_plogp_part, &nparts, c->st));
+    CK(c, launch_softmax_fp32(c->d_LL, R, N, c->d_plogp_part, &nparts, c->d_lse32, c->st));
     CK(c, launch_sum_f64(c->d_plogp_part, nparts, c->d_stats + 2, c->st));
+    CK(c, launch_sum_f64(c->d_lse32, N, c->d_stats + 3, c->st));
     int64_t nden = 0;
     if (c->gauss) {
       CrossArgs x{};
@@ -482,7 +476,7 @@ emc_status emc_maximize(emc_context* c) {
     CK(c, launch_scaling_finish(c->gauss ? c->d_patsq : c->d_patsum, c->d_den, nden, N,
                                 c->d_scaling, c->st));
     CK(c, launch_row_sums(c->d_LL, R, N, c->d_T, c->st));
-    c->launches += 7;
+    c->launches += 8;
   } else {
     MaxEpiArgs e{};
     e.N = N;
@@ -513,19 +507,17 @@ emc_status emc_maximize(emc_context* c) {
     a.patsum = c->d_patsum;
     a.gauss_inv = e.gauss_inv;
     a.lse = c->d_lse;
-    a.den_part = c->d_den2;
-    a.plogp_part = c->d_plogp2;
+    a.plogp = c->d_plogp;
     a.new_scaling = c->d_scaling;
     a.c0 = 1.0f;
     a.Phi = c->d_Phi;
     a.Plo = c->d_Plo;
-    a.Tpart = c->d_Tpart;
     a.T = c->d_T;
     a.P32 = nullptr;
-    CK(c, launch_resp_pass(a, kRespChunk, c->st));
-    CK(c, launch_sum_f64(c->d_plogp2, N, c->d_stats + 2, c->st));
+    CK(c, launch_resp_pass(a, c->st));
+    CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
     CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
-    c->launches += 9;
+    c->launches += 5;  // maximize contraction, combine, row sweep, 2 sums
   }
   c->mark(3);
   c->stage = 2;
@@ -630,7 +622,7 @@ emc_status emc_iterate(emc_context* c, emc_iter_stats* stats) {
     for (float v : t) T += v;
     stats->model_max = h[1];
     stats->sum_plogp = h[2];
-    stats->total_loglik = c->mixed ? h[3] : 0.0;
+    stats->total_loglik = h[3];
     stats->total_resp = T;
   }
   return EMC_OK;

@@ -45,9 +45,10 @@ struct LLArgs {
 cudaError_t launch_ll_fp32(const LLArgs& a, cudaStream_t st);
 
 // Per-pattern softmax over r of X[r][p] (in place), FP32 arithmetic as the
-// reference; plogp_part[blockIdx] receives sum P log P partials (FP64).
+// reference; plogp_part[blockIdx] receives sum P log P partials (FP64) and
+// lse[p] (optional) the pattern's log-sum-exp.
 cudaError_t launch_softmax_fp32(float* X, int64_t R, int64_t N, double* plogp_part,
-                                int* nparts, cudaStream_t st);
+                                int* nparts, double* lse, cudaStream_t st);
 // sum of x log x over n floats into *out (FP64).
 cudaError_t launch_xlogx_sum(const float* x, int64_t n, double* out, double* scratch,
                              cudaStream_t st);

@@ -52,40 +52,54 @@ __device__ float block_max(float v, float* red) {
 // ------------------------------------------------------------------ expand --
 // One block per rotation; threads stride over pixels.  emc_cuda.cu:51-111 for
 // the nearest mode (exclusive lower bound), trilinear otherwise.
+// Four pixels per thread and iteration: their gathers are independent, so
+// four L2 round trips are in flight per thread.
+constexpr int kExpandUnroll = 4;
 __global__ void __launch_bounds__(kBlock) expand_kernel(const ExpandArgs a) {
   __shared__ double red[32];
   const int64_t r = blockIdx.x;
   float m[9];
   emc_voxel::rotation_matrix(a.quat + 4 * r, m);
   double stat = 0.0;
-  for (int64_t i = threadIdx.x; i < a.ld; i += blockDim.x) {
-    float w = 0.0f;
-    const bool real = i < a.npix;
-    if (real) {
-      float u[3];
-      emc_voxel::position(m, a.side, a.cx[i], a.cy[i], a.cz[i], u);
-      if (a.interp == 0) {
-        int64_t v;
-        if (emc_voxel::nearest(u, a.side, 1, &v)) w = __ldg(a.model + v);
-      } else {
-        int64_t v[8];
-        float ww[8];
-        const int n = emc_voxel::trilinear(u, a.side, v, ww);
-        for (int c = 0; c < n; ++c) w = fmaf(ww[c], __ldg(a.model + v[c]), w);
+  const int64_t step = (int64_t)blockDim.x * kExpandUnroll;
+  for (int64_t i0 = threadIdx.x; i0 < a.ld; i0 += step) {
+    float w[kExpandUnroll];
+#pragma unroll
+    for (int u = 0; u < kExpandUnroll; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x;
+      w[u] = 0.0f;
+      if (i < a.npix) {
+        float pos[3];
+        emc_voxel::position(m, a.side, __ldg(a.cx + i), __ldg(a.cy + i), __ldg(a.cz + i), pos);
+        if (a.interp == 0) {
+          int64_t v;
+          if (emc_voxel::nearest(pos, a.side, 1, &v)) w[u] = __ldg(a.model + v);
+        } else {
+          int64_t v[8];
+          float ww[8];
+          const int n = emc_voxel::trilinear(pos, a.side, v, ww);
+          for (int c = 0; c < n; ++c) w[u] = fmaf(ww[c], __ldg(a.model + v[c]), w[u]);
+        }
       }
-      if (a.stat != STAT_NONE && (!a.stat_mask || a.stat_mask[i] != 0))
-        stat += a.stat == STAT_SUMSQ ? (double)w * w : (double)w;
     }
-    const int64_t o = r * a.ld + i;
-    if (a.out == EXP_F32) {
-      a.out_f32[o] = w;
-    } else if (a.out == EXP_LOG_F32) {
-      a.out_f32[o] = real ? logf(fmaxf(w, a.floor_)) : 0.0f;
-    } else {
-      const float x = real ? (a.log_split ? logf(fmaxf(w, a.floor_)) : w) : 0.0f;
-      const __half hi = __float2half_rn(x);
-      a.out_hi[o] = hi;
-      a.out_lo[o] = __float2half_rn(x - __half2float(hi));
+#pragma unroll
+    for (int u = 0; u < kExpandUnroll; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x;
+      if (i >= a.ld) break;
+      const bool real = i < a.npix;
+      if (real && a.stat != STAT_NONE && (!a.stat_mask || a.stat_mask[i] != 0))
+        stat += a.stat == STAT_SUMSQ ? (double)w[u] * w[u] : (double)w[u];
+      const int64_t o = r * a.ld + i;
+      if (a.out == EXP_F32) {
+        a.out_f32[o] = w[u];
+      } else if (a.out == EXP_LOG_F32) {
+        a.out_f32[o] = real ? logf(fmaxf(w[u], a.floor_)) : 0.0f;
+      } else {
+        const float x = real ? (a.log_split ? logf(fmaxf(w[u], a.floor_)) : w[u]) : 0.0f;
+        const __half hi = __float2half_rn(x);
+        a.out_hi[o] = hi;
+        a.out_lo[o] = __float2half_rn(x - __half2float(hi));
+      }
     }
   }
   if (a.rowstat) {
@@ -288,7 +302,7 @@ struct OpCompress {
 // ----------------------------------------------------------------- softmax --
 // 32 patterns per block (lane == pattern), 8 warps share the rotations.
 __global__ void __launch_bounds__(kBlock) softmax_kernel(float* X, int64_t R, int64_t N,
-                                                         double* plogp_part) {
+                                                         double* plogp_part, double* lse) {
   __shared__ float smax[8][32];
   __shared__ float ssum[8][32];
   __shared__ double sred[8][32];
@@ -313,6 +327,7 @@ __global__ void __launch_bounds__(kBlock) softmax_kernel(float* X, int64_t R, in
   s = 0.0f;
   for (int k = 0; k < 8; ++k) s += ssum[k][lane];
   const float inv = 1.0f / s;
+  if (lse && ok && w == 0) lse[p] = (double)mx + log((double)s);
   double pl = 0.0;
   if (ok)
     for (int64_t r = w; r < R; r += 8) {
@@ -534,10 +549,10 @@ cudaError_t launch_ll_fp32(const LLArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_softmax_fp32(float* X, int64_t R, int64_t N, double* plogp_part, int* nparts,
-                                cudaStream_t st) {
+                                double* lse, cudaStream_t st) {
   const int64_t nb = (N + 31) / 32;
   if (nparts) *nparts = (int)nb;
-  softmax_kernel<<<(unsigned)nb, kBlock, 0, st>>>(X, R, N, plogp_part);
+  softmax_kernel<<<(unsigned)nb, kBlock, 0, st>>>(X, R, N, plogp_part, lse);
   return cudaGetLastError();
 }
 

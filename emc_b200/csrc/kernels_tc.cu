@@ -335,13 +335,18 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // --------------------------------------------------------------- epilogues --
 
-// maximize: row = pattern, column = rotation.
+// maximize: row = pattern, column = rotation.  Besides Y it emits, per
+// pattern and 256-rotation tile k, the partials of an online log-sum-exp
+// relative to the tile maximum m_k:
+//   s_k = sum e^(LL-m_k),  d_k = sum e^(LL-m_k) X,  q_k = sum e^(LL-m_k) (LL-m_k)
+// with X the scaling denominator term (gaussian: C_rp, poisson: sum W_r).  The
+// combine kernel turns them into lse_p, the new scaling and sum P log P.
 struct EpiMax {
   static constexpr int kSmemBytes = BN * 8;
   MaxEpiArgs a;
   int64_t n0, ntile, p;
   bool pv;
-  float phi, mx, sm;
+  float phi, mx, sm, sd, sq;
   double c1, c0;
 
   __device__ void tile_begin(int64_t mt, int64_t nt, int tid, uint8_t* smem) {
@@ -361,7 +366,7 @@ struct EpiMax {
     pv = p < a.N;
     phi = pv ? a.scaling[p] : 1.0f;
     mx = -FLT_MAX;
-    sm = 0.0f;
+    sm = sd = sq = 0.0f;
     if (!a.poisson) {
       // LL = (2 C / phi - sum S^2 - sum K^2 / phi^2) / (2 cnt sigma^2)
       c1 = 2.0 * a.gauss_inv / (double)phi;
@@ -370,7 +375,7 @@ struct EpiMax {
   }
   __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) {
     const double* rs = reinterpret_cast<const double*>(smem);
-    float ll[16];
+    float ll[16], xs[16];
     float cmax = -FLT_MAX;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
@@ -379,6 +384,7 @@ struct EpiMax {
       const double l = a.poisson ? (double)x - (double)phi * rs[c + k]
                                  : fma((double)x, c1, c0 - rs[c + k]);
       ll[k] = (float)l;
+      xs[k] = a.poisson ? (float)rs[c + k] : x;
       const bool ok = pv && r < a.R;
       if (ok) {
         a.Y[r * a.ldY + p] = a.poisson ? ll[k] : x;
@@ -389,16 +395,25 @@ struct EpiMax {
     }
     if (cmax > -FLT_MAX) {
       if (cmax > mx) {
-        sm *= expf(mx - cmax);
+        const float f = mx > -FLT_MAX ? expf(mx - cmax) : 0.0f;
+        sq = f * (sq + (mx - cmax) * sm);
+        sm *= f;
+        sd *= f;
         mx = cmax;
       }
 #pragma unroll
       for (int k = 0; k < 16; ++k)
-        if (ll[k] > -FLT_MAX) sm += expf(ll[k] - mx);
+        if (ll[k] > -FLT_MAX) {
+          const float dl = ll[k] - mx;
+          const float e = expf(dl);
+          sm += e;
+          sd = fmaf(e, xs[k], sd);
+          sq = fmaf(e, dl, sq);
+        }
     }
   }
   __device__ void row_end() {
-    if (pv) a.part[ntile * a.N + p] = make_float2(mx, sm);
+    if (pv) a.part[ntile * a.N + p] = make_float4(mx, sm, sd, sq);
   }
 };
 
@@ -432,7 +447,7 @@ struct EpiCmp {
         active = true;
         const float rw = a.rotw[r];
         wT = rw * T;
-        wU = rw * a.inv_c0;
+        wU = wT * a.inv_c0;  // accumulator holds U_r / T_r (rows of P' are divided by T_r)
         emc_voxel::rotation_matrix(a.quat + 4 * r, m);
       }
     }
@@ -490,17 +505,37 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-__global__ void lse_kernel(const float2* part, int64_t nparts, int64_t N, double* lse) {
+// Per pattern: lse_p, the new scaling and sum P log P from the tile partials.
+//   lse = M + log sum_k s_k e^(m_k - M)
+//   D   = sum_k d_k e^(m_k - lse)                       (= sum_r P_rp X_rp)
+//   sum_r P log P = sum_k e^(m_k - lse) (q_k + (m_k - lse) s_k)
+__global__ void combine_kernel(const RespArgs a) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= N) return;
+  if (p >= a.N) return;
   float M = -FLT_MAX;
-  for (int64_t k = 0; k < nparts; ++k) M = fmaxf(M, part[k * N + p].x);
+  for (int64_t k = 0; k < a.nparts; ++k) M = fmaxf(M, a.part[k * a.N + p].x);
   double S = 0.0;
-  for (int64_t k = 0; k < nparts; ++k) {
-    const float2 v = part[k * N + p];
+  for (int64_t k = 0; k < a.nparts; ++k) {
+    const float4 v = a.part[k * a.N + p];
     if (v.y > 0.0f) S += (double)v.y * exp((double)v.x - (double)M);
   }
-  lse[p] = (double)M + log(S);
+  const double lse = (double)M + log(S);
+  double D = 0.0, Q = 0.0;
+  for (int64_t k = 0; k < a.nparts; ++k) {
+    const float4 v = a.part[k * a.N + p];
+    if (!(v.y > 0.0f)) continue;
+    const double dm = (double)v.x - lse;
+    const double f = exp(dm);
+    D += (double)v.z * f;
+    Q += f * ((double)v.w + dm * (double)v.y);
+  }
+  a.lse[p] = lse;
+  a.plogp[p] = Q;
+  // emc_cuda.cu:226 for gaussian; poisson MLE sum K / sum_r P_rp sum W_r
+  const double num = a.poisson ? a.patsum[p] : a.patstat[p];
+  float phi = a.scaling[p];
+  if (num > 0.0 && D > 0.0) phi = (float)(num / D);
+  a.new_scaling[p] = phi;
 }
 
 // LL of one element from the stored Y (poisson: LL itself; gaussian: C).
@@ -525,125 +560,72 @@ __device__ __forceinline__ LLFromY make_llf(const RespArgs& a, int64_t p) {
   return f;
 }
 
-// Sweep 1: for each pattern, D_p = sum_r P_rp X_rp and sum P log P over a chunk
-// of rotations.  Lane handles patterns 2l, 2l+1 of a 64-pattern block; the 8
-// warps interleave over the chunk's rotations.
-__global__ void __launch_bounds__(256) sweep1_kernel(const RespArgs a, int64_t rchunk) {
-  __shared__ double sden[8][64], spl[8][64];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t p0 = (int64_t)blockIdx.x * 64 + 2 * lane;
-  const int64_t r0 = (int64_t)blockIdx.y * rchunk;
-  const int64_t r1 = min(a.R, r0 + rchunk);
-  const bool v0 = p0 < a.N, v1 = p0 + 1 < a.N;
-  const LLFromY f0 = make_llf(a, p0), f1 = make_llf(a, p0 + 1);
-  const double l0 = v0 ? a.lse[p0] : 0.0, l1 = v1 ? a.lse[p0 + 1] : 0.0;
-  double d0 = 0, d1 = 0, q0 = 0, q1 = 0;
-  for (int64_t r = r0 + w; r < r1; r += 8) {
-    const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
-    const float* yr = a.Y + r * a.ldY + p0;
-    float y0 = 0.f, y1 = 0.f;
-    if (v1) {
-      const float2 y = *reinterpret_cast<const float2*>(yr);
-      y0 = y.x;
-      y1 = y.y;
-    } else if (v0) {
-      y0 = yr[0];
-    }
-    if (v0) {
-      const double e = f0(y0, rs) - l0;
-      const double P = (double)expf((float)e);
-      d0 += P * (a.poisson ? a.rowstat[r] : (double)y0);
-      q0 += P * e;
-    }
-    if (v1) {
-      const double e = f1(y1, rs) - l1;
-      const double P = (double)expf((float)e);
-      d1 += P * (a.poisson ? a.rowstat[r] : (double)y1);
-      q1 += P * e;
-    }
-  }
-  sden[w][2 * lane] = d0;
-  sden[w][2 * lane + 1] = d1;
-  spl[w][2 * lane] = q0;
-  spl[w][2 * lane + 1] = q1;
-  __syncthreads();
-  if (threadIdx.x < 64) {
-    const int64_t p = (int64_t)blockIdx.x * 64 + threadIdx.x;
-    double d = 0, q = 0;
-    for (int k = 0; k < 8; ++k) {
-      d += sden[k][threadIdx.x];
-      q += spl[k][threadIdx.x];
-    }
-    if (p < a.N) {
-      a.den_part[(int64_t)blockIdx.y * a.N + p] = d;
-      a.plogp_part[(int64_t)blockIdx.y * a.N + p] = q;
-    }
-  }
-}
-
-// new phi (emc_cuda.cu:226 for gaussian; poisson MLE sum K / sum_r P_rp sum W_r)
-__global__ void finish_scaling_kernel(const RespArgs a, int64_t nchunk) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= a.N) return;
-  double d = 0, q = 0;
-  for (int64_t k = 0; k < nchunk; ++k) {
-    d += a.den_part[k * a.N + p];
-    q += a.plogp_part[k * a.N + p];
-  }
-  a.plogp_part[p] = q;  // per-pattern sum P log P (row 0 reused)
-  const double num = a.poisson ? a.patsum[p] : a.patstat[p];
-  float phi = a.scaling[p];
-  if (num > 0.0 && d > 0.0) phi = (float)(num / d);
-  a.new_scaling[p] = phi;
-}
-
-// Sweep 2: P' = c0 P / phi_new split into FP16 hi + lo, T_r partial sums.
-__global__ void __launch_bounds__(256) sweep2_kernel(const RespArgs a, int64_t rchunk) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t p0 = (int64_t)blockIdx.x * 64 + 2 * lane;
-  const int64_t r0 = (int64_t)blockIdx.y * rchunk;
-  const int64_t r1 = min(a.R, r0 + rchunk);
-  const bool v0 = p0 < a.N, v1 = p0 + 1 < a.N;
-  const LLFromY f0 = make_llf(a, p0), f1 = make_llf(a, p0 + 1);
-  const double l0 = v0 ? a.lse[p0] : 0.0, l1 = v1 ? a.lse[p0 + 1] : 0.0;
-  const float g0 = v0 ? a.c0 / a.new_scaling[p0] : 0.0f;
-  const float g1 = v1 ? a.c0 / a.new_scaling[p0 + 1] : 0.0f;
-  for (int64_t r = r0 + w; r < r1; r += 8) {
-    const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
-    const float* yr = a.Y + r * a.ldY + p0;
-    float P0 = 0.f, P1 = 0.f;
-    if (v1) {
-      const float2 y = *reinterpret_cast<const float2*>(yr);
-      P0 = expf((float)(f0(y.x, rs) - l0));
-      P1 = expf((float)(f1(y.y, rs) - l1));
-    } else if (v0) {
-      P0 = expf((float)(f0(yr[0], rs) - l0));
-    }
-    const float x0 = P0 * g0, x1 = P1 * g1;
-    const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-    const __half e0 = __float2half_rn(x0 - __half2float(h0));
-    const __half e1 = __float2half_rn(x1 - __half2float(h1));
-    const int64_t o = r * a.ldP + p0;
-    if (p0 < a.ldP) {
-      *reinterpret_cast<__half2*>(a.Phi + o) = __halves2half2(h0, h1);
-      *reinterpret_cast<__half2*>(a.Plo + o) = __halves2half2(e0, e1);
+// One block per rotation r.  Pass 1 reads the row of Y once from HBM, forms
+// P_rp = exp(LL_rp - lse_p), keeps it in shared memory and sums T_r.  Pass 2
+// writes P'_rp = c0 P_rp / (T_r phi_p) as FP16 hi + lo.  Dividing by T_r (the
+// slice average of emc_atomic.cu:105-111) keeps every entry of the row in
+// [0, c0/phi_p], so rotations with a tiny total responsibility keep their
+// relative precision instead of underflowing FP16.  Rows longer than the
+// shared buffer recompute P from Y in pass 2.
+constexpr int kRowThreads = 512;
+__global__ void __launch_bounds__(kRowThreads) row_kernel(const RespArgs a, int use_smem) {
+  extern __shared__ float prow[];
+  __shared__ double red[kRowThreads / 32];
+  const int64_t r = blockIdx.x;
+  const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
+  const float* yrow = a.Y + r * a.ldY;
+  const int64_t npair = (a.N + 1) / 2;
+  auto prob = [&](int64_t p, float y) -> float {
+    const LLFromY f = make_llf(a, p);
+    return expf((float)(f(y, rs) - a.lse[p]));
+  };
+  double t = 0.0;
+  for (int64_t q = threadIdx.x; q < npair; q += kRowThreads) {
+    const int64_t p = 2 * q;
+    const float2 y = *reinterpret_cast<const float2*>(yrow + p);
+    const float P0 = prob(p, y.x);
+    const float P1 = p + 1 < a.N ? prob(p + 1, y.y) : 0.0f;
+    if (use_smem) {
+      prow[p] = P0;
+      prow[p + 1] = P1;
     }
     if (a.P32) {
-      if (v0) a.P32[r * a.N + p0] = P0;
-      if (v1) a.P32[r * a.N + p0 + 1] = P1;
+      a.P32[r * a.N + p] = P0;
+      if (p + 1 < a.N) a.P32[r * a.N + p + 1] = P1;
     }
-    double t = (double)P0 + (double)P1;
-    t = warp_sum_d(t);
-    if (lane == 0) a.Tpart[(int64_t)blockIdx.x * a.R + r] = (float)t;  // one writer per (block, r)
+    t += (double)P0 + (double)P1;
   }
-}
-
-__global__ void treduce_kernel(const float* Tpart, int64_t nb, int64_t R, float* T) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= R) return;
-  double s = 0;
-  for (int64_t b = 0; b < nb; ++b) s += Tpart[b * R + r];
-  T[r] = (float)s;
+  t = warp_sum_d(t);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  double T = 0.0;
+  for (int i = 0; i < kRowThreads / 32; ++i) T += red[i];
+  if (threadIdx.x == 0) a.T[r] = (float)T;
+  const float invT = T > 1e-10 ? (float)(1.0 / T) : 0.0f;
+  const int64_t lpair = a.ldP / 2;
+  __half2* hi = reinterpret_cast<__half2*>(a.Phi + r * a.ldP);
+  __half2* lo = reinterpret_cast<__half2*>(a.Plo + r * a.ldP);
+  for (int64_t q = threadIdx.x; q < lpair; q += kRowThreads) {
+    const int64_t p = 2 * q;
+    float P0 = 0.0f, P1 = 0.0f;
+    if (p < a.N) {
+      if (use_smem) {
+        P0 = prow[p];
+        P1 = prow[p + 1];
+      } else {
+        const float2 y = *reinterpret_cast<const float2*>(yrow + p);
+        P0 = prob(p, y.x);
+        P1 = p + 1 < a.N ? prob(p + 1, y.y) : 0.0f;
+      }
+    }
+    const float g0 = p < a.N ? a.c0 / a.new_scaling[p] : 0.0f;
+    const float g1 = p + 1 < a.N ? a.c0 / a.new_scaling[p + 1] : 0.0f;
+    const float x0 = P0 * invT * g0, x1 = P1 * invT * g1;
+    const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+    hi[q] = __halves2half2(h0, h1);
+    lo[q] = __halves2half2(__float2half_rn(x0 - __half2float(h0)),
+                           __float2half_rn(x1 - __half2float(h1)));
+  }
 }
 
 __global__ void export_kernel(const RespArgs a, float* P) {
@@ -733,18 +715,16 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
                                   status, num_sms, st);
 }
 
-cudaError_t launch_resp_pass(RespArgs& a, int64_t rchunk, cudaStream_t st) {
-  lse_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, st>>>(a.part, a.nparts, a.N, a.lse);
-  const int64_t nchunk = (a.R + rchunk - 1) / rchunk;
-  const int64_t pblocks = (a.ldP + 63) / 64;
-  dim3 grid((unsigned)((a.N + 63) / 64), (unsigned)nchunk);
-  sweep1_kernel<<<grid, 256, 0, st>>>(a, rchunk);
-  finish_scaling_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, st>>>(a, nchunk);
-  cudaError_t e = cudaMemsetAsync(a.Tpart, 0, sizeof(float) * pblocks * a.R, st);
+cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {
+  combine_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, st>>>(a);
+  // the row buffer holds N floats (N rounded up to even) when it fits in shared memory
+  const size_t row_bytes = sizeof(float) * (size_t)((a.N + 1) / 2 * 2);
+  const int use_smem = row_bytes <= 200 * 1024 ? 1 : 0;
+  const size_t dyn = use_smem ? row_bytes : 0;
+  cudaError_t e = cudaFuncSetAttribute(row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(dyn > 0 ? dyn : 1024));
   if (e != cudaSuccess) return e;
-  dim3 grid2((unsigned)pblocks, (unsigned)nchunk);
-  sweep2_kernel<<<grid2, 256, 0, st>>>(a, rchunk);
-  treduce_kernel<<<(unsigned)((a.R + 255) / 256), 256, 0, st>>>(a.Tpart, pblocks, a.R, a.T);
+  row_kernel<<<(unsigned)a.R, kRowThreads, dyn, st>>>(a, use_smem);
   return cudaGetLastError();
 }
 

@@ -202,7 +202,8 @@ void cuda_normalize_responsabilities(real* d_respons, int N_slices, int N_images
     return;
   }
   int np = 0;
-  ok(launch_softmax_fp32(d_respons, N_slices, N_images, part, &np, 0), "normalize_responsabilities");
+  ok(launch_softmax_fp32(d_respons, N_slices, N_images, part, &np, nullptr, 0),
+     "normalize_responsabilities");
 }
 
 real cuda_total_respons(real* d_respons, real* respons, int n) {

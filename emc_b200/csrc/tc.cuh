@@ -22,8 +22,8 @@ bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t ro
 
 // Maximize contraction: acc[p][r] = sum_j K[p][j] (B_hi[r][j] + B_lo[r][j]),
 // 128 patterns x 256 rotations per tile.  Epilogue writes Y[r][p] (LL for
-// poisson, the cross term C for gaussian) and per-pattern partial
-// (max, sum exp) of LL over the tile's rotations.
+// poisson, the cross term C for gaussian) and per pattern and rotation tile
+// the online log-sum-exp partials (m, s, d, q) described in kernels_tc.cu.
 struct MaxEpiArgs {
   int64_t N, R, ldY;
   int poisson;
@@ -32,15 +32,16 @@ struct MaxEpiArgs {
   const double* patstat;   // [N] gaussian: sum K_p^2
   double gauss_inv;        // 1 / (2 cnt sigma^2)
   float* Y;                // [R][ldY]
-  float2* part;            // [ceil(R/256)][N] (max, sum exp(LL - max))
+  float4* part;            // [ceil(R/256)][N]
 };
 cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
                                const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
                                int64_t Kpad, const MaxEpiArgs& e, TcStatus* status,
                                int num_sms, cudaStream_t st);
 
-// Compress contraction: acc[r][j] = sum_p (P'_hi + P'_lo)[r][p] Kt[j][p],
-// 128 rotations x 256 pixels per tile, inserted in the epilogue.
+// Compress contraction: acc[r][j] = sum_p (P'_hi + P'_lo)[r][p] Kt[j][p] with
+// P' = c0 P / (T_r phi_p), i.e. the averaged slice U_r / T_r; 128 rotations x
+// 256 pixels per tile, inserted in the epilogue.
 struct CmpEpiArgs {
   int64_t R, npa;
   int side, interp;
@@ -60,29 +61,30 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
                                int64_t Npad, const CmpEpiArgs& e, TcStatus* status, int num_sms,
                                cudaStream_t st);
 
-// Responsibility pass of the mixed path.
+// Responsibility pass of the mixed path: combine the tile partials per
+// pattern (lse, new scaling, sum P log P), then one sweep over the rows of Y
+// that writes T_r and the compress operand P' = c0 P / (T_r phi_new) as FP16
+// hi + lo.
 struct RespArgs {
   int64_t N, R, ldY, ldP, nparts;  // nparts = number of 256-rotation tiles
   int poisson;
   const float* Y;
-  const float2* part;
+  const float4* part;
   const float* scaling;    // phi used for LL
   const double* rowstat;
   const double* patstat;   // gaussian: sum K^2 (also the scaling numerator)
   const double* patsum;    // poisson: sum K (scaling numerator)
   double gauss_inv;
   double* lse;             // [N]
-  double* den_part;        // [nchunk][N]
-  double* plogp_part;      // [nchunk][N]
+  double* plogp;           // [N] per-pattern sum P log P
   float* new_scaling;      // [N]
   float c0;                // global scale of P'
   __half* Phi;             // [Rpad][ldP]
   __half* Plo;
-  float* Tpart;            // [ceil(N/64)][R]
   float* T;                // [R]
   float* P32;              // optional [R][N] FP32 responsibilities
 };
-cudaError_t launch_resp_pass(RespArgs& a, int64_t rchunk, cudaStream_t st);
+cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st);
 // FP32 responsibilities [R][N] from Y and lse (readback / tests).
 cudaError_t launch_resp_export(const RespArgs& a, float* P, cudaStream_t st);
 // Builds the FP16 pattern operands: Kh[Npad][Ppad] and Kt[Ppad][Npad] from
