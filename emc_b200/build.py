@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "libemc_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = ["host.cpp", "kernels_fp32.cu", "kernels_tc.cu", "context.cu", "legacy.cu"]
+SOURCES = ["host.cpp", "kernels_fp32.cu", "kernels_tc.cu", "context.cu", "legacy.cu", "noalloc.cu"]
 HEADERS = ["voxel.h", "kernels.cuh", "tc.cuh"]
 PUBLIC = [os.path.join(REPO, "include", h) for h in ("emc.h", "emc_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

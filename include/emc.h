@@ -91,6 +91,25 @@ void cuda_allocate_scaling(real **scaling, int N_images);
 void cuda_normalize_responsabilities(real *d_respons, int N_slices, int N_images);
 real cuda_total_respons(real *d_respons, real *respons, int n);
 
+/* No counterpart in the reference.  cuda_normalize_responsabilities followed
+ * by cuda_total_respons, for callers that cannot call cudaMalloc: code that
+ * runs while a stream is being captured into a CUDA graph, processes held to a
+ * fixed device-memory budget, or an allocator-owning host framework that
+ * forbids allocations behind its back.  The kernels' scratch (one FP64
+ * partial per 32 patterns) is a fixed 512 KB array in the library's device
+ * image instead of memory the library allocates, so this function allocates
+ * nothing; every GPU that loads the library holds that array until exit.
+ * Limit: N_images <= 2,097,152; larger calls are rejected with status 1.
+ * d_respons [N_slices][N_images] is normalised in place on `stream` (a
+ * cudaStream_t, NULL for the default stream); if sum_plogp is not NULL it
+ * receives sum P log P and the call waits for the stream.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (other streams, other host threads) race.
+ * Returns 0 on success, 1 for invalid or too large sizes, 2 for a CUDA error. */
+int cuda_normalize_responsabilities_noalloc(real *d_respons, int N_slices, int N_images,
+                                            void *stream, double *sum_plogp);
+
 /* Status of the last call made through this header on the calling thread
  * (0 = success).  The reference reports errors only by printf
  * (emc_cuda.cu:178-181); this adds a way to read them. */
