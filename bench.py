@@ -316,13 +316,20 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(ext):
             e0.record()
+        parts = np.zeros(4)
         for _ in range(steps_e):
+            t0 = time.perf_counter()
             ctx.set_patterns(host_counts)
+            t1 = time.perf_counter()
             ctx.set_model(pm)
             ctx.set_scaling(ps)
             ctx.iterate(stats=False)
+            t2 = time.perf_counter()
             m = ctx.get_model()
+            t3 = time.perf_counter()
             s = ctx.get_scaling()
+            t4 = time.perf_counter()
+            parts += [t1 - t0, t2 - t1, t3 - t2, t4 - t3]
         with torch.cuda.stream(ext):
             e1.record()
         torch.cuda.synchronize()
@@ -335,7 +342,9 @@ def main():
         e2e = {"value": N * R * world / (ms_e / 1e3), "unit": UNIT, "ms_per_step": ms_e,
                "h2d_bytes_per_step": int(host_counts.nbytes + pm.nbytes + ps.nbytes),
                "d2h_bytes_per_step": int(m.nbytes + s.nbytes),
-               "api": "emc_set_patterns/model/scaling + emc_iterate + emc_get_model/scaling"}
+               "api": "emc_set_patterns/model/scaling + emc_iterate + emc_get_model/scaling",
+               "host_ms": dict(zip(["set_patterns", "enqueue_iteration", "get_model",
+                                    "get_scaling"], [round(x * 1e3 / steps_e, 3) for x in parts]))}
 
     # responsibility error of this path vs the FP64 oracle on a sample, and the CPU baseline
     cpu = None

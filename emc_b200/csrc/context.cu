@@ -55,7 +55,8 @@ struct emc_context {
   // rotations
   float *d_quat = nullptr, *d_rotw = nullptr;
   // patterns
-  float* d_K = nullptr;  // [N][npa] FP32 (FP32 path)
+  float* d_K = nullptr;      // [N][npa] FP32 counts on the active pixels
+  float* d_stage = nullptr;  // [N][side^2] upload staging
   double *d_patsq = nullptr, *d_patsum = nullptr;
   // model state
   float *d_model = nullptr, *d_weight = nullptr, *d_scaling = nullptr, *d_scaling_prev = nullptr;
@@ -75,7 +76,9 @@ struct emc_context {
   __half *d_Phi = nullptr, *d_Plo = nullptr;
   float* d_Y = nullptr;
   float4* d_part = nullptr;
+  float2* d_acc = nullptr;  // interleaved (model, weight) accumulators
   double *d_lse = nullptr, *d_plogp = nullptr;
+  float* d_Tpart = nullptr;
   CUtensorMap tmKh, tmKt, tmBhi, tmBlo, tmPhi, tmPlo;
   TcStatus* d_status = nullptr;
   // profiling: events at stage boundaries, kernel launch count
@@ -266,6 +269,7 @@ static emc_status alloc_work(emc_context* c) {
   c->Ppad = round_up(npa, 256);
   c->Rpad = round_up(R, 256);
   c->nrt = c->Rpad / 256;
+  TRY(c->alloc(&c->d_acc, c->M, true));
   TRY(c->alloc(&c->d_Kh, c->Npad * c->Ppad, true));
   TRY(c->alloc(&c->d_Kt, c->Ppad * c->Npad, true));
   TRY(c->alloc(&c->d_Bhi, c->Rpad * c->Ppad, true));
@@ -276,12 +280,13 @@ static emc_status alloc_work(emc_context* c) {
   TRY(c->alloc(&c->d_part, c->nrt * N));
   TRY(c->alloc(&c->d_lse, N));
   TRY(c->alloc(&c->d_plogp, N));
-  bool ok = tc_encode_2d(&c->tmKh, c->d_Kh, c->Ppad, c->Npad, 128) &&
-            tc_encode_2d(&c->tmBhi, c->d_Bhi, c->Ppad, c->Rpad, 256) &&
-            tc_encode_2d(&c->tmBlo, c->d_Blo, c->Ppad, c->Rpad, 256) &&
-            tc_encode_2d(&c->tmPhi, c->d_Phi, c->Npad, c->Rpad, 128) &&
-            tc_encode_2d(&c->tmPlo, c->d_Plo, c->Npad, c->Rpad, 128) &&
-            tc_encode_2d(&c->tmKt, c->d_Kt, c->Npad, c->Ppad, 256);
+  TRY(c->alloc(&c->d_Tpart, ((N + 1023) / 1024) * R));
+  bool ok = tc_encode_2d(&c->tmKh, c->d_Kh, c->Ppad, c->Npad, 128, kMaximizeBK) &&
+            tc_encode_2d(&c->tmBhi, c->d_Bhi, c->Ppad, c->Rpad, 256, kMaximizeBK) &&
+            tc_encode_2d(&c->tmBlo, c->d_Blo, c->Ppad, c->Rpad, 256, kMaximizeBK) &&
+            tc_encode_2d(&c->tmPhi, c->d_Phi, c->Npad, c->Rpad, 128, kCompressBK) &&
+            tc_encode_2d(&c->tmPlo, c->d_Plo, c->Npad, c->Rpad, 128, kCompressBK) &&
+            tc_encode_2d(&c->tmKt, c->d_Kt, c->Npad, c->Ppad, 256, kCompressBK);
   if (!ok) return c->fail(EMC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   return EMC_OK;
 }
@@ -330,16 +335,12 @@ emc_status emc_set_patterns(emc_context* c, const float* counts) {
   if (!c || !counts) return EMC_ERR_ARG;
   if (!c->have_geom) return c->fail(EMC_ERR_STATE, "set the geometry before the patterns");
   const int64_t N = c->N, npa = c->npa;
-  // full images to the device, then gathered to the active pixels there
-  float* full = nullptr;
-  CK(c, cudaMallocAsync((void**)&full, sizeof(float) * N * c->npix, c->st));
+  // full images to the device, then gathered to the active pixels there;
+  // the staging buffers are allocated on the first call and kept
+  if (!c->d_stage) TRY(c->alloc(&c->d_stage, N * c->npix));
+  if (c->mixed && !c->d_K) TRY(c->alloc(&c->d_K, N * npa));
+  float* full = c->d_stage;
   float* compact = c->d_K;
-  emc_status s = EMC_OK;
-  if (c->mixed && (s = c->cuda(cudaMallocAsync((void**)&compact, sizeof(float) * N * npa, c->st),
-                               "cudaMallocAsync")) != EMC_OK) {
-    cudaFreeAsync(full, c->st);
-    return s;
-  }
   cudaError_t e = cudaMemcpyAsync(full, counts, sizeof(float) * N * c->npix,
                                   cudaMemcpyHostToDevice, c->st);
   if (e == cudaSuccess) {
@@ -361,8 +362,6 @@ emc_status emc_set_patterns(emc_context* c, const float* counts) {
       e = launch_pack_patterns(compact, N, npa, c->Npad, c->Ppad, c->d_Kh, c->d_Kt, d_bad, c->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
   }
-  cudaFreeAsync(full, c->st);
-  if (c->mixed) cudaFreeAsync(compact, c->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return c->cuda(e, "emc_set_patterns");
   if (bad)
@@ -512,12 +511,13 @@ emc_status emc_maximize(emc_context* c) {
     a.c0 = 1.0f;
     a.Phi = c->d_Phi;
     a.Plo = c->d_Plo;
+    a.Tpart = c->d_Tpart;
     a.T = c->d_T;
     a.P32 = nullptr;
     CK(c, launch_resp_pass(a, c->st));
     CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
     CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
-    c->launches += 5;  // maximize contraction, combine, row sweep, 2 sums
+    c->launches += 6;  // maximize contraction, combine, 2 sweeps, 2 sums
   }
   c->mark(3);
   c->stage = 2;
@@ -528,8 +528,12 @@ emc_status emc_compress(emc_context* c) {
   if (!c) return EMC_ERR_ARG;
   if (c->stage != 2) return c->fail(EMC_ERR_STATE, "compress called before maximize");
   // emc.c:1025-1026 reset, then emc_cuda.cu:292-362 insert, :414-433 normalise
-  CK(c, cudaMemsetAsync(c->d_model, 0, sizeof(float) * c->M, c->st));
-  CK(c, cudaMemsetAsync(c->d_weight, 0, sizeof(float) * c->M, c->st));
+  if (!c->mixed) {
+    CK(c, cudaMemsetAsync(c->d_model, 0, sizeof(float) * c->M, c->st));
+    CK(c, cudaMemsetAsync(c->d_weight, 0, sizeof(float) * c->M, c->st));
+  } else {
+    CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
+  }
   if (!c->mixed) {
     CompressArgs a{};
     a.P = c->d_LL;
@@ -575,14 +579,17 @@ emc_status emc_compress(emc_context* c) {
     e.cy = c->d_cy;
     e.cz = c->d_cz;
     e.ins = c->d_ins;
-    e.model = c->d_model;
-    e.weight = c->d_weight;
+    e.acc = c->d_acc;
     CK(c, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
                              c->d_status, c->num_sms, c->st));
     c->launches += 1;
   }
   c->mark(4);
-  CK(c, launch_normalize_model(c->d_model, c->d_weight, c->M, c->mixed ? 1 : 0, c->d_scratch,
+  if (!c->mixed)
+    CK(c, launch_normalize_model(c->d_model, c->d_weight, c->M, 0, c->d_scratch, c->d_stats,
+                                 c->st));
+  else
+    CK(c, launch_normalize_acc(c->d_acc, c->d_model, c->d_weight, c->M, c->d_scratch,
                                c->d_stats, c->st));
   c->launches += 4;
   c->mark(5);

@@ -110,6 +110,9 @@ cudaError_t launch_insert(const InsertArgs& a, cudaStream_t st);
 // stats[1] = max after normalisation.  fp64 selects the FP64 division.
 cudaError_t launch_normalize_model(float* model, const float* weight, int64_t M, int fp64,
                                    double* scratch, double* stats, cudaStream_t st);
+// Same from interleaved (model, weight) accumulators; writes model and weight.
+cudaError_t launch_normalize_acc(const float2* acc, float* model, float* weight, int64_t M,
+                                 double* scratch, double* stats, cudaStream_t st);
 cudaError_t launch_model_max(const float* model, int64_t M, double* scratch, double* out,
                              cudaStream_t st);
 cudaError_t launch_fill(float* x, int64_t n, float v, cudaStream_t st);

@@ -52,9 +52,28 @@ __device__ float block_max(float v, float* red) {
 // ------------------------------------------------------------------ expand --
 // One block per rotation; threads stride over pixels.  emc_cuda.cu:51-111 for
 // the nearest mode (exclusive lower bound), trilinear otherwise.
+// Slice value W at continuous voxel position u (0 outside the grid).
+template <int INTERP>
+__device__ __forceinline__ float gather(const float* __restrict__ model, const float* u, int side) {
+  if (INTERP == 0) {
+    int64_t v;
+    return emc_voxel::nearest(u, side, 1, &v) ? __ldg(model + v) : 0.0f;
+  }
+  float acc = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    int64_t v;
+    float w;
+    if (emc_voxel::trilinear_corner(u, side, c, &v, &w) && w != 0.0f)
+      acc = fmaf(w, __ldg(model + v), acc);
+  }
+  return acc;
+}
+
 // Four pixels per thread and iteration: their gathers are independent, so
 // four L2 round trips are in flight per thread.
 constexpr int kExpandUnroll = 4;
+template <int INTERP, int OUT>
 __global__ void __launch_bounds__(kBlock) expand_kernel(const ExpandArgs a) {
   __shared__ double red[32];
   const int64_t r = blockIdx.x;
@@ -71,34 +90,27 @@ __global__ void __launch_bounds__(kBlock) expand_kernel(const ExpandArgs a) {
       if (i < a.npix) {
         float pos[3];
         emc_voxel::position(m, a.side, __ldg(a.cx + i), __ldg(a.cy + i), __ldg(a.cz + i), pos);
-        if (a.interp == 0) {
-          int64_t v;
-          if (emc_voxel::nearest(pos, a.side, 1, &v)) w[u] = __ldg(a.model + v);
-        } else {
-          int64_t v[8];
-          float ww[8];
-          const int n = emc_voxel::trilinear(pos, a.side, v, ww);
-          for (int c = 0; c < n; ++c) w[u] = fmaf(ww[c], __ldg(a.model + v[c]), w[u]);
-        }
+        w[u] = gather<INTERP>(a.model, pos, a.side);
       }
     }
 #pragma unroll
     for (int u = 0; u < kExpandUnroll; ++u) {
       const int64_t i = i0 + (int64_t)u * blockDim.x;
-      if (i >= a.ld) break;
-      const bool real = i < a.npix;
-      if (real && a.stat != STAT_NONE && (!a.stat_mask || a.stat_mask[i] != 0))
-        stat += a.stat == STAT_SUMSQ ? (double)w[u] * w[u] : (double)w[u];
-      const int64_t o = r * a.ld + i;
-      if (a.out == EXP_F32) {
-        a.out_f32[o] = w[u];
-      } else if (a.out == EXP_LOG_F32) {
-        a.out_f32[o] = real ? logf(fmaxf(w[u], a.floor_)) : 0.0f;
-      } else {
-        const float x = real ? (a.log_split ? logf(fmaxf(w[u], a.floor_)) : w[u]) : 0.0f;
-        const __half hi = __float2half_rn(x);
-        a.out_hi[o] = hi;
-        a.out_lo[o] = __float2half_rn(x - __half2float(hi));
+      if (i < a.ld) {
+        const bool real = i < a.npix;
+        if (real && a.stat != STAT_NONE && (!a.stat_mask || a.stat_mask[i] != 0))
+          stat += a.stat == STAT_SUMSQ ? (double)w[u] * w[u] : (double)w[u];
+        const int64_t o = r * a.ld + i;
+        if (OUT == EXP_F32) {
+          a.out_f32[o] = w[u];
+        } else if (OUT == EXP_LOG_F32) {
+          a.out_f32[o] = real ? logf(fmaxf(w[u], a.floor_)) : 0.0f;
+        } else {
+          const float x = real ? (a.log_split ? logf(fmaxf(w[u], a.floor_)) : w[u]) : 0.0f;
+          const __half hi = __float2half_rn(x);
+          a.out_hi[o] = hi;
+          a.out_lo[o] = __float2half_rn(x - __half2float(hi));
+        }
       }
     }
   }
@@ -441,12 +453,13 @@ __global__ void __launch_bounds__(kBlock) insert_kernel(const InsertArgs a) {
       atomicAdd(a.model + v, w * s);
       atomicAdd(a.weight + v, w);
     } else {
-      int64_t v[8];
-      float ww[8];
-      const int n = emc_voxel::trilinear(u, a.side, v, ww);
-      for (int c = 0; c < n; ++c) {
-        atomicAdd(a.model + v[c], ww[c] * w * s);
-        atomicAdd(a.weight + v[c], ww[c] * w);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        int64_t v;
+        float wc;
+        if (!emc_voxel::trilinear_corner(u, a.side, c, &v, &wc) || wc == 0.0f) continue;
+        atomicAdd(a.model + v, wc * w * s);
+        atomicAdd(a.weight + v, wc * w);
       }
     }
   }
@@ -466,6 +479,23 @@ __global__ void divide_kernel(float* model, const float* weight, int64_t M, int 
     else
       v = 0.0f;
     model[i] = v;
+    s += v;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// Mixed path: model/weight from the interleaved accumulators (FP64 division).
+__global__ void divide_acc_kernel(const float2* acc, float* model, float* weight, int64_t M,
+                                  double* part) {
+  __shared__ double red[32];
+  double s = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 a = acc[i];
+    const float v = a.y > 0.0f ? (float)((double)a.x / (double)a.y) : 0.0f;  // emc_cuda.cu:416-420
+    model[i] = v;
+    weight[i] = a.y;
     s += v;
   }
   s = block_sum(s, red);
@@ -527,9 +557,22 @@ inline int grid_for(int64_t n) {
 
 // ------------------------------------------------------------- launchers --
 
+template <int INTERP>
+void expand_dispatch(const ExpandArgs& a, cudaStream_t st) {
+  if (a.out == EXP_F32)
+    expand_kernel<INTERP, EXP_F32><<<(unsigned)a.R, kBlock, 0, st>>>(a);
+  else if (a.out == EXP_LOG_F32)
+    expand_kernel<INTERP, EXP_LOG_F32><<<(unsigned)a.R, kBlock, 0, st>>>(a);
+  else
+    expand_kernel<INTERP, EXP_F16_SPLIT><<<(unsigned)a.R, kBlock, 0, st>>>(a);
+}
+
 cudaError_t launch_expand(const ExpandArgs& a, cudaStream_t st) {
   if (a.R <= 0) return cudaSuccess;
-  expand_kernel<<<(unsigned)a.R, kBlock, 0, st>>>(a);
+  if (a.interp == 0)
+    expand_dispatch<0>(a, st);
+  else
+    expand_dispatch<1>(a, st);
   return cudaGetLastError();
 }
 
@@ -621,6 +664,16 @@ cudaError_t launch_normalize_model(float* model, const float* weight, int64_t M,
   divide_kernel<<<g, kBlock, 0, st>>>(model, weight, M, fp64, scratch);
   sum_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, scratch + kReduceBlocks);
   scale_max_kernel<<<g, kBlock, 0, st>>>(model, M, scratch + kReduceBlocks, fp64, stats, scratch);
+  max_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, stats + 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normalize_acc(const float2* acc, float* model, float* weight, int64_t M,
+                                 double* scratch, double* stats, cudaStream_t st) {
+  const int g = grid_for(M);
+  divide_acc_kernel<<<g, kBlock, 0, st>>>(acc, model, weight, M, scratch);
+  sum_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, scratch + kReduceBlocks);
+  scale_max_kernel<<<g, kBlock, 0, st>>>(model, M, scratch + kReduceBlocks, 1, stats, scratch);
   max_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, stats + 1);
   return cudaGetLastError();
 }

@@ -22,12 +22,10 @@
 namespace emc {
 namespace {
 
-constexpr int BM = 128, BN = 256, BK = 64;
+constexpr int BM = 128, BN = 256;
 constexpr int kThreads = 192;
 constexpr int kTmemCols = 512;
 constexpr uint64_t kWaitLimitNs = 10ull * 1000ull * 1000ull * 1000ull;
-constexpr uint32_t A_BYTES = BM * BK * 2;  // 16 KB
-constexpr uint32_t B_BYTES = BN * BK * 2;  // 32 KB
 
 // ------------------------------------------------------------ PTX helpers --
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -100,15 +98,18 @@ __device__ __forceinline__ void tmem_ld_wait() {
 }
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
-// Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, rows of
-// 128 bytes, 8-row core groups 1024 bytes apart (SBO); LBO unused for this
-// layout; version 1 (sm_100).
+// Shared-memory matrix descriptor of a K-major operand whose rows are BK FP16
+// elements (BK = 64: 128-byte rows, 128B swizzle; BK = 32: 64-byte rows, 64B
+// swizzle, as TMA writes them); 8-row core groups 8 * row bytes apart (SBO);
+// LBO unused for swizzled K-major layouts; version 1 (sm_100).
+template <int BKT>
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
+  static_assert(BKT == 64 || BKT == 32, "row of 128 or 64 bytes");
   uint64_t d = (uint64_t)((addr & 0x3FFFFu) >> 4);
   d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)((8 * BKT * 2) >> 4) << 32;
   d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;
+  d |= (uint64_t)(BKT == 64 ? 2 : 4) << 61;
   return d;
 }
 // Instruction descriptor, kind::f16: D = F32, A = B = F16, both K-major.
@@ -140,13 +141,15 @@ __device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int si
 }
 
 // ---------------------------------------------------------------- kernel --
-template <int NA, int NB, int STAGES, bool M_INNER, class Epi>
+template <int NA, int NB, int STAGES, bool M_INNER, int BK, class Epi>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1,
                    const __grid_constant__ CUtensorMap tmB0, const __grid_constant__ CUtensorMap tmB1,
                    const int64_t m_tiles, const int64_t n_tiles, const int64_t k_blocks,
                    const Epi epi, TcStatus* status) {
   static_assert(NA * NB == 2, "one hi/lo split per contraction");
+  constexpr uint32_t A_BYTES = BM * BK * 2;
+  constexpr uint32_t B_BYTES = BN * BK * 2;
   constexpr uint32_t STAGE_BYTES = NA * A_BYTES + NB * B_BYTES;
   extern __shared__ uint8_t dyn_smem[];
   __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES];
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int q = 0; q < 2; ++q) {
               const uint32_t ao = base + (NA == 2 ? q : 0) * A_BYTES + k * 32;
               const uint32_t bo = bbase + (NB == 2 ? q : 0) * B_BYTES + k * 32;
-              mma_f16(d, sdesc(ao), sdesc(bo), kIdesc, (kb | k | q) != 0);
+              mma_f16(d, sdesc<BK>(ao), sdesc<BK>(bo), kIdesc, (kb | k | q) != 0);
             }
           }
           mma_commit(smem_u32(&empty_bar[s]));
@@ -321,6 +324,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       e.row_end();
       tc_fence_before();
       mbar_arrive(smem_u32(&tempty_bar[acc]));
+      e.tile_end(mt, nt, ep_tid, epi_smem);
     }
   }
   tc_fence_before();
@@ -387,7 +391,8 @@ struct EpiMax {
       xs[k] = a.poisson ? (float)rs[c + k] : x;
       const bool ok = pv && r < a.R;
       if (ok) {
-        a.Y[r * a.ldY + p] = a.poisson ? ll[k] : x;
+        // streamed (evict-first): Y is 1 GB and must not push operand tiles out of L2
+        __stcs(a.Y + r * a.ldY + p, a.poisson ? ll[k] : x);
         cmax = fmaxf(cmax, ll[k]);
       } else {
         ll[k] = -FLT_MAX;
@@ -415,7 +420,13 @@ struct EpiMax {
   __device__ void row_end() {
     if (pv) a.part[ntile * a.N + p] = make_float4(mx, sm, sd, sq);
   }
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
 };
+
+// (model, weight) += (x, y) at one voxel as a single vector reduction.
+__device__ __forceinline__ void red_add_v2(float2* p, float x, float y) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(x), "f"(y) : "memory");
+}
 
 // compress: row = rotation, column = active pixel; inserts into model/weight.
 struct EpiCmp {
@@ -465,29 +476,29 @@ struct EpiCmp {
       if (a.interp == 0) {
         int64_t vox;
         if (!emc_voxel::nearest(u, a.side, 0, &vox)) continue;
-        atomicAdd(a.model + vox, val);
-        atomicAdd(a.weight + vox, wT);
+        red_add_v2(a.acc + vox, val, wT);
       } else {
-        int64_t vv[8];
-        float ww[8];
-        const int n = emc_voxel::trilinear(u, a.side, vv, ww);
-        for (int cc = 0; cc < n; ++cc) {
-          atomicAdd(a.model + vv[cc], ww[cc] * val);
-          atomicAdd(a.weight + vv[cc], ww[cc] * wT);
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+          int64_t vox;
+          float wc;
+          if (!emc_voxel::trilinear_corner(u, a.side, cc, &vox, &wc) || wc == 0.0f) continue;
+          red_add_v2(a.acc + vox, wc * val, wc * wT);
         }
       }
     }
   }
   __device__ void row_end() {}
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
 };
 
-template <int NA, int NB, int STAGES, bool M_INNER, class Epi>
+template <int NA, int NB, int STAGES, bool M_INNER, int BK, class Epi>
 cudaError_t run_gemm(const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
                      const CUtensorMap& b1, int64_t m_tiles, int64_t n_tiles, int64_t k_blocks,
                      const Epi& epi, TcStatus* st, int num_sms, cudaStream_t stream) {
-  constexpr uint32_t stage = NA * A_BYTES + NB * B_BYTES;
+  constexpr uint32_t stage = NA * BM * BK * 2 + NB * BN * BK * 2;
   const size_t dyn = (size_t)STAGES * stage + 1024;
-  auto kern = tc_gemm_kernel<NA, NB, STAGES, M_INNER, Epi>;
+  auto kern = tc_gemm_kernel<NA, NB, STAGES, M_INNER, BK, Epi>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e != cudaSuccess) return e;
   const int64_t tiles = m_tiles * n_tiles;
@@ -560,71 +571,146 @@ __device__ __forceinline__ LLFromY make_llf(const RespArgs& a, int64_t p) {
   return f;
 }
 
-// One block per rotation r.  Pass 1 reads the row of Y once from HBM, forms
-// P_rp = exp(LL_rp - lse_p), keeps it in shared memory and sums T_r.  Pass 2
-// writes P'_rp = c0 P_rp / (T_r phi_p) as FP16 hi + lo.  Dividing by T_r (the
-// slice average of emc_atomic.cu:105-111) keeps every entry of the row in
-// [0, c0/phi_p], so rotations with a tiny total responsibility keep their
-// relative precision instead of underflowing FP16.  Rows longer than the
-// shared buffer recompute P from Y in pass 2.
-constexpr int kRowThreads = 512;
-__global__ void __launch_bounds__(kRowThreads) row_kernel(const RespArgs a, int use_smem) {
-  extern __shared__ float prow[];
-  __shared__ double red[kRowThreads / 32];
-  const int64_t r = blockIdx.x;
-  const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
-  const float* yrow = a.Y + r * a.ldY;
-  const int64_t npair = (a.N + 1) / 2;
-  auto prob = [&](int64_t p, float y) -> float {
-    const LLFromY f = make_llf(a, p);
-    return expf((float)(f(y, rs) - a.lse[p]));
-  };
-  double t = 0.0;
-  for (int64_t q = threadIdx.x; q < npair; q += kRowThreads) {
-    const int64_t p = 2 * q;
-    const float2 y = *reinterpret_cast<const float2*>(yrow + p);
-    const float P0 = prob(p, y.x);
-    const float P1 = p + 1 < a.N ? prob(p + 1, y.y) : 0.0f;
-    if (use_smem) {
-      prow[p] = P0;
-      prow[p + 1] = P1;
-    }
-    if (a.P32) {
-      a.P32[r * a.N + p] = P0;
-      if (p + 1 < a.N) a.P32[r * a.N + p + 1] = P1;
-    }
-    t += (double)P0 + (double)P1;
+// The two sweeps over Y are tiled 32 rotations x 1024 patterns per block:
+// each thread owns four consecutive patterns (one float4 of Y per row), loads
+// their constants (lse, LL coefficients, 1/phi) once and reuses them for the
+// block's 32 rows.
+constexpr int kSweepRows = 32;
+constexpr int kSweepThreads = 256;
+constexpr int kSweepPatterns = 4 * kSweepThreads;
+
+struct PatConst {
+  double lse[4];
+  LLFromY f[4];
+  bool ok[4];
+};
+
+__device__ __forceinline__ void load_consts(const RespArgs& a, int64_t p0, PatConst& k) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t p = p0 + i;
+    k.ok[i] = p < a.N;
+    k.lse[i] = k.ok[i] ? a.lse[p] : 0.0;
+    k.f[i] = make_llf(a, p);
   }
-  t = warp_sum_d(t);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
-  __syncthreads();
-  double T = 0.0;
-  for (int i = 0; i < kRowThreads / 32; ++i) T += red[i];
-  if (threadIdx.x == 0) a.T[r] = (float)T;
-  const float invT = T > 1e-10 ? (float)(1.0 / T) : 0.0f;
-  const int64_t lpair = a.ldP / 2;
-  __half2* hi = reinterpret_cast<__half2*>(a.Phi + r * a.ldP);
-  __half2* lo = reinterpret_cast<__half2*>(a.Plo + r * a.ldP);
-  for (int64_t q = threadIdx.x; q < lpair; q += kRowThreads) {
-    const int64_t p = 2 * q;
-    float P0 = 0.0f, P1 = 0.0f;
-    if (p < a.N) {
-      if (use_smem) {
-        P0 = prow[p];
-        P1 = prow[p + 1];
-      } else {
-        const float2 y = *reinterpret_cast<const float2*>(yrow + p);
-        P0 = prob(p, y.x);
-        P1 = p + 1 < a.N ? prob(p + 1, y.y) : 0.0f;
+}
+
+__device__ __forceinline__ void probs_from(const PatConst& k, float4 y, double rs, float (&P)[4]) {
+  const float yy[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    P[i] = k.ok[i] ? expf((float)(k.f[i](yy[i], rs) - k.lse[i])) : 0.0f;
+}
+
+// Sweep A: Tpart[pattern block][r] = sum over the block's patterns of P_rp.
+__global__ void __launch_bounds__(kSweepThreads) rowsum_kernel(const RespArgs a) {
+  __shared__ float red[kSweepThreads / 32][kSweepRows];
+  const int64_t p0 = (int64_t)blockIdx.x * kSweepPatterns + 4 * threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.y * kSweepRows;
+  const bool any = p0 < a.N;
+  PatConst k;
+  load_consts(a, p0, k);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  // four rows per step: their loads are issued before any result is needed
+  for (int i0 = 0; i0 < kSweepRows; i0 += 4) {
+    float t[4];
+    float4 y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t r = r0 + i0 + u;
+      y[u] = (r < a.R && any) ? *reinterpret_cast<const float4*>(a.Y + r * a.ldY + p0)
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t r = r0 + i0 + u;
+      t[u] = 0.0f;
+      if (r < a.R && any) {
+        const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
+        float P[4];
+        probs_from(k, y[u], rs, P);
+        t[u] = (P[0] + P[1]) + (P[2] + P[3]);
       }
     }
-    const float g0 = p < a.N ? a.c0 / a.new_scaling[p] : 0.0f;
-    const float g1 = p + 1 < a.N ? a.c0 / a.new_scaling[p + 1] : 0.0f;
-    const float x0 = P0 * invT * g0, x1 = P1 * invT * g1;
-    const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-    hi[q] = __halves2half2(h0, h1);
-    lo[q] = __halves2half2(__float2half_rn(x0 - __half2float(h0)),
-                           __float2half_rn(x1 - __half2float(h1)));
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t[u] += __shfl_xor_sync(0xffffffffu, t[u], o);
+      if (lane == 0) red[w][i0 + u] = t[u];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kSweepRows) {
+    const int64_t r = r0 + threadIdx.x;
+    float t = 0.0f;
+    for (int i = 0; i < kSweepThreads / 32; ++i) t += red[i][threadIdx.x];
+    if (r < a.R) a.Tpart[(int64_t)blockIdx.x * a.R + r] = t;
+  }
+}
+
+// Sweep B: P'_rp = c0 P_rp / (T_r phi_p) as FP16 hi + lo.  Dividing each row
+// by its total responsibility T_r (the slice average of emc_atomic.cu:105-111)
+// keeps every entry in [0, c0/phi_p], so rotations with a tiny T_r keep their
+// relative precision instead of underflowing FP16.
+__global__ void __launch_bounds__(kSweepThreads) write_kernel(const RespArgs a, int64_t nblk) {
+  __shared__ float invT[kSweepRows];
+  const int64_t p0 = (int64_t)blockIdx.x * kSweepPatterns + 4 * threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.y * kSweepRows;
+  if (threadIdx.x < kSweepRows) {
+    const int64_t r = r0 + threadIdx.x;
+    double T = 0.0;
+    if (r < a.R) {
+      for (int64_t b = 0; b < nblk; ++b) T += a.Tpart[b * a.R + r];
+      if (blockIdx.x == 0) a.T[r] = (float)T;
+    }
+    invT[threadIdx.x] = T > 1e-10 ? (float)(1.0 / T) : 0.0f;
+  }
+  __syncthreads();
+  if (p0 >= a.ldP) return;
+  PatConst k;
+  load_consts(a, p0, k);
+  float g[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) g[i] = k.ok[i] ? a.c0 / a.new_scaling[p0 + i] : 0.0f;
+  const bool any = p0 < a.N;
+  for (int i0 = 0; i0 < kSweepRows; i0 += 4) {
+    float4 y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t r = r0 + i0 + u;
+      y[u] = (r < a.R && any) ? *reinterpret_cast<const float4*>(a.Y + r * a.ldY + p0)
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+    const int i = i0 + u;
+    const int64_t r = r0 + i;
+    if (r >= a.R) break;
+    float P[4] = {0.f, 0.f, 0.f, 0.f};
+    if (any) {
+      const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
+      probs_from(k, y[u], rs, P);
+    }
+    __half h[4], l[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float x = P[j] * invT[i] * g[j];
+      h[j] = __float2half_rn(x);
+      l[j] = __float2half_rn(x - __half2float(h[j]));
+    }
+    uint2 hv, lv;
+    hv.x = (uint32_t)__half_as_ushort(h[0]) | ((uint32_t)__half_as_ushort(h[1]) << 16);
+    hv.y = (uint32_t)__half_as_ushort(h[2]) | ((uint32_t)__half_as_ushort(h[3]) << 16);
+    lv.x = (uint32_t)__half_as_ushort(l[0]) | ((uint32_t)__half_as_ushort(l[1]) << 16);
+    lv.y = (uint32_t)__half_as_ushort(l[2]) | ((uint32_t)__half_as_ushort(l[3]) << 16);
+    __stcs(reinterpret_cast<uint2*>(a.Phi + r * a.ldP + p0), hv);
+    __stcs(reinterpret_cast<uint2*>(a.Plo + r * a.ldP + p0), lv);
+    if (a.P32) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (k.ok[j]) a.P32[r * a.N + p0 + j] = P[j];
+    }
+    }
   }
 }
 
@@ -669,7 +755,7 @@ __global__ void pack_kernel(const float* K, int64_t N, int64_t npa, int64_t Npad
 // ------------------------------------------------------------- host side --
 
 bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
-                  uint32_t box_rows) {
+                  uint32_t box_rows, uint32_t box_inner) {
   typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -686,10 +772,12 @@ bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t ro
   }
   const cuuint64_t dims[2] = {inner, rows};
   const cuuint64_t strides[1] = {inner * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)BK, box_rows};
+  if (box_inner != 64 && box_inner != 32) return false;
+  const cuuint32_t box[2] = {box_inner, box_rows};
   const cuuint32_t estr[2] = {1, 1};
   return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box,
-            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            box_inner == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -699,9 +787,12 @@ cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
                                cudaStream_t st) {
   EpiMax epi;
   epi.a = e;
-  // patterns are the inner tile index: the 148 CTAs in flight share B tiles
-  return run_gemm<1, 2, 2, true>(tmK, tmK, tmBhi, tmBlo, Mpad / BM, Rpad / BN, Kpad / BK, epi,
-                                 status, num_sms, st);
+  // rows = patterns (counts, 8 KB per stage), columns = rotations (hi and lo,
+  // 2 x 16 KB); pattern tiles are the inner index, so the CTAs in flight share
+  // each rotation tile in L2.  K-steps of 32 (64-byte rows) keep five 40 KB
+  // stages in flight.
+  return run_gemm<1, 2, 5, true, kMaximizeBK>(tmK, tmK, tmBhi, tmBlo, Mpad / BM, Rpad / BN,
+                                              Kpad / kMaximizeBK, epi, status, num_sms, st);
 }
 
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
@@ -711,20 +802,17 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
   EpiCmp epi;
   epi.a = e;
   // pixel tiles are the inner index: CTAs in flight share the P' tiles
-  return run_gemm<2, 1, 3, false>(tmPhi, tmPlo, tmKt, tmKt, Rpad / BM, Ppad / BN, Npad / BK, epi,
-                                  status, num_sms, st);
+  return run_gemm<2, 1, 3, false, kCompressBK>(tmPhi, tmPlo, tmKt, tmKt, Rpad / BM, Ppad / BN,
+                                               Npad / kCompressBK, epi, status, num_sms, st);
 }
 
 cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {
   combine_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, st>>>(a);
-  // the row buffer holds N floats (N rounded up to even) when it fits in shared memory
-  const size_t row_bytes = sizeof(float) * (size_t)((a.N + 1) / 2 * 2);
-  const int use_smem = row_bytes <= 200 * 1024 ? 1 : 0;
-  const size_t dyn = use_smem ? row_bytes : 0;
-  cudaError_t e = cudaFuncSetAttribute(row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(dyn > 0 ? dyn : 1024));
-  if (e != cudaSuccess) return e;
-  row_kernel<<<(unsigned)a.R, kRowThreads, dyn, st>>>(a, use_smem);
+  const int64_t nblk = (a.N + kSweepPatterns - 1) / kSweepPatterns;
+  const int64_t rblk = (a.R + kSweepRows - 1) / kSweepRows;
+  rowsum_kernel<<<dim3((unsigned)nblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a);
+  const int64_t wblk = (a.ldP + kSweepPatterns - 1) / kSweepPatterns;
+  write_kernel<<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
   return cudaGetLastError();
 }
 

@@ -17,8 +17,13 @@ struct TcStatus {
 };
 enum { TC_OK = 0, TC_TIMEOUT = 1 };
 
+// K-step (FP16 elements per shared-memory row) of the two contractions; the
+// tensor maps of their operands use it as the inner box size.
+constexpr int kMaximizeBK = 32;
+constexpr int kCompressBK = 64;
+
 bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
-                  uint32_t box_rows);
+                  uint32_t box_rows, uint32_t box_inner);
 
 // Maximize contraction: acc[p][r] = sum_j K[p][j] (B_hi[r][j] + B_lo[r][j]),
 // 128 patterns x 256 rotations per tile.  Epilogue writes Y[r][p] (LL for
@@ -32,7 +37,7 @@ struct MaxEpiArgs {
   const double* patstat;   // [N] gaussian: sum K_p^2
   double gauss_inv;        // 1 / (2 cnt sigma^2)
   float* Y;                // [R][ldY]
-  float4* part;            // [ceil(R/256)][N]
+  float4* part;            // [Rpad/256][N]
 };
 cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
                                const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
@@ -53,8 +58,7 @@ struct CmpEpiArgs {
   const float* cy;
   const float* cz;
   const int32_t* ins;      // [npa] insert flag (mask == 1)
-  float* model;
-  float* weight;
+  float2* acc;             // [side^3] interleaved (model, weight) accumulators
 };
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
                                const CUtensorMap& tmKt, int64_t Rpad, int64_t Ppad,
@@ -62,9 +66,8 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
                                cudaStream_t st);
 
 // Responsibility pass of the mixed path: combine the tile partials per
-// pattern (lse, new scaling, sum P log P), then one sweep over the rows of Y
-// that writes T_r and the compress operand P' = c0 P / (T_r phi_new) as FP16
-// hi + lo.
+// pattern (lse, new scaling, sum P log P), then two sweeps over Y: row sums
+// T_r, and the compress operand P' = c0 P / (T_r phi_new) as FP16 hi + lo.
 struct RespArgs {
   int64_t N, R, ldY, ldP, nparts;  // nparts = number of 256-rotation tiles
   int poisson;
@@ -81,6 +84,7 @@ struct RespArgs {
   float c0;                // global scale of P'
   __half* Phi;             // [Rpad][ldP]
   __half* Plo;
+  float* Tpart;            // [ceil(N/1024)][R] partial sums of T_r
   float* T;                // [R]
   float* P32;              // optional [R][N] FP32 responsibilities
 };

@@ -83,6 +83,20 @@ EMC_HD bool nearest(const float* u, int side, int lower, int64_t* v) {
   return true;
 }
 
+// Corner c (0..7, bit 0 = x, 1 = y, 2 = z) of the trilinear stencil: its voxel
+// and weight, false when it lies outside the grid.  Callers unroll over c, so
+// no stencil array is kept.
+EMC_HD bool trilinear_corner(const float* u, int side, int c, int64_t* v, float* w) {
+  const float fx = floorf(u[0]), fy = floorf(u[1]), fz = floorf(u[2]);
+  const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
+  const int kx = (int)fx + bx, ky = (int)fy + by, kz = (int)fz + bz;
+  if (kx < 0 || kx >= side || ky < 0 || ky >= side || kz < 0 || kz >= side) return false;
+  const float ax = u[0] - fx, ay = u[1] - fy, az = u[2] - fz;
+  *w = (bx ? ax : 1.0f - ax) * (by ? ay : 1.0f - ay) * (bz ? az : 1.0f - az);
+  *v = ((int64_t)kz * side + ky) * side + kx;
+  return true;
+}
+
 // Returns the number of in-grid corners written to v/w (at most 8).
 EMC_HD int trilinear(const float* u, int side, int64_t* v, float* w) {
   const float fx = floorf(u[0]), fy = floorf(u[1]), fz = floorf(u[2]);
