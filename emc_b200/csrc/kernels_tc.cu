@@ -354,13 +354,22 @@ struct EpiMax {
   double c1, c0;
 
   __device__ void tile_begin(int64_t mt, int64_t nt, int tid, uint8_t* smem) {
+    // per column: gaussian sum S^2 * inv (FP64); poisson sum W as an FP32
+    // hi + lo pair, so LL = x - phi (hi + lo) takes two FP32 FMAs
     double* rs = reinterpret_cast<double*>(smem);
+    float2* rs2 = reinterpret_cast<float2*>(smem);
     n0 = nt * BN;
     ntile = nt;
     epi_bar();
     for (int c = tid; c < BN; c += 128) {
       const int64_t r = n0 + c;
-      rs[c] = r < a.R ? (a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv) : 0.0;
+      const double w = r < a.R ? a.rowstat[r] : 0.0;
+      if (a.poisson) {
+        const float hi = (float)w;
+        rs2[c] = make_float2(hi, (float)(w - (double)hi));
+      } else {
+        rs[c] = w * a.gauss_inv;
+      }
     }
     epi_bar();
     (void)mt;
@@ -379,16 +388,21 @@ struct EpiMax {
   }
   __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) {
     const double* rs = reinterpret_cast<const double*>(smem);
+    const float2* rs2 = reinterpret_cast<const float2*>(smem);
     float ll[16], xs[16];
     float cmax = -FLT_MAX;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       const float x = __uint_as_float(v[k]);
       const int64_t r = n0 + c + k;
-      const double l = a.poisson ? (double)x - (double)phi * rs[c + k]
-                                 : fma((double)x, c1, c0 - rs[c + k]);
-      ll[k] = (float)l;
-      xs[k] = a.poisson ? (float)rs[c + k] : x;
+      if (a.poisson) {
+        const float2 w = rs2[c + k];
+        ll[k] = fmaf(-phi, w.y, fmaf(-phi, w.x, x));
+        xs[k] = w.x + w.y;
+      } else {
+        ll[k] = (float)fma((double)x, c1, c0 - rs[c + k]);
+        xs[k] = x;
+      }
       const bool ok = pv && r < a.R;
       if (ok) {
         // streamed (evict-first): Y is 1 GB and must not push operand tiles out of L2
@@ -400,7 +414,7 @@ struct EpiMax {
     }
     if (cmax > -FLT_MAX) {
       if (cmax > mx) {
-        const float f = mx > -FLT_MAX ? expf(mx - cmax) : 0.0f;
+        const float f = mx > -FLT_MAX ? __expf(mx - cmax) : 0.0f;
         sq = f * (sq + (mx - cmax) * sm);
         sm *= f;
         sd *= f;
@@ -410,7 +424,7 @@ struct EpiMax {
       for (int k = 0; k < 16; ++k)
         if (ll[k] > -FLT_MAX) {
           const float dl = ll[k] - mx;
-          const float e = expf(dl);
+          const float e = __expf(dl);
           sm += e;
           sd = fmaf(e, xs[k], sd);
           sq = fmaf(e, dl, sq);
