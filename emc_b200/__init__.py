@@ -22,7 +22,7 @@ _NAMES = {
     "gauss": GAUSS, "poisson": POISSON, "nearest": NEAREST, "trilinear": TRILINEAR,
     "fp32": FP32, "mixed": MIXED,
 }
-BUF_MODEL, BUF_WEIGHT, BUF_SCALING, BUF_RESP, BUF_SLICES, BUF_TOTALRESP = range(6)
+BUF_MODEL, BUF_WEIGHT, BUF_SCALING, BUF_RESP, BUF_SLICES, BUF_TOTALRESP, BUF_ACCUM = range(7)
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
           4: "device wait timed out", 5: "call out of order", 6: "data out of exact range",
           7: "unsupported"}
@@ -50,7 +50,7 @@ class SynthConfig(C.Structure):
     _fields_ = [("side", C.c_int32), ("n_scatterers", C.c_int32), ("object_radius", C.c_double),
                 ("n_patterns", C.c_int64), ("mean_photons", C.c_double),
                 ("scale_sigma", C.c_double), ("beamstop_radius", C.c_double),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("first_pattern", C.c_int64)]
 
 
 _lib = None
@@ -84,6 +84,8 @@ def lib():
             ("emc_legacy_last_status", [], C.c_int),
             ("emc_set_profiling", [P, C.c_int], C.c_int), ("emc_stage_times", [P, P], C.c_int),
             ("emc_launch_count", [P], I64),
+            ("emc_compress_insert", [P], C.c_int), ("emc_normalize", [P], C.c_int),
+            ("emc_partial_stats", [P, P, P], C.c_int),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -131,10 +133,13 @@ def random_model(side, seed=0):
 
 
 def synthesize(side, n_patterns, x, y, z, mean_photons=1000.0, scale_sigma=0.3,
-               beamstop_radius=0.0, n_scatterers=40, object_radius=0.3, seed=0):
-    """Seeded synthetic dataset: returns dict(model, counts, mask, rotations, scales)."""
+               beamstop_radius=0.0, n_scatterers=40, object_radius=0.3, seed=0, first_pattern=0):
+    """Seeded synthetic dataset: returns dict(model, counts, mask, rotations, scales).
+
+    Patterns first_pattern .. first_pattern + n_patterns - 1 of the seeded
+    sequence, so shards of one dataset can be generated independently."""
     sc = SynthConfig(side, n_scatterers, object_radius, n_patterns, mean_photons, scale_sigma,
-                     beamstop_radius, seed)
+                     beamstop_radius, seed, first_pattern)
     npix = side * side
     model = np.zeros(side ** 3, np.float32)
     counts = np.zeros((n_patterns, npix), np.float32)
@@ -145,6 +150,14 @@ def synthesize(side, n_patterns, x, y, z, mean_photons=1000.0, scale_sigma=0.3,
     _check(lib().emc_synthesize(C.byref(sc), _ptr(x), _ptr(y), _ptr(z), _ptr(model), _ptr(counts),
                                 _ptr(mask), _ptr(rot), _ptr(scales)))
     return dict(model=model, counts=counts, mask=mask, rotations=rot, scales=scales)
+
+
+class _CudaArray:
+    """__cuda_array_interface__ of a float32 device buffer owned by the library."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False),
+                                         "version": 2, "strides": None}
 
 
 # --------------------------------------------------------------- context --
@@ -229,6 +242,24 @@ class Context:
 
     def compress(self):
         self._c(lib().emc_compress(self._h))
+
+    def compress_insert(self):
+        self._c(lib().emc_compress_insert(self._h))
+
+    def normalize(self):
+        self._c(lib().emc_normalize(self._h))
+
+    def partial_stats(self):
+        a, b = C.c_double(), C.c_double()
+        self._c(lib().emc_partial_stats(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def accumulator_tensor(self):
+        """Zero-copy torch view (CUDA, float32 [2*side^3]) of the insertion
+        accumulators, valid between compress_insert() and normalize()."""
+        import torch
+        ptr, nbytes = self.device_buffer(BUF_ACCUM)
+        return torch.as_tensor(_CudaArray(ptr, nbytes // 4), device="cuda")
 
     def synchronize(self):
         self._c(lib().emc_synchronize(self._h))

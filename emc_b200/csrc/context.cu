@@ -201,7 +201,9 @@ emc_status emc_create(const emc_config* cfg, emc_context** out) {
   e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(c->cuda(e, "cudaStreamCreate"));
   emc_status s;
-  if ((s = c->alloc(&c->d_model, c->M, true)) || (s = c->alloc(&c->d_weight, c->M, true)) ||
+  // model and weight are adjacent: on the FP32 path they are the insertion
+  // accumulators, reduced across ranks as one buffer of 2*M floats
+  if ((s = c->alloc(&c->d_model, 2 * c->M, true)) ||
       (s = c->alloc(&c->d_scaling, c->N)) || (s = c->alloc(&c->d_scaling_prev, c->N)) ||
       (s = c->alloc(&c->d_quat, 4 * c->R)) || (s = c->alloc(&c->d_rotw, c->R)) ||
       (s = c->alloc(&c->d_T, c->R, true)) || (s = c->alloc(&c->d_rowstat, c->R, true)) ||
@@ -209,6 +211,7 @@ emc_status emc_create(const emc_config* cfg, emc_context** out) {
       (s = c->alloc(&c->d_patsq, c->N, true)) || (s = c->alloc(&c->d_patsum, c->N, true)) ||
       (s = c->alloc(&c->d_status, 1, true)))
     return bail(s);
+  c->d_weight = c->d_model + c->M;
   if ((s = c->cuda(launch_fill(c->d_scaling, c->N, 1.0f, c->st), "fill")) != EMC_OK) return bail(s);
   *out = c;
   return EMC_OK;
@@ -524,7 +527,7 @@ emc_status emc_maximize(emc_context* c) {
   return EMC_OK;
 }
 
-emc_status emc_compress(emc_context* c) {
+emc_status emc_compress_insert(emc_context* c) {
   if (!c) return EMC_ERR_ARG;
   if (c->stage != 2) return c->fail(EMC_ERR_STATE, "compress called before maximize");
   // emc.c:1025-1026 reset, then emc_cuda.cu:292-362 insert, :414-433 normalise
@@ -585,6 +588,13 @@ emc_status emc_compress(emc_context* c) {
     c->launches += 1;
   }
   c->mark(4);
+  c->stage = 3;
+  return EMC_OK;
+}
+
+emc_status emc_normalize(emc_context* c) {
+  if (!c) return EMC_ERR_ARG;
+  if (c->stage != 3) return c->fail(EMC_ERR_STATE, "normalize called before compress_insert");
   if (!c->mixed)
     CK(c, launch_normalize_model(c->d_model, c->d_weight, c->M, 0, c->d_scratch, c->d_stats,
                                  c->st));
@@ -595,6 +605,11 @@ emc_status emc_compress(emc_context* c) {
   c->mark(5);
   c->stage = 0;
   return EMC_OK;
+}
+
+emc_status emc_compress(emc_context* c) {
+  TRY(emc_compress_insert(c));
+  return emc_normalize(c);
 }
 
 static emc_status check_status(emc_context* c) {
@@ -635,6 +650,16 @@ emc_status emc_iterate(emc_context* c, emc_iter_stats* stats) {
   return EMC_OK;
 }
 
+emc_status emc_partial_stats(emc_context* c, double* plogp, double* loglik) {
+  if (!c) return EMC_ERR_ARG;
+  double h[4] = {0, 0, 0, 0};
+  CK(c, cudaMemcpyAsync(h, c->d_stats, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  if (plogp) *plogp = h[2];
+  if (loglik) *loglik = h[3];
+  return EMC_OK;
+}
+
 emc_status emc_get_model(emc_context* c, float* model) {
   return emc_get_buffer(c, EMC_BUF_MODEL, model, sizeof(float) * (c ? c->M : 0));
 }
@@ -652,6 +677,10 @@ emc_status emc_device_buffer(emc_context* c, emc_buffer which, void** dptr, size
     case EMC_BUF_WEIGHT: p = c->d_weight; n = sizeof(float) * c->M; break;
     case EMC_BUF_SCALING: p = c->d_scaling; n = sizeof(float) * c->N; break;
     case EMC_BUF_TOTALRESP: p = c->d_T; n = sizeof(float) * c->R; break;
+    case EMC_BUF_ACCUM:
+      p = c->mixed ? (void*)c->d_acc : (void*)c->d_model;
+      n = sizeof(float) * 2 * c->M;
+      break;
     case EMC_BUF_RESP:
       if (c->mixed) return c->fail(EMC_ERR_UNSUPPORTED, "mixed path keeps no FP32 responsibility matrix");
       p = c->d_LL; n = sizeof(float) * c->R * c->N; break;

@@ -248,7 +248,7 @@ emc_status emc_synthesize(const emc_synth_config* sc, const float* x, const floa
                           const float* z, float* true_model, float* counts, int32_t* mask,
                           float* true_rot, float* true_scale) {
   if (!sc || !x || !y || !z || !counts || !mask || sc->side < 2 || sc->n_patterns < 1 ||
-      sc->n_scatterers < 1)
+      sc->n_scatterers < 1 || sc->first_pattern < 0)
     return EMC_ERR_ARG;
   const int side = sc->side;
   const int64_t npix = (int64_t)side * side, M = npix * side, N = sc->n_patterns;
@@ -294,7 +294,8 @@ emc_status emc_synthesize(const emc_synth_config* sc, const float* x, const floa
   if (active == 0) return EMC_ERR_ARG;
 #pragma omp parallel for schedule(dynamic, 8)
   for (int64_t p = 0; p < N; ++p) {
-    Stream s(sc->seed, 0x70617474ull, (uint64_t)p);
+    const uint64_t gp = (uint64_t)(p + sc->first_pattern);  // index in the whole dataset
+    Stream s(sc->seed, 0x70617474ull, gp);
     // uniform random rotation (Shoemake's subgroup algorithm)
     const double u1 = s.uniform(), u2 = s.uniform(), u3 = s.uniform();
     float q[4] = {(float)(std::sqrt(1 - u1) * std::sin(2 * M_PI * u2)),
@@ -318,7 +319,7 @@ emc_status emc_synthesize(const emc_synth_config* sc, const float* x, const floa
       if (mask[i]) tot += acc;
     }
     const double f = tot > 0 ? sc->mean_photons * scale / tot : 0.0;
-    Stream d(sc->seed, 0x636f756eull, (uint64_t)p);
+    Stream d(sc->seed, 0x636f756eull, gp);
     float* out = counts + p * npix;
     for (int64_t i = 0; i < npix; ++i) out[i] = (float)d.poisson(sl[i] * f);
     if (true_rot)

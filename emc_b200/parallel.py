@@ -1,0 +1,67 @@
+"""Pattern-sharded EMC across ranks (one process per GPU).
+
+An EMC iteration is per pattern everywhere except insertion: every rank
+expands the same model against the same rotations, evaluates its own patterns
+(responsibilities, scaling), and inserts their slice averages into its own
+accumulators.  The only exchange is the element-wise sum of those
+accumulators -- 2 x side^3 floats, model and weight sums -- before
+normalisation; the ranks then normalise identical sums and hold identical
+models.  The reference is single-GPU; this follows the sharding SURVEY.md's
+multi-GPU row describes, with one all-reduce per iteration.
+
+The per-iteration statistics (sum P log P, sum of log-sum-exps) are sums over
+patterns and are reduced the same way.
+"""
+from __future__ import annotations
+
+import torch
+import torch.distributed as dist
+
+
+def shard_range(n_total: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous, balanced (first pattern, count) of rank's share."""
+    base, extra = divmod(n_total, world)
+    count = base + (1 if rank < extra else 0)
+    first = rank * base + min(rank, extra)
+    return first, count
+
+
+class ShardedIteration:
+    """Drives one EMC iteration over a pattern shard and sums the insertion
+    accumulators across the process group.
+
+    `ctx` is an emc_b200.Context (or any object with the same stage methods:
+    expand, maximize, compress_insert, accumulator_tensor, synchronize,
+    normalize, partial_stats)."""
+
+    def __init__(self, ctx, group=None):
+        self.ctx = ctx
+        self.group = group
+
+    def __call__(self) -> None:
+        c = self.ctx
+        c.expand()
+        c.maximize()
+        c.compress_insert()
+        if dist.is_initialized() and dist.get_world_size(self.group) > 1:
+            acc = c.accumulator_tensor()
+            if acc.is_cuda:
+                # enqueued on the library's stream: it waits for the insertion
+                # and normalise (enqueued next on that stream) waits for it
+                with torch.cuda.stream(torch.cuda.ExternalStream(c.stream)):
+                    dist.all_reduce(acc, op=dist.ReduceOp.SUM, group=self.group)
+            else:
+                c.synchronize()
+                dist.all_reduce(acc, op=dist.ReduceOp.SUM, group=self.group)
+        c.normalize()
+
+    def stats(self) -> dict:
+        plogp, loglik = self.ctx.partial_stats()
+        t = torch.tensor([plogp, loglik], dtype=torch.float64)
+        if dist.is_initialized() and dist.get_world_size(self.group) > 1:
+            backend = dist.get_backend(self.group)
+            if backend == "nccl":
+                t = t.cuda()
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+            t = t.cpu()
+        return {"sum_plogp": float(t[0]), "total_loglik": float(t[1])}

@@ -50,14 +50,17 @@ def pixel_size(side: int) -> float:
     return math.tan(math.radians(EDGE_ANGLE_DEG)) * DISTANCE / (side / 2)
 
 
-def make(w: Workload | str, n_patterns: int | None = None):
-    """Returns dict(x, y, z, mask, counts, rotations q, weights w, model0, true_model, ...)."""
+def make(w: Workload | str, n_patterns: int | None = None, first_pattern: int = 0):
+    """Returns dict(x, y, z, mask, counts, rotations q, weights w, model0, true_model, ...).
+
+    first_pattern selects a shard of the seeded pattern sequence (the model,
+    mask and rotations do not depend on it)."""
     if isinstance(w, str):
         w = WORKLOADS[w]
     N = n_patterns or w.n_patterns
     x, y, z = detector_coordinates(w.side, WAVELENGTH, pixel_size(w.side), DISTANCE)
     d = synthesize(w.side, N, x, y, z, mean_photons=w.mean_photons, scale_sigma=w.scale_sigma,
-                   beamstop_radius=w.beamstop, seed=w.seed)
+                   beamstop_radius=w.beamstop, seed=w.seed, first_pattern=first_pattern)
     q, wt = generate_rotations(w.rot_n, halve=True)
     return dict(workload=w, x=x, y=y, z=z, mask=d["mask"], counts=d["counts"], q=q, w=wt,
                 model0=random_model(w.side, w.seed), true_model=d["model"],

@@ -66,7 +66,9 @@ typedef enum {
   EMC_BUF_SCALING = 2,  /* float [N] */
   EMC_BUF_RESP = 3,     /* float [R][N] responsibilities after maximize */
   EMC_BUF_SLICES = 4,   /* float [R][Pa] expanded slices (FP32 path), Pa = active pixels */
-  EMC_BUF_TOTALRESP = 5 /* float [R] T_r */
+  EMC_BUF_TOTALRESP = 5, /* float [R] T_r */
+  EMC_BUF_ACCUM = 6      /* float [2*side^3] insertion accumulators (model and weight sums)
+                            between emc_compress_insert and emc_normalize */
 } emc_buffer;
 
 const char *emc_status_string(emc_status s);
@@ -95,6 +97,15 @@ emc_status emc_iterate(emc_context *ctx, emc_iter_stats *stats);
 emc_status emc_expand(emc_context *ctx);
 emc_status emc_maximize(emc_context *ctx);
 emc_status emc_compress(emc_context *ctx);
+/* emc_compress in two halves: insertion into the accumulators
+ * (EMC_BUF_ACCUM), then model = sum / weight normalised to mean 1.  Between
+ * them a pattern-sharded run sums the accumulators across ranks (the only
+ * exchange of an EMC iteration: every other quantity is per pattern or per
+ * rotation). */
+emc_status emc_compress_insert(emc_context *ctx);
+emc_status emc_normalize(emc_context *ctx);
+/* sum P log P and sum_p lse_p of this context's patterns in the last iteration. */
+emc_status emc_partial_stats(emc_context *ctx, double *sum_plogp, double *total_loglik);
 
 emc_status emc_synchronize(emc_context *ctx);
 emc_status emc_get_model(emc_context *ctx, float *model);
@@ -137,6 +148,7 @@ typedef struct {
   double scale_sigma;        /* lognormal sigma of the per-pattern scale */
   double beamstop_radius;    /* pixels; mask = 0 within this radius */
   uint64_t seed;
+  int64_t first_pattern;     /* index of counts[0] in the seeded pattern sequence (shards) */
 } emc_synth_config;
 
 /* Synthetic dataset: |F|^2 of point scatterers on a side^3 grid (model, may be

@@ -128,3 +128,30 @@ def test_stage_order_is_enforced(tiny):
         assert ei.value.status == 5
         ctx.iterate()
         ctx.synchronize()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_accumulator_view_and_split_compress(tiny, prec):
+    """compress == compress_insert + normalize, and the zero-copy torch view of
+    the accumulators (what a pattern-sharded run all-reduces) holds the model
+    and weight sums."""
+    import torch
+    d = tiny
+    M = d["workload"].side ** 3
+    with make_ctx(d, precision=prec) as a, make_ctx(d, precision=prec) as b:
+        a.iterate()
+        b.expand()
+        b.maximize()
+        b.compress_insert()
+        b.synchronize()
+        acc = b.accumulator_tensor()
+        assert acc.is_cuda and acc.numel() == 2 * M
+        h = acc.double().cpu().numpy()
+        msum, wsum = (h[:M], h[M:]) if prec == "fp32" else (h[0::2], h[1::2])
+        expect = np.where(wsum > 0, msum / np.where(wsum > 0, wsum, 1), 0.0)
+        expect /= expect.mean()
+        b.normalize()
+        model = b.get_model()
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(model, a.get_model(), rtol=1e-6, atol=1e-6)
+        np.testing.assert_allclose(model, expect, rtol=1e-5, atol=1e-6)
