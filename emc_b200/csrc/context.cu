@@ -11,6 +11,7 @@
 
 #include "../../include/emc_b200.h"
 #include "kernels.cuh"
+#include "proposal.cuh"
 #include "tc.cuh"
 
 using namespace emc;
@@ -82,6 +83,18 @@ struct emc_context {
   CUtensorMap tmKh, tmKt, tmBhi, tmBlo, tmPhi, tmPlo;
   TcStatus* d_status = nullptr;
   // profiling: events at stage boundaries, kernel launch count
+  // learned proposal: rotation cells and the candidate-iteration buffers
+  int32_t n_cells = 0, cand_m = 0;
+  int64_t max_members = 0;
+  std::vector<int64_t> h_mbeg;
+  std::vector<int32_t> h_mcnt;
+  int32_t* d_cell = nullptr;
+  int64_t* d_mbeg = nullptr;
+  int32_t* d_mcnt = nullptr;
+  int32_t *d_cand = nullptr, *d_gpair = nullptr, *d_gcnt = nullptr;
+  int64_t *d_ppos = nullptr, *d_gbeg = nullptr, *d_goff = nullptr;
+  float *d_mass = nullptr, *d_Yc = nullptr, *d_Pt = nullptr, *d_U = nullptr;
+  double *d_lse_c = nullptr, *d_plogp_c = nullptr;
   // Two event sets alternate between iterations, so the times of iteration
   // i-1 can be read while iteration i is still queued.
   bool prof = false;
@@ -744,4 +757,244 @@ emc_status emc_get_buffer(emc_context* c, emc_buffer which, void* host, size_t b
   return EMC_OK;
 }
 
+
+// ----------------------------------------------------- learned proposal --
+
+emc_status emc_set_cells(emc_context* c, const int32_t* cell, int32_t n_cells) {
+  if (!c || !cell || n_cells < 1) return EMC_ERR_ARG;
+  if (n_cells > 1024) return c->fail(EMC_ERR_RANGE, "at most 1024 cells");
+  std::vector<int64_t> beg(n_cells, -1);
+  std::vector<int32_t> cnt(n_cells, 0);
+  for (int64_t r = 0; r < c->R; ++r) {
+    if (cell[r] < 0 || cell[r] >= n_cells) return c->fail(EMC_ERR_ARG, "cell id out of range");
+    if (r > 0 && cell[r] < cell[r - 1])
+      return c->fail(EMC_ERR_ARG, "rotations must be sorted by cell (cell ids non-decreasing)");
+    if (beg[cell[r]] < 0) beg[cell[r]] = r;
+    cnt[cell[r]]++;
+  }
+  for (int32_t k = 0; k < n_cells; ++k)
+    if (beg[k] < 0) beg[k] = 0;
+  if (!c->d_cell) TRY(c->alloc(&c->d_cell, c->R));
+  if (c->n_cells != n_cells) {
+    TRY(c->alloc(&c->d_mbeg, n_cells));
+    TRY(c->alloc(&c->d_mcnt, n_cells));
+    TRY(c->alloc(&c->d_gbeg, n_cells));
+    TRY(c->alloc(&c->d_gcnt, n_cells));
+    TRY(c->alloc(&c->d_goff, n_cells));
+  }
+  CK(c, cudaMemcpyAsync(c->d_cell, cell, sizeof(int32_t) * c->R, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_mbeg, beg.data(), sizeof(int64_t) * n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_mcnt, cnt.data(), sizeof(int32_t) * n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  c->n_cells = n_cells;
+  c->h_mbeg = beg;
+  c->h_mcnt = cnt;
+  c->max_members = 0;
+  c->cand_m = 0;  // the candidate buffers are sized by the largest cell: reallocate
+  for (int32_t k : cnt) c->max_members = k > c->max_members ? k : c->max_members;
+  return EMC_OK;
+}
+
+emc_status emc_pattern_features(emc_context* c, int32_t in_side, float* x) {
+  if (!c || !x) return EMC_ERR_ARG;
+  if (!c->have_pat) return c->fail(EMC_ERR_STATE, "patterns are not set");
+  if (in_side * 2 != c->cfg.side) return c->fail(EMC_ERR_ARG, "in_side must be side / 2");
+  CK(c, launch_features(c->d_K, c->d_pix, c->N, c->npa, c->cfg.side, in_side, x, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  return EMC_OK;
+}
+
+emc_status emc_cell_targets(emc_context* c, float* t) {
+  if (!c || !t) return EMC_ERR_ARG;
+  if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
+  if (c->stage == 1) return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+  TargetArgs a{};
+  a.N = c->N;
+  a.R = c->R;
+  a.n_cells = c->n_cells;
+  a.cell = c->d_cell;
+  if (!c->mixed) {
+    a.P = c->d_LL;
+    a.ldP = c->N;
+  } else {
+    a.Y = c->d_Y;
+    a.ldY = c->Npad;
+    a.poisson = c->gauss ? 0 : 1;
+    a.lse = c->d_lse;
+    a.scaling = c->d_scaling_prev;
+    a.rowstat = c->d_rowstat;
+    a.patstat = c->d_patsq;
+    a.gauss_inv = gauss_inv(c);
+  }
+  a.t = t;
+  CK(c, launch_targets(a, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  return EMC_OK;
+}
+
+emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, float threshold,
+                                emc_proposal_stats* stats) {
+  if (!c || !probs || m < 1 || m > 32) return EMC_ERR_ARG;
+  if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
+  if (m > c->n_cells) return c->fail(EMC_ERR_ARG, "more cells per pattern than cells");
+  const int64_t N = c->N, R = c->R, pairs = N * m;
+  if (c->cand_m != m) {
+    for (void* p : {(void*)c->d_cand, (void*)c->d_ppos, (void*)c->d_gpair, (void*)c->d_Yc, (void*)c->d_Pt})
+      if (p) c->release(p);
+    TRY(c->alloc(&c->d_cand, pairs));
+    TRY(c->alloc(&c->d_ppos, pairs));
+    TRY(c->alloc(&c->d_gpair, pairs));
+    if (!c->d_mass) {
+      TRY(c->alloc(&c->d_mass, N));
+      TRY(c->alloc(&c->d_lse_c, N));
+      TRY(c->alloc(&c->d_plogp_c, N));
+    }
+    TRY(c->alloc(&c->d_Yc, pairs * c->max_members));
+    TRY(c->alloc(&c->d_Pt, pairs * c->max_members));
+    if (c->mixed && !c->d_U) TRY(c->alloc(&c->d_U, R * c->npa));
+    c->cand_m = m;
+  }
+  TRY(emc_expand(c));
+  if (!c->mixed && c->gauss)  // the grouped gaussian LL uses the expanded form: sum_j S_rj^2
+    CK(c, launch_pattern_stats(c->d_S, nullptr, R, c->npa, c->npa, 1, c->d_rowstat, c->st));
+  // candidate cells of every pattern and the proposal's mass on them
+  CK(c, launch_select(probs, N, c->n_cells, m, c->d_cand, c->d_mass, c->st));
+  std::vector<int32_t> cand(pairs);
+  std::vector<float> mass(N);
+  CK(c, cudaMemcpyAsync(cand.data(), c->d_cand, sizeof(int32_t) * pairs, cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaMemcpyAsync(mass.data(), c->d_mass, sizeof(float) * N, cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  double msum = 0.0, mmin = 1e300;
+  for (float v : mass) {
+    msum += v;
+    mmin = v < mmin ? v : mmin;
+  }
+  emc_proposal_stats st{};
+  st.mean_mass = msum / (double)N;
+  st.min_mass = mmin;
+  if (st.mean_mass < threshold) {
+    // the proposal is not confident enough: the dense iteration runs instead
+    TRY(emc_maximize(c));
+    TRY(emc_compress(c));
+    st.fallback = 1;
+    st.pairs = 0;
+    st.evaluations = N * R;
+    if (stats) *stats = st;
+    return EMC_OK;
+  }
+  // group the (pattern, cell) pairs by cell (stable counting sort on the host)
+  std::vector<int32_t> gcnt(c->n_cells, 0);
+  for (int32_t k : cand) {
+    if (k < 0 || k >= c->n_cells) return c->fail(EMC_ERR_ARG, "cell probabilities must be finite");
+    gcnt[k]++;
+  }
+  std::vector<int64_t> gbeg(c->n_cells), goff(c->n_cells), fill(c->n_cells);
+  int64_t acc = 0, off = 0, maxp = 0, evals = 0;
+  for (int32_t k = 0; k < c->n_cells; ++k) {
+    gbeg[k] = acc;
+    fill[k] = acc;
+    acc += gcnt[k];
+    goff[k] = off;
+    off += (int64_t)gcnt[k] * c->h_mcnt[k];
+    maxp = gcnt[k] > maxp ? gcnt[k] : maxp;
+    evals += (int64_t)gcnt[k] * c->h_mcnt[k];
+  }
+  std::vector<int32_t> gpair(pairs);
+  std::vector<int64_t> ppos(pairs);
+  for (int64_t p = 0; p < N; ++p)
+    for (int32_t i = 0; i < m; ++i) {
+      const int32_t k = cand[p * m + i];
+      const int64_t q = fill[k]++;
+      gpair[q] = (int32_t)p;
+      ppos[p * m + i] = q;
+    }
+  CK(c, cudaMemcpyAsync(c->d_gpair, gpair.data(), sizeof(int32_t) * pairs, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_ppos, ppos.data(), sizeof(int64_t) * pairs, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_gbeg, gbeg.data(), sizeof(int64_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_gcnt, gcnt.data(), sizeof(int32_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_goff, goff.data(), sizeof(int64_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * N, cudaMemcpyDeviceToDevice, c->st));
+  CK(c, cudaMemsetAsync(c->d_T, 0, sizeof(float) * R, c->st));
+  GroupArgs g{};
+  g.N = N;
+  g.npa = c->npa;
+  g.MM = c->max_members;
+  g.n_cells = c->n_cells;
+  g.m = m;
+  g.poisson = c->gauss ? 0 : 1;
+  g.mbeg = c->d_mbeg;
+  g.mcnt = c->d_mcnt;
+  g.gbeg = c->d_gbeg;
+  g.gcnt = c->d_gcnt;
+  g.gpair = c->d_gpair;
+  g.ppos = c->d_ppos;
+  g.cand = c->d_cand;
+  g.goff = c->d_goff;
+  if (!c->mixed) {
+    g.S = c->d_S;
+    g.ldS = c->npa;
+  } else {
+    g.hi = c->d_Bhi;
+    g.lo = c->d_Blo;
+    g.ldS = c->Ppad;
+  }
+  g.K = c->d_K;
+  g.scaling = c->d_scaling_prev;
+  g.rowstat = c->d_rowstat;
+  g.patstat = c->d_patsq;
+  g.patsum = c->d_patsum;
+  g.gauss_inv = gauss_inv(c);
+  g.Y = c->d_Yc;
+  g.Pt = c->d_Pt;
+  g.T = c->d_T;
+  g.lse = c->d_lse_c;
+  g.plogp = c->d_plogp_c;
+  g.new_scaling = c->d_scaling;
+  g.U = c->mixed ? c->d_U : c->d_S;
+  if (!c->gauss && !c->mixed) {
+    // the FP32 poisson expand stores log W; insertion needs the averaged slices in a separate buffer
+    if (!c->d_U) TRY(c->alloc(&c->d_U, R * c->npa));
+    g.U = c->d_U;
+  }
+  c->mark(1);
+  CK(c, launch_group_maximize(g, maxp, c->max_members, c->st));
+  c->mark(2);
+  c->mark(3);
+  CK(c, launch_group_compress(g, c->max_members, c->st));
+  CK(c, cudaMemsetAsync(c->d_model, 0, sizeof(float) * 2 * c->M, c->st));
+  InsertArgs in{};
+  in.U = g.U;
+  in.T = c->d_T;
+  in.rotw = c->d_rotw;
+  in.quat = c->d_quat;
+  in.cx = c->d_cx;
+  in.cy = c->d_cy;
+  in.cz = c->d_cz;
+  in.ins = c->d_ins;
+  in.R = R;
+  in.npix = c->npa;
+  in.ldU = c->npa;
+  in.side = c->cfg.side;
+  in.interp = c->cfg.interp;
+  in.model = c->d_model;
+  in.weight = c->d_weight;
+  CK(c, launch_insert(in, c->st));
+  c->mark(4);
+  CK(c, launch_normalize_model(c->d_model, c->d_weight, c->M, 1, c->d_scratch, c->d_stats, c->st));
+  CK(c, launch_sum_f64(c->d_plogp_c, N, c->d_stats + 2, c->st));
+  CK(c, launch_sum_f64(c->d_lse_c, N, c->d_stats + 3, c->st));
+  c->mark(5);
+  c->launches += 11;
+  c->stage = 0;
+  TRY(check_status(c));
+  double h[4];
+  CK(c, cudaMemcpy(h, c->d_stats, sizeof(h), cudaMemcpyDeviceToHost));
+  st.sum_plogp = h[2];
+  st.total_loglik = h[3];
+  st.pairs = pairs;
+  st.evaluations = evals;
+  st.fallback = 0;
+  if (stats) *stats = st;
+  return EMC_OK;
+}
 }  // extern "C"

@@ -1,0 +1,73 @@
+// Learned rotation proposal: launch interface (kernels in proposal.cu).
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace emc {
+
+// x[p][S*S] = log(1 + sum of the counts of each 2x2 pixel block), S = side/2.
+cudaError_t launch_features(const float* K, const int32_t* pix, int64_t N, int64_t npa, int side,
+                            int S, float* x, cudaStream_t st);
+
+// t[p][c] = sum of the responsibilities of cell c's fine rotations.
+struct TargetArgs {
+  int64_t N, R;
+  int n_cells;
+  const int32_t* cell;     // [R] cell of every fine rotation
+  const float* P;          // FP32 responsibilities [R][ldP] (FP32 path) or nullptr
+  int64_t ldP;
+  const float* Y;          // otherwise from the mixed path's Y and lse
+  int64_t ldY;
+  int poisson;
+  const double* lse;
+  const float* scaling;    // phi used for LL (gaussian)
+  const double* rowstat;
+  const double* patstat;
+  double gauss_inv;
+  float* t;                // [N][n_cells]
+};
+cudaError_t launch_targets(const TargetArgs& a, cudaStream_t st);
+
+// cand[p][0..m) = the m most probable cells of probs[p][0..C); mass[p] = their total.
+cudaError_t launch_select(const float* probs, int64_t N, int C, int m, int32_t* cand, float* mass,
+                          cudaStream_t st);
+
+// Pairs (pattern, selected cell) grouped by cell: group c holds pairs
+// gbeg[c] .. gbeg[c]+gcnt[c]-1, pair q belongs to pattern gpair[q]; pattern
+// p's i-th selected cell is cand[p*m+i] and its pair is ppos[p*m+i].  Cell c's
+// fine rotations are mbeg[c] .. mbeg[c]+mcnt[c]-1.
+struct GroupArgs {
+  int64_t N, npa, MM;      // MM: row stride of Y (>= largest cell)
+  int n_cells, m, poisson;
+  const int64_t* mbeg;
+  const int32_t* mcnt;
+  const int64_t* gbeg;
+  const int32_t* gcnt;
+  const int32_t* gpair;
+  const int64_t* ppos;
+  const int32_t* cand;
+  const int64_t* goff;     // offset of cell c's [mcnt][gcnt] block in Pt
+  const float* S;          // FP32 slice operand [R][ldS] (log W or S), or nullptr ->
+  const __half* hi;        // FP16 hi + lo [Rpad][ldS]
+  const __half* lo;
+  int64_t ldS;
+  const float* K;          // [N][npa]
+  const float* scaling;    // phi used for LL
+  const double* rowstat;   // poisson: sum W_r; gaussian: sum S_r^2
+  const double* patstat;   // sum K^2
+  const double* patsum;    // sum K
+  double gauss_inv;
+  float* Y;                // [pairs][MM]
+  float* Pt;               // per cell [mcnt][gcnt]: P / phi_new
+  float* T;                // [R] (zeroed by the caller)
+  double* lse;             // [N]
+  double* plogp;           // [N]
+  float* new_scaling;      // [N]
+  float* U;                // [R][npa] averaged slices
+};
+cudaError_t launch_group_maximize(const GroupArgs& g, int64_t max_pairs, int64_t max_members,
+                                  cudaStream_t st);
+cudaError_t launch_group_compress(const GroupArgs& g, int64_t max_members, cudaStream_t st);
+
+}  // namespace emc

@@ -128,6 +128,58 @@ void *emc_stream(emc_context *ctx);
 /* Number of active (mask != 0) pixels. */
 int64_t emc_active_pixels(const emc_context *ctx);
 
+/* ---- learned rotation proposal ----
+ * Fine rotations are grouped into coarse cells (e.g. the nearest rotation of
+ * the 420-rotation 600-cell sampling); the rotation list given to
+ * emc_set_rotations must be sorted by cell.  A proposal network predicts, per
+ * pattern, a posterior over the cells; emc_iterate_proposed then evaluates
+ * each pattern only against the fine rotations of its m most probable cells,
+ * or runs the dense iteration when the mean predicted mass on those cells is
+ * below `threshold`. */
+typedef struct {
+  double mean_mass, min_mass;  /* predicted posterior mass on the evaluated cells */
+  int64_t pairs;               /* (pattern, cell) pairs evaluated */
+  int64_t evaluations;         /* (pattern, rotation) evaluations */
+  int32_t fallback;            /* 1: the dense iteration ran instead */
+  int32_t pad_;
+  double sum_plogp, total_loglik;
+} emc_proposal_stats;
+
+/* cell[r] for every rotation (non-decreasing), n_cells cells. */
+emc_status emc_set_cells(emc_context *ctx, const int32_t *cell, int32_t n_cells);
+/* x [N][in_side^2] (device): log(1 + counts summed over 2x2 pixel blocks),
+ * in_side = side / 2; the proposal network's input. */
+emc_status emc_pattern_features(emc_context *ctx, int32_t in_side, float *x_device);
+/* t [N][n_cells] (device): the last maximize's responsibilities summed over
+ * each cell's rotations; the proposal network's training target. */
+emc_status emc_cell_targets(emc_context *ctx, float *t_device);
+/* One iteration restricted to the proposal's top-m cells per pattern.
+ * cell_probs: device [N][n_cells]. */
+emc_status emc_iterate_proposed(emc_context *ctx, const float *cell_probs_device, int32_t m,
+                                float threshold, emc_proposal_stats *stats);
+
+/* Proposal network: three 3x3 stride-2 convolutions (16, 32, 64 channels,
+ * ReLU) and a fully connected layer to n_out logits, softmax.  BF16 weights
+ * and activations (bf16 = 0: FP32, for gradient checks), FP32 accumulation,
+ * FP32 master weights, Adam.  All data pointers are device pointers. */
+typedef struct emc_net emc_net;
+emc_status emc_net_create(int in_side, int n_out, int bf16, uint64_t seed, int device,
+                          emc_net **out);
+emc_status emc_net_destroy(emc_net *net);
+int64_t emc_net_num_params(const emc_net *net);
+emc_status emc_net_get_params(emc_net *net, float *host);
+emc_status emc_net_set_params(emc_net *net, const float *host);
+/* probs [batch][n_out] from x [batch][in_side^2]. */
+emc_status emc_net_forward(emc_net *net, const float *x, int64_t batch, float *probs);
+/* Mean soft-target cross-entropy of (x, t [batch][n_out]) and its gradient
+ * (kept inside; copied to grad_host when not NULL, layout as the parameters). */
+emc_status emc_net_gradients(emc_net *net, const float *x, const float *t, int64_t batch,
+                             double *loss, float *grad_host);
+/* emc_net_gradients followed by one Adam step with learning rate lr. */
+emc_status emc_net_train_step(emc_net *net, const float *x, const float *t, int64_t batch,
+                              float lr, double *loss);
+const char *emc_net_last_error(const emc_net *net);
+
 /* ---- host-side input generators (reference host code, C++ here) ---- */
 
 int64_t emc_n_to_samples(int n); /* emc.c:43 */

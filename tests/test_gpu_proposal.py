@@ -1,0 +1,117 @@
+"""Learned rotation proposal: the network's gradients against a float64 torch
+autograd reference of the same architecture, and the proposal end to end
+(trained on dense responsibilities; captured responsibility mass; model of a
+proposed iteration against the dense iteration; fallback)."""
+import numpy as np
+import pytest
+
+from parity import make_ctx, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch_reference(params, x, t, in_side, n_out):
+    """Forward + backward of the network in float64 (CPU), same parameter layout:
+    W[co][ci][3][3] then b[co] for three stride-2 convolutions, Wfc[c][f], bfc[c]."""
+    import torch
+    import torch.nn.functional as F
+    ch = [1, 16, 32, 64]
+    p = torch.tensor(params, dtype=torch.float64)
+    off, views = 0, []
+    for l in range(3):
+        n = ch[l + 1] * ch[l] * 9
+        views.append(p[off:off + n].view(ch[l + 1], ch[l], 3, 3))
+        off += n
+        views.append(p[off:off + ch[l + 1]])
+        off += ch[l + 1]
+    nf = 64 * (in_side // 8) ** 2
+    views.append(p[off:off + n_out * nf].view(n_out, nf))
+    off += n_out * nf
+    views.append(p[off:off + n_out])
+    leaves = [v.clone().requires_grad_(True) for v in views]
+    h = torch.tensor(x, dtype=torch.float64).view(-1, 1, in_side, in_side)
+    for l in range(3):
+        h = F.relu(F.conv2d(h, leaves[2 * l], leaves[2 * l + 1], stride=2, padding=1))
+    z = h.reshape(h.shape[0], -1) @ leaves[6].T + leaves[7]
+    tt = torch.tensor(t, dtype=torch.float64)
+    loss = -(tt * F.log_softmax(z, dim=1)).sum(1).mean()
+    loss.backward()
+    return float(loss.detach()), np.concatenate([v.grad.reshape(-1).numpy() for v in leaves])
+
+
+@pytest.mark.parametrize("bf16,tol", [(False, 1e-4), (True, 5e-2)])
+def test_network_gradients_match_float64_reference(bf16, tol):
+    import torch
+    from emc_b200.proposal import ProposalNet
+    in_side, n_out, B = 16, 10, 5
+    net = ProposalNet(in_side, n_out, bf16=bf16, seed=3)
+    rng = np.random.default_rng(0)
+    params = (rng.standard_normal(net.num_params) * 0.2).astype(np.float32)
+    if bf16:  # the forward pass sees bf16 weights: give the reference the same values
+        params = torch.tensor(params).bfloat16().float().numpy()
+    net.set_params(params)
+    x = rng.uniform(0, 2, (B, in_side * in_side)).astype(np.float32)
+    t = rng.uniform(0, 1, (B, n_out)).astype(np.float32)
+    t /= t.sum(1, keepdims=True)
+    loss, g = net.gradients(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda())
+    loss_ref, g_ref = _torch_reference(params.astype(np.float64), x.astype(np.float64),
+                                       t.astype(np.float64), in_side, n_out)
+    assert abs(loss - loss_ref) <= tol * abs(loss_ref)
+    # per tensor relative error (layout W1 b1 W2 b2 W3 b3 Wfc bfc)
+    sizes = [16 * 9, 16, 32 * 144, 32, 64 * 288, 64, n_out * 64 * 4, n_out]
+    o = 0
+    for sz in sizes:
+        assert rel(g[o:o + sz], g_ref[o:o + sz]) <= tol, (o, rel(g[o:o + sz], g_ref[o:o + sz]))
+        o += sz
+    net.close()
+
+
+def test_learned_proposal_end_to_end():
+    import torch
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    d = W.make("b200_64", n_patterns=3000)
+    q, w, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=2)
+    d = dict(d, q=q, w=w)
+    members = np.bincount(cell, minlength=n_cells)
+    m = int(np.ceil(512 / members.mean()))  # about 512 fine rotations per pattern
+    with make_ctx(d, likelihood="poisson", precision="mixed") as ctx:
+        for _ in range(3):
+            ctx.iterate()
+        lp = LearnedProposal(ctx, cell, n_cells, bf16=True, seed=1)
+        x, t = lp.features(), lp.targets()
+        np.testing.assert_allclose(t.sum(1).cpu().numpy(), 1.0, atol=1e-4)
+
+        def captured(probs):
+            top = torch.topk(probs, m, dim=1).indices
+            return torch.gather(t, 1, top).sum(1).cpu().numpy()
+
+        before = captured(lp.predict(x))
+        losses = lp.train(x, t, epochs=25, batch=256, lr=2e-3)
+        probs = lp.predict(x)
+        after = captured(probs)
+        assert losses[-1] < losses[0]
+        # what the trained network gains over the untrained one: the true
+        # responsibility mass on the evaluated rotations
+        assert after.mean() > 0.95 and after.mean() > before.mean() + 0.3, (before.mean(), after.mean())
+        m0, s0 = ctx.get_model(), ctx.get_scaling()
+        st = lp.iterate(probs, m, threshold=0.0)
+        assert st["fallback"] == 0
+        assert st["mean_mass"] > 0.9 and st["pairs"] == 3000 * m
+        frac = st["evaluations"] / (3000 * len(q))
+        assert frac < 0.03, frac
+        m_prop = ctx.get_model()
+        ctx.set_model(m0)
+        ctx.set_scaling(s0)
+        ctx.iterate()
+        m_dense = ctx.get_model()
+        err = rel(m_prop, m_dense)
+        print(f"proposal: captured mass untrained {before.mean():.4f} trained {after.mean():.4f} "
+              f"(min {after.min():.4f}); evaluated fraction {frac:.4f}; model error vs dense {err:.2e}")
+        assert err < 2e-2, err
+        # the fallback runs the dense iteration
+        ctx.set_model(m0)
+        ctx.set_scaling(s0)
+        st = lp.iterate(probs, m, threshold=1.01)
+        assert st["fallback"] == 1
+        assert rel(ctx.get_model(), m_dense) < 1e-5
