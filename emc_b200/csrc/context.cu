@@ -13,6 +13,7 @@
 #include "kernels.cuh"
 #include "proposal.cuh"
 #include "tc.cuh"
+#include "tile.cuh"
 
 using namespace emc;
 
@@ -85,6 +86,8 @@ struct emc_context {
   // profiling: events at stage boundaries, kernel launch count
   // learned proposal: rotation cells and the candidate-iteration buffers
   int32_t n_cells = 0, cand_m = 0;
+  int resp_source = 0;  // responsibilities of the last maximize: 1 dense, 2 proposed
+  float* d_cmass = nullptr;
   int64_t max_members = 0;
   std::vector<int64_t> h_mbeg;
   std::vector<int32_t> h_mcnt;
@@ -93,7 +96,9 @@ struct emc_context {
   int32_t* d_mcnt = nullptr;
   int32_t *d_cand = nullptr, *d_gpair = nullptr, *d_gcnt = nullptr;
   int64_t *d_ppos = nullptr, *d_gbeg = nullptr, *d_goff = nullptr;
-  float *d_mass = nullptr, *d_Yc = nullptr, *d_Pt = nullptr, *d_U = nullptr;
+  float *d_mass = nullptr, *d_Yc = nullptr, *d_Pt = nullptr;
+  int4 *d_mtiles = nullptr, *d_ctiles = nullptr;
+  int64_t mtiles_cap = 0, ctiles_cap = 0;
   double *d_lse_c = nullptr, *d_plogp_c = nullptr;
   // Two event sets alternate between iterations, so the times of iteration
   // i-1 can be read while iteration i is still queued.
@@ -536,6 +541,7 @@ emc_status emc_maximize(emc_context* c) {
     c->launches += 6;  // maximize contraction, combine, 2 sweeps, 2 sums
   }
   c->mark(3);
+  c->resp_source = 1;
   c->stage = 2;
   return EMC_OK;
 }
@@ -807,7 +813,13 @@ emc_status emc_pattern_features(emc_context* c, int32_t in_side, float* x) {
 emc_status emc_cell_targets(emc_context* c, float* t) {
   if (!c || !t) return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
-  if (c->stage == 1) return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+  if (c->resp_source == 0 || c->stage == 1)
+    return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+  if (c->resp_source == 2) {
+    CK(c, launch_scatter_targets(c->d_cand, c->d_cmass, c->N, c->cand_m, c->n_cells, t, c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    return EMC_OK;
+  }
   TargetArgs a{};
   a.N = c->N;
   a.R = c->R;
@@ -832,9 +844,9 @@ emc_status emc_cell_targets(emc_context* c, float* t) {
   return EMC_OK;
 }
 
-emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, float threshold,
-                                emc_proposal_stats* stats) {
-  if (!c || !probs || m < 1 || m > 32) return EMC_ERR_ARG;
+emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, float mass_target,
+                                float threshold, emc_proposal_stats* stats) {
+  if (!c || !probs || m < 1) return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
   if (m > c->n_cells) return c->fail(EMC_ERR_ARG, "more cells per pattern than cells");
   const int64_t N = c->N, R = c->R, pairs = N * m;
@@ -849,16 +861,18 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
       TRY(c->alloc(&c->d_lse_c, N));
       TRY(c->alloc(&c->d_plogp_c, N));
     }
+    if (c->d_cmass) c->release(c->d_cmass);
+    TRY(c->alloc(&c->d_cmass, pairs));
     TRY(c->alloc(&c->d_Yc, pairs * c->max_members));
     TRY(c->alloc(&c->d_Pt, pairs * c->max_members));
-    if (c->mixed && !c->d_U) TRY(c->alloc(&c->d_U, R * c->npa));
+    if (!c->d_acc) TRY(c->alloc(&c->d_acc, c->M));
     c->cand_m = m;
   }
   TRY(emc_expand(c));
   if (!c->mixed && c->gauss)  // the grouped gaussian LL uses the expanded form: sum_j S_rj^2
     CK(c, launch_pattern_stats(c->d_S, nullptr, R, c->npa, c->npa, 1, c->d_rowstat, c->st));
   // candidate cells of every pattern and the proposal's mass on them
-  CK(c, launch_select(probs, N, c->n_cells, m, c->d_cand, c->d_mass, c->st));
+  CK(c, launch_select(probs, N, c->n_cells, m, mass_target, c->d_cand, c->d_mass, c->st));
   std::vector<int32_t> cand(pairs);
   std::vector<float> mass(N);
   CK(c, cudaMemcpyAsync(cand.data(), c->d_cand, sizeof(int32_t) * pairs, cudaMemcpyDeviceToHost, c->st));
@@ -884,10 +898,18 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
   }
   // group the (pattern, cell) pairs by cell (stable counting sort on the host)
   std::vector<int32_t> gcnt(c->n_cells, 0);
-  for (int32_t k : cand) {
-    if (k < 0 || k >= c->n_cells) return c->fail(EMC_ERR_ARG, "cell probabilities must be finite");
-    gcnt[k]++;
-  }
+  int64_t npairs = 0;
+  for (int64_t p = 0; p < N; ++p)
+    for (int32_t i = 0; i < m; ++i) {
+      const int32_t k = cand[p * m + i];
+      if (k < 0) {
+        if (i == 0) return c->fail(EMC_ERR_ARG, "cell probabilities must be finite");
+        break;
+      }
+      if (k >= c->n_cells) return c->fail(EMC_ERR_ARG, "cell index out of range");
+      gcnt[k]++;
+      npairs++;
+    }
   std::vector<int64_t> gbeg(c->n_cells), goff(c->n_cells), fill(c->n_cells);
   int64_t acc = 0, off = 0, maxp = 0, evals = 0;
   for (int32_t k = 0; k < c->n_cells; ++k) {
@@ -899,16 +921,38 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     maxp = gcnt[k] > maxp ? gcnt[k] : maxp;
     evals += (int64_t)gcnt[k] * c->h_mcnt[k];
   }
-  std::vector<int32_t> gpair(pairs);
-  std::vector<int64_t> ppos(pairs);
+  std::vector<int32_t> gpair(npairs);
+  std::vector<int64_t> ppos(pairs, -1);
   for (int64_t p = 0; p < N; ++p)
     for (int32_t i = 0; i < m; ++i) {
       const int32_t k = cand[p * m + i];
+      if (k < 0) break;
       const int64_t q = fill[k]++;
       gpair[q] = (int32_t)p;
       ppos[p * m + i] = q;
     }
-  CK(c, cudaMemcpyAsync(c->d_gpair, gpair.data(), sizeof(int32_t) * pairs, cudaMemcpyHostToDevice, c->st));
+  // tile lists of the grouped contractions: only cells that some pattern selected
+  std::vector<int4> mt, ct;
+  for (int32_t k = 0; k < c->n_cells; ++k) {
+    if (gcnt[k] == 0) continue;
+    for (int32_t r0 = 0; r0 < c->h_mcnt[k]; r0 += TM) {
+      ct.push_back(make_int4(k, r0, 0, 0));
+      for (int32_t q0 = 0; q0 < gcnt[k]; q0 += TN) mt.push_back(make_int4(k, r0, q0, 0));
+    }
+  }
+  if ((int64_t)mt.size() > c->mtiles_cap) {
+    if (c->d_mtiles) c->release(c->d_mtiles);
+    TRY(c->alloc(&c->d_mtiles, mt.size()));
+    c->mtiles_cap = (int64_t)mt.size();
+  }
+  if ((int64_t)ct.size() > c->ctiles_cap) {
+    if (c->d_ctiles) c->release(c->d_ctiles);
+    TRY(c->alloc(&c->d_ctiles, ct.size()));
+    c->ctiles_cap = (int64_t)ct.size();
+  }
+  CK(c, cudaMemcpyAsync(c->d_mtiles, mt.data(), sizeof(int4) * mt.size(), cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_ctiles, ct.data(), sizeof(int4) * ct.size(), cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_gpair, gpair.data(), sizeof(int32_t) * npairs, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_ppos, ppos.data(), sizeof(int64_t) * pairs, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_gbeg, gbeg.data(), sizeof(int64_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_gcnt, gcnt.data(), sizeof(int32_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
@@ -950,48 +994,40 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
   g.lse = c->d_lse_c;
   g.plogp = c->d_plogp_c;
   g.new_scaling = c->d_scaling;
-  g.U = c->mixed ? c->d_U : c->d_S;
-  if (!c->gauss && !c->mixed) {
-    // the FP32 poisson expand stores log W; insertion needs the averaged slices in a separate buffer
-    if (!c->d_U) TRY(c->alloc(&c->d_U, R * c->npa));
-    g.U = c->d_U;
-  }
+  g.cmass = c->d_cmass;
+  g.mtiles = c->d_mtiles;
+  g.ctiles = c->d_ctiles;
+  g.rotw = c->d_rotw;
+  g.quat = c->d_quat;
+  g.cx = c->d_cx;
+  g.cy = c->d_cy;
+  g.cz = c->d_cz;
+  g.ins = c->d_ins;
+  g.side = c->cfg.side;
+  g.interp = c->cfg.interp;
+  g.acc = c->d_acc;
   c->mark(1);
-  CK(c, launch_group_maximize(g, maxp, c->max_members, c->st));
+  CK(c, launch_group_maximize(g, (int64_t)mt.size(), c->st));
+  c->resp_source = 2;
   c->mark(2);
   c->mark(3);
-  CK(c, launch_group_compress(g, c->max_members, c->st));
-  CK(c, cudaMemsetAsync(c->d_model, 0, sizeof(float) * 2 * c->M, c->st));
-  InsertArgs in{};
-  in.U = g.U;
-  in.T = c->d_T;
-  in.rotw = c->d_rotw;
-  in.quat = c->d_quat;
-  in.cx = c->d_cx;
-  in.cy = c->d_cy;
-  in.cz = c->d_cz;
-  in.ins = c->d_ins;
-  in.R = R;
-  in.npix = c->npa;
-  in.ldU = c->npa;
-  in.side = c->cfg.side;
-  in.interp = c->cfg.interp;
-  in.model = c->d_model;
-  in.weight = c->d_weight;
-  CK(c, launch_insert(in, c->st));
+  CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
+  CK(c, launch_group_compress(g, (int64_t)ct.size(), c->st));
   c->mark(4);
-  CK(c, launch_normalize_model(c->d_model, c->d_weight, c->M, 1, c->d_scratch, c->d_stats, c->st));
+  CK(c, launch_normalize_acc(c->d_acc, c->d_model, c->d_weight, c->M, c->d_scratch, c->d_stats,
+                             c->st));
   CK(c, launch_sum_f64(c->d_plogp_c, N, c->d_stats + 2, c->st));
   CK(c, launch_sum_f64(c->d_lse_c, N, c->d_stats + 3, c->st));
   c->mark(5);
-  c->launches += 11;
+  // select, grouped contraction + softmax, grouped compress, normalise (4), two sums
+  c->launches += 10 + ((!c->mixed && c->gauss) ? 1 : 0);
   c->stage = 0;
   TRY(check_status(c));
   double h[4];
   CK(c, cudaMemcpy(h, c->d_stats, sizeof(h), cudaMemcpyDeviceToHost));
   st.sum_plogp = h[2];
   st.total_loglik = h[3];
-  st.pairs = pairs;
+  st.pairs = npairs;
   st.evaluations = evals;
   st.fallback = 0;
   if (stats) *stats = st;

@@ -41,6 +41,10 @@ __device__ __forceinline__ void st(T* p, float v) {
 }
 
 // C[r*scr + n*scn] (+)= sum_k A[r*sar + k*sak] B[n*sbn + k*sbk] (+ bias[r]) (relu)
+// With kchunk > 0 the reduction is split: block z sums k in
+// [z*kchunk, (z+1)*kchunk) and adds its partial into C atomically (C float,
+// zeroed by the caller) -- the weight gradients, whose reduction runs over
+// every output position of the batch.
 template <class TA, class TB, class TC, bool BKMAJOR>
 struct GemmOp {
   using Acc = float;
@@ -51,11 +55,19 @@ struct GemmOp {
   int64_t M, N, K, sar, sak, sbn, sbk, scr, scn;
   const float* bias;
   int relu, accumulate;
-  __device__ int64_t ksize() const { return K; }
+  int64_t kchunk;
+  __device__ int64_t koff() const { return kchunk ? (int64_t)blockIdx.z * kchunk : 0; }
+  __device__ int64_t ksize() const {
+    if (!kchunk) return K;
+    const int64_t left = K - koff();
+    return left < kchunk ? left : kchunk;
+  }
   __device__ float a(int64_t r, int64_t k) const {
+    k += koff();
     return (r < M && k < K) ? ld(A + r * sar + k * sak) : 0.0f;
   }
   __device__ float b(int64_t n, int64_t k) const {
+    k += koff();
     return (n < N && k < K) ? ld(B + n * sbn + k * sbk) : 0.0f;
   }
   static __device__ __forceinline__ float inner(float acc, float a, float b) { return fmaf(a, b, acc); }
@@ -69,6 +81,12 @@ struct GemmOp {
         const int64_t n = n0 + j;
         if (n >= N) continue;
         TC* c = C + r * scr + n * scn;
+        if constexpr (sizeof(TC) == 4) {
+          if (kchunk) {
+            atomicAdd(c, acc[i][j]);
+            continue;
+          }
+        }
         float v = acc[i][j] + (bias ? bias[r] : 0.0f);
         if (accumulate) v += ld(c);
         if (relu) v = fmaxf(v, 0.0f);
@@ -83,8 +101,31 @@ cudaError_t gemm(const TA* A, int64_t sar, int64_t sak, const TB* B, int64_t sbn
                  TC* C, int64_t scr, int64_t scn, int64_t M, int64_t N, int64_t K,
                  const float* bias, int relu, int accumulate, cudaStream_t st) {
   GemmOp<TA, TB, TC, BKMAJOR> op{A, B, C, M, N, K, sar, sak, sbn, sbk, scr, scn, bias, relu,
-                                 accumulate};
+                                 accumulate, 0};
   dim3 grid((unsigned)((N + TN - 1) / TN), (unsigned)((M + TM - 1) / TM));
+  tile_kernel<<<grid, kTileThreads, 0, st>>>(op);
+  return cudaGetLastError();
+}
+
+// C[M][N] (row stride scr) = A B^T with the reduction split over enough
+// blocks to fill the GPU (about 4 per SM); C is zeroed here.
+template <class TA, class TB, bool BKMAJOR>
+cudaError_t gemm_splitk(const TA* A, int64_t sar, int64_t sak, const TB* B, int64_t sbn,
+                        int64_t sbk, float* C, int64_t scr, int64_t M, int64_t N, int64_t K,
+                        int num_sms, cudaStream_t st) {
+  const int64_t base = ((N + TN - 1) / TN) * ((M + TM - 1) / TM);
+  int64_t splits = (4 * (int64_t)num_sms + base - 1) / base;
+  const int64_t max_splits = (K + 255) / 256;  // at least 256 terms per block
+  if (splits > max_splits) splits = max_splits;
+  if (splits < 1) splits = 1;
+  int64_t chunk = (K + splits - 1) / splits;
+  chunk = (chunk + TK - 1) / TK * TK;
+  splits = (K + chunk - 1) / chunk;
+  cudaError_t e = cudaMemsetAsync(C, 0, sizeof(float) * M * scr, st);
+  if (e != cudaSuccess) return e;
+  GemmOp<TA, TB, float, BKMAJOR> op{A, B, C, M, N, K, sar, sak, sbn, sbk, scr, 1, nullptr, 0, 0,
+                                    chunk};
+  dim3 grid((unsigned)((N + TN - 1) / TN), (unsigned)((M + TM - 1) / TM), (unsigned)splits);
   tile_kernel<<<grid, kTileThreads, 0, st>>>(op);
   return cudaGetLastError();
 }
@@ -237,7 +278,7 @@ inline unsigned blocks_for(int64_t n) {
 using namespace emc;
 
 struct emc_net {
-  int S = 0, C = 0, bf16 = 1;
+  int S = 0, C = 0, bf16 = 1, num_sms = 148;
   int ch[4] = {1, 16, 32, 64};
   int64_t off[9] = {0};  // parameter offsets: W1 b1 W2 b2 W3 b3 Wfc bfc, total
   int64_t F = 0, cap = 0;  // fc input features, batch capacity
@@ -347,8 +388,8 @@ cudaError_t net_backward(emc_net* n, int64_t B) {
   float* g = n->g;
   cudaError_t e;
   // fc: dWfc[c][f] = dz[c][b] feat[f][b];  dbfc = sum_b dz;  dfeat[f][b] = Wfc[c][f] dz[c][b]
-  e = gemm<float, T, float, true>(n->dz, B, 1, (const T*)n->feat, B, 1, g + n->off[6], n->F, 1,
-                                  n->C, n->F, B, nullptr, 0, 0, st);
+  e = gemm_splitk<float, T, true>(n->dz, B, 1, (const T*)n->feat, B, 1, g + n->off[6], n->F, n->C,
+                                  n->F, B, n->num_sms, st);
   if (e != cudaSuccess) return e;
   rowsum_grad_kernel<<<(unsigned)n->C, 256, 0, st>>>(n->dz, n->C, B, g + n->off[7]);
   e = gemm<T, float, float, false>(wc + n->off[6], 1, n->F, n->dz, 1, B, n->dfeat, B, 1, n->F, B,
@@ -365,8 +406,8 @@ cudaError_t net_backward(emc_net* n, int64_t B) {
     relu_back_kernel<T><<<blocks_for(cout * NN), 256, 0, st>>>(n->dout[l], (const T*)n->out[l],
                                                                cout * NN);
     // dW[co][k] = dout[co][n] col[k][n];  db[co] = sum_n dout[co][n]
-    e = gemm<float, T, float, true>(n->dout[l], NN, 1, (const T*)n->col[l], NN, 1, g + n->off[2 * l],
-                                    K9, 1, cout, K9, NN, nullptr, 0, 0, st);
+    e = gemm_splitk<float, T, true>(n->dout[l], NN, 1, (const T*)n->col[l], NN, 1,
+                                    g + n->off[2 * l], K9, cout, K9, NN, n->num_sms, st);
     if (e != cudaSuccess) return e;
     rowsum_grad_kernel<<<(unsigned)cout, 256, 0, st>>>(n->dout[l], cout, NN, g + n->off[2 * l + 1]);
     if (l == 0) break;
@@ -390,6 +431,7 @@ emc_status emc_net_create(int in_side, int n_out, int bf16, uint64_t seed, int d
   *out = nullptr;
   if (cudaSetDevice(device) != cudaSuccess) return EMC_ERR_CUDA;
   emc_net* n = new emc_net();
+  cudaDeviceGetAttribute(&n->num_sms, cudaDevAttrMultiProcessorCount, device);
   n->S = in_side;
   n->C = n_out;
   n->bf16 = bf16 ? 1 : 0;

@@ -15,9 +15,14 @@
 
 #include "proposal.cuh"
 #include "tile.cuh"
+#include "voxel.h"
 
 namespace emc {
 namespace {
+
+__device__ __forceinline__ void red_add_v2(float2* p, float x, float y) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(x), "f"(y) : "memory");
+}
 
 __global__ void features_kernel(const float* K, const int32_t* pix, int64_t N, int64_t npa, int side,
                                 int S, float* x) {
@@ -67,21 +72,24 @@ __global__ void __launch_bounds__(256) targets_kernel(const TargetArgs a) {
     for (int c = w; c < a.n_cells; c += 8) a.t[p * a.n_cells + c] = tc[c * 32 + lane];
 }
 
-// One warp per pattern: the m most probable cells, and their total probability.
-__global__ void select_kernel(const float* probs, int64_t N, int C, int m, int32_t* cand,
-                              float* mass) {
+// One warp per pattern: its most probable cells in order, until their total
+// probability reaches mass_target or m cells are taken; unused slots -1.
+__global__ void select_kernel(const float* probs, int64_t N, int C, int m, float mass_target,
+                              int32_t* cand, float* mass) {
   const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (p >= N) return;
   const float* row = probs + p * C;
   uint32_t taken = 0;  // bit i: cell lane + 32 i already selected (C <= 1024)
   float tot = 0.0f;
-  for (int s = 0; s < m; ++s) {
-    float best = -1.0f;
+  const bool adaptive = mass_target < 1.0f;  // else always m cells
+  int s = 0;
+  for (; s < m && !(adaptive && tot >= mass_target); ++s) {
+    float best = -INFINITY;
     int bi = -1;
     for (int i = 0; lane + 32 * i < C; ++i) {
       const float v = row[lane + 32 * i];
-      if (!((taken >> i) & 1u) && v > best) {
+      if (!((taken >> i) & 1u) && (v > best || (bi < 0 && v == v))) {
         best = v;
         bi = lane + 32 * i;
       }
@@ -89,7 +97,7 @@ __global__ void select_kernel(const float* probs, int64_t N, int C, int m, int32
     for (int o = 16; o > 0; o >>= 1) {
       const float ov = __shfl_xor_sync(0xffffffffu, best, o);
       const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ov > best || (ov == best && oi >= 0 && (bi < 0 || oi < bi))) {
+      if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) {
         best = ov;
         bi = oi;
       }
@@ -98,41 +106,52 @@ __global__ void select_kernel(const float* probs, int64_t N, int C, int m, int32
     if (lane == 0) cand[p * m + s] = bi;
     tot += best > 0.0f ? best : 0.0f;
   }
+  for (int k = s + lane; k < m; k += 32) cand[p * m + k] = -1;
   if (lane == 0) mass[p] = tot;
 }
 
-// Grouped maximize, one contraction per cell (blockIdx.z): rows = the cell's
-// fine rotations, columns = its (pattern, cell) pairs, reduction over pixels.
-// Writes Y[pair][member]: poisson LL, gaussian cross term C.
+// Grouped maximize, one contraction per cell: rows = the cell's fine
+// rotations, columns = its (pattern, cell) pairs, reduction over pixels.
+// Blocks come from a tile list (cell, row offset, column offset) holding only
+// the tiles of cells that some pattern selected.  Writes Y[pair][member]:
+// poisson LL, gaussian cross term.
 struct OpGroupLL {
   using Acc = double;
   static constexpr bool kBKMajor = true;
   GroupArgs g;
+  __device__ int cell() const { return __ldg(&g.mtiles[blockIdx.x].x); }
+  __device__ bool origin(int64_t& m0, int64_t& n0) const {
+    const int4 t = g.mtiles[blockIdx.x];
+    m0 = t.y;
+    n0 = t.z;
+    return true;
+  }
   __device__ int64_t ksize() const { return g.npa; }
   __device__ float a(int64_t row, int64_t j) const {
-    const int c = blockIdx.z;
-    if (row >= g.mcnt[c] || j >= g.npa) return 0.0f;
-    const int64_t r = g.mbeg[c] + row;
+    const int c = cell();
+    if (row >= __ldg(g.mcnt + c) || j >= g.npa) return 0.0f;
+    const int64_t r = __ldg(g.mbeg + c) + row;
     if (g.S) return __ldg(g.S + r * g.ldS + j);
     return __half2float(g.hi[r * g.ldS + j]) + __half2float(g.lo[r * g.ldS + j]);
   }
   __device__ float b(int64_t col, int64_t j) const {
-    const int c = blockIdx.z;
-    if (col >= g.gcnt[c] || j >= g.npa) return 0.0f;
-    return __ldg(g.K + (int64_t)g.gpair[g.gbeg[c] + col] * g.npa + j);
+    const int c = cell();
+    if (col >= __ldg(g.gcnt + c) || j >= g.npa) return 0.0f;
+    return __ldg(g.K + (int64_t)__ldg(g.gpair + __ldg(g.gbeg + c) + col) * g.npa + j);
   }
   static __device__ __forceinline__ float inner(float acc, float a, float b) { return fmaf(a, b, acc); }
   __device__ void epilogue(double (&acc)[8][4], int64_t r0, int64_t n0, float*) const {
-    const int c = blockIdx.z;
+    const int c = cell();
+    const int32_t mc = g.mcnt[c], gc = g.gcnt[c];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int64_t row = r0 + i;
-      if (row >= g.mcnt[c]) continue;
+      if (row >= mc) continue;
       const int64_t r = g.mbeg[c] + row;
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
         const int64_t col = n0 + jj;
-        if (col >= g.gcnt[c]) continue;
+        if (col >= gc) continue;
         const int64_t q = g.gbeg[c] + col;
         const int p = g.gpair[q];
         const double v = g.poisson ? acc[i][jj] - (double)g.scaling[p] * g.rowstat[r] : acc[i][jj];
@@ -159,6 +178,7 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
   double mx = -INFINITY;
   for (int i = 0; i < g.m; ++i) {
     const int c = g.cand[p * g.m + i];
+    if (c < 0) break;
     const int64_t q = g.ppos[p * g.m + i];
     for (int k = lane; k < g.mcnt[c]; k += 32) mx = fmax(mx, ll_of(c, q, k));
   }
@@ -166,6 +186,7 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
   double s = 0.0, d = 0.0, pl = 0.0;
   for (int i = 0; i < g.m; ++i) {
     const int c = g.cand[p * g.m + i];
+    if (c < 0) break;
     const int64_t q = g.ppos[p * g.m + i];
     for (int k = lane; k < g.mcnt[c]; k += 32) {
       const double l = ll_of(c, q, k);
@@ -192,47 +213,101 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
   }
   for (int i = 0; i < g.m; ++i) {
     const int c = g.cand[p * g.m + i];
+    if (c < 0) break;
     const int64_t q = g.ppos[p * g.m + i];
     const int64_t col = q - g.gbeg[c];
+    float cm = 0.0f;
     for (int k = lane; k < g.mcnt[c]; k += 32) {
       const float P = (float)exp(ll_of(c, q, k) - lse);
       g.Pt[g.goff[c] + (int64_t)k * g.gcnt[c] + col] = (float)(P / phi_new);
       atomicAdd(g.T + g.mbeg[c] + k, P);
+      cm += P;
     }
+    for (int o = 16; o > 0; o >>= 1) cm += __shfl_xor_sync(0xffffffffu, cm, o);
+    if (lane == 0) g.cmass[p * g.m + i] = cm;
   }
 }
 
+// t[p][c] from a proposed iteration: the responsibility mass of each
+// candidate cell, 0 elsewhere (t zeroed by the caller).
+__global__ void scatter_targets_kernel(const int32_t* cand, const float* cmass, int64_t N, int m,
+                                       int n_cells, float* t) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= N * m) return;
+  const int c = cand[e];
+  if (c >= 0) t[(e / m) * n_cells + c] = cmass[e];
+}
+
 // Grouped compress, one contraction per cell: rows = the cell's rotations,
-// columns = pixels, reduction over the cell's pairs: U_r / T_r.
+// columns = pixels, reduction over the cell's pairs, giving T_r U_r; the
+// epilogue inserts it into the interleaved (model, weight) accumulators
+// (emc_atomic.cu:115-133: weight w = rotw T_r, so model += rotw (T_r U_r)),
+// skipping rotations with T_r <= 1e-10.  blockIdx.x indexes the (cell, row
+// offset) list, blockIdx.y the pixel tile.
 struct OpGroupCmp {
   using Acc = float;
   static constexpr bool kBKMajor = false;
   GroupArgs g;
-  __device__ int64_t ksize() const { return g.gcnt[blockIdx.z]; }
+  __device__ int cell() const { return __ldg(&g.ctiles[blockIdx.x].x); }
+  __device__ bool origin(int64_t& m0, int64_t& n0) const {
+    m0 = g.ctiles[blockIdx.x].y;
+    n0 = (int64_t)blockIdx.y * TN;
+    return true;
+  }
+  __device__ int64_t ksize() const { return g.gcnt[cell()]; }
   __device__ float a(int64_t row, int64_t k) const {
-    const int c = blockIdx.z;
-    if (row >= g.mcnt[c] || k >= g.gcnt[c]) return 0.0f;
-    return g.Pt[g.goff[c] + row * g.gcnt[c] + k];
+    const int c = cell();
+    const int32_t gc = __ldg(g.gcnt + c);
+    if (row >= __ldg(g.mcnt + c) || k >= gc) return 0.0f;
+    return g.Pt[__ldg(g.goff + c) + row * gc + k];
   }
   __device__ float b(int64_t j, int64_t k) const {
-    const int c = blockIdx.z;
-    if (j >= g.npa || k >= g.gcnt[c]) return 0.0f;
-    return __ldg(g.K + (int64_t)g.gpair[g.gbeg[c] + k] * g.npa + j);
+    const int c = cell();
+    if (j >= g.npa || k >= __ldg(g.gcnt + c)) return 0.0f;
+    return __ldg(g.K + (int64_t)__ldg(g.gpair + __ldg(g.gbeg + c) + k) * g.npa + j);
   }
   static __device__ __forceinline__ float inner(float acc, float a, float b) { return fmaf(a, b, acc); }
   __device__ void epilogue(float (&acc)[8][4], int64_t r0, int64_t j0, float*) const {
-    const int c = blockIdx.z;
+    const int c = cell();
+    const int32_t mc = g.mcnt[c];
+    float cx[4], cy[4], cz[4];
+    bool use[4];
 #pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int64_t j = j0 + jj;
+      use[jj] = j < g.npa && g.ins[j] == 1;
+      cx[jj] = use[jj] ? g.cx[j] : 0.0f;
+      cy[jj] = use[jj] ? g.cy[j] : 0.0f;
+      cz[jj] = use[jj] ? g.cz[j] : 0.0f;
+    }
+#pragma unroll 1
     for (int i = 0; i < 8; ++i) {
       const int64_t row = r0 + i;
-      if (row >= g.mcnt[c]) continue;
+      if (row >= mc) break;
       const int64_t r = g.mbeg[c] + row;
       const float T = g.T[r];
+      if (!(T > 1e-10f)) continue;
+      const float rw = g.rotw[r], wT = rw * T;
+      float m[9];
+      emc_voxel::rotation_matrix(g.quat + 4 * r, m);
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
-        const int64_t j = j0 + jj;
-        if (j >= g.npa) continue;
-        g.U[r * g.npa + j] = T > 1e-10f ? acc[i][jj] / T : acc[i][jj];
+        if (!use[jj]) continue;
+        float u[3];
+        emc_voxel::position(m, g.side, cx[jj], cy[jj], cz[jj], u);
+        const float val = rw * acc[i][jj];
+        if (g.interp == 0) {
+          int64_t v;
+          if (emc_voxel::nearest(u, g.side, 0, &v)) red_add_v2(g.acc + v, val, wT);
+        } else {
+#pragma unroll
+          for (int cc = 0; cc < 8; ++cc) {
+            int64_t v;
+            float wc;
+            if (!emc_voxel::trilinear_corner(u, g.side, cc, &v, &wc) || wc == 0.0f) continue;
+            red_add_v2(g.acc + v, wc * val, wc * wT);
+          }
+        }
       }
     }
   }
@@ -263,28 +338,35 @@ cudaError_t launch_targets(const TargetArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_select(const float* probs, int64_t N, int C, int m, int32_t* cand, float* mass,
-                          cudaStream_t st) {
-  select_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(probs, N, C, m, cand, mass);
+cudaError_t launch_scatter_targets(const int32_t* cand, const float* cmass, int64_t N, int m,
+                                  int n_cells, float* t, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(t, 0, sizeof(float) * N * n_cells, st);
+  if (e != cudaSuccess) return e;
+  scatter_targets_kernel<<<(unsigned)((N * m + 255) / 256), 256, 0, st>>>(cand, cmass, N, m, n_cells, t);
   return cudaGetLastError();
 }
 
-cudaError_t launch_group_maximize(const GroupArgs& g, int64_t max_pairs, int64_t max_members,
-                                  cudaStream_t st) {
-  OpGroupLL op{g};
-  dim3 grid((unsigned)((max_pairs + TN - 1) / TN), (unsigned)((max_members + TM - 1) / TM),
-            (unsigned)g.n_cells);
-  tile_kernel<<<grid, kTileThreads, 0, st>>>(op);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+cudaError_t launch_select(const float* probs, int64_t N, int C, int m, float mass_target,
+                          int32_t* cand, float* mass, cudaStream_t st) {
+  select_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(probs, N, C, m, mass_target, cand, mass);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_maximize(const GroupArgs& g, int64_t n_mtiles, cudaStream_t st) {
+  if (n_mtiles > 0) {
+    OpGroupLL op{g};
+    tile_kernel<<<(unsigned)n_mtiles, kTileThreads, 0, st>>>(op);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   group_softmax_kernel<<<(unsigned)((g.N + 7) / 8), 256, 0, st>>>(g);
   return cudaGetLastError();
 }
 
-cudaError_t launch_group_compress(const GroupArgs& g, int64_t max_members, cudaStream_t st) {
+cudaError_t launch_group_compress(const GroupArgs& g, int64_t n_ctiles, cudaStream_t st) {
+  if (n_ctiles == 0) return cudaSuccess;
   OpGroupCmp op{g};
-  dim3 grid((unsigned)((g.npa + TN - 1) / TN), (unsigned)((max_members + TM - 1) / TM),
-            (unsigned)g.n_cells);
+  dim3 grid((unsigned)n_ctiles, (unsigned)((g.npa + TN - 1) / TN));
   tile_kernel<<<grid, kTileThreads, 0, st>>>(op);
   return cudaGetLastError();
 }

@@ -28,14 +28,20 @@ struct TargetArgs {
   float* t;                // [N][n_cells]
 };
 cudaError_t launch_targets(const TargetArgs& a, cudaStream_t st);
+// The same after a proposed iteration: t[p][cand[p][i]] = cmass[p][i], 0 elsewhere.
+cudaError_t launch_scatter_targets(const int32_t* cand, const float* cmass, int64_t N, int m,
+                                   int n_cells, float* t, cudaStream_t st);
 
-// cand[p][0..m) = the m most probable cells of probs[p][0..C); mass[p] = their total.
-cudaError_t launch_select(const float* probs, int64_t N, int C, int m, int32_t* cand, float* mass,
-                          cudaStream_t st);
+// cand[p][0..m): the most probable cells of probs[p][0..C) in order, until
+// their total reaches mass_target or m cells are taken (then -1);
+// mass[p] = their total.
+cudaError_t launch_select(const float* probs, int64_t N, int C, int m, float mass_target,
+                          int32_t* cand, float* mass, cudaStream_t st);
 
 // Pairs (pattern, selected cell) grouped by cell: group c holds pairs
 // gbeg[c] .. gbeg[c]+gcnt[c]-1, pair q belongs to pattern gpair[q]; pattern
-// p's i-th selected cell is cand[p*m+i] and its pair is ppos[p*m+i].  Cell c's
+// p's i-th selected cell is cand[p*m+i] (-1: none, and none after it) and
+// its pair is ppos[p*m+i].  Cell c's
 // fine rotations are mbeg[c] .. mbeg[c]+mcnt[c]-1.
 struct GroupArgs {
   int64_t N, npa, MM;      // MM: row stride of Y (>= largest cell)
@@ -64,10 +70,20 @@ struct GroupArgs {
   double* lse;             // [N]
   double* plogp;           // [N]
   float* new_scaling;      // [N]
-  float* U;                // [R][npa] averaged slices
+  float* cmass;            // [N][m] responsibility mass of each candidate cell
+  // tile lists: mtiles (cell, member offset, pair offset) of the grouped
+  // maximize; ctiles (cell, member offset) of the grouped compress
+  const int4* mtiles;
+  const int4* ctiles;
+  // insertion (compress epilogue) into interleaved (model, weight) accumulators
+  const float* rotw;       // [R]
+  const float* quat;       // [R][4]
+  const float *cx, *cy, *cz;
+  const int32_t* ins;      // [npa] insertion mask (== 1)
+  int side, interp;
+  float2* acc;             // [M] zeroed by the caller
 };
-cudaError_t launch_group_maximize(const GroupArgs& g, int64_t max_pairs, int64_t max_members,
-                                  cudaStream_t st);
-cudaError_t launch_group_compress(const GroupArgs& g, int64_t max_members, cudaStream_t st);
+cudaError_t launch_group_maximize(const GroupArgs& g, int64_t n_mtiles, cudaStream_t st);
+cudaError_t launch_group_compress(const GroupArgs& g, int64_t n_ctiles, cudaStream_t st);
 
 }  // namespace emc

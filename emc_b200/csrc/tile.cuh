@@ -3,6 +3,7 @@
 // proposal, and the proposal network's layers).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 namespace emc {
 
@@ -12,16 +13,28 @@ constexpr int kTileThreads = 256;
 // of 32, 256 threads with an 8x4 register tile each.  Op supplies the operand
 // loads (a(row, k), b(col, k)), the per-element update, the epilogue, and may
 // read blockIdx.z (grouped contractions).  The K extent comes from
-// op.ksize() and may be 0 for an empty group.
+// op.ksize() and may be 0 for an empty group.  An Op with a member
+// origin(m0, n0) places its blocks itself (a list of tiles of uneven groups,
+// indexed by blockIdx.x); a block whose origin() returns false exits.
 constexpr int TM = 128, TN = 64, TK = 32;
+
+template <class Op, class = void>
+struct has_origin : std::false_type {};
+template <class Op>
+struct has_origin<Op, std::void_t<decltype(&Op::origin)>> : std::true_type {};
 
 template <class Op>
 __global__ void __launch_bounds__(kTileThreads) tile_kernel(const Op op) {
   __shared__ __align__(16) float As[TK][TM + 4];
   __shared__ __align__(16) float Bs[TK][TN + 4];
   const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-  const int64_t m0 = (int64_t)blockIdx.y * TM;
-  const int64_t n0 = (int64_t)blockIdx.x * TN;
+  int64_t m0, n0;
+  if constexpr (has_origin<Op>::value) {
+    if (!op.origin(m0, n0)) return;  // uniform over the block
+  } else {
+    m0 = (int64_t)blockIdx.y * TM;
+    n0 = (int64_t)blockIdx.x * TN;
+  }
   using Acc = typename Op::Acc;
   Acc acc[8][4];
   float tacc[8][4];

@@ -29,7 +29,7 @@ def _bind():
         ("emc_set_cells", [P, P, C.c_int32], C.c_int),
         ("emc_pattern_features", [P, C.c_int32, P], C.c_int),
         ("emc_cell_targets", [P, P], C.c_int),
-        ("emc_iterate_proposed", [P, P, C.c_int32, C.c_float, P], C.c_int),
+        ("emc_iterate_proposed", [P, P, C.c_int32, C.c_float, C.c_float, P], C.c_int),
         ("emc_net_create", [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, P], C.c_int),
         ("emc_net_destroy", [P], C.c_int),
         ("emc_net_num_params", [P], I64),
@@ -156,7 +156,8 @@ class LearnedProposal:
         return x
 
     def targets(self):
-        """Cell posterior of the last dense maximize, [N][n_cells]."""
+        """Cell posterior of the last maximize (dense, or proposed: 0 outside
+        the candidate cells), [N][n_cells]."""
         import torch
         t = torch.empty((self.ctx.N, self.n_cells), dtype=torch.float32, device="cuda")
         torch.cuda.synchronize()
@@ -187,11 +188,23 @@ class LearnedProposal:
         torch.cuda.synchronize()
         return out
 
-    def iterate(self, probs, cells_per_pattern, threshold=0.99):
-        """One proposed iteration; returns its statistics as a dict."""
+    @staticmethod
+    def blend(probs, previous=None, weight=0.5):
+        """Cell probabilities to select from: the network's prediction mixed
+        with the previous iteration's cell posterior (emc_cell_targets), so
+        the cells holding a pattern's last responsibilities stay candidates."""
+        if previous is None:
+            return probs
+        return (1.0 - weight) * probs + weight * previous
+
+    def iterate(self, probs, max_cells, mass_target=1.0, threshold=0.99):
+        """One proposed iteration (emc_iterate_proposed): per pattern, its most
+        probable cells until their predicted mass reaches mass_target, at most
+        max_cells; the dense iteration when the mean predicted mass is below
+        threshold.  Returns the iteration's statistics as a dict."""
         import torch
         torch.cuda.synchronize()
         st = ProposalStats()
-        self.ctx._c(lib().emc_iterate_proposed(self.ctx._h, probs.data_ptr(), cells_per_pattern,
-                                               threshold, C.byref(st)))
+        self.ctx._c(lib().emc_iterate_proposed(self.ctx._h, probs.data_ptr(), max_cells,
+                                               mass_target, threshold, C.byref(st)))
         return {k: getattr(st, k) for k, _ in ProposalStats._fields_ if k != "pad_"}

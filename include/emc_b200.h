@@ -133,7 +133,7 @@ int64_t emc_active_pixels(const emc_context *ctx);
  * the 420-rotation 600-cell sampling); the rotation list given to
  * emc_set_rotations must be sorted by cell.  A proposal network predicts, per
  * pattern, a posterior over the cells; emc_iterate_proposed then evaluates
- * each pattern only against the fine rotations of its m most probable cells,
+ * each pattern only against the fine rotations of its most probable cells,
  * or runs the dense iteration when the mean predicted mass on those cells is
  * below `threshold`. */
 typedef struct {
@@ -150,13 +150,18 @@ emc_status emc_set_cells(emc_context *ctx, const int32_t *cell, int32_t n_cells)
 /* x [N][in_side^2] (device): log(1 + counts summed over 2x2 pixel blocks),
  * in_side = side / 2; the proposal network's input. */
 emc_status emc_pattern_features(emc_context *ctx, int32_t in_side, float *x_device);
-/* t [N][n_cells] (device): the last maximize's responsibilities summed over
+/* t [N][n_cells] (device): the responsibilities of the last maximize (dense,
+ * or proposed: then 0 outside each pattern's candidate cells) summed over
  * each cell's rotations; the proposal network's training target. */
 emc_status emc_cell_targets(emc_context *ctx, float *t_device);
-/* One iteration restricted to the proposal's top-m cells per pattern.
- * cell_probs: device [N][n_cells]. */
-emc_status emc_iterate_proposed(emc_context *ctx, const float *cell_probs_device, int32_t m,
-                                float threshold, emc_proposal_stats *stats);
+/* One iteration restricted, per pattern, to its most probable cells: cells in
+ * order of predicted probability until their predicted mass reaches
+ * mass_target (>= 1: always max_cells cells), at most max_cells.  The dense
+ * iteration runs instead when the mean predicted mass of the selected cells
+ * is below `threshold`.  cell_probs: device [N][n_cells]. */
+emc_status emc_iterate_proposed(emc_context *ctx, const float *cell_probs_device,
+                                int32_t max_cells, float mass_target, float threshold,
+                                emc_proposal_stats *stats);
 
 /* Proposal network: three 3x3 stride-2 convolutions (16, 32, 64 channels,
  * ReLU) and a fully connected layer to n_out logits, softmax.  BF16 weights

@@ -539,12 +539,23 @@ void orc_normalize_model(int64_t M, double* model, const double* weight) {
 void orc_iterate(const orc_config* c, const float* images, const int32_t* mask, const float* rot,
                  const float* rotw, const float* cx, const float* cy, const float* cz,
                  double* model, double* scaling, double* resp_out, orc_stats* stats) {
+  orc_iterate_restricted(c, images, mask, rot, rotw, cx, cy, cz, nullptr, model, scaling,
+                         resp_out, stats);
+}
+
+void orc_iterate_restricted(const orc_config* c, const float* images, const int32_t* mask,
+                            const float* rot, const float* rotw, const float* cx, const float* cy,
+                            const float* cz, const uint8_t* allowed, double* model,
+                            double* scaling, double* resp_out, orc_stats* stats) {
   const int64_t R = c->n_rotations, N = c->n_patterns;
   const int64_t npix = (int64_t)c->side * c->side;
   const int64_t M = npix * c->side;
   std::vector<double> S(R * npix), P(R * N), lse(N), T(R);
   orc_expand(c, model, rot, cx, cy, cz, S.data());
   orc_loglik(c, S.data(), images, mask, scaling, P.data());
+  if (allowed)  // rotations outside a pattern's candidate set get no responsibility
+    for (int64_t i = 0; i < R * N; ++i)
+      if (!allowed[i]) P[i] = -INFINITY;
   const double plogp = orc_softmax(R, N, P.data(), lse.data());
   orc_update_scaling(c, S.data(), images, mask, P.data(), scaling);
   std::vector<double> wacc(M, 0.0);

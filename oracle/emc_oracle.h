@@ -98,6 +98,16 @@ void orc_iterate(const orc_config* c, const float* images, const int32_t* mask,
                  const float* rot, const float* rotw, const float* cx, const float* cy,
                  const float* cz, double* model, double* scaling, double* resp_out,
                  orc_stats* stats);
+/* The same iteration with the softmax restricted, per pattern, to a candidate
+   set of rotations: allowed[r][p] != 0 (every pattern needs at least one).
+   Log-likelihoods outside the set are -inf, so those responsibilities are 0
+   and the scaling update and compress sum over the candidates only.  This is
+   the iteration the learned orientation proposal evaluates (a top-k of the
+   rotations per pattern); with every pair allowed it equals orc_iterate. */
+void orc_iterate_restricted(const orc_config* c, const float* images, const int32_t* mask,
+                            const float* rot, const float* rotw, const float* cx, const float* cy,
+                            const float* cz, const uint8_t* allowed, double* model,
+                            double* scaling, double* resp_out, orc_stats* stats);
 
 #ifdef __cplusplus
 }

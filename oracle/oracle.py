@@ -74,6 +74,7 @@ def lib():
         _lib.orc_insert.argtypes = [P] * 11
         _lib.orc_normalize_model.argtypes = [C.c_int64, P, P]
         _lib.orc_iterate.argtypes = [P] * 12
+        _lib.orc_iterate_restricted.argtypes = [P] * 13
     return _lib
 
 
@@ -219,17 +220,27 @@ def normalize_model(model, weight):
     return m
 
 
-def iterate(cfg, images, mask, rot, rotw, cx, cy, cz, model, scaling, want_resp=False):
+def iterate(cfg, images, mask, rot, rotw, cx, cy, cz, model, scaling, want_resp=False,
+            allowed=None):
     """One EMC iteration in the order of emc.c:989-1084.
 
+    allowed: optional [R][N] mask restricting each pattern's softmax to a
+    candidate set of rotations (orc_iterate_restricted).
     Returns (model, scaling, P or None, stats dict)."""
     k = _Keep()
     m = _f64(model).copy()
     sc = _f64(scaling).copy()
     P = np.zeros((cfg.n_rotations, cfg.n_patterns), np.float64) if want_resp else None
     st = Stats()
-    lib().orc_iterate(C.byref(cfg), k(_f32(images)), k(_i32(mask)), k(_f32(rot)),
-                      k(_f32(rotw)), k(_f32(cx)), k(_f32(cy)), k(_f32(cz)), _p(m), _p(sc),
-                      _p(P), C.byref(st))
+    if allowed is None:
+        lib().orc_iterate(C.byref(cfg), k(_f32(images)), k(_i32(mask)), k(_f32(rot)),
+                          k(_f32(rotw)), k(_f32(cx)), k(_f32(cy)), k(_f32(cz)), _p(m), _p(sc),
+                          _p(P), C.byref(st))
+    else:
+        al = k(np.ascontiguousarray(allowed, np.uint8))
+        assert allowed.shape == (cfg.n_rotations, cfg.n_patterns)
+        lib().orc_iterate_restricted(C.byref(cfg), k(_f32(images)), k(_i32(mask)), k(_f32(rot)),
+                                     k(_f32(rotw)), k(_f32(cx)), k(_f32(cy)), k(_f32(cz)), al,
+                                     _p(m), _p(sc), _p(P), C.byref(st))
     stats = {k: getattr(st, k) for k, _ in Stats._fields_}
     return m, sc, P, stats

@@ -115,3 +115,85 @@ def test_learned_proposal_end_to_end():
         st = lp.iterate(probs, m, threshold=1.01)
         assert st["fallback"] == 1
         assert rel(ctx.get_model(), m_dense) < 1e-5
+
+
+def _proposal_case(d, max_cells, mass_target=1.0, seed=0):
+    """Rotations sorted by coarse cell (n=1: 60 uneven cells), distinct random
+    cell probabilities, and the allowed[r][p] mask of the selected cells: in
+    order of probability until their (FP32) sum reaches mass_target, at most
+    max_cells."""
+    from emc_b200.proposal import sorted_rotations
+    q, w, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=1)
+    d = dict(d, q=q, w=w)
+    N = d["counts"].shape[0]
+    rng = np.random.default_rng(seed)
+    z = rng.standard_normal((N, n_cells)) * 2.0
+    probs = np.exp(z - z.max(1, keepdims=True))
+    probs = (probs / probs.sum(1, keepdims=True)).astype(np.float32)
+    sel = np.zeros((N, n_cells), bool)
+    for p in range(N):
+        tot = np.float32(0)
+        for k in np.argsort(-probs[p], kind="stable")[:max_cells]:
+            if mass_target < 1.0 and tot >= mass_target:
+                break
+            sel[p, k] = True
+            tot = np.float32(tot + probs[p, k])
+    allowed = sel[:, cell].T.astype(np.uint8)  # [R][N]
+    return d, cell, n_cells, probs, allowed
+
+
+@pytest.mark.parametrize("lik,interp,prec,tol,max_cells,mass_target", [
+    ("poisson", "nearest", "fp32", 1e-5, 7, 1.0),
+    ("gauss", "nearest", "fp32", 1e-4, 7, 1.0),
+    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0),
+    ("gauss", "nearest", "mixed", 1e-4, 7, 1.0),
+    ("poisson", "trilinear", "mixed", 1e-4, 7, 1.0),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.6),
+])
+def test_proposed_iteration_matches_restricted_oracle(lik, interp, prec, tol, max_cells,
+                                                      mass_target):
+    """One proposed iteration (the top cells of 60 uneven cells per pattern:
+    a fixed 7, or adaptive up to a predicted mass of 0.6) against the FP64
+    oracle's iteration restricted to the same candidate rotations."""
+    import torch
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal
+    from oracle import oracle as O
+    from parity import oracle_cfg
+    d, cell, n_cells, probs, allowed = _proposal_case(W.make("tiny16"), max_cells, mass_target)
+    cfg = oracle_cfg(d, lik, interp)
+    m_ref, s_ref, P_ref, st_ref = O.iterate(cfg, d["counts"], d["mask"], d["q"], d["w"], d["x"],
+                                            d["y"], d["z"], d["model0"].astype(np.float64),
+                                            d["scaling0"].astype(np.float64), want_resp=True,
+                                            allowed=allowed)
+    t_ref = np.zeros((P_ref.shape[1], n_cells))
+    np.add.at(t_ref.T, cell, P_ref)  # responsibility mass per (pattern, cell)
+    with make_ctx(d, lik, interp, prec) as ctx:
+        lp = LearnedProposal(ctx, cell, n_cells, bf16=True)
+        st = lp.iterate(torch.from_numpy(probs).cuda(), max_cells, mass_target, threshold=0.0)
+        assert st["fallback"] == 0
+        assert st["evaluations"] == int(allowed.sum())
+        assert rel(ctx.get_scaling(), s_ref) <= tol, rel(ctx.get_scaling(), s_ref)
+        assert rel(ctx.get_model(), m_ref) <= tol, rel(ctx.get_model(), m_ref)
+        assert abs(st["sum_plogp"] - st_ref["sum_plogp"]) <= 1e-3 * abs(st_ref["sum_plogp"]) + 1e-3
+        assert abs(st["total_loglik"] - st_ref["total_loglik"]) <= 1e-5 * abs(st_ref["total_loglik"])
+        t = lp.targets().cpu().numpy()
+        assert np.abs(t - t_ref).max() <= 1e-3
+
+
+def test_proposed_iteration_with_every_cell_is_the_dense_iteration():
+    import torch
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal
+    d, cell, n_cells, probs, _ = _proposal_case(W.make("tiny16"), 60)
+    with make_ctx(d, "poisson", "nearest", "mixed") as ctx:
+        m0, s0 = ctx.get_model(), ctx.get_scaling()
+        ctx.iterate()
+        m_dense, s_dense = ctx.get_model(), ctx.get_scaling()
+        ctx.set_model(m0)
+        ctx.set_scaling(s0)
+        lp = LearnedProposal(ctx, cell, n_cells)
+        st = lp.iterate(torch.from_numpy(probs).cuda(), n_cells, threshold=0.0)
+        assert st["evaluations"] == ctx.N * ctx.R
+        assert rel(ctx.get_model(), m_dense) <= 1e-4
+        assert rel(ctx.get_scaling(), s_dense) <= 1e-4
