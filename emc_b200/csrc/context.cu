@@ -3,6 +3,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -98,7 +99,11 @@ struct emc_context {
   int64_t *d_ppos = nullptr, *d_gbeg = nullptr, *d_goff = nullptr;
   float *d_mass = nullptr, *d_Yc = nullptr, *d_Pt = nullptr;
   int4 *d_mtiles = nullptr, *d_ctiles = nullptr;
-  int64_t mtiles_cap = 0, ctiles_cap = 0;
+  TileDesc *d_gmt = nullptr, *d_gct = nullptr;   // tcgen05 grouped tile lists
+  __half *d_Kg = nullptr, *d_KgT = nullptr, *d_Ahi = nullptr, *d_Alo = nullptr;
+  // capacities (elements) of the per-iteration proposal buffers
+  int64_t mtiles_cap = 0, ctiles_cap = 0, gmt_cap = 0, gct_cap = 0, pairs_cap = 0, slots_cap = 0,
+          yc_cap = 0, pt_cap = 0, kg_cap = 0, kgt_ld = 0, a_ld = 0;
   double *d_lse_c = nullptr, *d_plogp_c = nullptr;
   // Two event sets alternate between iterations, so the times of iteration
   // i-1 can be read while iteration i is still queued.
@@ -796,7 +801,6 @@ emc_status emc_set_cells(emc_context* c, const int32_t* cell, int32_t n_cells) {
   c->h_mbeg = beg;
   c->h_mcnt = cnt;
   c->max_members = 0;
-  c->cand_m = 0;  // the candidate buffers are sized by the largest cell: reallocate
   for (int32_t k : cnt) c->max_members = k > c->max_members ? k : c->max_members;
   return EMC_OK;
 }
@@ -844,28 +848,43 @@ emc_status emc_cell_targets(emc_context* c, float* t) {
   return EMC_OK;
 }
 
+}  // extern "C"
+
+// Grows a proposal buffer to hold at least `need` elements (contents not kept).
+template <class T>
+static emc_status grow(emc_context* c, T** p, int64_t& cap, int64_t need) {
+  if (need <= cap && *p) return EMC_OK;
+  if (*p) c->release(*p);
+  *p = nullptr;
+  cap = 0;
+  const int64_t n = need + need / 4 + 64;
+  TRY(c->alloc(p, n));
+  cap = n;
+  return EMC_OK;
+}
+
+extern "C" {
+
 emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, float mass_target,
                                 float threshold, emc_proposal_stats* stats) {
   if (!c || !probs || m < 1) return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
   if (m > c->n_cells) return c->fail(EMC_ERR_ARG, "more cells per pattern than cells");
   const int64_t N = c->N, R = c->R, pairs = N * m;
-  if (c->cand_m != m) {
-    for (void* p : {(void*)c->d_cand, (void*)c->d_ppos, (void*)c->d_gpair, (void*)c->d_Yc, (void*)c->d_Pt})
-      if (p) c->release(p);
-    TRY(c->alloc(&c->d_cand, pairs));
-    TRY(c->alloc(&c->d_ppos, pairs));
-    TRY(c->alloc(&c->d_gpair, pairs));
-    if (!c->d_mass) {
-      TRY(c->alloc(&c->d_mass, N));
-      TRY(c->alloc(&c->d_lse_c, N));
-      TRY(c->alloc(&c->d_plogp_c, N));
-    }
-    if (c->d_cmass) c->release(c->d_cmass);
-    TRY(c->alloc(&c->d_cmass, pairs));
-    TRY(c->alloc(&c->d_Yc, pairs * c->max_members));
-    TRY(c->alloc(&c->d_Pt, pairs * c->max_members));
-    if (!c->d_acc) TRY(c->alloc(&c->d_acc, c->M));
+  if (!c->d_mass) {
+    TRY(c->alloc(&c->d_mass, N));
+    TRY(c->alloc(&c->d_lse_c, N));
+    TRY(c->alloc(&c->d_plogp_c, N));
+  }
+  if (!c->d_acc) TRY(c->alloc(&c->d_acc, c->M));
+  if (pairs > c->pairs_cap || c->cand_m != m) {
+    int64_t cap = c->pairs_cap;
+    TRY(grow(c, &c->d_cand, cap, pairs));
+    cap = c->pairs_cap;
+    TRY(grow(c, &c->d_ppos, cap, pairs));
+    cap = c->pairs_cap;
+    TRY(grow(c, &c->d_cmass, cap, pairs));
+    c->pairs_cap = cap;
     c->cand_m = m;
   }
   TRY(emc_expand(c));
@@ -896,8 +915,12 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     if (stats) *stats = st;
     return EMC_OK;
   }
-  // group the (pattern, cell) pairs by cell (stable counting sort on the host)
-  std::vector<int32_t> gcnt(c->n_cells, 0);
+  // Group the (pattern, cell) pairs by cell (stable counting sort on the
+  // host).  Pairs live in slots: cell c owns slots gbeg[c] .. gbeg[c]+gcnt[c]-1,
+  // its first slot a multiple of 8 (16-byte aligned FP16 columns of KgT);
+  // the slots between cells are padding (pattern -1).
+  const int n_cells = c->n_cells;
+  std::vector<int32_t> gcnt(n_cells, 0);
   int64_t npairs = 0;
   for (int64_t p = 0; p < N; ++p)
     for (int32_t i = 0; i < m; ++i) {
@@ -906,22 +929,22 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
         if (i == 0) return c->fail(EMC_ERR_ARG, "cell probabilities must be finite");
         break;
       }
-      if (k >= c->n_cells) return c->fail(EMC_ERR_ARG, "cell index out of range");
+      if (k >= n_cells) return c->fail(EMC_ERR_ARG, "cell index out of range");
       gcnt[k]++;
       npairs++;
     }
-  std::vector<int64_t> gbeg(c->n_cells), goff(c->n_cells), fill(c->n_cells);
-  int64_t acc = 0, off = 0, maxp = 0, evals = 0;
-  for (int32_t k = 0; k < c->n_cells; ++k) {
-    gbeg[k] = acc;
-    fill[k] = acc;
-    acc += gcnt[k];
+  std::vector<int64_t> gbeg(n_cells), goff(n_cells), fill(n_cells);
+  int64_t S = 0, off = 0, evals = 0, kw = 0;
+  for (int32_t k = 0; k < n_cells; ++k) {
+    gbeg[k] = S;
+    fill[k] = S;
+    S += (gcnt[k] + 7) / 8 * 8;
     goff[k] = off;
     off += (int64_t)gcnt[k] * c->h_mcnt[k];
-    maxp = gcnt[k] > maxp ? gcnt[k] : maxp;
     evals += (int64_t)gcnt[k] * c->h_mcnt[k];
+    kw = std::max<int64_t>(kw, (gcnt[k] + 63) / 64 * 64);
   }
-  std::vector<int32_t> gpair(npairs);
+  std::vector<int32_t> gpair(S, -1);
   std::vector<int64_t> ppos(pairs, -1);
   for (int64_t p = 0; p < N; ++p)
     for (int32_t i = 0; i < m; ++i) {
@@ -931,39 +954,77 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
       gpair[q] = (int32_t)p;
       ppos[p * m + i] = q;
     }
-  // tile lists of the grouped contractions: only cells that some pattern selected
+  // tcgen05 grouped contractions: mixed precision, cells of at most 256 rotations
+  const bool tc = c->mixed && c->max_members <= 256 && S > 0 && (S + 31) / 32 <= 65535;
+  const int64_t MM = tc ? 256 : c->max_members;
+  TRY(grow(c, &c->d_gpair, c->slots_cap, S));
+  TRY(grow(c, &c->d_Yc, c->yc_cap, S * MM));
+  TRY(grow(c, &c->d_Pt, c->pt_cap, evals));
   std::vector<int4> mt, ct;
-  for (int32_t k = 0; k < c->n_cells; ++k) {
-    if (gcnt[k] == 0) continue;
-    for (int32_t r0 = 0; r0 < c->h_mcnt[k]; r0 += TM) {
-      ct.push_back(make_int4(k, r0, 0, 0));
-      for (int32_t q0 = 0; q0 < gcnt[k]; q0 += TN) mt.push_back(make_int4(k, r0, q0, 0));
+  std::vector<TileDesc> gmt, gct;
+  if (tc) {
+    const int64_t ptiles = (c->npa + 255) / 256;
+    for (int32_t k = 0; k < n_cells; ++k) {
+      if (gcnt[k] == 0) continue;
+      for (int32_t q0 = 0; q0 < gcnt[k]; q0 += 128)
+        gmt.push_back(TileDesc{(int32_t)(gbeg[k] + q0), 0, (int32_t)c->h_mbeg[k], 0,
+                               (int32_t)(c->Ppad / kMaximizeBK), k, q0, 0});
+      for (int32_t r0 = 0; r0 < c->h_mcnt[k]; r0 += 128)
+        for (int64_t nt = 0; nt < ptiles; ++nt)
+          gct.push_back(TileDesc{(int32_t)(c->h_mbeg[k] + r0), 0, (int32_t)(nt * 256),
+                                 (int32_t)gbeg[k], (gcnt[k] + 63) / 64, k, r0, 0});
     }
+    TRY(grow(c, &c->d_gmt, c->gmt_cap, (int64_t)gmt.size()));
+    TRY(grow(c, &c->d_gct, c->gct_cap, (int64_t)gct.size()));
+    TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
+    if (S > c->kgt_ld) {
+      if (c->d_KgT) c->release(c->d_KgT);
+      c->d_KgT = nullptr;
+      c->kgt_ld = 0;
+      const int64_t ld = (S + S / 4 + 63) / 64 * 64;
+      TRY(c->alloc(&c->d_KgT, ld * c->Ppad));
+      c->kgt_ld = ld;
+    }
+    if (kw > c->a_ld) {
+      for (__half** q : {&c->d_Ahi, &c->d_Alo})
+        if (*q) {
+          c->release(*q);
+          *q = nullptr;
+        }
+      c->a_ld = 0;
+      const int64_t ld = (kw + kw / 4 + 63) / 64 * 64;
+      TRY(c->alloc(&c->d_Ahi, R * ld));
+      TRY(c->alloc(&c->d_Alo, R * ld));
+      c->a_ld = ld;
+    }
+    CK(c, cudaMemcpyAsync(c->d_gmt, gmt.data(), sizeof(TileDesc) * gmt.size(), cudaMemcpyHostToDevice, c->st));
+    CK(c, cudaMemcpyAsync(c->d_gct, gct.data(), sizeof(TileDesc) * gct.size(), cudaMemcpyHostToDevice, c->st));
+  } else {
+    // CUDA-core grouped contractions: tile lists over the selected cells
+    for (int32_t k = 0; k < n_cells; ++k) {
+      if (gcnt[k] == 0) continue;
+      for (int32_t r0 = 0; r0 < c->h_mcnt[k]; r0 += TM) {
+        ct.push_back(make_int4(k, r0, 0, 0));
+        for (int32_t q0 = 0; q0 < gcnt[k]; q0 += TN) mt.push_back(make_int4(k, r0, q0, 0));
+      }
+    }
+    TRY(grow(c, &c->d_mtiles, c->mtiles_cap, (int64_t)mt.size()));
+    TRY(grow(c, &c->d_ctiles, c->ctiles_cap, (int64_t)ct.size()));
+    CK(c, cudaMemcpyAsync(c->d_mtiles, mt.data(), sizeof(int4) * mt.size(), cudaMemcpyHostToDevice, c->st));
+    CK(c, cudaMemcpyAsync(c->d_ctiles, ct.data(), sizeof(int4) * ct.size(), cudaMemcpyHostToDevice, c->st));
   }
-  if ((int64_t)mt.size() > c->mtiles_cap) {
-    if (c->d_mtiles) c->release(c->d_mtiles);
-    TRY(c->alloc(&c->d_mtiles, mt.size()));
-    c->mtiles_cap = (int64_t)mt.size();
-  }
-  if ((int64_t)ct.size() > c->ctiles_cap) {
-    if (c->d_ctiles) c->release(c->d_ctiles);
-    TRY(c->alloc(&c->d_ctiles, ct.size()));
-    c->ctiles_cap = (int64_t)ct.size();
-  }
-  CK(c, cudaMemcpyAsync(c->d_mtiles, mt.data(), sizeof(int4) * mt.size(), cudaMemcpyHostToDevice, c->st));
-  CK(c, cudaMemcpyAsync(c->d_ctiles, ct.data(), sizeof(int4) * ct.size(), cudaMemcpyHostToDevice, c->st));
-  CK(c, cudaMemcpyAsync(c->d_gpair, gpair.data(), sizeof(int32_t) * npairs, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_gpair, gpair.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_ppos, ppos.data(), sizeof(int64_t) * pairs, cudaMemcpyHostToDevice, c->st));
-  CK(c, cudaMemcpyAsync(c->d_gbeg, gbeg.data(), sizeof(int64_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
-  CK(c, cudaMemcpyAsync(c->d_gcnt, gcnt.data(), sizeof(int32_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
-  CK(c, cudaMemcpyAsync(c->d_goff, goff.data(), sizeof(int64_t) * c->n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_gbeg, gbeg.data(), sizeof(int64_t) * n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_gcnt, gcnt.data(), sizeof(int32_t) * n_cells, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_goff, goff.data(), sizeof(int64_t) * n_cells, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * N, cudaMemcpyDeviceToDevice, c->st));
   CK(c, cudaMemsetAsync(c->d_T, 0, sizeof(float) * R, c->st));
   GroupArgs g{};
   g.N = N;
   g.npa = c->npa;
-  g.MM = c->max_members;
-  g.n_cells = c->n_cells;
+  g.MM = MM;
+  g.n_cells = n_cells;
   g.m = m;
   g.poisson = c->gauss ? 0 : 1;
   g.mbeg = c->d_mbeg;
@@ -1006,21 +1067,68 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
   g.side = c->cfg.side;
   g.interp = c->cfg.interp;
   g.acc = c->d_acc;
-  c->mark(1);
-  CK(c, launch_group_maximize(g, (int64_t)mt.size(), c->st));
+  int launches = 0;
+  if (tc) {
+    CUtensorMap tmKg, tmKgT, tmAhi, tmAlo;
+    if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, kMaximizeBK) ||
+        !tc_encode_2d_strided(&tmKgT, c->d_KgT, S, c->Ppad, c->kgt_ld, 256, kCompressBK) ||
+        !tc_encode_2d_strided(&tmAhi, c->d_Ahi, c->a_ld, R, c->a_ld, 128, kCompressBK) ||
+        !tc_encode_2d_strided(&tmAlo, c->d_Alo, c->a_ld, R, c->a_ld, 128, kCompressBK))
+      return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
+    CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->kgt_ld, c->d_KgT, c->st));
+    c->mark(1);
+    GMaxEpiArgs ge{};
+    ge.tiles = c->d_gmt;
+    ge.mcnt = c->d_mcnt;
+    ge.gcnt = c->d_gcnt;
+    ge.gpair = c->d_gpair;
+    ge.poisson = g.poisson;
+    ge.scaling = c->d_scaling_prev;
+    ge.rowstat = c->d_rowstat;
+    ge.Y = c->d_Yc;
+    ge.ldY = MM;
+    CK(c, launch_group_maximize_tc(tmKg, c->tmBhi, c->tmBlo, (int64_t)gmt.size(), ge, c->d_status,
+                                   c->num_sms, c->st));
+    c->mark(2);
+    CK(c, launch_group_softmax(g, c->st));
+    CK(c, launch_p_split(g, c->d_cell, R, c->d_T, c->a_ld, c->d_Ahi, c->d_Alo, c->st));
+    c->mark(3);
+    CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
+    GCmpEpiArgs ce{};
+    ce.tiles = c->d_gct;
+    ce.mcnt = c->d_mcnt;
+    ce.npa = c->npa;
+    ce.side = c->cfg.side;
+    ce.interp = c->cfg.interp;
+    ce.quat = c->d_quat;
+    ce.rotw = c->d_rotw;
+    ce.T = c->d_T;
+    ce.cx = c->d_cx;
+    ce.cy = c->d_cy;
+    ce.cz = c->d_cz;
+    ce.ins = c->d_ins;
+    ce.acc = c->d_acc;
+    CK(c, launch_group_compress_tc(tmAhi, tmAlo, tmKgT, (int64_t)gct.size(), ce, c->d_status,
+                                   c->num_sms, c->st));
+    launches = 6;  // gather (2), contraction, softmax, split, contraction
+  } else {
+    c->mark(1);
+    CK(c, launch_group_maximize(g, (int64_t)mt.size(), c->st));
+    c->mark(2);
+    c->mark(3);
+    CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
+    CK(c, launch_group_compress(g, (int64_t)ct.size(), c->st));
+    launches = 3;  // contraction, softmax, contraction
+  }
   c->resp_source = 2;
-  c->mark(2);
-  c->mark(3);
-  CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
-  CK(c, launch_group_compress(g, (int64_t)ct.size(), c->st));
   c->mark(4);
   CK(c, launch_normalize_acc(c->d_acc, c->d_model, c->d_weight, c->M, c->d_scratch, c->d_stats,
                              c->st));
   CK(c, launch_sum_f64(c->d_plogp_c, N, c->d_stats + 2, c->st));
   CK(c, launch_sum_f64(c->d_lse_c, N, c->d_stats + 3, c->st));
   c->mark(5);
-  // select, grouped contraction + softmax, grouped compress, normalise (4), two sums
-  c->launches += 10 + ((!c->mixed && c->gauss) ? 1 : 0);
+  // select, the grouped stages, normalise (4), two sums
+  c->launches += 1 + launches + 6 + ((!c->mixed && c->gauss) ? 1 : 0);
   c->stage = 0;
   TRY(check_status(c));
   double h[4];

@@ -200,6 +200,27 @@ __global__ void __launch_bounds__(kThreads, 1)
       n = t - m * n_tiles;
     }
   };
+  // TMA origins (row and k offset of each operand) and k-block count of tile
+  // t: a regular m_tiles x n_tiles grid, or an epilogue-supplied tile list
+  // (grouped contractions of uneven groups)
+  auto coords = [&](int64_t t, int& ar, int& ak, int& br, int& bk, int64_t& kbs) {
+    if constexpr (Epi::kListed) {
+      const TileDesc d = epi.a.tiles[t];
+      ar = d.a_row;
+      ak = d.a_k0;
+      br = d.b_row;
+      bk = d.b_k0;
+      kbs = d.k_blocks;
+    } else {
+      int64_t mt, nt;
+      tile_mn(t, mt, nt);
+      ar = (int)(mt * BM);
+      ak = 0;
+      br = (int)(nt * BN);
+      bk = 0;
+      kbs = k_blocks;
+    }
+  };
 
   if (warp == 0) {
     if (lane == 0) {
@@ -209,9 +230,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       int64_t issued = 0;
       bool ok = true;
       for (int64_t t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        int64_t mt, nt;
-        tile_mn(t, mt, nt);
-        for (int64_t kb = 0; kb < k_blocks; ++kb) {
+        int ar, ak, br, bk;
+        int64_t kbs;
+        coords(t, ar, ak, br, bk, kbs);
+        for (int64_t kb = 0; kb < kbs; ++kb) {
           if (!bounded_wait(smem_u32(&empty_bar[s]), ph ^ 1, ctl, 1)) {
             ok = false;
             break;
@@ -220,11 +242,11 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_expect_tx(fb, STAGE_BYTES);
           const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
           const int kc = (int)(kb * BK);
-          tma_load_2d(base, &tmA0, kc, (int)(mt * BM), fb);
-          if (NA == 2) tma_load_2d(base + A_BYTES, &tmA1, kc, (int)(mt * BM), fb);
+          tma_load_2d(base, &tmA0, ak + kc, ar, fb);
+          if (NA == 2) tma_load_2d(base + A_BYTES, &tmA1, ak + kc, ar, fb);
           const uint32_t bbase = base + NA * A_BYTES;
-          tma_load_2d(bbase, &tmB0, kc, (int)(nt * BN), fb);
-          if (NB == 2) tma_load_2d(bbase + B_BYTES, &tmB1, kc, (int)(nt * BN), fb);
+          tma_load_2d(bbase, &tmB0, bk + kc, br, fb);
+          if (NB == 2) tma_load_2d(bbase + B_BYTES, &tmB1, bk + kc, br, fb);
           ++issued;
           if (++s == STAGES) {
             s = 0;
@@ -261,7 +283,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!bounded_wait(smem_u32(&tempty_bar[acc]), aph ^ 1, ctl, 2)) break;
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
-        for (int64_t kb = 0; kb < k_blocks; ++kb) {
+        int ar, ak, br, bk;
+        int64_t kbs;
+        coords(t, ar, ak, br, bk, kbs);
+        for (int64_t kb = 0; kb < kbs; ++kb) {
           if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3)) {
             ok = false;
             break;
@@ -310,7 +335,12 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (epi_abort) break;
       tc_fence_after();
       int64_t mt, nt;
-      tile_mn(t, mt, nt);
+      if constexpr (Epi::kListed) {
+        mt = t;  // listed epilogues read their tile descriptor
+        nt = 0;
+      } else {
+        tile_mn(t, mt, nt);
+      }
       e.tile_begin(mt, nt, ep_tid, epi_smem);
       e.row_begin(mt * BM + quarter * 32 + lane);
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
@@ -346,6 +376,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 // with X the scaling denominator term (gaussian: C_rp, poisson: sum W_r).  The
 // combine kernel turns them into lse_p, the new scaling and sum P log P.
 struct EpiMax {
+  static constexpr bool kListed = false;
   static constexpr int kSmemBytes = BN * 8;
   MaxEpiArgs a;
   int64_t n0, ntile, p;
@@ -444,6 +475,7 @@ __device__ __forceinline__ void red_add_v2(float2* p, float x, float y) {
 
 // compress: row = rotation, column = active pixel; inserts into model/weight.
 struct EpiCmp {
+  static constexpr bool kListed = false;
   static constexpr int kSmemBytes = BN * 16;
   CmpEpiArgs a;
   int64_t j0;
@@ -487,6 +519,136 @@ struct EpiCmp {
       float u[3];
       emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
       const float val = __uint_as_float(v[k]) * wU;
+      if (a.interp == 0) {
+        int64_t vox;
+        if (!emc_voxel::nearest(u, a.side, 0, &vox)) continue;
+        red_add_v2(a.acc + vox, val, wT);
+      } else {
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+          int64_t vox;
+          float wc;
+          if (!emc_voxel::trilinear_corner(u, a.side, cc, &vox, &wc) || wc == 0.0f) continue;
+          red_add_v2(a.acc + vox, wc * val, wc * wT);
+        }
+      }
+    }
+  }
+  __device__ void row_end() {}
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
+};
+
+// Grouped maximize of the learned proposal, one tile list over the selected
+// cells: row = slot (a (pattern, cell) pair; the cell's slots are contiguous),
+// column = member rotation of the cell (<= 256).  Writes Y[slot][member]:
+// poisson LL = x - phi_p sum W_r, gaussian cross term x.
+struct EpiGMax {
+  static constexpr bool kListed = true;
+  static constexpr int kSmemBytes = BN * 8;
+  GMaxEpiArgs a;
+  TileDesc d;
+  int32_t mc, gc;
+  int64_t slot;
+  bool rv;
+  float phi;
+
+  __device__ void tile_begin(int64_t t, int64_t, int tid, uint8_t* smem) {
+    float2* rs2 = reinterpret_cast<float2*>(smem);
+    d = a.tiles[t];
+    mc = a.mcnt[d.cell];
+    gc = a.gcnt[d.cell];
+    epi_bar();
+    for (int c = tid; c < BN; c += 128) {
+      const double w = (a.poisson && c < mc) ? a.rowstat[d.b_row + c] : 0.0;
+      const float hi = (float)w;
+      rs2[c] = make_float2(hi, (float)(w - (double)hi));
+    }
+    epi_bar();
+  }
+  __device__ void row_begin(int64_t row) {
+    const int local = (int)(row % BM);
+    rv = d.local0 + local < gc;
+    slot = (int64_t)d.a_row + local;
+    phi = rv ? a.scaling[a.gpair[slot]] : 1.0f;
+  }
+  __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) {
+    if (!rv || c >= mc) return;
+    const float2* rs2 = reinterpret_cast<const float2*>(smem);
+    float y[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const float x = __uint_as_float(v[k]);
+      if (a.poisson) {
+        const float2 w = rs2[c + k];
+        y[k] = fmaf(-phi, w.y, fmaf(-phi, w.x, x));
+      } else {
+        y[k] = x;
+      }
+    }
+    float* dst = a.Y + slot * a.ldY + c;
+    if (c + 16 <= mc) {
+#pragma unroll
+      for (int k = 0; k < 16; k += 4)
+        *reinterpret_cast<float4*>(dst + k) = make_float4(y[k], y[k + 1], y[k + 2], y[k + 3]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k)
+        if (c + k < mc) dst[k] = y[k];
+    }
+  }
+  __device__ void row_end() {}
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
+};
+
+// Grouped compress: row = member rotation r of the tile's cell, column =
+// active pixel; acc = U_r (the operand rows are P / (T_r phi)), inserted with
+// weight rotw T_r as in EpiCmp.
+struct EpiGCmp {
+  static constexpr bool kListed = true;
+  static constexpr int kSmemBytes = BN * 16;
+  GCmpEpiArgs a;
+  TileDesc d;
+  int32_t mc;
+  bool active;
+  float m[9];
+  float wT;
+
+  __device__ void tile_begin(int64_t t, int64_t, int tid, uint8_t* smem) {
+    float4* cs = reinterpret_cast<float4*>(smem);
+    d = a.tiles[t];
+    mc = a.mcnt[d.cell];
+    epi_bar();
+    for (int c = tid; c < BN; c += 128) {
+      const int64_t j = (int64_t)d.b_row + c;
+      cs[c] = j < a.npa ? make_float4(a.cx[j], a.cy[j], a.cz[j], a.ins[j] == 1 ? 1.0f : 0.0f)
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    epi_bar();
+  }
+  __device__ void row_begin(int64_t row) {
+    const int local = (int)(row % BM);
+    active = false;
+    if (d.local0 + local < mc) {
+      const int64_t r = (int64_t)d.a_row + local;
+      const float T = a.T[r];
+      // emc_atomic.cu:128: rotations with T_r <= 1e-10 are skipped; weight w = rotw T
+      if (T > 1e-10f) {
+        active = true;
+        wT = a.rotw[r] * T;
+        emc_voxel::rotation_matrix(a.quat + 4 * r, m);
+      }
+    }
+  }
+  __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) {
+    if (!active) return;
+    const float4* cs = reinterpret_cast<const float4*>(smem);
+#pragma unroll 4
+    for (int k = 0; k < 16; ++k) {
+      const float4 q = cs[c + k];
+      if (q.w == 0.0f) continue;
+      float u[3];
+      emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
+      const float val = __uint_as_float(v[k]) * wT;
       if (a.interp == 0) {
         int64_t vox;
         if (!emc_voxel::nearest(u, a.side, 0, &vox)) continue;
@@ -770,6 +932,11 @@ __global__ void pack_kernel(const float* K, int64_t N, int64_t npa, int64_t Npad
 
 bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
                   uint32_t box_rows, uint32_t box_inner) {
+  return tc_encode_2d_strided(tm, base, inner, rows, inner, box_rows, box_inner);
+}
+
+bool tc_encode_2d_strided(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
+                          uint64_t ld, uint32_t box_rows, uint32_t box_inner) {
   typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -785,8 +952,9 @@ bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t ro
     fn = (EncodeFn)p;
   }
   const cuuint64_t dims[2] = {inner, rows};
-  const cuuint64_t strides[1] = {inner * 2};
+  const cuuint64_t strides[1] = {ld * 2};
   if (box_inner != 64 && box_inner != 32) return false;
+  if (ld < inner || (ld * 2) % 16 != 0) return false;
   const cuuint32_t box[2] = {box_inner, box_rows};
   const cuuint32_t estr[2] = {1, 1};
   return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box,
@@ -818,6 +986,26 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
   // pixel tiles are the inner index: CTAs in flight share the P' tiles
   return run_gemm<2, 1, 3, false, kCompressBK>(tmPhi, tmPlo, tmKt, tmKt, Rpad / BM, Ppad / BN,
                                                Npad / kCompressBK, epi, status, num_sms, st);
+}
+
+cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap& tmBhi,
+                                     const CUtensorMap& tmBlo, int64_t n_tiles,
+                                     const GMaxEpiArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st) {
+  EpiGMax epi;
+  epi.a = e;
+  return run_gemm<1, 2, 5, true, kMaximizeBK>(tmKg, tmKg, tmBhi, tmBlo, n_tiles, 1, 0, epi,
+                                              status, num_sms, st);
+}
+
+cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap& tmAlo,
+                                     const CUtensorMap& tmKgT, int64_t n_tiles,
+                                     const GCmpEpiArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st) {
+  EpiGCmp epi;
+  epi.a = e;
+  return run_gemm<2, 1, 3, false, kCompressBK>(tmAhi, tmAlo, tmKgT, tmKgT, n_tiles, 1, 0, epi,
+                                               status, num_sms, st);
 }
 
 cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {

@@ -313,6 +313,62 @@ struct OpGroupCmp {
   }
 };
 
+// Kg[slot][j] = Kh[pattern of slot][j] (FP16 counts, rows of Ppad; zero rows
+// for the padding slots), 16-byte copies.
+__global__ void gather_rows_kernel(const __half* Kh, int64_t Ppad, const int32_t* slot_pat,
+                                   int64_t S, __half* Kg) {
+  const int64_t s = blockIdx.x;  // one block per slot
+  if (s >= S) return;
+  const int p = slot_pat[s];
+  const int64_t n16 = Ppad / 8;
+  const uint4* src = reinterpret_cast<const uint4*>(Kh + (int64_t)(p < 0 ? 0 : p) * Ppad);
+  uint4* dst = reinterpret_cast<uint4*>(Kg + s * Ppad);
+  for (int64_t i = threadIdx.x; i < n16; i += blockDim.x)
+    dst[i] = p < 0 ? make_uint4(0, 0, 0, 0) : src[i];
+}
+
+// KgT[j][slot] = Kh[pattern of slot][j] for j < Ppad, slot < S (zero for the
+// padding slots): 32 x 32 tiles transposed through shared memory.
+__global__ void gather_transpose_kernel(const __half* Kh, int64_t Ppad, const int32_t* slot_pat,
+                                        int64_t S, int64_t ldT, __half* KgT) {
+  __shared__ __half tile[32][33];
+  const int64_t j0 = (int64_t)blockIdx.x * 32, s0 = (int64_t)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t s = s0 + i, j = j0 + tx;
+    const int p = s < S ? slot_pat[s] : -1;
+    tile[i][tx] = (p >= 0 && j < Ppad) ? Kh[(int64_t)p * Ppad + j] : __float2half_rn(0.0f);
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t j = j0 + i, s = s0 + tx;
+    if (j < Ppad && s < S) KgT[j * ldT + s] = tile[tx][i];
+  }
+}
+
+// The grouped compress operand: A[r][q] = P / (T_r phi) of rotation r and the
+// q-th slot of its cell as FP16 hi + lo, zero from the cell's slot count up to
+// the next multiple of 64 (the contraction's k-blocks), and zero rows for
+// rotations with T_r <= 1e-10.  One block per rotation.
+__global__ void p_split_kernel(const GroupArgs g, const int32_t* cell_of, const float* T,
+                               int64_t ldA, __half* Ahi, __half* Alo) {
+  const int64_t r = blockIdx.x;
+  const int c = cell_of[r];
+  const int32_t gc = g.gcnt[c];
+  if (gc == 0) return;
+  const int64_t k = r - g.mbeg[c];
+  const float Tr = T[r];
+  const float inv = Tr > 1e-10f ? 1.0f / Tr : 0.0f;
+  const int32_t width = (gc + 63) / 64 * 64;
+  const float* src = g.Pt + g.goff[c] + k * gc;
+  for (int32_t q = threadIdx.x; q < width; q += blockDim.x) {
+    const float v = q < gc ? src[q] * inv : 0.0f;
+    const __half hi = __float2half_rn(v);
+    Ahi[r * ldA + q] = hi;
+    Alo[r * ldA + q] = __float2half_rn(v - __half2float(hi));
+  }
+}
+
 inline unsigned blocks_for(int64_t n) {
   const int64_t b = (n + 255) / 256;
   return (unsigned)(b < 8192 ? (b > 0 ? b : 1) : 8192);
@@ -360,6 +416,28 @@ cudaError_t launch_group_maximize(const GroupArgs& g, int64_t n_mtiles, cudaStre
     if (e != cudaSuccess) return e;
   }
   group_softmax_kernel<<<(unsigned)((g.N + 7) / 8), 256, 0, st>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_softmax(const GroupArgs& g, cudaStream_t st) {
+  group_softmax_kernel<<<(unsigned)((g.N + 7) / 8), 256, 0, st>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* slot_pat, int64_t S,
+                                __half* Kg, int64_t ldT, __half* KgT, cudaStream_t st) {
+  if (S == 0) return cudaSuccess;
+  if (Kg) gather_rows_kernel<<<(unsigned)S, 256, 0, st>>>(Kh, Ppad, slot_pat, S, Kg);
+  if (KgT) {
+    dim3 grid((unsigned)((Ppad + 31) / 32), (unsigned)((S + 31) / 32));
+    gather_transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(Kh, Ppad, slot_pat, S, ldT, KgT);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p_split(const GroupArgs& g, const int32_t* cell_of, int64_t R, const float* T,
+                           int64_t ldA, __half* Ahi, __half* Alo, cudaStream_t st) {
+  p_split_kernel<<<(unsigned)R, 128, 0, st>>>(g, cell_of, T, ldA, Ahi, Alo);
   return cudaGetLastError();
 }
 

@@ -24,6 +24,10 @@ constexpr int kCompressBK = 64;
 
 bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
                   uint32_t box_rows, uint32_t box_inner);
+// The same for a matrix whose rows are ld >= inner elements apart (reads past
+// `inner` are zero-filled).
+bool tc_encode_2d_strided(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
+                          uint64_t ld, uint32_t box_rows, uint32_t box_inner);
 
 // Maximize contraction: acc[p][r] = sum_j K[p][j] (B_hi[r][j] + B_lo[r][j]),
 // 128 patterns x 256 rotations per tile.  Epilogue writes Y[r][p] (LL for
@@ -64,6 +68,55 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
                                const CUtensorMap& tmKt, int64_t Rpad, int64_t Ppad,
                                int64_t Npad, const CmpEpiArgs& e, TcStatus* status, int num_sms,
                                cudaStream_t st);
+
+// Tile of a grouped contraction (learned proposal): TMA origins of the two
+// operands (row, k offset), its k-block count, and the group (cell) with the
+// tile's first row inside the group.
+struct TileDesc {
+  int32_t a_row, a_k0, b_row, b_k0;
+  int32_t k_blocks, cell, local0, pad;
+};
+
+// Grouped maximize: acc[slot][member] = sum_j Kg[slot][j] (B_hi + B_lo)[mbeg_c + member][j]
+// over the selected cells; 128 slots x 256 members per tile (a cell has at
+// most 256 members).  Writes Y[slot][member] (poisson LL, gaussian C).
+struct GMaxEpiArgs {
+  const TileDesc* tiles;
+  const int32_t* mcnt;     // [n_cells] members per cell
+  const int32_t* gcnt;     // [n_cells] slots (pairs) per cell
+  const int32_t* gpair;    // [slots] pattern of each slot
+  int poisson;
+  const float* scaling;    // [N] phi used for LL
+  const double* rowstat;   // [R] poisson: sum W_r
+  float* Y;                // [slots][ldY]
+  int64_t ldY;
+};
+cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap& tmBhi,
+                                     const CUtensorMap& tmBlo, int64_t n_tiles,
+                                     const GMaxEpiArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st);
+
+// Grouped compress: acc[member][j] = sum_q A[mbeg_c + member][q] KgT[j][slot0_c + q]
+// with A = P / (T_r phi) as FP16 hi + lo (zero beyond the cell's slots);
+// 128 members x 256 pixels per tile, inserted in the epilogue.
+struct GCmpEpiArgs {
+  const TileDesc* tiles;
+  const int32_t* mcnt;
+  int64_t npa;
+  int side, interp;
+  const float* quat;
+  const float* rotw;
+  const float* T;
+  const float* cx;
+  const float* cy;
+  const float* cz;
+  const int32_t* ins;
+  float2* acc;
+};
+cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap& tmAlo,
+                                     const CUtensorMap& tmKgT, int64_t n_tiles,
+                                     const GCmpEpiArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st);
 
 // Responsibility pass of the mixed path: combine the tile partials per
 // pattern (lse, new scaling, sum P log P), then two sweeps over Y: row sums
