@@ -6,9 +6,16 @@ over every pattern and rotation of the workload, inputs resident in HBM.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Default workload: 64^3 model, 64x64 detector with a radius-4 beamstop (4044
-active pixels), 25,680 rotations (600-cell n=8, halved), 10,000 seeded
-synthetic Poisson patterns (mean 2000 photons, lognormal scale sigma 0.5).
+Default workload: 128^3 model, 128x128 detector with a radius-6 beamstop
+(16,272 active pixels), 86,520 rotations (600-cell n=12, halved), 50,000
+seeded synthetic Poisson patterns (mean 500 photons, ~3% non-zero pixels,
+lognormal scale sigma 0.5).  The headline is the dense mixed-precision
+iteration (every pattern x rotation pair evaluated); beside it the line
+reports the plain FP32 iteration, the learned orientation proposal (top
+cells of a BF16 network's coarse posterior, the dense iteration as
+fallback) with its captured responsibility mass and model error, the error
+of the mixed path against the FP64 oracle on a sample, and the oracle's CPU
+rate on that sample.
 Multi-GPU (torchrun): patterns are sharded across ranks (each rank holds its
 own N patterns of one seeded dataset: weak scaling) and every iteration sums
 the model/weight insertion accumulators with one NCCL all-reduce before
@@ -34,18 +41,19 @@ sys.path.insert(0, REPO)
 METRIC = "pattern×rotation evals/s"
 UNIT = "evals/s"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
-# DRAM bytes per launch of the maximize contraction on the default workload,
-# from the ncu capture summarised in profiles/ (None until captured).
-MAXIMIZE_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) per launch of the maximize contraction on the
+# default workload (128^3, 86,520 rotations, 50,000 patterns), from the ncu
+# capture summarised in profiles/tc_gemm_dram_large128.md.
+MAXIMIZE_TRAFFIC_BYTES = 709_666_040_320 + 17_586_104_576
 
 
 def parse():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="b200_64")
+    ap.add_argument("--workload", default="large128")
     ap.add_argument("--patterns", type=int, default=None, help="override the pattern count")
     ap.add_argument("--likelihood", default="poisson", choices=["poisson", "gauss"])
     ap.add_argument("--interp", default="nearest", choices=["nearest", "trilinear"])
@@ -54,6 +62,11 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-steps", type=int, default=10)
+    ap.add_argument("--train-iters", type=int, default=5,
+                    help="dense iterations whose responsibilities train the proposal network")
+    ap.add_argument("--train-epochs", type=int, default=12)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -120,27 +133,43 @@ class ClockSampler:
 
 # ------------------------------------------------------------ CPU baseline --
 
-def cpu_oracle_rate(d, likelihood, interp, seconds, want_resp_rows=None):
+def sample_indices(d, max_rotations=2048):
+    """An evenly strided subset of the rotations (every k-th): the CPU sample
+    and the oracle parity sample of large workloads."""
+    R = d["q"].shape[0]
+    k = max(1, -(-R // max_rotations))
+    return np.arange(0, R, k)
+
+
+def cpu_oracle_rate(d, likelihood, interp, seconds, rot=None):
     """FP64 C++/OpenMP oracle (oracle/) on a bounded sample of the workload:
-    every rotation, the first n patterns.  Returns (evals/s, sample text, P)."""
+    the rotations `rot` (default: an evenly strided subset of at most 2048) and
+    the first n patterns, n sized for about `seconds` of CPU work.  Returns
+    (evals/s, sample text, oracle output (model, scaling, P, stats), n, rot)."""
     from oracle import oracle as O
     w = d["workload"]
-    R = d["q"].shape[0]
+    rot = sample_indices(d) if rot is None else rot
+    r = len(rot)
 
     def run(n):
-        cfg = O.make_config(w.side, n, R, likelihood=O.LL_POISSON if likelihood == "poisson"
+        cfg = O.make_config(w.side, n, r, likelihood=O.LL_POISSON if likelihood == "poisson"
                             else O.LL_GAUSS, interp=O.NEAREST if interp == "nearest"
                             else O.TRILINEAR)
         t = time.perf_counter()
-        _, _, P, _ = O.iterate(cfg, d["counts"][:n], d["mask"], d["q"], d["w"], d["x"], d["y"],
-                               d["z"], d["model0"], d["scaling0"][:n], want_resp=True)
-        return time.perf_counter() - t, P
+        out = O.iterate(cfg, d["counts"][:n], d["mask"], d["q"][rot], d["w"][rot], d["x"],
+                        d["y"], d["z"], d["model0"], d["scaling0"][:n], want_resp=True)
+        return time.perf_counter() - t, out
 
     t8, _ = run(8)
-    n = int(max(8, min(d["counts"].shape[0], 8 * seconds / max(t8, 1e-3) * 0.8)))
+    t64, _ = run(64) if t8 < seconds / 8 else (None, None)
+    # per-pattern cost from two sizes (the fixed expand / insert cost cancels)
+    per = (t64 - t8) / 56 if t64 is not None and t64 > t8 else t8 / 8
+    n = int(max(8, min(d["counts"].shape[0], (seconds - t8) / max(per, 1e-4))))
     n = max(8, (n // 8) * 8)
-    t, P = run(n)
-    return n * R / t, f"1 FP64 iteration, {n} patterns x {R} rotations ({t:.1f} s)", P, n
+    t, out = run(n)
+    R = d["q"].shape[0]
+    return (n * r / t, f"1 FP64 iteration, {n} patterns x {r} rotations (every "
+            f"{-(-R // r)}th of {R}; {t:.1f} s)", out, n, rot)
 
 
 def cores():
@@ -165,9 +194,9 @@ def reference_arm(a):
     for _ in range(max(0, min(a.warmup, 1))):
         cpu_oracle_rate(d, a.likelihood, a.interp, 2.0)
     rates, samples = [], []
-    per = max(2.0, 60.0 / max(1, a.steps))
+    per = max(2.0, 90.0 / max(1, a.steps))
     for _ in range(a.steps):
-        r, s, _, _ = cpu_oracle_rate(d, a.likelihood, a.interp, per)
+        r, s, _, _, _ = cpu_oracle_rate(d, a.likelihood, a.interp, per)
         rates.append(r)
         samples.append(s)
     v = statistics.median(rates)
@@ -194,6 +223,123 @@ def config_desc(a, d):
                         f"{a.likelihood} likelihood, {a.interp} interpolation",
             "precision": a.precision, "patterns": N, "rotations": R, "active_pixels": npa,
             "l2": "inputs larger than L2 (responsibility matrix and slice operands > 126 MB)"}
+
+
+# ------------------------------------------------------- learned proposal --
+
+def learned_proposal(a, E, W, d, device, dense_ms):
+    """The learned orientation proposal on the same data: rotations sorted by
+    their coarse cell (the 420 rotations of the n=2 sampling), --train-iters
+    dense iterations whose responsibilities train the BF16 network, then
+    --learned-steps proposed iterations.  Each proposed iteration selects, per
+    pattern, the cells of the blended posterior (network prediction and the
+    previous iteration's cell responsibilities) up to a predicted mass of
+    0.999 (at most 16 cells); the dense iteration runs instead when the mean
+    predicted mass falls below 0.99."""
+    import torch
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    w = d["workload"]
+    q, wt, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=2)
+    N, R = d["counts"].shape[0], q.shape[0]
+    ctx = E.Context(w.side, N, R, likelihood=a.likelihood, interp=a.interp, precision="mixed",
+                    device=device)
+    ctx.set_geometry(d["x"], d["y"], d["z"], d["mask"])
+    ctx.set_rotations(q, wt)
+    ctx.set_patterns(d["counts"])
+    ctx.set_model(d["model0"])
+    ctx.set_scaling(d["scaling0"])
+    for _ in range(a.train_iters):
+        ctx.iterate(stats=False)
+    lp = LearnedProposal(ctx, cell, n_cells, bf16=True, seed=1)
+    t0 = time.perf_counter()
+    x, t_dense = lp.features(), lp.targets()
+    losses = lp.train(x, t_dense, epochs=a.train_epochs, batch=256, lr=2e-3)
+    probs = lp.predict(x)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    max_cells, target, threshold = 16, 0.999, 0.99
+
+    # accuracy of one proposed iteration against the dense iteration from the
+    # same state, and the true responsibility mass its candidate cells hold
+    m0, s0 = ctx.get_model(), ctx.get_scaling()
+    ctx.iterate(stats=False)
+    m_dense, w_dense = ctx.get_model(), ctx.get_buffer(E.BUF_WEIGHT).copy()
+    t_next = lp.targets()
+    ctx.set_model(m0)
+    ctx.set_scaling(s0)
+    sel_probs = LearnedProposal.blend(probs, t_dense)
+    st = lp.iterate(sel_probs, max_cells, target, threshold)
+    m_prop = ctx.get_model()
+    srt = torch.sort(sel_probs, dim=1, descending=True)
+    k = torch.clamp((torch.cumsum(srt.values, 1) < target).sum(1) + 1, max=max_cells)
+    keep = torch.arange(n_cells, device=sel_probs.device)[None, :] < k[:, None]
+    captured = (torch.gather(t_next, 1, srt.indices) * keep).sum(1)
+    heavy = w_dense > np.quantile(w_dense[w_dense > 0], 0.1)
+    acc = {"captured_mass_mean": float(captured.mean()), "captured_mass_min": float(captured.min()),
+           "patterns_below_0.99": float((captured < 0.99).float().mean()),
+           "model_rel_err_vs_dense": float(np.linalg.norm(m_prop - m_dense) /
+                                           np.linalg.norm(m_dense)),
+           "model_rel_err_vs_dense_weight_gt_p10": float(
+               np.linalg.norm((m_prop - m_dense)[heavy]) / np.linalg.norm(m_dense[heavy])),
+           "predicted_mass_mean": st["mean_mass"]}
+    untrained = LearnedProposal(ctx, cell, n_cells, bf16=True, seed=2).predict(x)
+    srt_u = torch.sort(untrained, dim=1, descending=True)
+    ku = torch.clamp((torch.cumsum(srt_u.values, 1) < target).sum(1) + 1, max=max_cells)
+    keep_u = torch.arange(n_cells, device=x.device)[None, :] < ku[:, None]
+    acc["untrained_network_captured_mass_mean"] = float(
+        (torch.gather(t_next, 1, srt_u.indices) * keep_u).sum(1).mean())
+
+    # timed: proposed iterations, each selecting from the blend of the network
+    # and the previous iteration's cell responsibilities
+    ctx.set_model(m0)
+    ctx.set_scaling(s0)
+    prev = t_dense
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    for _ in range(2):
+        lp.iterate(LearnedProposal.blend(probs, prev), max_cells, target, threshold)
+        prev = lp.targets()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(ext):
+        e0.record()
+    evals = fallbacks = 0
+    t0 = time.perf_counter()
+    for _ in range(a.learned_steps):
+        st = lp.iterate(LearnedProposal.blend(probs, prev), max_cells, target, threshold)
+        prev = lp.targets()
+        evals += st["evaluations"]
+        fallbacks += st["fallback"]
+    with torch.cuda.stream(ext):
+        e1.record()
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / a.learned_steps
+    ms = e0.elapsed_time(e1) / a.learned_steps
+    ctx.set_profiling(True)
+    stage = np.zeros(5)
+    for i in range(3):
+        lp.iterate(LearnedProposal.blend(probs, prev), max_cells, target, threshold)
+        if i >= 1:
+            stage += ctx.stage_times()
+    ctx.set_profiling(False)
+    ctx.close()
+    lp.net.close()
+    return {
+        "ms_per_step": ms, "s_per_iter": ms / 1e3, "wall_ms_per_step": wall * 1e3,
+        "value_dense_equivalent": N * R / (ms / 1e3),
+        "value_evaluated": evals / a.learned_steps / (ms / 1e3),
+        "unit": UNIT, "evaluated_fraction": evals / a.learned_steps / (N * R),
+        "fallback_iterations": fallbacks, "speedup_vs_dense_mixed": dense_ms / ms,
+        "stages_ms": dict(zip(["expand_select_gather", "grouped_maximize", "softmax_split",
+                               "grouped_compress_insert", "normalise"],
+                              [round(float(v) / 2, 3) for v in stage])),
+        "accuracy": acc,
+        "selection": f"per pattern, cells of the blended posterior up to predicted mass {target} "
+                     f"(at most {max_cells} of {n_cells}); dense fallback below mean mass {threshold}",
+        "network": "BF16 CNN: 3 conv 3x3 stride 2 (16/32/64) + FC -> 420-way softmax on "
+                   f"{w.side // 2}^2 log(1+K) (2x2 binned); trained {a.train_epochs} epochs on "
+                   f"the responsibilities of {a.train_iters} dense iterations "
+                   f"({train_s:.1f} s incl. features, loss {losses[0]:.3f} -> {losses[-1]:.4f})",
+    }
 
 
 # ------------------------------------------------------------------ ours --
@@ -291,7 +437,8 @@ def main():
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if achieved else None,
             "peak_kind": f"{pk_kind} bf16 dense, sustained",
-            "traffic": MAXIMIZE_TRAFFIC_BYTES,
+            "traffic": MAXIMIZE_TRAFFIC_BYTES if a.workload == "large128" and N == 50_000
+            and a.precision == "mixed" else None,
             "algorithmic_flops_per_launch": flops,
             "launch_ms": gemm_ms}
     stages = dict(zip(["expand", "maximize_contraction", "responsibility_pass", "compress_insert",
@@ -354,33 +501,54 @@ def main():
                "host_ms": dict(zip(["set_patterns", "enqueue_iteration", "get_model",
                                     "get_scaling"], [round(x * 1e3 / steps_e, 3) for x in parts]))}
 
-    # responsibility error of this path vs the FP64 oracle on a sample, and the CPU baseline
+    ctx.close()
+
+    # The error of this path against the FP64 oracle on a sample (the oracle
+    # cannot run the full workload in seconds): the same patterns and an
+    # evenly strided subset of the rotations through a context of that size;
+    # the oracle's time on it is the CPU baseline.
     cpu = None
     err = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        ctx.set_model(d["model0"])
-        ctx.set_scaling(d["scaling0"])
-        ctx.set_patterns(d["counts"])
-        ctx.expand()
-        ctx.maximize()
-        P = ctx.get_buffer(E.BUF_RESP)
-        rate, sample, P_ref, n = cpu_oracle_rate(d, a.likelihood, a.interp, a.cpu_seconds)
+        rate, sample, (m_ref, s_ref, P_ref, _), n, rot = cpu_oracle_rate(
+            d, a.likelihood, a.interp, a.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": cores(), "kind": "port",
                "sample": sample + " (C++/OpenMP FP64 oracle)"}
-        diff = np.abs(P[:, :n].astype(np.float64) - P_ref).sum(0)
+        sub = E.Context(wl.side, n, len(rot), likelihood=a.likelihood, interp=a.interp,
+                        precision=a.precision, device=local)
+        sub.set_geometry(d["x"], d["y"], d["z"], d["mask"])
+        sub.set_rotations(d["q"][rot], d["w"][rot])
+        sub.set_patterns(d["counts"][:n])
+        sub.set_model(d["model0"])
+        sub.set_scaling(d["scaling0"][:n])
+        sub.expand()
+        sub.maximize()
+        P = sub.get_buffer(E.BUF_RESP)
+        sub.compress()
+        m_sub = sub.get_model()
+        sub.close()
+        diff = np.abs(P.astype(np.float64) - P_ref).sum(0)
         err = {"resp_l1_max": float(diff.max()), "resp_l1_mean": float(diff.mean()),
-               "sample_patterns": n, "vs": "FP64 oracle, same model and scaling"}
-        ctx.compress()
-    ctx.close()
+               "model_rel_err": float(np.linalg.norm(m_sub - m_ref) / np.linalg.norm(m_ref)),
+               "sample": f"{n} patterns x {len(rot)} rotations (every {-(-R // len(rot))}th), "
+                         "one iteration from the same model and scaling",
+               "vs": "FP64 oracle"}
+
+    learned = None
+    if rank == 0 and world == 1 and not a.no_learned and a.precision == "mixed":
+        learned = learned_proposal(a, E, W, d, local, ms_step)
 
     fp32 = None
-    if not a.no_fp32 and a.precision == "mixed":
+    if rank == 0 and world == 1 and not a.no_fp32 and a.precision == "mixed":
         c32 = make_ctx("fp32")
         ms32, st32, _ = timed(c32, a.fp32_steps, 1)
         c32.close()
         fp32 = {"value": N * R * world / (ms32 / 1e3), "ms_per_step": ms32,
+                "s_per_iter": ms32 / 1e3,
                 "stages_ms": [round(float(x), 3) for x in st32],
                 "speedup_of_mixed": ms32 / ms_step}
+        if learned:
+            learned["speedup_vs_plain_fp32"] = ms32 / learned["ms_per_step"]
 
     if dist:
         dist.barrier()
@@ -395,7 +563,8 @@ def main():
         "data": "synthetic (seeded point-scatterer model, Poisson patterns)",
         "config": config_desc(a, d),
         "stages_ms": stages, "roofline": roof, "cpu_baseline": cpu, "error": err,
-        "plain_fp32": fp32, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        "plain_fp32": fp32, "learned_proposal": learned, "e2e": e2e, "clocks": clk,
+        "gpu_launches": launches,
     }
     print(json.dumps(line))
     return 0

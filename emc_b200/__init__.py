@@ -46,6 +46,10 @@ class IterStats(C.Structure):
                 ("model_max", C.c_double), ("total_resp", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("maximize_raster", C.c_int32), ("compress_raster", C.c_int32)]
+
+
 class SynthConfig(C.Structure):
     _fields_ = [("side", C.c_int32), ("n_scatterers", C.c_int32), ("object_radius", C.c_double),
                 ("n_patterns", C.c_int64), ("mean_photons", C.c_double),
@@ -86,6 +90,8 @@ def lib():
             ("emc_launch_count", [P], I64),
             ("emc_compress_insert", [P], C.c_int), ("emc_normalize", [P], C.c_int),
             ("emc_partial_stats", [P, P, P], C.c_int),
+            ("emc_get_tuning", [P, P], C.c_int), ("emc_set_tuning", [P, P], C.c_int),
+            ("emc_autotune", [P, P, C.c_int32, P, P], C.c_int),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -302,6 +308,24 @@ class Context:
     @property
     def launch_count(self):
         return int(lib().emc_launch_count(self._h))
+
+    def get_tuning(self):
+        """(maximize_raster, compress_raster) of the tensor-core tile orders."""
+        t = Tuning()
+        self._c(lib().emc_get_tuning(self._h, C.byref(t)))
+        return t.maximize_raster, t.compress_raster
+
+    def set_tuning(self, maximize_raster, compress_raster):
+        t = Tuning(maximize_raster, compress_raster)
+        self._c(lib().emc_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, candidates=(1, 2, 4, 8, 16)):
+        """emc_autotune: returns (best (maximize, compress), ms[2][n])."""
+        cand = np.ascontiguousarray(candidates, np.int32)
+        ms = np.zeros((2, len(cand)), np.float32)
+        t = Tuning()
+        self._c(lib().emc_autotune(self._h, _ptr(cand), len(cand), _ptr(ms), C.byref(t)))
+        return (t.maximize_raster, t.compress_raster), ms
 
     def device_buffer(self, which):
         p, n = C.c_void_p(), C.c_size_t()

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1,
                    const __grid_constant__ CUtensorMap tmB0, const __grid_constant__ CUtensorMap tmB1,
                    const int64_t m_tiles, const int64_t n_tiles, const int64_t k_blocks,
-                   const Epi epi, TcStatus* status) {
+                   const int raster, const Epi epi, TcStatus* status) {
   static_assert(NA * NB == 2, "one hi/lo split per contraction");
   constexpr uint32_t A_BYTES = BM * BK * 2;
   constexpr uint32_t B_BYTES = BN * BK * 2;
@@ -191,13 +191,26 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = tmem_slot;
   const int64_t num_tiles = m_tiles * n_tiles;
 
+  // Tile order.  The inner index (m for M_INNER, else n) runs fastest, in
+  // bands of `raster` outer tiles: the CTAs in flight then cover about
+  // gridDim / raster inner tiles x raster outer tiles, so each operand tile
+  // they load from HBM is shared through L2 by several of them (the K extent
+  // is long, so the panels themselves do not stay in L2).
   auto tile_mn = [&](int64_t t, int64_t& m, int64_t& n) {
+    const int64_t inner = M_INNER ? m_tiles : n_tiles;
+    const int64_t outer = M_INNER ? n_tiles : m_tiles;
+    const int64_t span = (int64_t)raster * inner;
+    const int64_t band = t / span;
+    const int64_t o0 = band * raster;
+    const int64_t g = outer - o0 < raster ? outer - o0 : raster;
+    const int64_t w = t - band * span;
+    const int64_t o = o0 + w % g, i = w / g;
     if (M_INNER) {
-      n = t / m_tiles;
-      m = t - n * m_tiles;
+      m = i;
+      n = o;
     } else {
-      m = t / n_tiles;
-      n = t - m * n_tiles;
+      m = o;
+      n = i;
     }
   };
   // TMA origins (row and k offset of each operand) and k-block count of tile
@@ -671,7 +684,9 @@ struct EpiGCmp {
 template <int NA, int NB, int STAGES, bool M_INNER, int BK, class Epi>
 cudaError_t run_gemm(const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
                      const CUtensorMap& b1, int64_t m_tiles, int64_t n_tiles, int64_t k_blocks,
-                     const Epi& epi, TcStatus* st, int num_sms, cudaStream_t stream) {
+                     const Epi& epi, TcStatus* st, int num_sms, cudaStream_t stream,
+                     int raster = 1) {
+  if (raster < 1) raster = 1;
   constexpr uint32_t stage = NA * BM * BK * 2 + NB * BN * BK * 2;
   const size_t dyn = (size_t)STAGES * stage + 1024;
   auto kern = tc_gemm_kernel<NA, NB, STAGES, M_INNER, BK, Epi>;
@@ -680,7 +695,8 @@ cudaError_t run_gemm(const CUtensorMap& a0, const CUtensorMap& a1, const CUtenso
   const int64_t tiles = m_tiles * n_tiles;
   if (tiles == 0) return cudaSuccess;
   const int grid = (int)(tiles < num_sms ? tiles : num_sms);
-  kern<<<grid, kThreads, dyn, stream>>>(a0, a1, b0, b1, m_tiles, n_tiles, k_blocks, epi, st);
+  kern<<<grid, kThreads, dyn, stream>>>(a0, a1, b0, b1, m_tiles, n_tiles, k_blocks, raster, epi,
+                                        st);
   return cudaGetLastError();
 }
 
@@ -966,7 +982,7 @@ bool tc_encode_2d_strided(CUtensorMap* tm, const void* base, uint64_t inner, uin
 cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
                                const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
                                int64_t Kpad, const MaxEpiArgs& e, TcStatus* status, int num_sms,
-                               cudaStream_t st) {
+                               cudaStream_t st, int raster) {
   EpiMax epi;
   epi.a = e;
   // rows = patterns (counts, 8 KB per stage), columns = rotations (hi and lo,
@@ -974,18 +990,20 @@ cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
   // each rotation tile in L2.  K-steps of 32 (64-byte rows) keep five 40 KB
   // stages in flight.
   return run_gemm<1, 2, 5, true, kMaximizeBK>(tmK, tmK, tmBhi, tmBlo, Mpad / BM, Rpad / BN,
-                                              Kpad / kMaximizeBK, epi, status, num_sms, st);
+                                              Kpad / kMaximizeBK, epi, status, num_sms, st,
+                                              raster);
 }
 
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
                                const CUtensorMap& tmKt, int64_t Rpad, int64_t Ppad, int64_t Npad,
                                const CmpEpiArgs& e, TcStatus* status, int num_sms,
-                               cudaStream_t st) {
+                               cudaStream_t st, int raster) {
   EpiCmp epi;
   epi.a = e;
   // pixel tiles are the inner index: CTAs in flight share the P' tiles
   return run_gemm<2, 1, 3, false, kCompressBK>(tmPhi, tmPlo, tmKt, tmKt, Rpad / BM, Ppad / BN,
-                                               Npad / kCompressBK, epi, status, num_sms, st);
+                                               Npad / kCompressBK, epi, status, num_sms, st,
+                                               raster);
 }
 
 cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap& tmBhi,

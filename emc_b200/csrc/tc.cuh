@@ -43,10 +43,11 @@ struct MaxEpiArgs {
   float* Y;                // [R][ldY]
   float4* part;            // [Rpad/256][N]
 };
+// raster: rotation tiles per band of the tile order (see kernels_tc.cu).
 cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
                                const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
                                int64_t Kpad, const MaxEpiArgs& e, TcStatus* status,
-                               int num_sms, cudaStream_t st);
+                               int num_sms, cudaStream_t st, int raster);
 
 // Compress contraction: acc[r][j] = sum_p (P'_hi + P'_lo)[r][p] Kt[j][p] with
 // P' = c0 P / (T_r phi_p), i.e. the averaged slice U_r / T_r; 128 rotations x
@@ -64,10 +65,11 @@ struct CmpEpiArgs {
   const int32_t* ins;      // [npa] insert flag (mask == 1)
   float2* acc;             // [side^3] interleaved (model, weight) accumulators
 };
+// raster: rotation tiles per band of the tile order.
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
                                const CUtensorMap& tmKt, int64_t Rpad, int64_t Ppad,
                                int64_t Npad, const CmpEpiArgs& e, TcStatus* status, int num_sms,
-                               cudaStream_t st);
+                               cudaStream_t st, int raster);
 
 // Tile of a grouped contraction (learned proposal): TMA origins of the two
 // operands (row, k offset), its k-block count, and the group (cell) with the

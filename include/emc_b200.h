@@ -128,6 +128,22 @@ void *emc_stream(emc_context *ctx);
 /* Number of active (mask != 0) pixels. */
 int64_t emc_active_pixels(const emc_context *ctx);
 
+/* Tile order of the two tensor-core contractions (mixed precision): the
+ * persistent CTAs walk the output tiles in bands of `raster` rotation tiles,
+ * the other index fastest, so operand tiles loaded from HBM are shared
+ * through L2 by the CTAs in flight.  1 = plain row order. */
+typedef struct {
+  int32_t maximize_raster, compress_raster;
+} emc_tuning;
+emc_status emc_get_tuning(const emc_context *ctx, emc_tuning *t);
+emc_status emc_set_tuning(emc_context *ctx, const emc_tuning *t);
+/* Autotuner: one iteration per candidate band size (both contractions at
+ * once, timed by stage events) from the current model and scaling, which are
+ * restored afterwards; keeps the fastest candidate of each contraction.
+ * ms (optional): [2][n], maximize then compress times.  FP32 contexts: no-op. */
+emc_status emc_autotune(emc_context *ctx, const int32_t *candidates, int32_t n, float *ms,
+                        emc_tuning *best);
+
 /* ---- learned rotation proposal ----
  * Fine rotations are grouped into coarse cells (e.g. the nearest rotation of
  * the 420-rotation 600-cell sampling); the rotation list given to

@@ -155,3 +155,24 @@ def test_accumulator_view_and_split_compress(tiny, prec):
         torch.cuda.synchronize()
         np.testing.assert_allclose(model, a.get_model(), rtol=1e-6, atol=1e-6)
         np.testing.assert_allclose(model, expect, rtol=1e-5, atol=1e-6)
+
+
+def test_autotune_keeps_results_and_restores_state(tiny):
+    """emc_autotune times candidate tile orders from the current state and
+    restores it; the tile order changes no result."""
+    d = tiny
+    with make_ctx(d, "poisson", "nearest", "mixed") as ctx:
+        m0 = ctx.get_model()
+        best, ms = ctx.autotune((1, 2, 4))
+        assert ms.shape == (2, 3) and np.all(ms > 0)
+        assert best[0] in (1, 2, 4) and best[1] in (1, 2, 4)
+        np.testing.assert_array_equal(ctx.get_model(), m0)
+        ctx.set_tuning(1, 1)
+        ctx.iterate()
+        m1 = ctx.get_model()
+        ctx.set_model(m0)
+        ctx.set_scaling(d["scaling0"])
+        ctx.set_tuning(3, 5)
+        assert ctx.get_tuning() == (3, 5)
+        ctx.iterate()
+        assert rel(ctx.get_model(), m1) < 1e-6
