@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="large128")
     ap.add_argument("--patterns", type=int, default=None, help="override the pattern count")
+    ap.add_argument("--rot-n", type=int, default=None,
+                    help="override the 600-cell refinement of the rotation sampling")
     ap.add_argument("--likelihood", default="poisson", choices=["poisson", "gauss"])
     ap.add_argument("--interp", default="nearest", choices=["nearest", "trilinear"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
@@ -188,7 +190,7 @@ def reference_arm(a):
     from emc_b200 import workloads as W
     from oracle import oracle as O
     O.build() if not os.path.isfile(O.LIB_PATH) else None
-    d = W.make(a.workload, n_patterns=a.patterns)
+    d = W.make(workload_of(a))
     w = d["workload"]
     N, R = d["counts"].shape[0], d["q"].shape[0]
     for _ in range(max(0, min(a.warmup, 1))):
@@ -212,6 +214,14 @@ def reference_arm(a):
     }
     print(json.dumps(line))
     return 0
+
+
+def workload_of(a):
+    """The named workload with the --patterns / --rot-n overrides."""
+    from emc_b200 import workloads as W
+    w0 = W.WORKLOADS[a.workload]
+    return W.Workload(w0.name, w0.side, a.rot_n or w0.rot_n, a.patterns or w0.n_patterns,
+                      w0.mean_photons, w0.scale_sigma, w0.beamstop, w0.iterations, seed=w0.seed)
 
 
 def config_desc(a, d):
@@ -361,9 +371,7 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    w0 = W.WORKLOADS[a.workload]
-    wl = W.Workload(w0.name, w0.side, w0.rot_n, a.patterns or w0.n_patterns, w0.mean_photons,
-                    w0.scale_sigma, w0.beamstop, w0.iterations, seed=w0.seed)
+    wl = workload_of(a)
     d = W.make(wl, first_pattern=rank * wl.n_patterns)  # this rank's shard of one dataset
     N, R = d["counts"].shape[0], d["q"].shape[0]
     npa = int((d["mask"] != 0).sum())
