@@ -91,6 +91,11 @@ def lib():
             ("emc_compress_insert", [P], C.c_int), ("emc_normalize", [P], C.c_int),
             ("emc_partial_stats", [P, P, P], C.c_int),
             ("emc_get_tuning", [P, P], C.c_int), ("emc_set_tuning", [P, P], C.c_int),
+            ("emc_orientation_stats", [P, P, P, P], C.c_int),
+            ("emc_model_random_orientations", [C.c_int, I64, P, P, P, P, P, C.c_uint64, P, P],
+             C.c_int),
+            ("emc_model_load", [C.c_char_p, C.c_int, P], C.c_int),
+            ("emc_model_save", [C.c_char_p, C.c_int, P], C.c_int),
             ("emc_autotune", [P, P, C.c_int32, P, P], C.c_int),
         ]:
             f = getattr(L, name)
@@ -130,6 +135,32 @@ def detector_coordinates(side, wavelength, pixel_size, detector_distance):
     lib().emc_detector_coordinates(side, wavelength, pixel_size, detector_distance, _ptr(x), _ptr(y),
                                    _ptr(z))
     return x, y, z
+
+
+def model_random_orientations(side, images, mask, x, y, z, seed=0, return_rotations=False):
+    """emc_model_random_orientations: every image inserted with weight 1 at a
+    uniformly random rotation, model = sum / weight (emc.c:896-914)."""
+    imgs = np.ascontiguousarray(images, np.float32).reshape(-1, side * side)
+    model = np.zeros(side ** 3, np.float32)
+    quat = np.zeros((imgs.shape[0], 4), np.float32)
+    _check(lib().emc_model_random_orientations(
+        side, imgs.shape[0], _ptr(imgs), _ptr(np.ascontiguousarray(mask, np.int32)),
+        _ptr(np.ascontiguousarray(x, np.float32)), _ptr(np.ascontiguousarray(y, np.float32)),
+        _ptr(np.ascontiguousarray(z, np.float32)), seed, _ptr(model), _ptr(quat)))
+    return (model, quat) if return_rotations else model
+
+
+def load_model(path, side):
+    """emc_model_load: raw float32 side^3 file, |value| (emc.c:915-925)."""
+    model = np.zeros(side ** 3, np.float32)
+    _check(lib().emc_model_load(os.fsencode(path), side, _ptr(model)))
+    return model
+
+
+def save_model(path, model, side):
+    m = np.ascontiguousarray(model, np.float32).reshape(-1)
+    assert m.size == side ** 3
+    _check(lib().emc_model_save(os.fsencode(path), side, _ptr(m)))
 
 
 def random_model(side, seed=0):
@@ -308,6 +339,14 @@ class Context:
     @property
     def launch_count(self):
         return int(lib().emc_launch_count(self._h))
+
+    def orientation_stats(self):
+        """emc_orientation_stats: dict(best_rot [N], best_resp [N], avg_resp [R])."""
+        best = np.zeros(self.N, np.int32)
+        bp = np.zeros(self.N, np.float32)
+        avg = np.zeros(self.R, np.float32)
+        self._c(lib().emc_orientation_stats(self._h, _ptr(best), _ptr(bp), _ptr(avg)))
+        return {"best_rot": best, "best_resp": bp, "avg_resp": avg}
 
     def get_tuning(self):
         """(maximize_raster, compress_raster) of the tensor-core tile orders."""

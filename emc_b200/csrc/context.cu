@@ -89,6 +89,8 @@ struct emc_context {
   int32_t n_cells = 0, cand_m = 0;
   int resp_source = 0;  // responsibilities of the last maximize: 1 dense, 2 proposed
   float* d_cmass = nullptr;
+  int32_t* d_best = nullptr;  // orientation diagnostics: most probable rotation per pattern
+  float* d_bestp = nullptr;
   int64_t max_members = 0;
   std::vector<int64_t> h_mbeg;
   std::vector<int32_t> h_mcnt;
@@ -754,6 +756,50 @@ emc_status emc_autotune(emc_context* c, const int32_t* cand, int32_t n, float* m
   return EMC_OK;
 }
 
+emc_status emc_orientation_stats(emc_context* c, int32_t* best_rot, float* best_resp,
+                                 float* avg_resp) {
+  if (!c) return EMC_ERR_ARG;
+  if (c->resp_source == 0 || c->stage == 1)
+    return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+  const int64_t N = c->N, R = c->R;
+  if (!c->d_best) {
+    TRY(c->alloc(&c->d_best, N));
+    TRY(c->alloc(&c->d_bestp, N));
+  }
+  if (c->resp_source == 1) {
+    if (!c->mixed) {
+      CK(c, launch_col_argmax(c->d_LL, R, N, c->d_best, c->d_bestp, c->st));
+    } else {
+      RespArgs a{};
+      a.N = N;
+      a.R = R;
+      a.ldY = c->Npad;
+      a.poisson = c->gauss ? 0 : 1;
+      a.Y = c->d_Y;
+      a.scaling = c->d_scaling_prev;
+      a.rowstat = c->d_rowstat;
+      a.patstat = c->d_patsq;
+      a.gauss_inv = gauss_inv(c);
+      a.lse = c->d_lse;
+      CK(c, launch_resp_argmax(a, c->d_best, c->d_bestp, c->st));
+    }
+    c->launches += 1;
+  }  // a proposed iteration recorded its best candidates itself
+  if (best_rot)
+    CK(c, cudaMemcpyAsync(best_rot, c->d_best, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, c->st));
+  if (best_resp)
+    CK(c, cudaMemcpyAsync(best_resp, c->d_bestp, sizeof(float) * N, cudaMemcpyDeviceToHost, c->st));
+  std::vector<float> T;
+  if (avg_resp) {
+    T.resize(R);
+    CK(c, cudaMemcpyAsync(T.data(), c->d_T, sizeof(float) * R, cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(c, cudaStreamSynchronize(c->st));
+  // average responsibility of each rotation over the patterns: T_r / N
+  for (int64_t r = 0; r < (avg_resp ? R : 0); ++r) avg_resp[r] = (float)((double)T[r] / (double)N);
+  return EMC_OK;
+}
+
 emc_status emc_partial_stats(emc_context* c, double* plogp, double* loglik) {
   if (!c) return EMC_ERR_ARG;
   double h[4] = {0, 0, 0, 0};
@@ -956,6 +1002,10 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     TRY(c->alloc(&c->d_lse_c, N));
     TRY(c->alloc(&c->d_plogp_c, N));
   }
+  if (!c->d_best) {
+    TRY(c->alloc(&c->d_best, N));
+    TRY(c->alloc(&c->d_bestp, N));
+  }
   if (!c->d_acc) TRY(c->alloc(&c->d_acc, c->M));
   if (pairs > c->pairs_cap || c->cand_m != m) {
     int64_t cap = c->pairs_cap;
@@ -1136,6 +1186,8 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
   g.plogp = c->d_plogp_c;
   g.new_scaling = c->d_scaling;
   g.cmass = c->d_cmass;
+  g.best_rot = c->d_best;
+  g.best_p = c->d_bestp;
   g.mtiles = c->d_mtiles;
   g.ctiles = c->d_ctiles;
   g.rotw = c->d_rotw;

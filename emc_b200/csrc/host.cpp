@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -327,6 +328,80 @@ emc_status emc_synthesize(const emc_synth_config* sc, const float* x, const floa
     if (true_scale) true_scale[p] = (float)scale;
   }
   return EMC_OK;
+}
+
+// ------------------------------------------------ model initialisation ---
+
+emc_status emc_model_random_orientations(int side, int64_t n_images, const float* images,
+                                         const int32_t* mask, const float* x, const float* y,
+                                         const float* z, uint64_t seed, float* model,
+                                         float* quat_out) {
+  // emc.c:896-914 (model_input == 1): every image inserted with weight 1 at a
+  // uniformly random rotation (Shoemake's subgroup algorithm, as
+  // quaternion_random emc.c:27-38), nearest voxel with the insertion bound,
+  // mask == 1 pixels; then model = sum / weight, 0 where no weight.
+  if (side < 2 || n_images < 0 || (n_images && !images) || !mask || !x || !y || !z || !model)
+    return EMC_ERR_ARG;
+  const int64_t npix = (int64_t)side * side, M = npix * side;
+  std::vector<double> acc(M, 0.0), wt(M, 0.0);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t p = 0; p < n_images; ++p) {
+    Stream s(seed, 0x726f7469ull, (uint64_t)p);
+    const double u1 = s.uniform(), u2 = s.uniform(), u3 = s.uniform();
+    float q[4] = {(float)(std::sqrt(1 - u1) * std::sin(2 * M_PI * u2)),
+                  (float)(std::sqrt(1 - u1) * std::cos(2 * M_PI * u2)),
+                  (float)(std::sqrt(u1) * std::sin(2 * M_PI * u3)),
+                  (float)(std::sqrt(u1) * std::cos(2 * M_PI * u3))};
+    if (quat_out)
+      for (int k = 0; k < 4; ++k) quat_out[4 * p + k] = q[k];
+    float m[9];
+    emc_voxel::rotation_matrix(q, m);
+    const float* img = images + p * npix;
+    for (int64_t i = 0; i < npix; ++i) {
+      if (mask[i] != 1) continue;
+      float u[3];
+      emc_voxel::position(m, side, x[i], y[i], z[i], u);
+      int64_t v;
+      if (!emc_voxel::nearest(u, side, 0, &v)) continue;
+#pragma omp atomic
+      acc[v] += (double)img[i];
+#pragma omp atomic
+      wt[v] += 1.0;
+    }
+  }
+  for (int64_t v = 0; v < M; ++v) model[v] = wt[v] > 0.0 ? (float)(acc[v] / wt[v]) : 0.0f;
+  return EMC_OK;
+}
+
+emc_status emc_model_load(const char* path, int side, float* model) {
+  // emc.c:915-925 (model_input == 2) reads |value| of a side^3 image; here the
+  // file is raw little-endian float32 in [z][y][x] order.
+  if (!path || side < 2 || !model) return EMC_ERR_ARG;
+  const int64_t M = (int64_t)side * side * side;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return EMC_ERR_ARG;
+  std::fseek(f, 0, SEEK_END);
+  const long bytes = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  if (bytes != (long)(M * 4)) {
+    std::fclose(f);
+    return EMC_ERR_RANGE;
+  }
+  const size_t got = std::fread(model, 4, (size_t)M, f);
+  std::fclose(f);
+  if (got != (size_t)M) return EMC_ERR_ARG;
+  for (int64_t i = 0; i < M; ++i) model[i] = std::fabs(model[i]);
+  return EMC_OK;
+}
+
+emc_status emc_model_save(const char* path, int side, const float* model) {
+  if (!path || side < 2 || !model) return EMC_ERR_ARG;
+  const int64_t M = (int64_t)side * side * side;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return EMC_ERR_ARG;
+  const size_t put = std::fwrite(model, 4, (size_t)M, f);
+  const int rc = std::fclose(f);
+  return (put == (size_t)M && rc == 0) ? EMC_OK : EMC_ERR_ARG;
 }
 
 // ------------------------------------------------- reference CPU routine ---

@@ -75,6 +75,9 @@ cudaError_t launch_pattern_stats(const float* K, const int32_t* pix, int64_t N, 
 
 // T[r] = sum_p P[r][p].
 cudaError_t launch_row_sums(const float* P, int64_t R, int64_t N, float* T, cudaStream_t st);
+// best[p] = argmax_r P[r][p], bestv[p] = its value.
+cudaError_t launch_col_argmax(const float* P, int64_t R, int64_t N, int32_t* best, float* bestv,
+                              cudaStream_t st);
 
 // U[r][pix j] = sum_p P_rp K_pj / phi_p, divided by T_r where T_r > 1e-10.
 struct CompressArgs {

@@ -346,6 +346,38 @@ __global__ void pattern_stats_kernel(const float* K, const int32_t* pix, int64_t
   if (lane == 0) num[p] = s;
 }
 
+// best[p] = argmax_r P[r][p] (first on ties), bestv[p] = that value: 32
+// patterns per block (lane), the 8 warps split the rotations.
+__global__ void __launch_bounds__(256) col_argmax_kernel(const float* P, int64_t R, int64_t N,
+                                                         int32_t* best, float* bestv) {
+  __shared__ float sv[8][32];
+  __shared__ int32_t si[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t p = (int64_t)blockIdx.x * 32 + lane;
+  float bv = -INFINITY;
+  int32_t bi = -1;
+  if (p < N)
+    for (int64_t r = w; r < R; r += 8) {
+      const float v = P[r * N + p];
+      if (v > bv) {
+        bv = v;
+        bi = (int32_t)r;
+      }
+    }
+  sv[w][lane] = bv;
+  si[w][lane] = bi;
+  __syncthreads();
+  if (w == 0 && p < N) {
+    for (int k = 1; k < 8; ++k)
+      if (sv[k][lane] > bv || (sv[k][lane] == bv && si[k][lane] >= 0 && si[k][lane] < bi)) {
+        bv = sv[k][lane];
+        bi = si[k][lane];
+      }
+    best[p] = bi;
+    bestv[p] = bv;
+  }
+}
+
 __global__ void row_sums_kernel(const float* P, int64_t R, int64_t N, float* T) {
   const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -558,6 +590,12 @@ cudaError_t launch_scaling_finish(const double* num, const double* den_part, int
 cudaError_t launch_pattern_stats(const float* K, const int32_t* pix, int64_t N, int64_t npa,
                                  int64_t ldK, int squares, double* num, cudaStream_t st) {
   pattern_stats_kernel<<<(unsigned)((N + 7) / 8), kBlock, 0, st>>>(K, pix, N, npa, ldK, squares, num);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_col_argmax(const float* P, int64_t R, int64_t N, int32_t* best, float* bestv,
+                              cudaStream_t st) {
+  col_argmax_kernel<<<(unsigned)((N + 31) / 32), 256, 0, st>>>(P, R, N, best, bestv);
   return cudaGetLastError();
 }
 

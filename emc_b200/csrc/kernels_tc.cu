@@ -916,6 +916,40 @@ __global__ void export_kernel(const RespArgs a, float* P) {
   }
 }
 
+// Most probable rotation of every pattern from Y: best[p] = argmax_r LL_rp,
+// bestp[p] = exp(LL - lse_p); 32 patterns per block, 8 warps split R.
+__global__ void __launch_bounds__(256) resp_argmax_kernel(const RespArgs a, int32_t* best,
+                                                          float* bestp) {
+  __shared__ double sv[8][32];
+  __shared__ int32_t si[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t p = (int64_t)blockIdx.x * 32 + lane;
+  const LLFromY f = make_llf(a, p < a.N ? p : 0);
+  double bv = -INFINITY;
+  int32_t bi = -1;
+  if (p < a.N)
+    for (int64_t r = w; r < a.R; r += 8) {
+      const double rs = a.poisson ? 0.0 : a.rowstat[r] * a.gauss_inv;
+      const double v = f(a.Y[r * a.ldY + p], rs);
+      if (v > bv) {
+        bv = v;
+        bi = (int32_t)r;
+      }
+    }
+  sv[w][lane] = bv;
+  si[w][lane] = bi;
+  __syncthreads();
+  if (w == 0 && p < a.N) {
+    for (int k = 1; k < 8; ++k)
+      if (sv[k][lane] > bv || (sv[k][lane] == bv && si[k][lane] >= 0 && si[k][lane] < bi)) {
+        bv = sv[k][lane];
+        bi = si[k][lane];
+      }
+    best[p] = bi;
+    bestp[p] = (float)exp(bv - a.lse[p]);
+  }
+}
+
 // Kh[p][j] and Kt[j][p] as FP16 through a 32x32 shared-memory transpose.
 __global__ void pack_kernel(const float* K, int64_t N, int64_t npa, int64_t Npad, int64_t Ppad,
                             __half* Kh, __half* Kt, int* bad) {
@@ -1039,6 +1073,11 @@ cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {
 cudaError_t launch_resp_export(const RespArgs& a, float* P, cudaStream_t st) {
   dim3 grid((unsigned)((a.N + 255) / 256), (unsigned)(a.R < 4096 ? a.R : 4096));
   export_kernel<<<grid, 256, 0, st>>>(a, P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_resp_argmax(const RespArgs& a, int32_t* best, float* bestp, cudaStream_t st) {
+  resp_argmax_kernel<<<(unsigned)((a.N + 31) / 32), 256, 0, st>>>(a, best, bestp);
   return cudaGetLastError();
 }
 

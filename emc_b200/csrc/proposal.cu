@@ -176,13 +176,27 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
     return fma((double)y, c1, c0 - g.rowstat[g.mbeg[c] + k] * g.gauss_inv);
   };
   double mx = -INFINITY;
+  int64_t arg = -1;  // rotation of the largest LL (first in candidate order on ties)
   for (int i = 0; i < g.m; ++i) {
     const int c = g.cand[p * g.m + i];
     if (c < 0) break;
     const int64_t q = g.ppos[p * g.m + i];
-    for (int k = lane; k < g.mcnt[c]; k += 32) mx = fmax(mx, ll_of(c, q, k));
+    for (int k = lane; k < g.mcnt[c]; k += 32) {
+      const double l = ll_of(c, q, k);
+      if (l > mx) {
+        mx = l;
+        arg = g.mbeg[c] + k;
+      }
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  for (int o = 16; o > 0; o >>= 1) {
+    const double om = __shfl_xor_sync(0xffffffffu, mx, o);
+    const long long oa = __shfl_xor_sync(0xffffffffu, (long long)arg, o);
+    if (om > mx || (om == mx && oa >= 0 && (arg < 0 || oa < arg))) {
+      mx = om;
+      arg = oa;
+    }
+  }
   double s = 0.0, d = 0.0, pl = 0.0;
   for (int i = 0; i < g.m; ++i) {
     const int c = g.cand[p * g.m + i];
@@ -210,6 +224,8 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
     g.lse[p] = lse;
     g.plogp[p] = pl / s - log(s);
     g.new_scaling[p] = (float)phi_new;
+    g.best_rot[p] = (int32_t)arg;
+    g.best_p[p] = (float)exp(mx - lse);
   }
   for (int i = 0; i < g.m; ++i) {
     const int c = g.cand[p * g.m + i];

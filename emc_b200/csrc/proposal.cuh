@@ -71,6 +71,8 @@ struct GroupArgs {
   double* plogp;           // [N]
   float* new_scaling;      // [N]
   float* cmass;            // [N][m] responsibility mass of each candidate cell
+  int32_t* best_rot;       // [N] most probable rotation among the candidates
+  float* best_p;           // [N] its responsibility
   // tile lists: mtiles (cell, member offset, pair offset) of the grouped
   // maximize; ctiles (cell, member offset) of the grouped compress
   const int4* mtiles;

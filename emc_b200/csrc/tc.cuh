@@ -146,6 +146,8 @@ struct RespArgs {
 cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st);
 // FP32 responsibilities [R][N] from Y and lse (readback / tests).
 cudaError_t launch_resp_export(const RespArgs& a, float* P, cudaStream_t st);
+// Most probable rotation of every pattern and its responsibility, from Y and lse.
+cudaError_t launch_resp_argmax(const RespArgs& a, int32_t* best, float* bestp, cudaStream_t st);
 // Builds the FP16 pattern operands: Kh[Npad][Ppad] and Kt[Ppad][Npad] from
 // compact FP32 counts [N][npa]; bad[0] counts entries that are not integers in [0, 2048].
 cudaError_t launch_pack_patterns(const float* K, int64_t N, int64_t npa, int64_t Npad,

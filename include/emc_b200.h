@@ -128,6 +128,15 @@ void *emc_stream(emc_context *ctx);
 /* Number of active (mask != 0) pixels. */
 int64_t emc_active_pixels(const emc_context *ctx);
 
+/* Orientation diagnostics of the last maximize (dense or proposed), host
+ * outputs, each optional: best_rot[N] the most probable rotation of every
+ * pattern (for a proposed iteration: among its candidates) and best_resp[N]
+ * its responsibility; avg_resp[R] the average responsibility of each
+ * rotation over the patterns (T_r / N).  The per-iteration record the
+ * reference's viewer reads (best rotations, average_resp, scaling). */
+emc_status emc_orientation_stats(emc_context *ctx, int32_t *best_rot, float *best_resp,
+                                 float *avg_resp);
+
 /* Tile order of the two tensor-core contractions (mixed precision): the
  * persistent CTAs walk the output tiles in bands of `raster` rotation tiles,
  * the other index fastest, so operand tiles loaded from HBM are shared
@@ -234,6 +243,19 @@ emc_status emc_synthesize(const emc_synth_config *sc, const float *x, const floa
                           float *true_rotations, float *true_scales);
 /* Uniform [0,1) initial model (emc.c:893-898 with a counter-based generator). */
 void emc_random_model(int side, uint64_t seed, float *model);
+/* Initial model from the data (emc.c:896-914, model_input 1): every image
+ * inserted with weight 1 at a uniformly random rotation (nearest voxel,
+ * mask == 1), then model = sum / weight (0 where no weight).  images:
+ * [n_images][side^2]; quat_out (optional): the rotations used, [n][4]. */
+emc_status emc_model_random_orientations(int side, int64_t n_images, const float *images,
+                                         const int32_t *mask, const float *x, const float *y,
+                                         const float *z, uint64_t seed, float *model,
+                                         float *quat_out);
+/* Model from / to a file (emc.c:915-925, model_input 2): raw little-endian
+ * float32, side^3 values in [z][y][x] order; load keeps |value|.
+ * EMC_ERR_RANGE when the file size is not 4 side^3 bytes. */
+emc_status emc_model_load(const char *path, int side, float *model);
+emc_status emc_model_save(const char *path, int side, const float *model);
 
 #ifdef __cplusplus
 }
