@@ -92,6 +92,7 @@ def lib():
             ("emc_partial_stats", [P, P, P], C.c_int),
             ("emc_get_tuning", [P, P], C.c_int), ("emc_set_tuning", [P, P], C.c_int),
             ("emc_orientation_stats", [P, P, P, P], C.c_int),
+            ("emc_set_patterns_sparse", [P, P, P, P], C.c_int),
             ("emc_model_random_orientations", [C.c_int, I64, P, P, P, P, P, C.c_uint64, P, P],
              C.c_int),
             ("emc_model_load", [C.c_char_p, C.c_int, P], C.c_int),
@@ -148,6 +149,16 @@ def model_random_orientations(side, images, mask, x, y, z, seed=0, return_rotati
         _ptr(np.ascontiguousarray(x, np.float32)), _ptr(np.ascontiguousarray(y, np.float32)),
         _ptr(np.ascontiguousarray(z, np.float32)), seed, _ptr(model), _ptr(quat)))
     return (model, quat) if return_rotations else model
+
+
+def photon_lists(counts):
+    """Dense patterns [N][side^2] -> CSR photon lists (row_ptr, pixels, counts)
+    of their non-zero pixels."""
+    K = np.asarray(counts).reshape(np.asarray(counts).shape[0], -1)
+    p, j = np.nonzero(K)
+    row_ptr = np.zeros(K.shape[0] + 1, np.int64)
+    np.cumsum(np.bincount(p, minlength=K.shape[0]), out=row_ptr[1:])
+    return row_ptr, j.astype(np.int32), K[p, j].astype(np.float32)
 
 
 def load_model(path, side):
@@ -252,6 +263,15 @@ class Context:
         k = self._f32(counts)
         assert k.size == self.N * self.side * self.side
         self._c(lib().emc_set_patterns(self._h, _ptr(k)))
+
+    def set_patterns_sparse(self, row_ptr, pixels, counts=None):
+        """emc_set_patterns_sparse: photon lists in CSR form (see photon_lists)."""
+        rp = np.ascontiguousarray(row_ptr, np.int64)
+        assert rp.size == self.N + 1
+        px = np.ascontiguousarray(pixels, np.int32)
+        ct = None if counts is None else np.ascontiguousarray(counts, np.float32)
+        self._c(lib().emc_set_patterns_sparse(self._h, _ptr(rp), _ptr(px),
+                                              None if ct is None else _ptr(ct)))
 
     def set_model(self, model):
         m = self._f32(model)

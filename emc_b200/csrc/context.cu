@@ -30,6 +30,30 @@ __global__ void gather_cols_kernel(const float* src, int64_t rows, int64_t ld, c
     dst[r * npa + j] = src[r * ld + pix[j]];
 }
 
+// Photon lists (CSR over patterns) into the compact counts: one warp per
+// pattern; entries on masked-out pixels are dropped, entries outside the
+// detector are counted in bad[0].  Counts are summed atomically (a pixel may
+// appear once per photon); integer counts make the order irrelevant.
+__global__ void scatter_photons_kernel(const int64_t* row_ptr, const int32_t* pix,
+                                       const float* val, int64_t N, int64_t npix,
+                                       const int32_t* compact_of, int64_t npa, float* K,
+                                       int* bad) {
+  const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= N) return;
+  int nbad = 0;
+  for (int64_t e = row_ptr[p] + lane; e < row_ptr[p + 1]; e += 32) {
+    const int32_t i = pix[e];
+    if (i < 0 || i >= npix) {
+      ++nbad;
+      continue;
+    }
+    const int32_t j = compact_of[i];
+    if (j >= 0) atomicAdd(K + p * npa + j, val ? val[e] : 1.0f);
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
 __global__ void split_sum_kernel(const __half* hi, const __half* lo, int64_t R, int64_t ld,
                                  int64_t npa, float* out) {
   const int64_t r = blockIdx.y;
@@ -60,6 +84,12 @@ struct emc_context {
   // patterns
   float* d_K = nullptr;      // [N][npa] FP32 counts on the active pixels
   float* d_stage = nullptr;  // [N][side^2] upload staging
+  // photon-list upload staging (CSR) and the detector pixel -> compact map
+  int64_t* d_sp_row = nullptr;
+  int32_t* d_sp_pix = nullptr;
+  float* d_sp_val = nullptr;
+  int64_t sp_cap = 0;
+  int32_t* d_compact_of = nullptr;
   double *d_patsq = nullptr, *d_patsum = nullptr;
   // model state
   float *d_model = nullptr, *d_weight = nullptr, *d_scaling = nullptr, *d_scaling_prev = nullptr;
@@ -362,6 +392,8 @@ emc_status emc_set_rotations(emc_context* c, const float* q, const float* w) {
   return EMC_OK;
 }
 
+static emc_status finish_patterns(emc_context* c);
+
 emc_status emc_set_patterns(emc_context* c, const float* counts) {
   if (!c || !counts) return EMC_ERR_ARG;
   if (!c->have_geom) return c->fail(EMC_ERR_STATE, "set the geometry before the patterns");
@@ -383,7 +415,15 @@ emc_status emc_set_patterns(emc_context* c, const float* counts) {
       e = cudaGetLastError();
     }
   }
-  if (e == cudaSuccess) e = launch_pattern_stats(compact, nullptr, N, npa, npa, 1, c->d_patsq, c->st);
+  if (e != cudaSuccess) return c->cuda(e, "emc_set_patterns");
+  return finish_patterns(c);
+}
+
+// Pattern statistics and the FP16 operands of the compact counts d_K.
+static emc_status finish_patterns(emc_context* c) {
+  const int64_t N = c->N, npa = c->npa;
+  float* compact = c->d_K;
+  cudaError_t e = launch_pattern_stats(compact, nullptr, N, npa, npa, 1, c->d_patsq, c->st);
   if (e == cudaSuccess) e = launch_pattern_stats(compact, nullptr, N, npa, npa, 0, c->d_patsum, c->st);
   int bad = 0;
   if (e == cudaSuccess && c->mixed) {
@@ -401,6 +441,59 @@ emc_status emc_set_patterns(emc_context* c, const float* counts) {
                    bad);
   c->have_pat = true;
   return EMC_OK;
+}
+
+emc_status emc_set_patterns_sparse(emc_context* c, const int64_t* row_ptr, const int32_t* pixels,
+                                   const float* counts) {
+  if (!c || !row_ptr) return EMC_ERR_ARG;
+  if (!c->have_geom) return c->fail(EMC_ERR_STATE, "set the geometry before the patterns");
+  const int64_t N = c->N, npa = c->npa;
+  const int64_t nnz = row_ptr[N];
+  if (row_ptr[0] != 0 || nnz < 0 || (nnz > 0 && !pixels))
+    return c->fail(EMC_ERR_ARG, "row_ptr must start at 0 and end at the entry count");
+  for (int64_t p = 0; p < N; ++p)
+    if (row_ptr[p + 1] < row_ptr[p]) return c->fail(EMC_ERR_ARG, "row_ptr must not decrease");
+  if (!c->d_compact_of) {
+    std::vector<int32_t> inv(c->npix, -1);
+    std::vector<int32_t> pix(npa);
+    CK(c, cudaMemcpyAsync(pix.data(), c->d_pix, sizeof(int32_t) * npa, cudaMemcpyDeviceToHost, c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    for (int64_t j = 0; j < npa; ++j) inv[pix[j]] = (int32_t)j;
+    TRY(c->alloc(&c->d_compact_of, c->npix));
+    CK(c, cudaMemcpyAsync(c->d_compact_of, inv.data(), sizeof(int32_t) * c->npix,
+                          cudaMemcpyHostToDevice, c->st));
+  }
+  if (!c->d_K) TRY(c->alloc(&c->d_K, N * npa));
+  if (!c->d_sp_row) TRY(c->alloc(&c->d_sp_row, N + 1));
+  if (nnz > c->sp_cap) {
+    for (void* q : {(void*)c->d_sp_pix, (void*)c->d_sp_val})
+      if (q) c->release(q);
+    c->d_sp_pix = nullptr;
+    c->d_sp_val = nullptr;
+    c->sp_cap = 0;
+    const int64_t cap = nnz + nnz / 4 + 1024;
+    TRY(c->alloc(&c->d_sp_pix, cap));
+    TRY(c->alloc(&c->d_sp_val, cap));
+    c->sp_cap = cap;
+  }
+  CK(c, cudaMemcpyAsync(c->d_sp_row, row_ptr, sizeof(int64_t) * (N + 1), cudaMemcpyHostToDevice, c->st));
+  if (nnz > 0) {
+    CK(c, cudaMemcpyAsync(c->d_sp_pix, pixels, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, c->st));
+    if (counts)
+      CK(c, cudaMemcpyAsync(c->d_sp_val, counts, sizeof(float) * nnz, cudaMemcpyHostToDevice, c->st));
+  }
+  int* d_bad = reinterpret_cast<int*>(c->d_scratch) + 1;
+  int bad = 0;
+  CK(c, cudaMemsetAsync(d_bad, 0, sizeof(int), c->st));
+  CK(c, cudaMemsetAsync(c->d_K, 0, sizeof(float) * N * npa, c->st));
+  scatter_photons_kernel<<<(unsigned)((N + 7) / 8), 256, 0, c->st>>>(
+      c->d_sp_row, c->d_sp_pix, counts ? c->d_sp_val : nullptr, N, c->npix, c->d_compact_of, npa,
+      c->d_K, d_bad);
+  CK(c, cudaGetLastError());
+  CK(c, cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  if (bad) return c->fail(EMC_ERR_ARG, "%d photon entries lie outside the detector", bad);
+  return finish_patterns(c);
 }
 
 emc_status emc_set_model(emc_context* c, const float* model) {

@@ -87,6 +87,14 @@ emc_status emc_set_geometry(emc_context *ctx, const float *x, const float *y, co
 emc_status emc_set_rotations(emc_context *ctx, const float *quaternions, const float *weights);
 /* Photon counts [N][side*side] (non-negative; the mixed path needs integers <= 2048). */
 emc_status emc_set_patterns(emc_context *ctx, const float *counts);
+/* The same from photon lists (sparse patterns, CSR over patterns): pattern p's
+ * entries are row_ptr[p] .. row_ptr[p+1]-1 (row_ptr[0] = 0, row_ptr[N] =
+ * entry count); pixels[e] is a detector pixel index (y * side + x) and
+ * counts[e] its count, or counts = NULL for one photon per entry (a pixel
+ * may repeat).  Entries on masked-out pixels are dropped; entries outside
+ * the detector are an error.  Only the lists cross the bus. */
+emc_status emc_set_patterns_sparse(emc_context *ctx, const int64_t *row_ptr,
+                                   const int32_t *pixels, const float *counts);
 emc_status emc_set_model(emc_context *ctx, const float *model);
 emc_status emc_set_scaling(emc_context *ctx, const float *scaling);
 

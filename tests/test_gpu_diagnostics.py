@@ -70,3 +70,39 @@ def test_output_files_read_back_like_the_viewer(tmp_path):
     avg = np.loadtxt(tmp_path / "average_resp_0001.data")
     assert avg.shape == (R,) and abs(avg.sum() - 1.0) < 1e-3
     np.testing.assert_array_equal(E.load_model(str(tmp_path / "model_0001.raw"), 16), model)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_photon_list_ingest_equals_dense_patterns(prec):
+    """emc_set_patterns_sparse (CSR photon lists, as (pixel, count) pairs or
+    one entry per photon) gives the iteration of the dense upload."""
+    import emc_b200 as E
+    from emc_b200 import workloads as W
+    d = W.make("small32")
+    with make_ctx(d, "poisson", "nearest", prec) as ctx:
+        m0 = ctx.get_model()
+        ctx.iterate()
+        m_dense, s_dense = ctx.get_model(), ctx.get_scaling()
+        rp, px, ct = E.photon_lists(d["counts"])
+        assert px.size == np.count_nonzero(d["counts"])
+        for photons in (False, True):
+            if photons:  # one entry per photon, in shuffled order within a pattern
+                rep = ct.astype(np.int64)
+                px2 = np.repeat(px, rep)
+                rp2 = np.zeros_like(rp)
+                np.cumsum(np.add.reduceat(rep, rp[:-1]) * (np.diff(rp) > 0), out=rp2[1:])
+                rng = np.random.default_rng(0)
+                for p in range(len(rp2) - 1):
+                    rng.shuffle(px2[rp2[p]:rp2[p + 1]])
+                ctx.set_patterns_sparse(rp2, px2)
+            else:
+                ctx.set_patterns_sparse(rp, px, ct)
+            ctx.set_model(m0)
+            ctx.set_scaling(d["scaling0"])
+            ctx.iterate()
+            assert rel(ctx.get_model(), m_dense) < 1e-6
+            assert rel(ctx.get_scaling(), s_dense) < 1e-6
+        bad = px.copy()
+        bad[0] = 32 * 32
+        with pytest.raises(E.EmcError):
+            ctx.set_patterns_sparse(rp, bad, ct)
