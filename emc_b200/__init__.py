@@ -93,6 +93,11 @@ def lib():
             ("emc_get_tuning", [P, P], C.c_int), ("emc_set_tuning", [P, P], C.c_int),
             ("emc_orientation_stats", [P, P, P, P], C.c_int),
             ("emc_set_patterns_sparse", [P, P, P, P], C.c_int),
+            ("emc_batch_create", [P, C.c_int32, P], C.c_int), ("emc_batch_destroy", [P], C.c_int),
+            ("emc_batch_iterate", [P], C.c_int), ("emc_batch_capture", [P], C.c_int),
+            ("emc_batch_launch", [P, C.c_int32], C.c_int),
+            ("emc_batch_synchronize", [P], C.c_int), ("emc_batch_stream", [P], P),
+            ("emc_batch_last_error", [P], C.c_char_p),
             ("emc_model_random_orientations", [C.c_int, I64, P, P, P, P, P, C.c_uint64, P, P],
              C.c_int),
             ("emc_model_load", [C.c_char_p, C.c_int, P], C.c_int),
@@ -390,3 +395,54 @@ class Context:
         p, n = C.c_void_p(), C.c_size_t()
         self._c(lib().emc_device_buffer(self._h, which, C.byref(p), C.byref(n)))
         return p.value, n.value
+
+
+class Batch:
+    """emc_batch: several mixed-precision contexts iterated with one
+    persistent launch per contraction, optionally replayed as a CUDA graph."""
+
+    def __init__(self, contexts):
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c._h for c in self.contexts])
+        h = C.c_void_p()
+        st = lib().emc_batch_create(arr, len(self.contexts), C.byref(h))
+        if st != 0:
+            raise EmcError(st, "emc_batch_create")
+        self._h = h
+
+    def _c(self, st):
+        if st != 0:
+            raise EmcError(st, lib().emc_batch_last_error(self._h).decode())
+
+    def iterate(self):
+        self._c(lib().emc_batch_iterate(self._h))
+
+    def capture(self):
+        self._c(lib().emc_batch_capture(self._h))
+
+    def launch(self, iterations=1):
+        self._c(lib().emc_batch_launch(self._h, iterations))
+
+    def synchronize(self):
+        self._c(lib().emc_batch_synchronize(self._h))
+
+    @property
+    def stream(self):
+        return lib().emc_batch_stream(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().emc_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -552,6 +552,79 @@ emc_status emc_expand(emc_context* c) {
   return EMC_OK;
 }
 
+}  // extern "C"
+
+// Epilogue arguments of the mixed maximize contraction.
+static MaxEpiArgs max_args(emc_context* c) {
+  MaxEpiArgs e{};
+  e.N = c->N;
+  e.R = c->R;
+  e.ldY = c->Npad;
+  e.poisson = c->gauss ? 0 : 1;
+  e.scaling = c->d_scaling_prev;
+  e.rowstat = c->d_rowstat;
+  e.patstat = c->d_patsq;
+  e.gauss_inv = gauss_inv(c);
+  e.Y = c->d_Y;
+  e.part = c->d_part;
+  return e;
+}
+
+// Epilogue arguments of the mixed compress contraction (insertion).
+static CmpEpiArgs cmp_args(emc_context* c) {
+  CmpEpiArgs e{};
+  e.R = c->R;
+  e.npa = c->npa;
+  e.side = c->cfg.side;
+  e.interp = c->cfg.interp;
+  e.inv_c0 = 1.0f;
+  e.quat = c->d_quat;
+  e.rotw = c->d_rotw;
+  e.T = c->d_T;
+  e.cx = c->d_cx;
+  e.cy = c->d_cy;
+  e.cz = c->d_cz;
+  e.ins = c->d_ins;
+  e.acc = c->d_acc;
+  return e;
+}
+
+// After the maximize contraction: lse, new scaling and sum P log P per
+// pattern, T_r, the compress operand P / (T_r phi), and the stats sums.
+static emc_status mixed_resp_pass(emc_context* c) {
+  const int64_t N = c->N;
+  RespArgs a{};
+  a.N = N;
+  a.R = c->R;
+  a.ldY = c->Npad;
+  a.ldP = c->Npad;
+  a.nparts = c->nrt;
+  a.poisson = c->gauss ? 0 : 1;
+  a.Y = c->d_Y;
+  a.part = c->d_part;
+  a.scaling = c->d_scaling_prev;
+  a.rowstat = c->d_rowstat;
+  a.patstat = c->d_patsq;
+  a.patsum = c->d_patsum;
+  a.gauss_inv = gauss_inv(c);
+  a.lse = c->d_lse;
+  a.plogp = c->d_plogp;
+  a.new_scaling = c->d_scaling;
+  a.c0 = 1.0f;
+  a.Phi = c->d_Phi;
+  a.Plo = c->d_Plo;
+  a.Tpart = c->d_Tpart;
+  a.T = c->d_T;
+  a.P32 = nullptr;
+  CK(c, launch_resp_pass(a, c->st));
+  CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
+  CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
+  c->launches += 5;  // combine, 2 sweeps, 2 sums
+  return EMC_OK;
+}
+
+extern "C" {
+
 emc_status emc_maximize(emc_context* c) {
   if (!c) return EMC_ERR_ARG;
   if (c->stage != 1) return c->fail(EMC_ERR_STATE, "maximize called before expand");
@@ -601,47 +674,12 @@ emc_status emc_maximize(emc_context* c) {
     CK(c, launch_row_sums(c->d_LL, R, N, c->d_T, c->st));
     c->launches += 8;
   } else {
-    MaxEpiArgs e{};
-    e.N = N;
-    e.R = R;
-    e.ldY = c->Npad;
-    e.poisson = c->gauss ? 0 : 1;
-    e.scaling = c->d_scaling_prev;
-    e.rowstat = c->d_rowstat;
-    e.patstat = c->d_patsq;
-    e.gauss_inv = gauss_inv(c);
-    e.Y = c->d_Y;
-    e.part = c->d_part;
+    MaxEpiArgs e = max_args(c);
     CK(c, launch_maximize_tc(c->tmKh, c->tmBhi, c->tmBlo, c->Npad, c->Rpad, c->Ppad, e,
                              c->d_status, c->num_sms, c->st, c->tune.maximize_raster));
     c->mark(2);
-    RespArgs a{};
-    a.N = N;
-    a.R = R;
-    a.ldY = c->Npad;
-    a.ldP = c->Npad;
-    a.nparts = c->nrt;
-    a.poisson = e.poisson;
-    a.Y = c->d_Y;
-    a.part = c->d_part;
-    a.scaling = c->d_scaling_prev;
-    a.rowstat = c->d_rowstat;
-    a.patstat = c->d_patsq;
-    a.patsum = c->d_patsum;
-    a.gauss_inv = e.gauss_inv;
-    a.lse = c->d_lse;
-    a.plogp = c->d_plogp;
-    a.new_scaling = c->d_scaling;
-    a.c0 = 1.0f;
-    a.Phi = c->d_Phi;
-    a.Plo = c->d_Plo;
-    a.Tpart = c->d_Tpart;
-    a.T = c->d_T;
-    a.P32 = nullptr;
-    CK(c, launch_resp_pass(a, c->st));
-    CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
-    CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
-    c->launches += 6;  // maximize contraction, combine, 2 sweeps, 2 sums
+    TRY(mixed_resp_pass(c));
+    c->launches += 1;  // the maximize contraction
   }
   c->mark(3);
   c->resp_source = 1;
@@ -691,20 +729,7 @@ emc_status emc_compress_insert(emc_context* c) {
     CK(c, launch_insert(in, c->st));
     c->launches += 2;
   } else {
-    CmpEpiArgs e{};
-    e.R = c->R;
-    e.npa = c->npa;
-    e.side = c->cfg.side;
-    e.interp = c->cfg.interp;
-    e.inv_c0 = 1.0f;
-    e.quat = c->d_quat;
-    e.rotw = c->d_rotw;
-    e.T = c->d_T;
-    e.cx = c->d_cx;
-    e.cy = c->d_cy;
-    e.cz = c->d_cz;
-    e.ins = c->d_ins;
-    e.acc = c->d_acc;
+    CmpEpiArgs e = cmp_args(c);
     CK(c, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
                              c->d_status, c->num_sms, c->st, c->tune.compress_raster));
     c->launches += 1;
@@ -1366,4 +1391,240 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
   if (stats) *stats = st;
   return EMC_OK;
 }
+}  // extern "C"
+
+// ------------------------------------------------ several datasets at once --
+// One iteration of several contexts with one persistent launch per
+// contraction (a tile list over all datasets), the per-dataset stages in
+// between on one shared stream, and optionally the whole iteration captured
+// into a CUDA graph.
+
+struct emc_batch {
+  std::vector<emc_context*> ctx;
+  std::vector<cudaStream_t> own;  // the contexts' own streams, given back by destroy
+  cudaStream_t st = nullptr;
+  TileDesc *d_mt = nullptr, *d_ct = nullptr;
+  int64_t n_mt = 0, n_ct = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string err;
+  emc_status fail(emc_status s, const std::string& m) {
+    err = m;
+    return s;
+  }
+  emc_status cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return EMC_OK;
+    return fail(e == cudaErrorMemoryAllocation ? EMC_ERR_OOM : EMC_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+  }
+};
+
+#define BCK(b, x)                                     \
+  do {                                                \
+    emc_status _s = (b)->cuda((x), #x);               \
+    if (_s != EMC_OK) return _s;                      \
+  } while (0)
+#define BTRY(b, c, x)                                 \
+  do {                                                \
+    emc_status _s = (x);                              \
+    if (_s != EMC_OK) return (b)->fail(_s, (c)->err); \
+  } while (0)
+
+extern "C" {
+
+emc_status emc_batch_destroy(emc_batch* b) {
+  if (!b) return EMC_OK;
+  if (b->st) cudaStreamSynchronize(b->st);
+  for (size_t i = 0; i < b->ctx.size(); ++i) b->ctx[i]->st = b->own[i];
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->d_mt) cudaFree(b->d_mt);
+  if (b->d_ct) cudaFree(b->d_ct);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return EMC_OK;
+}
+
+emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out) {
+  if (!ctxs || !out || n < 1 || n > kMaxBatch) return EMC_ERR_ARG;
+  *out = nullptr;
+  const int dev = ctxs[0]->cfg.device;
+  for (int32_t i = 0; i < n; ++i) {
+    emc_context* c = ctxs[i];
+    if (!c || !c->mixed || c->cfg.device != dev) return EMC_ERR_ARG;
+    if (!c->have_geom || !c->have_rot || !c->have_pat || !c->have_model || c->stage != 0)
+      return EMC_ERR_STATE;
+    for (int32_t k = 0; k < i; ++k)
+      if (ctxs[k] == c) return EMC_ERR_ARG;
+  }
+  emc_batch* b = new emc_batch();
+  if (cudaSetDevice(dev) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) {
+    emc_batch_destroy(b);
+    return EMC_ERR_CUDA;
+  }
+  for (int32_t i = 0; i < n; ++i) {
+    cudaStreamSynchronize(ctxs[i]->st);
+    b->ctx.push_back(ctxs[i]);
+    b->own.push_back(ctxs[i]->st);
+    ctxs[i]->st = b->st;  // every stage of every dataset on the batch's stream
+  }
+  // Tile lists, the costliest tiles first (a tile's time grows with its K
+  // extent), each dataset's tiles in the order of its own launch.
+  std::vector<int32_t> order(n);
+  std::vector<TileDesc> mt, ct;
+  for (int32_t i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t x, int32_t y) { return ctxs[x]->Ppad > ctxs[y]->Ppad; });
+  for (int32_t i : order) {
+    const emc_context* c = ctxs[i];
+    for (int64_t nt = 0; nt < c->Rpad / 256; ++nt)
+      for (int64_t m = 0; m < c->Npad / 128; ++m)
+        mt.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
+                              (int32_t)(c->Ppad / kMaximizeBK), (int32_t)nt, (int32_t)m, i});
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t x, int32_t y) { return ctxs[x]->Npad > ctxs[y]->Npad; });
+  for (int32_t i : order) {
+    const emc_context* c = ctxs[i];
+    for (int64_t m = 0; m < c->Rpad / 128; ++m)
+      for (int64_t nt = 0; nt < c->Ppad / 256; ++nt)
+        ct.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
+                              (int32_t)(c->Npad / kCompressBK), (int32_t)nt, (int32_t)m, i});
+  }
+  b->n_mt = (int64_t)mt.size();
+  b->n_ct = (int64_t)ct.size();
+  emc_status s = EMC_OK;
+  if ((s = b->cuda(cudaMalloc(&b->d_mt, sizeof(TileDesc) * mt.size()), "cudaMalloc")) != EMC_OK ||
+      (s = b->cuda(cudaMalloc(&b->d_ct, sizeof(TileDesc) * ct.size()), "cudaMalloc")) != EMC_OK ||
+      (s = b->cuda(cudaMemcpy(b->d_mt, mt.data(), sizeof(TileDesc) * mt.size(),
+                              cudaMemcpyHostToDevice), "tile list")) != EMC_OK ||
+      (s = b->cuda(cudaMemcpy(b->d_ct, ct.data(), sizeof(TileDesc) * ct.size(),
+                              cudaMemcpyHostToDevice), "tile list")) != EMC_OK) {
+    emc_batch_destroy(b);
+    return s;
+  }
+  *out = b;
+  return EMC_OK;
+}
+
+emc_status emc_batch_iterate(emc_batch* b) {
+  if (!b) return EMC_ERR_ARG;
+  const int n = (int)b->ctx.size();
+  emc_context* c0 = b->ctx[0];
+  TmapSet<kMaxBatch> maps;
+  BatchMaxArgs me{};
+  BatchCmpArgs ce{};
+  me.tiles = b->d_mt;
+  ce.tiles = b->d_ct;
+  for (int i = 0; i < n; ++i) {
+    emc_context* c = b->ctx[i];
+    if (c->stage != 0) return b->fail(EMC_ERR_STATE, "a dataset is between stages");
+    BTRY(b, c, emc_expand(c));
+    BCK(b, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * c->N,
+                           cudaMemcpyDeviceToDevice, b->st));
+    me.set[i] = max_args(c);
+    maps.a0[i] = c->tmKh;
+    maps.a1[i] = c->tmKh;
+    maps.b0[i] = c->tmBhi;
+    maps.b1[i] = c->tmBlo;
+  }
+  for (int i = n; i < kMaxBatch; ++i) {  // unused sets repeat the first (never indexed)
+    maps.a0[i] = maps.a0[0];
+    maps.a1[i] = maps.a1[0];
+    maps.b0[i] = maps.b0[0];
+    maps.b1[i] = maps.b1[0];
+  }
+  BCK(b, launch_batch_maximize_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
+  for (int i = 0; i < n; ++i) {
+    emc_context* c = b->ctx[i];
+    BTRY(b, c, mixed_resp_pass(c));
+    c->resp_source = 1;
+    c->stage = 2;
+    BCK(b, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, b->st));
+    ce.set[i] = cmp_args(c);
+    maps.a0[i] = c->tmPhi;
+    maps.a1[i] = c->tmPlo;
+    maps.b0[i] = c->tmKt;
+    maps.b1[i] = c->tmKt;
+  }
+  for (int i = n; i < kMaxBatch; ++i) {
+    maps.a0[i] = maps.a0[0];
+    maps.a1[i] = maps.a1[0];
+    maps.b0[i] = maps.b0[0];
+    maps.b1[i] = maps.b1[0];
+  }
+  BCK(b, launch_batch_compress_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
+  c0->launches += 2;
+  for (int i = 0; i < n; ++i) {
+    emc_context* c = b->ctx[i];
+    c->stage = 3;
+    BTRY(b, c, emc_normalize(c));
+  }
+  return EMC_OK;
+}
+
+emc_status emc_batch_capture(emc_batch* b) {
+  if (!b) return EMC_ERR_ARG;
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  std::vector<int64_t> l0;
+  std::vector<bool> prof;
+  for (emc_context* c : b->ctx) {
+    l0.push_back(c->launches);
+    prof.push_back(c->prof);
+    c->prof = false;  // no stage events inside the graph
+  }
+  BCK(b, cudaStreamSynchronize(b->st));
+  BCK(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  const emc_status s = emc_batch_iterate(b);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->st, &g);
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    b->ctx[i]->prof = prof[i];
+    b->ctx[i]->launches = l0[i];  // captured, not launched
+  }
+  if (s != EMC_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  BCK(b, e);
+  b->graph = g;
+  BCK(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+  // the per-launch bookkeeping of one iteration, applied per replay
+  for (emc_context* c : b->ctx) c->stage = 0;
+  return EMC_OK;
+}
+
+emc_status emc_batch_launch(emc_batch* b, int32_t iterations) {
+  if (!b || iterations < 0) return EMC_ERR_ARG;
+  if (!b->exec) return b->fail(EMC_ERR_STATE, "emc_batch_capture first");
+  for (int32_t k = 0; k < iterations; ++k) BCK(b, cudaGraphLaunch(b->exec, b->st));
+  // per dataset: expand, resp pass (5), normalise (4); two batched contractions
+  for (emc_context* c : b->ctx) {
+    c->launches += 10LL * iterations;
+    c->resp_source = 1;
+    c->stage = 0;
+  }
+  b->ctx[0]->launches += 2LL * iterations;
+  return EMC_OK;
+}
+
+emc_status emc_batch_synchronize(emc_batch* b) {
+  if (!b) return EMC_ERR_ARG;
+  BCK(b, cudaStreamSynchronize(b->st));
+  for (emc_context* c : b->ctx) BTRY(b, c, check_status(c));
+  return EMC_OK;
+}
+
+void* emc_batch_stream(emc_batch* b) { return b ? (void*)b->st : nullptr; }
+
+const char* emc_batch_last_error(const emc_batch* b) { return b ? b->err.c_str() : ""; }
+
 }  // extern "C"

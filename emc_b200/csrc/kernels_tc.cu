@@ -143,8 +143,7 @@ __device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int si
 // ---------------------------------------------------------------- kernel --
 template <int NA, int NB, int STAGES, bool M_INNER, int BK, class Epi>
 __global__ void __launch_bounds__(kThreads, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1,
-                   const __grid_constant__ CUtensorMap tmB0, const __grid_constant__ CUtensorMap tmB1,
+    tc_gemm_kernel(const __grid_constant__ TmapSet<Epi::kSets> maps,
                    const int64_t m_tiles, const int64_t n_tiles, const int64_t k_blocks,
                    const int raster, const Epi epi, TcStatus* status) {
   static_assert(NA * NB == 2, "one hi/lo split per contraction");
@@ -216,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   // TMA origins (row and k offset of each operand) and k-block count of tile
   // t: a regular m_tiles x n_tiles grid, or an epilogue-supplied tile list
   // (grouped contractions of uneven groups)
-  auto coords = [&](int64_t t, int& ar, int& ak, int& br, int& bk, int64_t& kbs) {
+  auto coords = [&](int64_t t, int& ar, int& ak, int& br, int& bk, int64_t& kbs, int& set) {
     if constexpr (Epi::kListed) {
       const TileDesc d = epi.a.tiles[t];
       ar = d.a_row;
@@ -224,6 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       br = d.b_row;
       bk = d.b_k0;
       kbs = d.k_blocks;
+      set = d.set;
     } else {
       int64_t mt, nt;
       tile_mn(t, mt, nt);
@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       br = (int)(nt * BN);
       bk = 0;
       kbs = k_blocks;
+      set = 0;
     }
   };
 
@@ -243,9 +244,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       int64_t issued = 0;
       bool ok = true;
       for (int64_t t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        int ar, ak, br, bk;
+        int ar, ak, br, bk, set;
         int64_t kbs;
-        coords(t, ar, ak, br, bk, kbs);
+        coords(t, ar, ak, br, bk, kbs, set);
+        const CUtensorMap* tA0 = &maps.a0[set];
+        const CUtensorMap* tA1 = &maps.a1[set];
+        const CUtensorMap* tB0 = &maps.b0[set];
+        const CUtensorMap* tB1 = &maps.b1[set];
         for (int64_t kb = 0; kb < kbs; ++kb) {
           if (!bounded_wait(smem_u32(&empty_bar[s]), ph ^ 1, ctl, 1)) {
             ok = false;
@@ -255,11 +260,11 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_expect_tx(fb, STAGE_BYTES);
           const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
           const int kc = (int)(kb * BK);
-          tma_load_2d(base, &tmA0, ak + kc, ar, fb);
-          if (NA == 2) tma_load_2d(base + A_BYTES, &tmA1, ak + kc, ar, fb);
+          tma_load_2d(base, tA0, ak + kc, ar, fb);
+          if (NA == 2) tma_load_2d(base + A_BYTES, tA1, ak + kc, ar, fb);
           const uint32_t bbase = base + NA * A_BYTES;
-          tma_load_2d(bbase, &tmB0, bk + kc, br, fb);
-          if (NB == 2) tma_load_2d(bbase + B_BYTES, &tmB1, bk + kc, br, fb);
+          tma_load_2d(bbase, tB0, bk + kc, br, fb);
+          if (NB == 2) tma_load_2d(bbase + B_BYTES, tB1, bk + kc, br, fb);
           ++issued;
           if (++s == STAGES) {
             s = 0;
@@ -296,9 +301,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!bounded_wait(smem_u32(&tempty_bar[acc]), aph ^ 1, ctl, 2)) break;
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
-        int ar, ak, br, bk;
+        int ar, ak, br, bk, set;
         int64_t kbs;
-        coords(t, ar, ak, br, bk, kbs);
+        coords(t, ar, ak, br, bk, kbs, set);
         for (int64_t kb = 0; kb < kbs; ++kb) {
           if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3)) {
             ok = false;
@@ -390,6 +395,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 // combine kernel turns them into lse_p, the new scaling and sum P log P.
 struct EpiMax {
   static constexpr bool kListed = false;
+  static constexpr int kSets = 1;
   static constexpr int kSmemBytes = BN * 8;
   MaxEpiArgs a;
   int64_t n0, ntile, p;
@@ -489,6 +495,7 @@ __device__ __forceinline__ void red_add_v2(float2* p, float x, float y) {
 // compress: row = rotation, column = active pixel; inserts into model/weight.
 struct EpiCmp {
   static constexpr bool kListed = false;
+  static constexpr int kSets = 1;
   static constexpr int kSmemBytes = BN * 16;
   CmpEpiArgs a;
   int64_t j0;
@@ -557,6 +564,7 @@ struct EpiCmp {
 // poisson LL = x - phi_p sum W_r, gaussian cross term x.
 struct EpiGMax {
   static constexpr bool kListed = true;
+  static constexpr int kSets = 1;
   static constexpr int kSmemBytes = BN * 8;
   GMaxEpiArgs a;
   TileDesc d;
@@ -618,6 +626,7 @@ struct EpiGMax {
 // weight rotw T_r as in EpiCmp.
 struct EpiGCmp {
   static constexpr bool kListed = true;
+  static constexpr int kSets = 1;
   static constexpr int kSmemBytes = BN * 16;
   GCmpEpiArgs a;
   TileDesc d;
@@ -681,11 +690,64 @@ struct EpiGCmp {
   __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
 };
 
+inline TmapSet<1> one_set(const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
+                          const CUtensorMap& b1) {
+  TmapSet<1> m;
+  m.a0[0] = a0;
+  m.a1[0] = a1;
+  m.b0[0] = b0;
+  m.b1[0] = b1;
+  return m;
+}
+
+// Several datasets in one launch: the tile list's `set` selects the tensor
+// maps and the epilogue arguments of its dataset; `local0` is the tile's row
+// tile and `cell` its column tile, so the single-dataset epilogues run as
+// they are.
+struct EpiBatchMax {
+  static constexpr bool kListed = true;
+  static constexpr int kSets = kMaxBatch;
+  static constexpr int kSmemBytes = EpiMax::kSmemBytes;
+  BatchMaxArgs a;
+  EpiMax inner;
+  int64_t row0;
+
+  __device__ void tile_begin(int64_t t, int64_t, int tid, uint8_t* smem) {
+    const TileDesc d = a.tiles[t];
+    inner.a = a.set[d.set];
+    row0 = (int64_t)d.local0 * BM;
+    inner.tile_begin(d.local0, d.cell, tid, smem);
+  }
+  __device__ void row_begin(int64_t row) { inner.row_begin(row0 + row % BM); }
+  __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) { inner.consume(c, v, smem); }
+  __device__ void row_end() { inner.row_end(); }
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
+};
+
+struct EpiBatchCmp {
+  static constexpr bool kListed = true;
+  static constexpr int kSets = kMaxBatch;
+  static constexpr int kSmemBytes = EpiCmp::kSmemBytes;
+  BatchCmpArgs a;
+  EpiCmp inner;
+  int64_t row0;
+
+  __device__ void tile_begin(int64_t t, int64_t, int tid, uint8_t* smem) {
+    const TileDesc d = a.tiles[t];
+    inner.a = a.set[d.set];
+    row0 = (int64_t)d.local0 * BM;
+    inner.tile_begin(d.local0, d.cell, tid, smem);
+  }
+  __device__ void row_begin(int64_t row) { inner.row_begin(row0 + row % BM); }
+  __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) { inner.consume(c, v, smem); }
+  __device__ void row_end() { inner.row_end(); }
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
+};
+
 template <int NA, int NB, int STAGES, bool M_INNER, int BK, class Epi>
-cudaError_t run_gemm(const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
-                     const CUtensorMap& b1, int64_t m_tiles, int64_t n_tiles, int64_t k_blocks,
-                     const Epi& epi, TcStatus* st, int num_sms, cudaStream_t stream,
-                     int raster = 1) {
+cudaError_t run_gemm(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n_tiles,
+                     int64_t k_blocks, const Epi& epi, TcStatus* st, int num_sms,
+                     cudaStream_t stream, int raster = 1) {
   if (raster < 1) raster = 1;
   constexpr uint32_t stage = NA * BM * BK * 2 + NB * BN * BK * 2;
   const size_t dyn = (size_t)STAGES * stage + 1024;
@@ -695,8 +757,7 @@ cudaError_t run_gemm(const CUtensorMap& a0, const CUtensorMap& a1, const CUtenso
   const int64_t tiles = m_tiles * n_tiles;
   if (tiles == 0) return cudaSuccess;
   const int grid = (int)(tiles < num_sms ? tiles : num_sms);
-  kern<<<grid, kThreads, dyn, stream>>>(a0, a1, b0, b1, m_tiles, n_tiles, k_blocks, raster, epi,
-                                        st);
+  kern<<<grid, kThreads, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks, raster, epi, st);
   return cudaGetLastError();
 }
 
@@ -1023,7 +1084,7 @@ cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
   // 2 x 16 KB); pattern tiles are the inner index, so the CTAs in flight share
   // each rotation tile in L2.  K-steps of 32 (64-byte rows) keep five 40 KB
   // stages in flight.
-  return run_gemm<1, 2, 5, true, kMaximizeBK>(tmK, tmK, tmBhi, tmBlo, Mpad / BM, Rpad / BN,
+  return run_gemm<1, 2, 5, true, kMaximizeBK>(one_set(tmK, tmK, tmBhi, tmBlo), Mpad / BM, Rpad / BN,
                                               Kpad / kMaximizeBK, epi, status, num_sms, st,
                                               raster);
 }
@@ -1035,7 +1096,7 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
   EpiCmp epi;
   epi.a = e;
   // pixel tiles are the inner index: CTAs in flight share the P' tiles
-  return run_gemm<2, 1, 3, false, kCompressBK>(tmPhi, tmPlo, tmKt, tmKt, Rpad / BM, Ppad / BN,
+  return run_gemm<2, 1, 3, false, kCompressBK>(one_set(tmPhi, tmPlo, tmKt, tmKt), Rpad / BM, Ppad / BN,
                                                Npad / kCompressBK, epi, status, num_sms, st,
                                                raster);
 }
@@ -1046,7 +1107,7 @@ cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap&
                                      cudaStream_t st) {
   EpiGMax epi;
   epi.a = e;
-  return run_gemm<1, 2, 5, true, kMaximizeBK>(tmKg, tmKg, tmBhi, tmBlo, n_tiles, 1, 0, epi,
+  return run_gemm<1, 2, 5, true, kMaximizeBK>(one_set(tmKg, tmKg, tmBhi, tmBlo), n_tiles, 1, 0, epi,
                                               status, num_sms, st);
 }
 
@@ -1056,8 +1117,24 @@ cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap
                                      cudaStream_t st) {
   EpiGCmp epi;
   epi.a = e;
-  return run_gemm<2, 1, 3, false, kCompressBK>(tmAhi, tmAlo, tmKgT, tmKgT, n_tiles, 1, 0, epi,
+  return run_gemm<2, 1, 3, false, kCompressBK>(one_set(tmAhi, tmAlo, tmKgT, tmKgT), n_tiles, 1, 0, epi,
                                                status, num_sms, st);
+}
+
+cudaError_t launch_batch_maximize_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                     const BatchMaxArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st) {
+  EpiBatchMax epi;
+  epi.a = e;
+  return run_gemm<1, 2, 5, true, kMaximizeBK>(maps, n_tiles, 1, 0, epi, status, num_sms, st);
+}
+
+cudaError_t launch_batch_compress_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                     const BatchCmpArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st) {
+  EpiBatchCmp epi;
+  epi.a = e;
+  return run_gemm<2, 1, 3, false, kCompressBK>(maps, n_tiles, 1, 0, epi, status, num_sms, st);
 }
 
 cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {

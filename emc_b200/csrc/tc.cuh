@@ -76,7 +76,14 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
 // tile's first row inside the group.
 struct TileDesc {
   int32_t a_row, a_k0, b_row, b_k0;
-  int32_t k_blocks, cell, local0, pad;
+  int32_t k_blocks, cell, local0, set;  // set: tensor maps / epilogue of the tile's dataset
+};
+
+// The four operand tensor maps of a contraction (A, A's hi/lo partner, B,
+// B's partner), NSET sets for launches over several datasets.
+template <int NSET>
+struct TmapSet {
+  CUtensorMap a0[NSET], a1[NSET], b0[NSET], b1[NSET];
 };
 
 // Grouped maximize: acc[slot][member] = sum_j Kg[slot][j] (B_hi + B_lo)[mbeg_c + member][j]
@@ -118,6 +125,25 @@ struct GCmpEpiArgs {
 cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap& tmAlo,
                                      const CUtensorMap& tmKgT, int64_t n_tiles,
                                      const GCmpEpiArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st);
+
+// Several datasets (contexts) in one persistent launch of each contraction:
+// a tile list over all of them (set = dataset, local0 = row tile, cell =
+// column tile) and each dataset's epilogue arguments.
+constexpr int kMaxBatch = 8;
+struct BatchMaxArgs {
+  const TileDesc* tiles;
+  MaxEpiArgs set[kMaxBatch];
+};
+struct BatchCmpArgs {
+  const TileDesc* tiles;
+  CmpEpiArgs set[kMaxBatch];
+};
+cudaError_t launch_batch_maximize_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                     const BatchMaxArgs& e, TcStatus* status, int num_sms,
+                                     cudaStream_t st);
+cudaError_t launch_batch_compress_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                     const BatchCmpArgs& e, TcStatus* status, int num_sms,
                                      cudaStream_t st);
 
 // Responsibility pass of the mixed path: combine the tile partials per

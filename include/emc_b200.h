@@ -145,6 +145,27 @@ int64_t emc_active_pixels(const emc_context *ctx);
 emc_status emc_orientation_stats(emc_context *ctx, int32_t *best_rot, float *best_resp,
                                  float *avg_resp);
 
+/* ---- several datasets in one launch ----
+ * Up to 8 mixed-precision contexts on one device (each set up with its own
+ * geometry, rotations, patterns and model; detector sizes may differ) iterate
+ * together: both contractions run as one persistent launch over a tile list
+ * spanning every dataset (costliest tiles first), the per-dataset stages
+ * between them on one shared stream.  The contexts keep that stream until
+ * emc_batch_destroy; their own calls (get_model, ...) stay ordered with the
+ * batch.  emc_batch_capture records one batched iteration into a CUDA graph;
+ * emc_batch_launch replays it.  Destroy a batch before its contexts. */
+typedef struct emc_batch emc_batch;
+emc_status emc_batch_create(emc_context *const *ctxs, int32_t n, emc_batch **out);
+emc_status emc_batch_destroy(emc_batch *batch);
+/* Enqueue one iteration of every dataset (no host synchronisation). */
+emc_status emc_batch_iterate(emc_batch *batch);
+emc_status emc_batch_capture(emc_batch *batch);
+emc_status emc_batch_launch(emc_batch *batch, int32_t iterations);
+/* Wait for the batch's stream; reports device wait timeouts of its kernels. */
+emc_status emc_batch_synchronize(emc_batch *batch);
+void *emc_batch_stream(emc_batch *batch);
+const char *emc_batch_last_error(const emc_batch *batch);
+
 /* Tile order of the two tensor-core contractions (mixed precision): the
  * persistent CTAs walk the output tiles in bands of `raster` rotation tiles,
  * the other index fastest, so operand tiles loaded from HBM are shared
