@@ -1405,6 +1405,8 @@ struct emc_batch {
   cudaStream_t st = nullptr;
   TileDesc *d_mt = nullptr, *d_ct = nullptr;
   int64_t n_mt = 0, n_ct = 0;
+  MaxEpiArgs* d_max = nullptr;  // per-dataset epilogue arguments (fixed per context)
+  CmpEpiArgs* d_cmp = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::string err;
@@ -1440,6 +1442,8 @@ emc_status emc_batch_destroy(emc_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->d_mt) cudaFree(b->d_mt);
   if (b->d_ct) cudaFree(b->d_ct);
+  if (b->d_max) cudaFree(b->d_max);
+  if (b->d_cmp) cudaFree(b->d_cmp);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
   return EMC_OK;
@@ -1476,26 +1480,47 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
   for (int32_t i = 0; i < n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(),
                    [&](int32_t x, int32_t y) { return ctxs[x]->Ppad > ctxs[y]->Ppad; });
+  // the order of the single-dataset launch (tile_mn in kernels_tc.cu): the
+  // inner index fastest, in bands of `raster` outer tiles
+  auto banded = [](int64_t inner, int64_t outer, int64_t raster, auto&& emit) {
+    raster = raster < 1 ? 1 : raster;
+    for (int64_t o0 = 0; o0 < outer; o0 += raster) {
+      const int64_t g = outer - o0 < raster ? outer - o0 : raster;
+      for (int64_t w = 0; w < g * inner; ++w) emit(w / g, o0 + w % g);
+    }
+  };
   for (int32_t i : order) {
     const emc_context* c = ctxs[i];
-    for (int64_t nt = 0; nt < c->Rpad / 256; ++nt)
-      for (int64_t m = 0; m < c->Npad / 128; ++m)
-        mt.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
-                              (int32_t)(c->Ppad / kMaximizeBK), (int32_t)nt, (int32_t)m, i});
+    banded(c->Npad / 128, c->Rpad / 256, c->tune.maximize_raster, [&](int64_t m, int64_t nt) {
+      mt.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
+                            (int32_t)(c->Ppad / kMaximizeBK), (int32_t)nt, (int32_t)m, i});
+    });
   }
   std::stable_sort(order.begin(), order.end(),
                    [&](int32_t x, int32_t y) { return ctxs[x]->Npad > ctxs[y]->Npad; });
   for (int32_t i : order) {
     const emc_context* c = ctxs[i];
-    for (int64_t m = 0; m < c->Rpad / 128; ++m)
-      for (int64_t nt = 0; nt < c->Ppad / 256; ++nt)
-        ct.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
-                              (int32_t)(c->Npad / kCompressBK), (int32_t)nt, (int32_t)m, i});
+    banded(c->Ppad / 256, c->Rpad / 128, c->tune.compress_raster, [&](int64_t nt, int64_t m) {
+      ct.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
+                            (int32_t)(c->Npad / kCompressBK), (int32_t)nt, (int32_t)m, i});
+    });
   }
   b->n_mt = (int64_t)mt.size();
   b->n_ct = (int64_t)ct.size();
+  std::vector<MaxEpiArgs> me(n);
+  std::vector<CmpEpiArgs> ce(n);
+  for (int32_t i = 0; i < n; ++i) {
+    me[i] = max_args(ctxs[i]);
+    ce[i] = cmp_args(ctxs[i]);
+  }
   emc_status s = EMC_OK;
-  if ((s = b->cuda(cudaMalloc(&b->d_mt, sizeof(TileDesc) * mt.size()), "cudaMalloc")) != EMC_OK ||
+  if ((s = b->cuda(cudaMalloc(&b->d_max, sizeof(MaxEpiArgs) * n), "cudaMalloc")) != EMC_OK ||
+      (s = b->cuda(cudaMalloc(&b->d_cmp, sizeof(CmpEpiArgs) * n), "cudaMalloc")) != EMC_OK ||
+      (s = b->cuda(cudaMemcpy(b->d_max, me.data(), sizeof(MaxEpiArgs) * n,
+                              cudaMemcpyHostToDevice), "epilogue arguments")) != EMC_OK ||
+      (s = b->cuda(cudaMemcpy(b->d_cmp, ce.data(), sizeof(CmpEpiArgs) * n,
+                              cudaMemcpyHostToDevice), "epilogue arguments")) != EMC_OK ||
+      (s = b->cuda(cudaMalloc(&b->d_mt, sizeof(TileDesc) * mt.size()), "cudaMalloc")) != EMC_OK ||
       (s = b->cuda(cudaMalloc(&b->d_ct, sizeof(TileDesc) * ct.size()), "cudaMalloc")) != EMC_OK ||
       (s = b->cuda(cudaMemcpy(b->d_mt, mt.data(), sizeof(TileDesc) * mt.size(),
                               cudaMemcpyHostToDevice), "tile list")) != EMC_OK ||
@@ -1516,14 +1541,15 @@ emc_status emc_batch_iterate(emc_batch* b) {
   BatchMaxArgs me{};
   BatchCmpArgs ce{};
   me.tiles = b->d_mt;
+  me.set = b->d_max;
   ce.tiles = b->d_ct;
+  ce.set = b->d_cmp;
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];
     if (c->stage != 0) return b->fail(EMC_ERR_STATE, "a dataset is between stages");
     BTRY(b, c, emc_expand(c));
     BCK(b, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * c->N,
                            cudaMemcpyDeviceToDevice, b->st));
-    me.set[i] = max_args(c);
     maps.a0[i] = c->tmKh;
     maps.a1[i] = c->tmKh;
     maps.b0[i] = c->tmBhi;
@@ -1542,7 +1568,6 @@ emc_status emc_batch_iterate(emc_batch* b) {
     c->resp_source = 1;
     c->stage = 2;
     BCK(b, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, b->st));
-    ce.set[i] = cmp_args(c);
     maps.a0[i] = c->tmPhi;
     maps.a1[i] = c->tmPlo;
     maps.b0[i] = c->tmKt;

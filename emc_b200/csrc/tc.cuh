@@ -133,11 +133,11 @@ cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap
 constexpr int kMaxBatch = 8;
 struct BatchMaxArgs {
   const TileDesc* tiles;
-  MaxEpiArgs set[kMaxBatch];
+  const MaxEpiArgs* set;  // device array, one per dataset
 };
 struct BatchCmpArgs {
   const TileDesc* tiles;
-  CmpEpiArgs set[kMaxBatch];
+  const CmpEpiArgs* set;  // device array, one per dataset
 };
 cudaError_t launch_batch_maximize_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
                                      const BatchMaxArgs& e, TcStatus* status, int num_sms,

@@ -46,6 +46,22 @@ WORKLOADS = {
 }
 
 
+# Batched case: six independent datasets of different detector sizes
+# (48 ... 128 px, 2k ... 20k patterns), each with its model side equal to the
+# detector side and an orientation sampling proportional to it (600-cell n
+# from 5 at 48 px to 12 at 128 px), beamstop radius 6 and 500 photons on
+# average as in large128.
+BATCH6 = [Workload(f"batch{s}", s, n, N, 500.0, 0.5, 6.0, 1, seed=10 + i)
+          for i, (s, n, N) in enumerate([(48, 5, 2000), (64, 6, 5000), (80, 8, 8000),
+                                         (96, 9, 11000), (112, 10, 14000), (128, 12, 20000)])]
+
+
+# The same detector sizes with 500 patterns and 3,240 rotations each: a
+# dataset whose contractions alone fill about a third of the GPU.
+BATCH6_SMALL = [Workload(f"small{s}", s, 4, 500, 500.0, 0.5, 6.0, 1, seed=20 + i)
+                for i, s in enumerate([48, 64, 80, 96, 112, 128])]
+
+
 def pixel_size(side: int) -> float:
     return math.tan(math.radians(EDGE_ANGLE_DEG)) * DISTANCE / (side / 2)
 
