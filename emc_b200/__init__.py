@@ -47,7 +47,8 @@ class IterStats(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("maximize_raster", C.c_int32), ("compress_raster", C.c_int32)]
+    _fields_ = [("maximize_raster", C.c_int32), ("compress_raster", C.c_int32),
+                ("maximize_pair", C.c_int32)]
 
 
 class SynthConfig(C.Structure):
@@ -374,13 +375,15 @@ class Context:
         return {"best_rot": best, "best_resp": bp, "avg_resp": avg}
 
     def get_tuning(self):
-        """(maximize_raster, compress_raster) of the tensor-core tile orders."""
+        """(maximize_raster, compress_raster, maximize_pair) of the tensor-core kernels."""
         t = Tuning()
         self._c(lib().emc_get_tuning(self._h, C.byref(t)))
-        return t.maximize_raster, t.compress_raster
+        return t.maximize_raster, t.compress_raster, t.maximize_pair
 
-    def set_tuning(self, maximize_raster, compress_raster):
-        t = Tuning(maximize_raster, compress_raster)
+    def set_tuning(self, maximize_raster, compress_raster, maximize_pair=None):
+        if maximize_pair is None:
+            maximize_pair = self.get_tuning()[2]
+        t = Tuning(maximize_raster, compress_raster, int(maximize_pair))
         self._c(lib().emc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, candidates=(1, 2, 4, 8, 16)):

@@ -761,6 +761,313 @@ cudaError_t run_gemm(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n
   return cudaGetLastError();
 }
 
+// ---------------------------------------------- two-SM maximize contraction --
+// The maximize contraction on SM pairs (cta_group::2, cluster of 2): a pair
+// computes a 256-pattern x 256-rotation tile with one tcgen05.mma per 16-wide
+// K step and operand half; each CTA loads its 128 patterns of the counts and
+// its 128 rotations of the hi and lo slice operand, so every SM moves half
+// the slice bytes of the one-SM kernel through shared memory, which leaves
+// room for 128-byte K-steps (4 stages of 48 KB).  The leader (rank 0) issues
+// the MMAs; both CTAs' TMA loads complete on the leader's barriers; the
+// leader's commits release both CTAs' stages and accumulators; each CTA's
+// epilogue drains its own 128 TMEM lanes (its patterns) x 256 rotations.
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// Address of the same shared-memory object in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t peer_addr(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// TMA load into this CTA's shared memory completing on the pair leader's barrier.
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* tm, int c0, int c1,
+                                                 uint32_t bar_cluster) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"((uint64_t)tm), "r"(c0), "r"(c1), "r"(bar_cluster)
+      : "memory");
+}
+__device__ __forceinline__ void mma_f16_pair(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                             uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accum)
+      : "memory");
+}
+// Arrive on an mbarrier (this CTA's or the peer's, shared::cluster address)
+// once every MMA this thread issued before has completed.
+__device__ __forceinline__ void mma_commit_pair(uint32_t bar_cluster) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar_cluster)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster)
+               : "memory");
+}
+
+// M = 256 (the pair), N = 256.
+constexpr uint32_t kIdescPair = (1u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+constexpr int kPairBK = 64;
+constexpr int kPairStages = 4;
+
+template <class Epi>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    tc_pair_maximize_kernel(const __grid_constant__ CUtensorMap tmA,
+                            const __grid_constant__ CUtensorMap tmB0,
+                            const __grid_constant__ CUtensorMap tmB1, const int64_t m_tiles,
+                            const int64_t n_tiles, const int64_t k_blocks, const int raster,
+                            const Epi epi, TcStatus* status) {
+  constexpr uint32_t A_BYTES = 128 * kPairBK * 2;   // this CTA's 128 patterns
+  constexpr uint32_t B_BYTES = 128 * kPairBK * 2;   // this CTA's 128 rotations, per half
+  constexpr uint32_t STAGE_BYTES = A_BYTES + 2 * B_BYTES;
+  constexpr int STAGES = kPairStages;
+  extern __shared__ uint8_t dyn_smem[];
+  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t tfull_bar[2], tempty_bar[2], drain_bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  __shared__ int epi_abort;
+  __shared__ __align__(16) uint8_t epi_smem[Epi::kSmemBytes];
+
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) &
+                                             ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  Ctl ctl{&abort_flag, status};
+  // stop the peer too: its waits then end at their next check
+  auto abort_pair = [&]() {
+    abort_flag = 1;
+    const uint32_t pa = peer_addr(smem_u32(&abort_flag), rank ^ 1u);
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(pa), "r"(1) : "memory");
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(smem_u32(&full_bar[s]), 1);
+      mbar_init(smem_u32(&empty_bar[s]), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(smem_u32(&tfull_bar[a]), 1);
+      mbar_init(smem_u32(&tempty_bar[a]), 2);  // one arrival per CTA's epilogue
+    }
+    mbar_init(smem_u32(&drain_bar), 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs' barriers exist before any remote arrival or load
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const int64_t num_tiles = m_tiles * n_tiles;
+  const int64_t cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
+
+  // pattern tiles (of 256) fastest, in bands of `raster` rotation tiles
+  auto tile_mn = [&](int64_t t, int64_t& m, int64_t& n) {
+    const int64_t span = (int64_t)raster * m_tiles;
+    const int64_t band = t / span;
+    const int64_t o0 = band * raster;
+    const int64_t g = n_tiles - o0 < raster ? n_tiles - o0 : raster;
+    const int64_t w = t - band * span;
+    n = o0 + w % g;
+    m = w / g;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ------------------------------------------------ TMA producer (both CTAs)
+      int s = 0;
+      uint32_t ph = 0;
+      int64_t issued = 0;
+      bool ok = true;
+      for (int64_t t = cid; t < num_tiles && ok; t += ncl) {
+        int64_t mt, nt;
+        tile_mn(t, mt, nt);
+        const int ar = (int)(mt * 256 + rank * 128), br = (int)(nt * 256 + rank * 128);
+        for (int64_t kb = 0; kb < k_blocks; ++kb) {
+          if (!bounded_wait(smem_u32(&empty_bar[s]), ph ^ 1, ctl, 1)) {
+            ok = false;
+            break;
+          }
+          const uint32_t fb = smem_u32(&full_bar[s]);
+          if (leader) mbar_expect_tx(fb, 2 * STAGE_BYTES);  // both CTAs' bytes
+          const uint32_t fb_leader = peer_addr(fb, 0);
+          const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
+          const int kc = (int)(kb * kPairBK);
+          tma_load_2d_pair(base, &tmA, kc, ar, fb_leader);
+          tma_load_2d_pair(base + A_BYTES, &tmB0, kc, br, fb_leader);
+          tma_load_2d_pair(base + A_BYTES + B_BYTES, &tmB1, kc, br, fb_leader);
+          ++issued;
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+      }
+      if (!ok) {
+        abort_pair();
+        if (leader) {
+          // the last min(issued, STAGES) stages must land (both CTAs' bytes
+          // complete on these barriers) before the pair exits
+          int64_t n = issued < STAGES ? issued : STAGES;
+          int ss = s;
+          uint32_t pp = ph;
+          for (int64_t i = 0; i < n; ++i) {
+            if (--ss < 0) {
+              ss = STAGES - 1;
+              pp ^= 1;
+            }
+            const uint64_t t0 = globaltimer();
+            while (!mbar_test(smem_u32(&full_bar[ss]), pp) && globaltimer() - t0 < kWaitLimitNs) {
+            }
+          }
+        } else {
+          // the peer cannot observe its loads; give them time to land
+          const uint64_t t0 = globaltimer();
+          while (globaltimer() - t0 < 2000000ull) {
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && leader) {
+      // ------------------------------------------------ MMA issuer (leader)
+      int s = 0;
+      uint32_t ph = 0;
+      int64_t i = 0;
+      bool ok = true;
+      for (int64_t t = cid; t < num_tiles && ok; t += ncl, ++i) {
+        const int acc = (int)(i & 1);
+        const uint32_t aph = (uint32_t)((i >> 1) & 1);
+        if (!bounded_wait(smem_u32(&tempty_bar[acc]), aph ^ 1, ctl, 2)) {
+          abort_pair();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * BN);
+        for (int64_t kb = 0; kb < k_blocks; ++kb) {
+          if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3)) {
+            ok = false;
+            abort_pair();
+            break;
+          }
+          tc_fence_after();
+          const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
+#pragma unroll
+          for (int k = 0; k < kPairBK / 16; ++k) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+              mma_f16_pair(d, sdesc<kPairBK>(base + k * 32),
+                           sdesc<kPairBK>(base + A_BYTES + q * B_BYTES + k * 32), kIdescPair,
+                           (kb | k | q) != 0);
+          }
+          // release this stage in both CTAs once its MMAs are done
+          const uint32_t eb = smem_u32(&empty_bar[s]);
+          mma_commit_pair(peer_addr(eb, 0));
+          mma_commit_pair(peer_addr(eb, 1));
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+        if (ok) {
+          const uint32_t tb = smem_u32(&tfull_bar[acc]);
+          mma_commit_pair(peer_addr(tb, 0));
+          mma_commit_pair(peer_addr(tb, 1));
+        }
+      }
+      mma_commit_pair(peer_addr(smem_u32(&drain_bar), 0));
+      const uint64_t t0 = globaltimer();
+      while (!mbar_test(smem_u32(&drain_bar), 0) && globaltimer() - t0 < kWaitLimitNs) {
+      }
+    }
+  } else {
+    // -------------------------------------------------- epilogue warps (both CTAs)
+    const int quarter = warp & 3;
+    const int ep_tid = threadIdx.x - 64;
+    Epi e = epi;
+    int64_t i = 0;
+    const uint32_t tempty_leader0 = peer_addr(smem_u32(&tempty_bar[0]), 0);
+    const uint32_t tempty_leader1 = peer_addr(smem_u32(&tempty_bar[1]), 0);
+    for (int64_t t = cid; t < num_tiles; t += ncl, ++i) {
+      const int acc = (int)(i & 1);
+      const uint32_t aph = (uint32_t)((i >> 1) & 1);
+      bounded_wait(smem_u32(&tfull_bar[acc]), aph, ctl, 4);
+      epi_bar();
+      if (ep_tid == 0) epi_abort = abort_flag;
+      epi_bar();
+      if (epi_abort) break;
+      tc_fence_after();
+      int64_t mt, nt;
+      tile_mn(t, mt, nt);
+      const int64_t mrow = mt * 2 + rank;  // this CTA's 128-pattern block
+      e.tile_begin(mrow, nt, ep_tid, epi_smem);
+      e.row_begin(mrow * BM + quarter * 32 + lane);
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
+#pragma unroll 1
+      for (int c = 0; c < BN; c += 16) {
+        uint32_t v[16];
+        tmem_ld16(taddr + c, v);
+        tmem_ld_wait();
+        e.consume(c, v, epi_smem);
+      }
+      e.row_end();
+      tc_fence_before();
+      epi_bar();  // the whole accumulator of this CTA has been read
+      if (ep_tid == 0) mbar_arrive_cluster(acc ? tempty_leader1 : tempty_leader0);
+      e.tile_end(mt, nt, ep_tid, epi_smem);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // neither CTA leaves while the pair's MMAs or loads may touch it
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+template <class Epi>
+cudaError_t run_pair_maximize(const CUtensorMap& a, const CUtensorMap& b0, const CUtensorMap& b1,
+                              int64_t m_tiles, int64_t n_tiles, int64_t k_blocks, const Epi& epi,
+                              TcStatus* st, int num_sms, cudaStream_t stream, int raster) {
+  constexpr uint32_t stage = 128 * kPairBK * 2 * 3;
+  const size_t dyn = (size_t)kPairStages * stage + 1024;
+  auto kern = tc_pair_maximize_kernel<Epi>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return e;
+  const int64_t tiles = m_tiles * n_tiles;
+  if (tiles == 0) return cudaSuccess;
+  const int64_t pairs = num_sms / 2;
+  const int grid = 2 * (int)(tiles < pairs ? tiles : pairs);
+  kern<<<grid, kThreads, dyn, stream>>>(a, b0, b1, m_tiles, n_tiles, k_blocks,
+                                        raster < 1 ? 1 : raster, epi, st);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------ responsibility pass --
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -1087,6 +1394,18 @@ cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
   return run_gemm<1, 2, 5, true, kMaximizeBK>(one_set(tmK, tmK, tmBhi, tmBlo), Mpad / BM, Rpad / BN,
                                               Kpad / kMaximizeBK, epi, status, num_sms, st,
                                               raster);
+}
+
+cudaError_t launch_maximize_pair_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
+                                    const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
+                                    int64_t Kpad, const MaxEpiArgs& e, TcStatus* status,
+                                    int num_sms, cudaStream_t st, int raster) {
+  EpiMax epi;
+  epi.a = e;
+  // 256-pattern pair tiles (the last may reach past Mpad: zero-filled by TMA,
+  // masked by the epilogue), 64-wide K-steps
+  return run_pair_maximize(tmK, tmBhi, tmBlo, (Mpad + 255) / 256, Rpad / BN, Kpad / kPairBK, epi,
+                           status, num_sms, st, raster);
 }
 
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,

@@ -49,6 +49,15 @@ cudaError_t launch_maximize_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
                                int64_t Kpad, const MaxEpiArgs& e, TcStatus* status,
                                int num_sms, cudaStream_t st, int raster);
 
+// The same contraction on SM pairs (cta_group::2): 256 patterns x 256
+// rotations per pair, 64-wide K-steps; the tensor maps have boxes of 128 rows
+// x 64 (kPairBoxK) for the counts and for each half of the slice operand.
+constexpr int kPairBoxK = 64;
+cudaError_t launch_maximize_pair_tc(const CUtensorMap& tmK, const CUtensorMap& tmBhi,
+                                    const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
+                                    int64_t Kpad, const MaxEpiArgs& e, TcStatus* status,
+                                    int num_sms, cudaStream_t st, int raster);
+
 // Compress contraction: acc[r][j] = sum_p (P'_hi + P'_lo)[r][p] Kt[j][p] with
 // P' = c0 P / (T_r phi_p), i.e. the averaged slice U_r / T_r; 128 rotations x
 // 256 pixels per tile, inserted in the epilogue.

@@ -172,13 +172,16 @@ const char *emc_batch_last_error(const emc_batch *batch);
  * through L2 by the CTAs in flight.  1 = plain row order. */
 typedef struct {
   int32_t maximize_raster, compress_raster;
+  int32_t maximize_pair; /* 1: the maximize contraction on SM pairs (cta_group::2) */
 } emc_tuning;
 emc_status emc_get_tuning(const emc_context *ctx, emc_tuning *t);
 emc_status emc_set_tuning(emc_context *ctx, const emc_tuning *t);
-/* Autotuner: one iteration per candidate band size (both contractions at
- * once, timed by stage events) from the current model and scaling, which are
- * restored afterwards; keeps the fastest candidate of each contraction.
- * ms (optional): [2][n], maximize then compress times.  FP32 contexts: no-op. */
+/* Autotuner: two iterations per candidate band size (the maximize on one SM
+ * and on SM pairs; both contractions timed by stage events) from the current
+ * model and scaling, which are restored afterwards; keeps the fastest band
+ * size of each contraction and the faster maximize form.  ms (optional):
+ * [2][n], the best maximize then compress time per candidate.  FP32
+ * contexts: no-op. */
 emc_status emc_autotune(emc_context *ctx, const int32_t *candidates, int32_t n, float *ms,
                         emc_tuning *best);
 
