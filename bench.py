@@ -41,10 +41,11 @@ sys.path.insert(0, REPO)
 METRIC = "pattern×rotation evals/s"
 UNIT = "evals/s"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
-# DRAM bytes (read + write) per launch of the maximize contraction on the
-# default workload (128^3, 86,520 rotations, 50,000 patterns), from the ncu
-# capture summarised in profiles/tc_gemm_dram_large128.md.
-MAXIMIZE_TRAFFIC_BYTES = 709_666_040_320 + 17_586_104_576
+# DRAM bytes (read + write) per launch of the maximize contraction (the
+# two-SM kernel the default workload selects) on the default workload (128^3,
+# 86,520 rotations, 50,000 patterns), from the ncu capture summarised in
+# profiles/tc_gemm_dram_large128.md.
+MAXIMIZE_TRAFFIC_BYTES = 671_161_542_400 + 17_579_778_304
 
 
 def parse():
@@ -505,7 +506,7 @@ def main():
     flops = 2.0 * N * R * npa
     achieved = flops / (gemm_ms / 1e3) / 1e12 if gemm_ms > 0 else None
     peak = pk["bf16_tflops_sustained"]
-    roof = {"bound": "tensor", "kernel": "maximize contraction (tcgen05, FP16 hi+lo)"
+    roof = {"bound": "tensor", "kernel": "maximize contraction (tcgen05 cta_group::2 pairs, FP16 hi+lo)"
             if a.precision == "mixed" else "maximize contraction (FP32 CUDA cores)",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if achieved else None,
