@@ -43,8 +43,8 @@ UNIT = "evals/s"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 # DRAM bytes (read + write) per launch of the maximize contraction (the
 # two-SM kernel the default workload selects) on the default workload (128^3,
-# 86,520 rotations, 50,000 patterns), from the ncu capture summarised in
-# profiles/tc_gemm_dram_large128.md.
+# 86,520 rotations, 50,000 patterns), measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, one pass).
 MAXIMIZE_TRAFFIC_BYTES = 671_161_542_400 + 17_579_778_304
 
 

@@ -157,6 +157,23 @@ struct emc_context {
     cudaEventRecord(ev[cur][i], st);
   }
 
+  // pinned host staging of the proposed iteration, reused between calls
+  void* hpin[6] = {nullptr};
+  size_t hcap[6] = {0};
+  template <class T>
+  T* pinned(int slot, size_t n) {
+    const size_t bytes = n * sizeof(T) + 16;
+    if (bytes > hcap[slot]) {
+      if (hpin[slot]) cudaFreeHost(hpin[slot]);
+      hpin[slot] = nullptr;
+      hcap[slot] = 0;
+      const size_t b = bytes + bytes / 4 + 4096;
+      if (cudaMallocHost(&hpin[slot], b) != cudaSuccess) return nullptr;
+      hcap[slot] = b;
+    }
+    return static_cast<T*>(hpin[slot]);
+  }
+
   emc_status fail(emc_status s, const char* fmt, ...) {
     char buf[512];
     va_list ap;
@@ -284,6 +301,8 @@ emc_status emc_destroy(emc_context* ctx) {
   for (auto& set : ctx->ev)
     for (auto& e : set)
       if (e) cudaEventDestroy(e);
+  for (void* h : ctx->hpin)
+    if (h) cudaFreeHost(h);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
   return EMC_OK;
@@ -1157,15 +1176,16 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     CK(c, launch_pattern_stats(c->d_S, nullptr, R, c->npa, c->npa, 1, c->d_rowstat, c->st));
   // candidate cells of every pattern and the proposal's mass on them
   CK(c, launch_select(probs, N, c->n_cells, m, mass_target, c->d_cand, c->d_mass, c->st));
-  std::vector<int32_t> cand(pairs);
-  std::vector<float> mass(N);
-  CK(c, cudaMemcpyAsync(cand.data(), c->d_cand, sizeof(int32_t) * pairs, cudaMemcpyDeviceToHost, c->st));
-  CK(c, cudaMemcpyAsync(mass.data(), c->d_mass, sizeof(float) * N, cudaMemcpyDeviceToHost, c->st));
+  int32_t* cand = c->pinned<int32_t>(0, pairs);
+  float* mass = c->pinned<float>(1, N);
+  if (!cand || !mass) return c->fail(EMC_ERR_OOM, "pinned host staging");
+  CK(c, cudaMemcpyAsync(cand, c->d_cand, sizeof(int32_t) * pairs, cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaMemcpyAsync(mass, c->d_mass, sizeof(float) * N, cudaMemcpyDeviceToHost, c->st));
   CK(c, cudaStreamSynchronize(c->st));
   double msum = 0.0, mmin = 1e300;
-  for (float v : mass) {
-    msum += v;
-    mmin = v < mmin ? v : mmin;
+  for (int64_t p = 0; p < N; ++p) {
+    msum += mass[p];
+    mmin = mass[p] < mmin ? mass[p] : mmin;
   }
   emc_proposal_stats st{};
   st.mean_mass = msum / (double)N;
@@ -1209,8 +1229,11 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     evals += (int64_t)gcnt[k] * c->h_mcnt[k];
     kw = std::max<int64_t>(kw, (gcnt[k] + 63) / 64 * 64);
   }
-  std::vector<int32_t> gpair(S, -1);
-  std::vector<int64_t> ppos(pairs, -1);
+  int32_t* gpair = c->pinned<int32_t>(2, S);
+  int64_t* ppos = c->pinned<int64_t>(3, pairs);
+  if (!gpair || !ppos) return c->fail(EMC_ERR_OOM, "pinned host staging");
+  std::fill(gpair, gpair + S, -1);
+  std::fill(ppos, ppos + pairs, (int64_t)-1);
   for (int64_t p = 0; p < N; ++p)
     for (int32_t i = 0; i < m; ++i) {
       const int32_t k = cand[p * m + i];
@@ -1226,21 +1249,31 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
   TRY(grow(c, &c->d_Yc, c->yc_cap, S * MM));
   TRY(grow(c, &c->d_Pt, c->pt_cap, evals));
   std::vector<int4> mt, ct;
-  std::vector<TileDesc> gmt, gct;
+  int64_t n_gmt = 0, n_gct = 0;
+  TileDesc *gmt = nullptr, *gct = nullptr;
   if (tc) {
     const int64_t ptiles = (c->npa + 255) / 256;
+    for (int32_t k = 0; k < n_cells; ++k)
+      if (gcnt[k] > 0) {
+        n_gmt += (gcnt[k] + 127) / 128;
+        n_gct += (int64_t)((c->h_mcnt[k] + 127) / 128) * ptiles;
+      }
+    gmt = c->pinned<TileDesc>(4, n_gmt);
+    gct = c->pinned<TileDesc>(5, n_gct);
+    if (!gmt || !gct) return c->fail(EMC_ERR_OOM, "pinned host staging");
+    int64_t im = 0, ic = 0;
     for (int32_t k = 0; k < n_cells; ++k) {
       if (gcnt[k] == 0) continue;
       for (int32_t q0 = 0; q0 < gcnt[k]; q0 += 128)
-        gmt.push_back(TileDesc{(int32_t)(gbeg[k] + q0), 0, (int32_t)c->h_mbeg[k], 0,
-                               (int32_t)(c->Ppad / kMaximizeBK), k, q0, 0});
+        gmt[im++] = TileDesc{(int32_t)(gbeg[k] + q0), 0, (int32_t)c->h_mbeg[k], 0,
+                             (int32_t)(c->Ppad / kMaximizeBK), k, q0, 0};
       for (int32_t r0 = 0; r0 < c->h_mcnt[k]; r0 += 128)
         for (int64_t nt = 0; nt < ptiles; ++nt)
-          gct.push_back(TileDesc{(int32_t)(c->h_mbeg[k] + r0), 0, (int32_t)(nt * 256),
-                                 (int32_t)gbeg[k], (gcnt[k] + 63) / 64, k, r0, 0});
+          gct[ic++] = TileDesc{(int32_t)(c->h_mbeg[k] + r0), 0, (int32_t)(nt * 256),
+                               (int32_t)gbeg[k], (gcnt[k] + 63) / 64, k, r0, 0};
     }
-    TRY(grow(c, &c->d_gmt, c->gmt_cap, (int64_t)gmt.size()));
-    TRY(grow(c, &c->d_gct, c->gct_cap, (int64_t)gct.size()));
+    TRY(grow(c, &c->d_gmt, c->gmt_cap, n_gmt));
+    TRY(grow(c, &c->d_gct, c->gct_cap, n_gct));
     TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
     if (S > c->kgt_ld) {
       if (c->d_KgT) c->release(c->d_KgT);
@@ -1262,8 +1295,8 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
       TRY(c->alloc(&c->d_Alo, R * ld));
       c->a_ld = ld;
     }
-    CK(c, cudaMemcpyAsync(c->d_gmt, gmt.data(), sizeof(TileDesc) * gmt.size(), cudaMemcpyHostToDevice, c->st));
-    CK(c, cudaMemcpyAsync(c->d_gct, gct.data(), sizeof(TileDesc) * gct.size(), cudaMemcpyHostToDevice, c->st));
+    CK(c, cudaMemcpyAsync(c->d_gmt, gmt, sizeof(TileDesc) * n_gmt, cudaMemcpyHostToDevice, c->st));
+    CK(c, cudaMemcpyAsync(c->d_gct, gct, sizeof(TileDesc) * n_gct, cudaMemcpyHostToDevice, c->st));
   } else {
     // CUDA-core grouped contractions: tile lists over the selected cells
     for (int32_t k = 0; k < n_cells; ++k) {
@@ -1278,8 +1311,8 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     CK(c, cudaMemcpyAsync(c->d_mtiles, mt.data(), sizeof(int4) * mt.size(), cudaMemcpyHostToDevice, c->st));
     CK(c, cudaMemcpyAsync(c->d_ctiles, ct.data(), sizeof(int4) * ct.size(), cudaMemcpyHostToDevice, c->st));
   }
-  CK(c, cudaMemcpyAsync(c->d_gpair, gpair.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, c->st));
-  CK(c, cudaMemcpyAsync(c->d_ppos, ppos.data(), sizeof(int64_t) * pairs, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_gpair, gpair, sizeof(int32_t) * S, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_ppos, ppos, sizeof(int64_t) * pairs, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_gbeg, gbeg.data(), sizeof(int64_t) * n_cells, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_gcnt, gcnt.data(), sizeof(int32_t) * n_cells, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_goff, goff.data(), sizeof(int64_t) * n_cells, cudaMemcpyHostToDevice, c->st));
@@ -1354,7 +1387,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     ge.rowstat = c->d_rowstat;
     ge.Y = c->d_Yc;
     ge.ldY = MM;
-    CK(c, launch_group_maximize_tc(tmKg, c->tmBhi, c->tmBlo, (int64_t)gmt.size(), ge, c->d_status,
+    CK(c, launch_group_maximize_tc(tmKg, c->tmBhi, c->tmBlo, n_gmt, ge, c->d_status,
                                    c->num_sms, c->st));
     c->mark(2);
     CK(c, launch_group_softmax(g, c->st));
@@ -1375,7 +1408,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     ce.cz = c->d_cz;
     ce.ins = c->d_ins;
     ce.acc = c->d_acc;
-    CK(c, launch_group_compress_tc(tmAhi, tmAlo, tmKgT, (int64_t)gct.size(), ce, c->d_status,
+    CK(c, launch_group_compress_tc(tmAhi, tmAlo, tmKgT, n_gct, ce, c->d_status,
                                    c->num_sms, c->st));
     launches = 6;  // gather (2), contraction, softmax, split, contraction
   } else {

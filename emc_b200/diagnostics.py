@@ -6,8 +6,8 @@ The viewer (viewer/*.py of the reference) loads, with numpy.loadtxt:
 rotations_module.py:87), ``average_resp_%04d.data`` (the average
 responsibility of every rotation, rotations_module.py:47).  The scaling
 history it reads from ``best_scaling.h5`` (scaling_module.py:19) is written
-here as text, ``best_scaling.data`` (one row per iteration), since HDF5 is not
-part of this build; the model goes to ``model_%04d.raw`` (emc_model_save:
+here as text, ``best_scaling.data`` (one row per iteration), since this
+package has no HDF5 writer; the model goes to ``model_%04d.raw`` (emc_model_save:
 raw float32, the format emc_model_load reads).
 """
 from __future__ import annotations

@@ -6,8 +6,8 @@ expands the same model against the same rotations, evaluates its own patterns
 accumulators.  The only exchange is the element-wise sum of those
 accumulators -- 2 x side^3 floats, model and weight sums -- before
 normalisation; the ranks then normalise identical sums and hold identical
-models.  The reference is single-GPU; this follows the sharding SURVEY.md's
-multi-GPU row describes, with one all-reduce per iteration.
+models.  The reference is single-GPU; patterns are the natural unit to
+shard, and this costs one all-reduce per iteration.
 
 The per-iteration statistics (sum P log P, sum of log-sum-exps) are sums over
 patterns and are reduced the same way.

@@ -3,7 +3,7 @@
  * needs in order to compile.  It lets oracle/Makefile build the reference's
  * own CPU path functions (rotation sampling, detector coordinates, get_slice,
  * insert_slice, update_slice, slice_weighting, the likelihood functions) as
- * a checker library under oracle/_ref/.  TEST INFRASTRUCTURE ONLY.
+ * a test library under oracle/_ref/.  TEST INFRASTRUCTURE ONLY.
  *
  * Storage follows libspimage's column-major convention, which is also what
  * the reference's CUDA kernels assume when they index the uploaded arrays
