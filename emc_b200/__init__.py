@@ -23,6 +23,7 @@ _NAMES = {
     "fp32": FP32, "mixed": MIXED,
 }
 BUF_MODEL, BUF_WEIGHT, BUF_SCALING, BUF_RESP, BUF_SLICES, BUF_TOTALRESP, BUF_ACCUM = range(7)
+BUF_TOTALRESP_ALL = 7
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
           4: "device wait timed out", 5: "call out of order", 6: "data out of exact range",
           7: "unsupported"}
@@ -316,6 +317,14 @@ class Context:
         a, b = C.c_double(), C.c_double()
         self._c(lib().emc_partial_stats(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def total_resp_all_tensor(self):
+        """Zero-copy torch view (CUDA, float32 [R]) of T_r as the insertion's
+        T_r <= 1e-10 skip test reads it, valid between maximize() and
+        compress_insert(): a pattern-sharded caller sums it over the shards."""
+        import torch
+        ptr, nbytes = self.device_buffer(BUF_TOTALRESP_ALL)
+        return torch.as_tensor(_CudaArray(ptr, nbytes // 4), device="cuda")
 
     def accumulator_tensor(self):
         """Zero-copy torch view (CUDA, float32 [2*side^3]) of the insertion

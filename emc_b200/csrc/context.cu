@@ -94,6 +94,7 @@ struct emc_context {
   // model state
   float *d_model = nullptr, *d_weight = nullptr, *d_scaling = nullptr, *d_scaling_prev = nullptr;
   float* d_T = nullptr;
+  float* d_Tskip = nullptr;  // T_r for the insertion skip: this context's T, or all shards' sum
   double* d_rowstat = nullptr;
   double* d_scratch = nullptr;  // reductions
   double* d_stats = nullptr;    // [0] mean [1] max [2] plogp [3] loglik
@@ -282,7 +283,8 @@ emc_status emc_create(const emc_config* cfg, emc_context** out) {
   if ((s = c->alloc(&c->d_model, 2 * c->M, true)) ||
       (s = c->alloc(&c->d_scaling, c->N)) || (s = c->alloc(&c->d_scaling_prev, c->N)) ||
       (s = c->alloc(&c->d_quat, 4 * c->R)) || (s = c->alloc(&c->d_rotw, c->R)) ||
-      (s = c->alloc(&c->d_T, c->R, true)) || (s = c->alloc(&c->d_rowstat, c->R, true)) ||
+      (s = c->alloc(&c->d_T, c->R, true)) || (s = c->alloc(&c->d_Tskip, c->R, true)) ||
+      (s = c->alloc(&c->d_rowstat, c->R, true)) ||
       (s = c->alloc(&c->d_scratch, 4096)) || (s = c->alloc(&c->d_stats, 16, true)) ||
       (s = c->alloc(&c->d_patsq, c->N, true)) || (s = c->alloc(&c->d_patsum, c->N, true)) ||
       (s = c->alloc(&c->d_status, 1, true)))
@@ -607,6 +609,7 @@ static CmpEpiArgs cmp_args(emc_context* c) {
   e.quat = c->d_quat;
   e.rotw = c->d_rotw;
   e.T = c->d_T;
+  e.Tskip = c->d_Tskip;
   e.cx = c->d_cx;
   e.cy = c->d_cy;
   e.cz = c->d_cz;
@@ -711,6 +714,9 @@ emc_status emc_maximize(emc_context* c) {
     TRY(mixed_resp_pass(c));
     c->launches += 1;  // the maximize contraction
   }
+  // the insertion skip test reads Tskip: this context's T_r unless a
+  // pattern-sharded caller replaces it by the sum over every shard
+  CK(c, cudaMemcpyAsync(c->d_Tskip, c->d_T, sizeof(float) * R, cudaMemcpyDeviceToDevice, c->st));
   c->mark(3);
   c->resp_source = 1;
   c->stage = 2;
@@ -743,6 +749,7 @@ emc_status emc_compress_insert(emc_context* c) {
     InsertArgs in{};
     in.U = c->d_S;
     in.T = c->d_T;
+    in.Tskip = c->d_Tskip;
     in.rotw = c->d_rotw;
     in.quat = c->d_quat;
     in.cx = c->d_cx;
@@ -981,6 +988,7 @@ emc_status emc_device_buffer(emc_context* c, emc_buffer which, void** dptr, size
     case EMC_BUF_WEIGHT: p = c->d_weight; n = sizeof(float) * c->M; break;
     case EMC_BUF_SCALING: p = c->d_scaling; n = sizeof(float) * c->N; break;
     case EMC_BUF_TOTALRESP: p = c->d_T; n = sizeof(float) * c->R; break;
+    case EMC_BUF_TOTALRESP_ALL: p = c->d_Tskip; n = sizeof(float) * c->R; break;
     case EMC_BUF_ACCUM:
       p = c->mixed ? (void*)c->d_acc : (void*)c->d_model;
       n = sizeof(float) * 2 * c->M;
@@ -1615,6 +1623,7 @@ emc_status emc_batch_iterate(emc_batch* b) {
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];
     BTRY(b, c, mixed_resp_pass(c));
+    BCK(b, cudaMemcpyAsync(c->d_Tskip, c->d_T, sizeof(float) * c->R, cudaMemcpyDeviceToDevice, b->st));
     c->resp_source = 1;
     c->stage = 2;
     BCK(b, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, b->st));

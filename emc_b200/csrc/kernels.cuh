@@ -96,6 +96,7 @@ cudaError_t launch_compress_fp32(const CompressArgs& a, cudaStream_t st);
 struct InsertArgs {
   const float* U;        // [R][ldU]
   const float* T;        // [R]
+  const float* Tskip;    // [R] T_r over all pattern shards for the <= 1e-10 skip (nullptr: T)
   const float* rotw;     // [R]
   const float* quat;
   const float* cx;

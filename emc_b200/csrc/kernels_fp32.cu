@@ -228,7 +228,7 @@ struct OpCompress {
         const int64_t jj = j0 + j;
         if (jj >= p.npa) continue;
         // emc_atomic.cu:105-111: divide by the slice's total responsibility
-        p.U[r * p.ldU + col_of(p.pix, jj)] = T > 1e-10f ? acc[i][j] / T : acc[i][j];
+        p.U[r * p.ldU + col_of(p.pix, jj)] = T > 1e-30f ? acc[i][j] / T : acc[i][j];
       }
     }
   }
@@ -393,7 +393,8 @@ __global__ void row_sums_kernel(const float* P, int64_t R, int64_t N, float* T) 
 __global__ void __launch_bounds__(kBlock) insert_kernel(const InsertArgs a) {
   const int64_t r = blockIdx.x;
   const float T = a.T[r];
-  if (!(T > 1e-10f)) return;
+  // emc_atomic.cu:128 skips T_r <= 1e-10 (T_r over every pattern shard)
+  if (!((a.Tskip ? a.Tskip[r] : T) > 1e-10f) || !(T > 0.0f)) return;
   const float w = a.rotw[r] * T;
   float m[9];
   emc_voxel::rotation_matrix(a.quat + 4 * r, m);

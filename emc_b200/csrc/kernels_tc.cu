@@ -519,8 +519,9 @@ struct EpiCmp {
     active = false;
     if (r < a.R) {
       const float T = a.T[r];
-      // emc_atomic.cu:128: rotations with T_r <= 1e-10 are skipped; weight w = rotw T
-      if (T > 1e-10f) {
+      // emc_atomic.cu:128: rotations with T_r <= 1e-10 are skipped (T_r over
+      // every pattern shard); weight w = rotw T with this shard's T
+      if ((a.Tskip ? a.Tskip[r] : T) > 1e-10f && T > 0.0f) {
         active = true;
         const float rw = a.rotw[r];
         wT = rw * T;
@@ -1223,7 +1224,8 @@ __global__ void __launch_bounds__(kSweepThreads) write_kernel(const RespArgs a, 
       for (int64_t b = 0; b < nblk; ++b) T += a.Tpart[b * a.R + r];
       if (blockIdx.x == 0) a.T[r] = (float)T;
     }
-    invT[threadIdx.x] = T > 1e-10 ? (float)(1.0 / T) : 0.0f;
+    // P <= T, so P / T stays finite; the insertion decides which rows count
+    invT[threadIdx.x] = T > 1e-30 ? (float)(1.0 / T) : 0.0f;
   }
   __syncthreads();
   if (p0 >= a.ldP) return;

@@ -68,6 +68,7 @@ struct CmpEpiArgs {
   const float* quat;       // [R][4]
   const float* rotw;       // [R]
   const float* T;          // [R]
+  const float* Tskip;      // [R] T_r over all pattern shards for the <= 1e-10 skip
   const float* cx;         // [npa] active-pixel coordinates
   const float* cy;
   const float* cz;

@@ -3,9 +3,10 @@
 An EMC iteration is per pattern everywhere except insertion: every rank
 expands the same model against the same rotations, evaluates its own patterns
 (responsibilities, scaling), and inserts their slice averages into its own
-accumulators.  The only exchange is the element-wise sum of those
+accumulators.  The exchanges are the element-wise sums of those
 accumulators -- 2 x side^3 floats, model and weight sums -- before
-normalisation; the ranks then normalise identical sums and hold identical
+normalisation, and of the R per-rotation responsibility totals that decide
+which rotations the insertion skips; the ranks then normalise identical sums and hold identical
 models.  The reference is single-GPU; patterns are the natural unit to
 shard, and this costs one all-reduce per iteration.
 
@@ -38,21 +39,29 @@ class ShardedIteration:
         self.ctx = ctx
         self.group = group
 
+    def _sum(self, t) -> None:
+        c = self.ctx
+        if t.is_cuda:
+            # enqueued on the library's stream: it waits for the stage that
+            # wrote t, and the next stage (enqueued after it) waits for it
+            with torch.cuda.stream(torch.cuda.ExternalStream(c.stream)):
+                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+        else:
+            c.synchronize()
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+
     def __call__(self) -> None:
         c = self.ctx
+        sharded = dist.is_initialized() and dist.get_world_size(self.group) > 1
         c.expand()
         c.maximize()
+        if sharded:
+            # the insertion skips rotations whose total responsibility over
+            # ALL patterns is <= 1e-10 (emc_atomic.cu:128): sum T_r first
+            self._sum(c.total_resp_all_tensor())
         c.compress_insert()
-        if dist.is_initialized() and dist.get_world_size(self.group) > 1:
-            acc = c.accumulator_tensor()
-            if acc.is_cuda:
-                # enqueued on the library's stream: it waits for the insertion
-                # and normalise (enqueued next on that stream) waits for it
-                with torch.cuda.stream(torch.cuda.ExternalStream(c.stream)):
-                    dist.all_reduce(acc, op=dist.ReduceOp.SUM, group=self.group)
-            else:
-                c.synchronize()
-                dist.all_reduce(acc, op=dist.ReduceOp.SUM, group=self.group)
+        if sharded:
+            self._sum(c.accumulator_tensor())
         c.normalize()
 
     def stats(self) -> dict:

@@ -67,8 +67,11 @@ typedef enum {
   EMC_BUF_RESP = 3,     /* float [R][N] responsibilities after maximize */
   EMC_BUF_SLICES = 4,   /* float [R][Pa] expanded slices (FP32 path), Pa = active pixels */
   EMC_BUF_TOTALRESP = 5, /* float [R] T_r */
-  EMC_BUF_ACCUM = 6      /* float [2*side^3] insertion accumulators (model and weight sums)
+  EMC_BUF_ACCUM = 6,     /* float [2*side^3] insertion accumulators (model and weight sums)
                             between emc_compress_insert and emc_normalize */
+  EMC_BUF_TOTALRESP_ALL = 7 /* float [R] T_r for the insertion's T_r <= 1e-10 skip: after
+                            maximize a copy of this context's T_r; a caller sharding the
+                            patterns over contexts replaces it by the sum over all of them */
 } emc_buffer;
 
 const char *emc_status_string(emc_status s);

@@ -490,15 +490,25 @@ void orc_slice_average(const orc_config* c, const double* resp, const float* ima
 void orc_insert(const orc_config* c, const double* U, const double* total_resp,
                 const int32_t* mask, const float* rot, const float* rotw, const float* cx,
                 const float* cy, const float* cz, double* model_acc, double* weight_acc) {
+  orc_insert_shard(c, U, total_resp, total_resp, mask, rot, rotw, cx, cy, cz, model_acc,
+                   weight_acc);
+}
+
+void orc_insert_shard(const orc_config* c, const double* U, const double* total_resp,
+                      const double* all_total_resp, const int32_t* mask, const float* rot,
+                      const float* rotw, const float* cx, const float* cy, const float* cz,
+                      double* model_acc, double* weight_acc) {
   // emc_atomic.cu:115-133 + :17-73: rotations with T_r <= 1e-10 are skipped;
   // model += w * U/T, weight += w with w = rotw_r * T_r, for mask == 1 pixels.
+  // For a shard of the patterns the skip test reads the total over all
+  // shards (all_total_resp), so the shards' sums add up to the unsharded one.
   // Serial, so the accumulation order is fixed.
   const int side = c->side;
   const int64_t npix = (int64_t)side * side;
   const std::vector<int64_t> ins = active_pixels(mask, npix, true);
   for (int64_t r = 0; r < c->n_rotations; ++r) {
     const double T = total_resp[r];
-    if (!(T > 1e-10)) continue;
+    if (!(all_total_resp[r] > 1e-10) || !(T > 0.0)) continue;
     const double w = (double)rotw[r] * T;
     float m[9];
     orc_rotation_matrix_f32(rot + 4 * r, m);

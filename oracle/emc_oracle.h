@@ -86,6 +86,12 @@ void orc_slice_average(const orc_config* c, const double* resp, const float* ima
 void orc_insert(const orc_config* c, const double* U, const double* total_resp,
                 const int32_t* mask, const float* rot, const float* rotw, const float* cx,
                 const float* cy, const float* cz, double* model_acc, double* weight_acc);
+/* The same for one shard of the patterns: the T_r <= 1e-10 skip reads
+   all_total_resp (T_r summed over every shard). */
+void orc_insert_shard(const orc_config* c, const double* U, const double* total_resp,
+                      const double* all_total_resp, const int32_t* mask, const float* rot,
+                      const float* rotw, const float* cx, const float* cy, const float* cz,
+                      double* model_acc, double* weight_acc);
 /* Slice average + insertion into zeroed accumulators; total_resp[r] = T_r. */
 void orc_compress(const orc_config* c, const double* resp, const float* images,
                   const int32_t* mask, const double* scaling, const float* rot,

@@ -75,6 +75,7 @@ def lib():
         _lib.orc_normalize_model.argtypes = [C.c_int64, P, P]
         _lib.orc_iterate.argtypes = [P] * 12
         _lib.orc_iterate_restricted.argtypes = [P] * 13
+        _lib.orc_insert_shard.argtypes = [P] * 12
     return _lib
 
 
@@ -200,15 +201,22 @@ def slice_average(cfg, P, images, mask, scaling):
     return U, T
 
 
-def insert(cfg, U, T, mask, rot, rotw, cx, cy, cz, model_acc=None, weight_acc=None):
-    """emc_atomic.cu:17-73,115-133; accumulates into (model_acc, weight_acc)."""
+def insert(cfg, U, T, mask, rot, rotw, cx, cy, cz, model_acc=None, weight_acc=None,
+           all_T=None):
+    """emc_atomic.cu:17-73,115-133; accumulates into (model_acc, weight_acc).
+    all_T: for a shard of the patterns, T_r over every shard (the skip test)."""
     k = _Keep()
     M = cfg.side ** 3
     model_acc = np.zeros(M, np.float64) if model_acc is None else model_acc
     weight_acc = np.zeros(M, np.float64) if weight_acc is None else weight_acc
-    lib().orc_insert(C.byref(cfg), k(_f64(U)), k(_f64(T)), k(_i32(mask)), k(_f32(rot)),
-                     k(_f32(rotw)), k(_f32(cx)), k(_f32(cy)), k(_f32(cz)), _p(model_acc),
-                     _p(weight_acc))
+    if all_T is None:
+        lib().orc_insert(C.byref(cfg), k(_f64(U)), k(_f64(T)), k(_i32(mask)), k(_f32(rot)),
+                         k(_f32(rotw)), k(_f32(cx)), k(_f32(cy)), k(_f32(cz)), _p(model_acc),
+                         _p(weight_acc))
+    else:
+        lib().orc_insert_shard(C.byref(cfg), k(_f64(U)), k(_f64(T)), k(_f64(all_T)),
+                               k(_i32(mask)), k(_f32(rot)), k(_f32(rotw)), k(_f32(cx)),
+                               k(_f32(cy)), k(_f32(cz)), _p(model_acc), _p(weight_acc))
     return model_acc, weight_acc
 
 

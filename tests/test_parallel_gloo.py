@@ -36,11 +36,16 @@ class OracleShard:
         self.loglik = float(lse.sum())
         self.scaling = O.update_scaling(self.cfg, self.S, self.K, self.d["mask"], self.P,
                                         self.scaling)
+        self.T_all = torch.from_numpy(self.P.sum(axis=1))
+
+    def total_resp_all_tensor(self):
+        return self.T_all
 
     def compress_insert(self):
         d = self.d
         U, T = O.slice_average(self.cfg, self.P, self.K, d["mask"], self.scaling)
-        acc_m, acc_w = O.insert(self.cfg, U, T, d["mask"], d["q"], d["w"], d["x"], d["y"], d["z"])
+        acc_m, acc_w = O.insert(self.cfg, U, T, d["mask"], d["q"], d["w"], d["x"], d["y"], d["z"],
+                                all_T=self.T_all.numpy())
         self.acc = torch.from_numpy(np.concatenate([acc_m, acc_w]))
 
     def accumulator_tensor(self):
