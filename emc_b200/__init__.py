@@ -49,7 +49,7 @@ class IterStats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("maximize_raster", C.c_int32), ("compress_raster", C.c_int32),
-                ("maximize_pair", C.c_int32)]
+                ("maximize_pair", C.c_int32), ("compress_pair", C.c_int32)]
 
 
 class SynthConfig(C.Structure):
@@ -384,15 +384,17 @@ class Context:
         return {"best_rot": best, "best_resp": bp, "avg_resp": avg}
 
     def get_tuning(self):
-        """(maximize_raster, compress_raster, maximize_pair) of the tensor-core kernels."""
+        """(maximize_raster, compress_raster, maximize_pair, compress_pair) of the
+        tensor-core kernels."""
         t = Tuning()
         self._c(lib().emc_get_tuning(self._h, C.byref(t)))
-        return t.maximize_raster, t.compress_raster, t.maximize_pair
+        return t.maximize_raster, t.compress_raster, t.maximize_pair, t.compress_pair
 
-    def set_tuning(self, maximize_raster, compress_raster, maximize_pair=None):
-        if maximize_pair is None:
-            maximize_pair = self.get_tuning()[2]
-        t = Tuning(maximize_raster, compress_raster, int(maximize_pair))
+    def set_tuning(self, maximize_raster, compress_raster, maximize_pair=None, compress_pair=None):
+        cur = self.get_tuning()
+        maximize_pair = cur[2] if maximize_pair is None else maximize_pair
+        compress_pair = cur[3] if compress_pair is None else compress_pair
+        t = Tuning(maximize_raster, compress_raster, int(maximize_pair), int(compress_pair))
         self._c(lib().emc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, candidates=(1, 2, 4, 8, 16)):

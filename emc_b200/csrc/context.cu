@@ -114,7 +114,7 @@ struct emc_context {
   double *d_lse = nullptr, *d_plogp = nullptr;
   float* d_Tpart = nullptr;
   CUtensorMap tmKh, tmKt, tmBhi, tmBlo, tmPhi, tmPlo;
-  CUtensorMap tmKh64, tmBhi64, tmBlo64;  // boxes of the two-SM maximize
+  CUtensorMap tmKh64, tmBhi64, tmBlo64, tmKt128;  // boxes of the two-SM contractions
   TcStatus* d_status = nullptr;
   // profiling: events at stage boundaries, kernel launch count
   // learned proposal: rotation cells and the candidate-iteration buffers
@@ -141,9 +141,10 @@ struct emc_context {
   double *d_lse_c = nullptr, *d_plogp_c = nullptr;
   // Two event sets alternate between iterations, so the times of iteration
   // i-1 can be read while iteration i is still queued.
-  // raster bands of the maximize / compress tile orders (measured at 128^3 /
-  // 86,520 rotations / 50k patterns: 1 and 6 were fastest; emc_autotune re-measures)
-  emc_tuning tune{1, 6, 0};
+  // raster bands of the maximize / compress tile orders and the SM-pair forms
+  // (defaults from measurements at 64^3 and 128^3, set per shape in
+  // alloc_work; emc_autotune re-measures)
+  emc_tuning tune{1, 6, 0, 0};
   bool prof = false;
   cudaEvent_t ev[2][6] = {{nullptr}};
   int cur = 0;
@@ -353,6 +354,9 @@ static emc_status alloc_work(emc_context* c) {
   // the two-SM maximize pays where the pixel extent is long (measured: 18%
   // faster at 16,384 padded pixels, 8% slower at 4,096); emc_autotune decides
   c->tune.maximize_pair = c->Ppad >= 8192 ? 1 : 0;
+  // the compress on pairs: 5% faster at 128^3 / 50k patterns (raster 2)
+  c->tune.compress_pair = (c->Ppad >= 8192 && c->Npad >= 8192) ? 1 : 0;
+  if (c->tune.compress_pair) c->tune.compress_raster = 2;
   c->Rpad = round_up(R, 256);
   c->nrt = c->Rpad / 256;
   TRY(c->alloc(&c->d_acc, c->M, true));
@@ -375,7 +379,8 @@ static emc_status alloc_work(emc_context* c) {
             tc_encode_2d(&c->tmKt, c->d_Kt, c->Npad, c->Ppad, 256, kCompressBK) &&
             tc_encode_2d(&c->tmKh64, c->d_Kh, c->Ppad, c->Npad, 128, kPairBoxK) &&
             tc_encode_2d(&c->tmBhi64, c->d_Bhi, c->Ppad, c->Rpad, 128, kPairBoxK) &&
-            tc_encode_2d(&c->tmBlo64, c->d_Blo, c->Ppad, c->Rpad, 128, kPairBoxK);
+            tc_encode_2d(&c->tmBlo64, c->d_Blo, c->Ppad, c->Rpad, 128, kPairBoxK) &&
+            tc_encode_2d(&c->tmKt128, c->d_Kt, c->Npad, c->Ppad, 128, kPairBoxK);
   if (!ok) return c->fail(EMC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   return EMC_OK;
 }
@@ -767,6 +772,10 @@ emc_status emc_compress_insert(emc_context* c) {
     c->launches += 2;
   } else {
     CmpEpiArgs e = cmp_args(c);
+    if (c->tune.compress_pair)
+      CK(c, launch_compress_pair_tc(c->tmPhi, c->tmPlo, c->tmKt128, c->Rpad, c->Ppad, c->Npad, e,
+                                    c->d_status, c->num_sms, c->st, c->tune.compress_raster));
+    else
     CK(c, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
                              c->d_status, c->num_sms, c->st, c->tune.compress_raster));
     c->launches += 1;
@@ -842,7 +851,8 @@ emc_status emc_get_tuning(const emc_context* c, emc_tuning* t) {
 
 emc_status emc_set_tuning(emc_context* c, const emc_tuning* t) {
   if (!c || !t || t->maximize_raster < 1 || t->compress_raster < 1 ||
-      (t->maximize_pair != 0 && t->maximize_pair != 1))
+      (t->maximize_pair != 0 && t->maximize_pair != 1) ||
+      (t->compress_pair != 0 && t->compress_pair != 1))
     return EMC_ERR_ARG;
   c->tune = *t;
   return EMC_OK;
@@ -884,7 +894,7 @@ emc_status emc_autotune(emc_context* c, const int32_t* cand, int32_t n, float* m
     for (int32_t i = 0; i < n && s == EMC_OK; ++i) {
       float tmax = 1e30f;
       for (int32_t pair = 0; pair < 2 && s == EMC_OK; ++pair) {
-        c->tune = emc_tuning{cand[i], cand[i], pair};
+        c->tune = emc_tuning{cand[i], cand[i], pair, pair};
         if ((s = restore()) != EMC_OK || (s = emc_iterate(c, nullptr)) != EMC_OK) break;
         float t[5];
         if ((s = c->cuda(cudaEventSynchronize(c->ev[c->cur][5]), "autotune")) != EMC_OK) break;
@@ -899,6 +909,7 @@ emc_status emc_autotune(emc_context* c, const int32_t* cand, int32_t n, float* m
         if (t[3] < bcmp) {
           bcmp = t[3];
           win.compress_raster = cand[i];
+          win.compress_pair = pair;
         }
         if (ms) ms[n + i] = pair == 0 ? t[3] : (t[3] < ms[n + i] ? t[3] : ms[n + i]);
       }

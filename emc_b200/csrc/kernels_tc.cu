@@ -823,16 +823,19 @@ constexpr uint32_t kIdescPair = (1u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint
 constexpr int kPairBK = 64;
 constexpr int kPairStages = 4;
 
-template <class Epi>
+// NA / NB: 1, or 2 for an operand split into FP16 hi + lo (one of them).
+template <int NA, int NB, bool M_INNER, class Epi>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
-    tc_pair_maximize_kernel(const __grid_constant__ CUtensorMap tmA,
-                            const __grid_constant__ CUtensorMap tmB0,
-                            const __grid_constant__ CUtensorMap tmB1, const int64_t m_tiles,
-                            const int64_t n_tiles, const int64_t k_blocks, const int raster,
-                            const Epi epi, TcStatus* status) {
-  constexpr uint32_t A_BYTES = 128 * kPairBK * 2;   // this CTA's 128 patterns
-  constexpr uint32_t B_BYTES = 128 * kPairBK * 2;   // this CTA's 128 rotations, per half
-  constexpr uint32_t STAGE_BYTES = A_BYTES + 2 * B_BYTES;
+    tc_pair_kernel(const __grid_constant__ CUtensorMap tmA0,
+                   const __grid_constant__ CUtensorMap tmA1,
+                   const __grid_constant__ CUtensorMap tmB0,
+                   const __grid_constant__ CUtensorMap tmB1, const int64_t m_tiles,
+                   const int64_t n_tiles, const int64_t k_blocks, const int raster,
+                   const Epi epi, TcStatus* status) {
+  static_assert(NA * NB == 2, "one hi/lo split per contraction");
+  constexpr uint32_t A_BYTES = 128 * kPairBK * 2;   // this CTA's 128 rows of A
+  constexpr uint32_t B_BYTES = 128 * kPairBK * 2;   // this CTA's 128 rows (half) of B
+  constexpr uint32_t STAGE_BYTES = NA * A_BYTES + NB * B_BYTES;
   constexpr int STAGES = kPairStages;
   extern __shared__ uint8_t dyn_smem[];
   __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES];
@@ -884,15 +887,24 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   const int64_t num_tiles = m_tiles * n_tiles;
   const int64_t cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
 
-  // pattern tiles (of 256) fastest, in bands of `raster` rotation tiles
+  // the inner index (m for M_INNER, else n) fastest, in bands of `raster`
+  // outer tiles (as tile_mn of tc_gemm_kernel)
   auto tile_mn = [&](int64_t t, int64_t& m, int64_t& n) {
-    const int64_t span = (int64_t)raster * m_tiles;
+    const int64_t inner = M_INNER ? m_tiles : n_tiles;
+    const int64_t outer = M_INNER ? n_tiles : m_tiles;
+    const int64_t span = (int64_t)raster * inner;
     const int64_t band = t / span;
     const int64_t o0 = band * raster;
-    const int64_t g = n_tiles - o0 < raster ? n_tiles - o0 : raster;
+    const int64_t g = outer - o0 < raster ? outer - o0 : raster;
     const int64_t w = t - band * span;
-    n = o0 + w % g;
-    m = w / g;
+    const int64_t o = o0 + w % g, i = w / g;
+    if (M_INNER) {
+      m = i;
+      n = o;
+    } else {
+      m = o;
+      n = i;
+    }
   };
 
   if (warp == 0) {
@@ -916,9 +928,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           const uint32_t fb_leader = peer_addr(fb, 0);
           const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
           const int kc = (int)(kb * kPairBK);
-          tma_load_2d_pair(base, &tmA, kc, ar, fb_leader);
-          tma_load_2d_pair(base + A_BYTES, &tmB0, kc, br, fb_leader);
-          tma_load_2d_pair(base + A_BYTES + B_BYTES, &tmB1, kc, br, fb_leader);
+          tma_load_2d_pair(base, &tmA0, kc, ar, fb_leader);
+          if (NA == 2) tma_load_2d_pair(base + A_BYTES, &tmA1, kc, ar, fb_leader);
+          const uint32_t bbase = base + NA * A_BYTES;
+          tma_load_2d_pair(bbase, &tmB0, kc, br, fb_leader);
+          if (NB == 2) tma_load_2d_pair(bbase + B_BYTES, &tmB1, kc, br, fb_leader);
           ++issued;
           if (++s == STAGES) {
             s = 0;
@@ -975,13 +989,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           }
           tc_fence_after();
           const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
+          const uint32_t bbase = base + NA * A_BYTES;
 #pragma unroll
           for (int k = 0; k < kPairBK / 16; ++k) {
 #pragma unroll
             for (int q = 0; q < 2; ++q)
-              mma_f16_pair(d, sdesc<kPairBK>(base + k * 32),
-                           sdesc<kPairBK>(base + A_BYTES + q * B_BYTES + k * 32), kIdescPair,
-                           (kb | k | q) != 0);
+              mma_f16_pair(d, sdesc<kPairBK>(base + (NA == 2 ? q : 0) * A_BYTES + k * 32),
+                           sdesc<kPairBK>(bbase + (NB == 2 ? q : 0) * B_BYTES + k * 32),
+                           kIdescPair, (kb | k | q) != 0);
           }
           // release this stage in both CTAs once its MMAs are done
           const uint32_t eb = smem_u32(&empty_bar[s]);
@@ -1051,20 +1066,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   }
 }
 
-template <class Epi>
-cudaError_t run_pair_maximize(const CUtensorMap& a, const CUtensorMap& b0, const CUtensorMap& b1,
-                              int64_t m_tiles, int64_t n_tiles, int64_t k_blocks, const Epi& epi,
-                              TcStatus* st, int num_sms, cudaStream_t stream, int raster) {
-  constexpr uint32_t stage = 128 * kPairBK * 2 * 3;
+template <int NA, int NB, bool M_INNER, class Epi>
+cudaError_t run_pair(const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
+                     const CUtensorMap& b1, int64_t m_tiles, int64_t n_tiles, int64_t k_blocks,
+                     const Epi& epi, TcStatus* st, int num_sms, cudaStream_t stream, int raster) {
+  constexpr uint32_t stage = 128 * kPairBK * 2 * (NA + NB);
   const size_t dyn = (size_t)kPairStages * stage + 1024;
-  auto kern = tc_pair_maximize_kernel<Epi>;
+  auto kern = tc_pair_kernel<NA, NB, M_INNER, Epi>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e != cudaSuccess) return e;
   const int64_t tiles = m_tiles * n_tiles;
   if (tiles == 0) return cudaSuccess;
   const int64_t pairs = num_sms / 2;
   const int grid = 2 * (int)(tiles < pairs ? tiles : pairs);
-  kern<<<grid, kThreads, dyn, stream>>>(a, b0, b1, m_tiles, n_tiles, k_blocks,
+  kern<<<grid, kThreads, dyn, stream>>>(a0, a1, b0, b1, m_tiles, n_tiles, k_blocks,
                                         raster < 1 ? 1 : raster, epi, st);
   return cudaGetLastError();
 }
@@ -1406,8 +1421,19 @@ cudaError_t launch_maximize_pair_tc(const CUtensorMap& tmK, const CUtensorMap& t
   epi.a = e;
   // 256-pattern pair tiles (the last may reach past Mpad: zero-filled by TMA,
   // masked by the epilogue), 64-wide K-steps
-  return run_pair_maximize(tmK, tmBhi, tmBlo, (Mpad + 255) / 256, Rpad / BN, Kpad / kPairBK, epi,
-                           status, num_sms, st, raster);
+  return run_pair<1, 2, true>(tmK, tmK, tmBhi, tmBlo, (Mpad + 255) / 256, Rpad / BN,
+                             Kpad / kPairBK, epi, status, num_sms, st, raster);
+}
+
+cudaError_t launch_compress_pair_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
+                                    const CUtensorMap& tmKt, int64_t Rpad, int64_t Ppad,
+                                    int64_t Npad, const CmpEpiArgs& e, TcStatus* status,
+                                    int num_sms, cudaStream_t st, int raster) {
+  EpiCmp epi;
+  epi.a = e;
+  // 256-rotation pair tiles (Rpad is a multiple of 256), pixel tiles inner
+  return run_pair<2, 1, false>(tmPhi, tmPlo, tmKt, tmKt, Rpad / 256, Ppad / BN, Npad / kPairBK,
+                               epi, status, num_sms, st, raster);
 }
 
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,

@@ -81,6 +81,13 @@ cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPl
                                int64_t Npad, const CmpEpiArgs& e, TcStatus* status, int num_sms,
                                cudaStream_t st, int raster);
 
+// The compress contraction on SM pairs: 256 rotations x 256 pixels per
+// pair, 64-wide K-steps; Kt's tensor map has boxes of 128 rows x 64.
+cudaError_t launch_compress_pair_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
+                                    const CUtensorMap& tmKt, int64_t Rpad, int64_t Ppad,
+                                    int64_t Npad, const CmpEpiArgs& e, TcStatus* status,
+                                    int num_sms, cudaStream_t st, int raster);
+
 // Tile of a grouped contraction (learned proposal): TMA origins of the two
 // operands (row, k offset), its k-block count, and the group (cell) with the
 // tile's first row inside the group.

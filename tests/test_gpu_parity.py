@@ -180,9 +180,9 @@ def test_autotune_keeps_results_and_restores_state(tiny):
 
 @pytest.mark.parametrize("lik", ["poisson", "gauss"])
 def test_pair_maximize_matches_oracle_and_one_sm_kernel(small, lik):
-    """The maximize contraction on SM pairs (cta_group::2, 256-pattern tiles,
-    half of the slice operand per SM) gives the responsibilities of the
-    one-SM kernel and of the oracle."""
+    """Both contractions on SM pairs (cta_group::2: 256-pattern / 256-rotation
+    tiles, half of the B operand per SM) give the responsibilities and the
+    model of the one-SM kernels and of the oracle."""
     import emc_b200 as E
     d = small
     cfg = oracle_cfg(d, lik, "nearest")
@@ -197,8 +197,8 @@ def test_pair_maximize_matches_oracle_and_one_sm_kernel(small, lik):
         m1 = ctx.get_model()
         ctx.set_model(d["model0"])
         ctx.set_scaling(d["scaling0"])
-        ctx.set_tuning(1, 6, 1)
-        assert ctx.get_tuning()[2] == 1
+        ctx.set_tuning(1, 6, 1, 1)
+        assert ctx.get_tuning()[2:] == (1, 1)
         ctx.expand()
         ctx.maximize()
         P2 = ctx.get_buffer(E.BUF_RESP)
@@ -219,7 +219,7 @@ def test_pair_maximize_at_size():
     out = []
     for pair in (0, 1):
         with make_ctx(d, "poisson", "nearest", "mixed") as ctx:
-            ctx.set_tuning(1, 6, pair)
+            ctx.set_tuning(1, 6, pair, pair)
             ctx.expand()
             ctx.maximize()
             P = ctx.get_buffer(E.BUF_RESP)
