@@ -1155,37 +1155,56 @@ constexpr int kSweepRows = 32;
 constexpr int kSweepThreads = 256;
 constexpr int kSweepPatterns = 4 * kSweepThreads;
 
+// Per-pattern constants of the sweeps.  Poisson Y is the LL itself, so only
+// lse is kept (fewer registers, more warps in flight); gaussian keeps the
+// coefficients of LL = (2 C / phi - sum S^2 - sum K^2 / phi^2) * inv.
+template <bool POISSON>
 struct PatConst {
   double lse[4];
-  LLFromY f[4];
+  double c1[4], c0[4];  // gaussian only
   bool ok[4];
 };
 
-__device__ __forceinline__ void load_consts(const RespArgs& a, int64_t p0, PatConst& k) {
+template <bool POISSON>
+__device__ __forceinline__ void load_consts(const RespArgs& a, int64_t p0, PatConst<POISSON>& k) {
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int64_t p = p0 + i;
     k.ok[i] = p < a.N;
     k.lse[i] = k.ok[i] ? a.lse[p] : 0.0;
-    k.f[i] = make_llf(a, p);
+    if constexpr (!POISSON) {
+      const LLFromY f = make_llf(a, p);
+      k.c1[i] = f.c1;
+      k.c0[i] = f.c0;
+    }
   }
 }
 
-__device__ __forceinline__ void probs_from(const PatConst& k, float4 y, double rs, float (&P)[4]) {
+// P = exp(LL - lse): the difference in FP64 (LL and lse are ~1e4), exp in FP32.
+template <bool POISSON>
+__device__ __forceinline__ void probs_from(const PatConst<POISSON>& k, float4 y, double rs,
+                                           float (&P)[4]) {
   const float yy[4] = {y.x, y.y, y.z, y.w};
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-    P[i] = k.ok[i] ? expf((float)(k.f[i](yy[i], rs) - k.lse[i])) : 0.0f;
+  for (int i = 0; i < 4; ++i) {
+    double ll;
+    if constexpr (POISSON)
+      ll = (double)yy[i];
+    else
+      ll = fma((double)yy[i], k.c1[i], k.c0[i] - rs);
+    P[i] = k.ok[i] ? expf((float)(ll - k.lse[i])) : 0.0f;
+  }
 }
 
 // Sweep A: Tpart[pattern block][r] = sum over the block's patterns of P_rp.
-__global__ void __launch_bounds__(kSweepThreads) rowsum_kernel(const RespArgs a) {
+template <bool POISSON>
+__global__ void __launch_bounds__(kSweepThreads, 4) rowsum_kernel(const RespArgs a) {
   __shared__ float red[kSweepThreads / 32][kSweepRows];
   const int64_t p0 = (int64_t)blockIdx.x * kSweepPatterns + 4 * threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.y * kSweepRows;
   const bool any = p0 < a.N;
-  PatConst k;
-  load_consts(a, p0, k);
+  PatConst<POISSON> k;
+  load_consts<POISSON>(a, p0, k);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   // four rows per step: their loads are issued before any result is needed
   for (int i0 = 0; i0 < kSweepRows; i0 += 4) {
@@ -1202,9 +1221,9 @@ __global__ void __launch_bounds__(kSweepThreads) rowsum_kernel(const RespArgs a)
       const int64_t r = r0 + i0 + u;
       t[u] = 0.0f;
       if (r < a.R && any) {
-        const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
+        const double rs = POISSON ? 0.0 : a.rowstat[r] * a.gauss_inv;
         float P[4];
-        probs_from(k, y[u], rs, P);
+        probs_from<POISSON>(k, y[u], rs, P);
         t[u] = (P[0] + P[1]) + (P[2] + P[3]);
       }
     }
@@ -1228,7 +1247,8 @@ __global__ void __launch_bounds__(kSweepThreads) rowsum_kernel(const RespArgs a)
 // by its total responsibility T_r (the slice average of emc_atomic.cu:105-111)
 // keeps every entry in [0, c0/phi_p], so rotations with a tiny T_r keep their
 // relative precision instead of underflowing FP16.
-__global__ void __launch_bounds__(kSweepThreads) write_kernel(const RespArgs a, int64_t nblk) {
+template <bool POISSON>
+__global__ void __launch_bounds__(kSweepThreads, 4) write_kernel(const RespArgs a, int64_t nblk) {
   __shared__ float invT[kSweepRows];
   const int64_t p0 = (int64_t)blockIdx.x * kSweepPatterns + 4 * threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.y * kSweepRows;
@@ -1244,8 +1264,8 @@ __global__ void __launch_bounds__(kSweepThreads) write_kernel(const RespArgs a, 
   }
   __syncthreads();
   if (p0 >= a.ldP) return;
-  PatConst k;
-  load_consts(a, p0, k);
+  PatConst<POISSON> k;
+  load_consts<POISSON>(a, p0, k);
   float g[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) g[i] = k.ok[i] ? a.c0 / a.new_scaling[p0 + i] : 0.0f;
@@ -1265,8 +1285,8 @@ __global__ void __launch_bounds__(kSweepThreads) write_kernel(const RespArgs a, 
     if (r >= a.R) break;
     float P[4] = {0.f, 0.f, 0.f, 0.f};
     if (any) {
-      const double rs = a.poisson ? a.rowstat[r] : a.rowstat[r] * a.gauss_inv;
-      probs_from(k, y[u], rs, P);
+      const double rs = POISSON ? 0.0 : a.rowstat[r] * a.gauss_inv;
+      probs_from<POISSON>(k, y[u], rs, P);
     }
     __half h[4], l[4];
 #pragma unroll
@@ -1488,9 +1508,15 @@ cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {
   combine_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, st>>>(a);
   const int64_t nblk = (a.N + kSweepPatterns - 1) / kSweepPatterns;
   const int64_t rblk = (a.R + kSweepRows - 1) / kSweepRows;
-  rowsum_kernel<<<dim3((unsigned)nblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a);
+  if (a.poisson)
+    rowsum_kernel<true><<<dim3((unsigned)nblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a);
+  else
+    rowsum_kernel<false><<<dim3((unsigned)nblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a);
   const int64_t wblk = (a.ldP + kSweepPatterns - 1) / kSweepPatterns;
-  write_kernel<<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
+  if (a.poisson)
+    write_kernel<true><<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
+  else
+    write_kernel<false><<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
   return cudaGetLastError();
 }
 
