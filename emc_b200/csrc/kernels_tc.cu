@@ -96,7 +96,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 __device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// Named barrier of the epilogue warps (n threads).
+__device__ __forceinline__ void epi_bar(int n = 128) {
+  asm volatile("bar.sync 1, %0;" ::"r"(n) : "memory");
+}
 
 // Shared-memory matrix descriptor of a K-major operand whose rows are BK FP16
 // elements (BK = 64: 128-byte rows, 128B swizzle; BK = 32: 64-byte rows, 64B
@@ -142,7 +145,7 @@ __device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int si
 
 // ---------------------------------------------------------------- kernel --
 template <int NA, int NB, int STAGES, bool M_INNER, int BK, class Epi>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
     tc_gemm_kernel(const __grid_constant__ TmapSet<Epi::kSets> maps,
                    const int64_t m_tiles, const int64_t n_tiles, const int64_t k_blocks,
                    const int raster, const Epi epi, TcStatus* status) {
@@ -170,7 +173,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(smem_u32(&tfull_bar[a]), 1);
-      mbar_init(smem_u32(&tempty_bar[a]), 128);
+      mbar_init(smem_u32(&tempty_bar[a]), 32 * Epi::kEpiWarps);
     }
     mbar_init(smem_u32(&drain_bar), 1);
     abort_flag = 0;
@@ -337,19 +340,24 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     // -------------------------------------------------- epilogue warps
+    // TMEM lane quarter = warp % 4; with 8 or 16 epilogue warps, 2 or 4 warps
+    // share a quarter and split the columns
+    constexpr int EW = Epi::kEpiWarps;
+    constexpr int COLS = BN / (EW / 4);
     const int quarter = warp & 3;
     const int ep_tid = threadIdx.x - 64;
+    const int col0 = ((warp - 2) / 4) * COLS;
     Epi e = epi;
     int64_t i = 0;
     for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, ++i) {
       const int acc = (int)(i & 1);
       const uint32_t aph = (uint32_t)((i >> 1) & 1);
       bounded_wait(smem_u32(&tfull_bar[acc]), aph, ctl, 4);
-      // the four epilogue warps leave together: a divergent exit would strand
-      // the others in the named barriers of tile_begin
-      epi_bar();
+      // the epilogue warps leave together: a divergent exit would strand the
+      // others in the named barriers of tile_begin
+      epi_bar(32 * EW);
       if (ep_tid == 0) epi_abort = abort_flag;
-      epi_bar();
+      epi_bar(32 * EW);
       if (epi_abort) break;
       tc_fence_after();
       int64_t mt, nt;
@@ -363,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       e.row_begin(mt * BM + quarter * 32 + lane);
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
-      for (int c = 0; c < BN; c += 16) {
+      for (int c = col0; c < col0 + COLS; c += 16) {
         uint32_t v[16];
         tmem_ld16(taddr + c, v);
         tmem_ld_wait();
@@ -396,6 +404,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 struct EpiMax {
   static constexpr bool kListed = false;
   static constexpr int kSets = 1;
+  static constexpr int kEpiWarps = 4;
   static constexpr int kSmemBytes = BN * 8;
   MaxEpiArgs a;
   int64_t n0, ntile, p;
@@ -496,6 +505,7 @@ __device__ __forceinline__ void red_add_v2(float2* p, float x, float y) {
 struct EpiCmp {
   static constexpr bool kListed = false;
   static constexpr int kSets = 1;
+  static constexpr int kEpiWarps = 4;
   static constexpr int kSmemBytes = BN * 16;
   CmpEpiArgs a;
   int64_t j0;
@@ -566,6 +576,7 @@ struct EpiCmp {
 struct EpiGMax {
   static constexpr bool kListed = true;
   static constexpr int kSets = 1;
+  static constexpr int kEpiWarps = 4;
   static constexpr int kSmemBytes = BN * 8;
   GMaxEpiArgs a;
   TileDesc d;
@@ -628,6 +639,9 @@ struct EpiGMax {
 struct EpiGCmp {
   static constexpr bool kListed = true;
   static constexpr int kSets = 1;
+  // insertion-heavy epilogue behind short K loops: 16 warps (four per TMEM
+  // lane quarter, a quarter of the columns each) keep more reductions in flight
+  static constexpr int kEpiWarps = 16;
   static constexpr int kSmemBytes = BN * 16;
   GCmpEpiArgs a;
   TileDesc d;
@@ -640,13 +654,13 @@ struct EpiGCmp {
     float4* cs = reinterpret_cast<float4*>(smem);
     d = a.tiles[t];
     mc = a.mcnt[d.cell];
-    epi_bar();
-    for (int c = tid; c < BN; c += 128) {
+    epi_bar(32 * kEpiWarps);
+    for (int c = tid; c < BN; c += 32 * kEpiWarps) {
       const int64_t j = (int64_t)d.b_row + c;
       cs[c] = j < a.npa ? make_float4(a.cx[j], a.cy[j], a.cz[j], a.ins[j] == 1 ? 1.0f : 0.0f)
                         : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    epi_bar();
+    epi_bar(32 * kEpiWarps);
   }
   __device__ void row_begin(int64_t row) {
     const int local = (int)(row % BM);
@@ -708,6 +722,7 @@ inline TmapSet<1> one_set(const CUtensorMap& a0, const CUtensorMap& a1, const CU
 struct EpiBatchMax {
   static constexpr bool kListed = true;
   static constexpr int kSets = kMaxBatch;
+  static constexpr int kEpiWarps = 4;
   static constexpr int kSmemBytes = EpiMax::kSmemBytes;
   BatchMaxArgs a;
   EpiMax inner;
@@ -728,6 +743,7 @@ struct EpiBatchMax {
 struct EpiBatchCmp {
   static constexpr bool kListed = true;
   static constexpr int kSets = kMaxBatch;
+  static constexpr int kEpiWarps = 4;
   static constexpr int kSmemBytes = EpiCmp::kSmemBytes;
   BatchCmpArgs a;
   EpiCmp inner;
@@ -758,7 +774,8 @@ cudaError_t run_gemm(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n
   const int64_t tiles = m_tiles * n_tiles;
   if (tiles == 0) return cudaSuccess;
   const int grid = (int)(tiles < num_sms ? tiles : num_sms);
-  kern<<<grid, kThreads, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks, raster, epi, st);
+  kern<<<grid, 64 + 32 * Epi::kEpiWarps, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks, raster,
+                                                       epi, st);
   return cudaGetLastError();
 }
 
