@@ -121,6 +121,7 @@ struct emc_context {
   int32_t n_cells = 0, cand_m = 0;
   int resp_source = 0;  // responsibilities of the last maximize: 1 dense, 2 proposed
   float* d_cmass = nullptr;
+  cudaEvent_t ev_sel = nullptr;  // the proposed iteration's selection has reached the host
   int32_t* d_best = nullptr;  // orientation diagnostics: most probable rotation per pattern
   float* d_bestp = nullptr;
   int64_t max_members = 0;
@@ -306,6 +307,7 @@ emc_status emc_destroy(emc_context* ctx) {
       if (e) cudaEventDestroy(e);
   for (void* h : ctx->hpin)
     if (h) cudaFreeHost(h);
+  if (ctx->ev_sel) cudaEventDestroy(ctx->ev_sel);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
   return EMC_OK;
@@ -1190,17 +1192,21 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, int32_t m, f
     c->pairs_cap = cap;
     c->cand_m = m;
   }
-  TRY(emc_expand(c));
-  if (!c->mixed && c->gauss)  // the grouped gaussian LL uses the expanded form: sum_j S_rj^2
-    CK(c, launch_pattern_stats(c->d_S, nullptr, R, c->npa, c->npa, 1, c->d_rowstat, c->st));
-  // candidate cells of every pattern and the proposal's mass on them
+  if (c->stage != 0) return c->fail(EMC_ERR_STATE, "proposed iteration between stages");
+  // candidate cells of every pattern and the proposal's mass on them; their
+  // copy to the host is waited for while the expansion runs behind it
   CK(c, launch_select(probs, N, c->n_cells, m, mass_target, c->d_cand, c->d_mass, c->st));
   int32_t* cand = c->pinned<int32_t>(0, pairs);
   float* mass = c->pinned<float>(1, N);
   if (!cand || !mass) return c->fail(EMC_ERR_OOM, "pinned host staging");
   CK(c, cudaMemcpyAsync(cand, c->d_cand, sizeof(int32_t) * pairs, cudaMemcpyDeviceToHost, c->st));
   CK(c, cudaMemcpyAsync(mass, c->d_mass, sizeof(float) * N, cudaMemcpyDeviceToHost, c->st));
-  CK(c, cudaStreamSynchronize(c->st));
+  if (!c->ev_sel) CK(c, cudaEventCreateWithFlags(&c->ev_sel, cudaEventDisableTiming));
+  CK(c, cudaEventRecord(c->ev_sel, c->st));
+  TRY(emc_expand(c));
+  if (!c->mixed && c->gauss)  // the grouped gaussian LL uses the expanded form: sum_j S_rj^2
+    CK(c, launch_pattern_stats(c->d_S, nullptr, R, c->npa, c->npa, 1, c->d_rowstat, c->st));
+  CK(c, cudaEventSynchronize(c->ev_sel));
   double msum = 0.0, mmin = 1e300;
   for (int64_t p = 0; p < N; ++p) {
     msum += mass[p];

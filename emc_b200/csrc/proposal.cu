@@ -344,21 +344,38 @@ __global__ void gather_rows_kernel(const __half* Kh, int64_t Ppad, const int32_t
 }
 
 // KgT[j][slot] = Kh[pattern of slot][j] for j < Ppad, slot < S (zero for the
-// padding slots): 32 x 32 tiles transposed through shared memory.
-__global__ void gather_transpose_kernel(const __half* Kh, int64_t Ppad, const int32_t* slot_pat,
-                                        int64_t S, int64_t ldT, __half* KgT) {
-  __shared__ __half tile[32][33];
-  const int64_t j0 = (int64_t)blockIdx.x * 32, s0 = (int64_t)blockIdx.y * 32;
-  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  for (int i = ty; i < 32; i += 8) {
-    const int64_t s = s0 + i, j = j0 + tx;
+// padding slots): 64 slots x 64 pixels per block, read and written as half2
+// (pairs of pixels in, pairs of slots out) through a shared-memory tile of
+// 32-bit words.
+__global__ void __launch_bounds__(256) gather_transpose_kernel(const __half* Kh, int64_t Ppad,
+                                                               const int32_t* slot_pat, int64_t S,
+                                                               int64_t ldT, __half* KgT) {
+  __shared__ uint32_t tile[64][33];  // [slot][pixel pair]
+  const int64_t j0 = (int64_t)blockIdx.x * 64, s0 = (int64_t)blockIdx.y * 64;
+  const int t = threadIdx.x;
+  // load: 64 slot rows x 32 pixel pairs
+  for (int e = t; e < 64 * 32; e += 256) {
+    const int sr = e >> 5, jp = e & 31;
+    const int64_t s = s0 + sr, j = j0 + 2 * jp;
     const int p = s < S ? slot_pat[s] : -1;
-    tile[i][tx] = (p >= 0 && j < Ppad) ? Kh[(int64_t)p * Ppad + j] : __float2half_rn(0.0f);
+    uint32_t v = 0;
+    if (p >= 0 && j + 1 < Ppad + 1)
+      v = *reinterpret_cast<const uint32_t*>(Kh + (int64_t)p * Ppad + j);
+    tile[sr][jp] = v;
   }
   __syncthreads();
-  for (int i = ty; i < 32; i += 8) {
-    const int64_t j = j0 + i, s = s0 + tx;
-    if (j < Ppad && s < S) KgT[j * ldT + s] = tile[tx][i];
+  // store: 64 pixel rows x 32 slot pairs
+  for (int e = t; e < 64 * 32; e += 256) {
+    const int jr = e >> 5, sp = e & 31;
+    const int64_t j = j0 + jr, s = s0 + 2 * sp;
+    if (j >= Ppad || s >= S) continue;
+    const uint32_t a = tile[2 * sp][jr >> 1], b = tile[2 * sp + 1][jr >> 1];
+    const uint32_t lo = (jr & 1) ? (a >> 16) : (a & 0xFFFFu);
+    const uint32_t hi = (jr & 1) ? (b >> 16) : (b & 0xFFFFu);
+    if (s + 1 < S)
+      *reinterpret_cast<uint32_t*>(KgT + j * ldT + s) = lo | (hi << 16);
+    else
+      KgT[j * ldT + s] = __ushort_as_half((unsigned short)lo);
   }
 }
 
@@ -445,8 +462,8 @@ cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* s
   if (S == 0) return cudaSuccess;
   if (Kg) gather_rows_kernel<<<(unsigned)S, 256, 0, st>>>(Kh, Ppad, slot_pat, S, Kg);
   if (KgT) {
-    dim3 grid((unsigned)((Ppad + 31) / 32), (unsigned)((S + 31) / 32));
-    gather_transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(Kh, Ppad, slot_pat, S, ldT, KgT);
+    dim3 grid((unsigned)((Ppad + 63) / 64), (unsigned)((S + 63) / 64));
+    gather_transpose_kernel<<<grid, 256, 0, st>>>(Kh, Ppad, slot_pat, S, ldT, KgT);
   }
   return cudaGetLastError();
 }
