@@ -166,10 +166,18 @@ def cpu_oracle_rate(d, likelihood, interp, seconds, rot=None):
         return time.perf_counter() - t, out
 
     t8, _ = run(8)
-    t64, _ = run(64) if t8 < seconds / 8 else (None, None)
     # per-pattern cost from two sizes (the fixed expand / insert cost cancels)
-    per = (t64 - t8) / 56 if t64 is not None and t64 > t8 else t8 / 8
-    n = int(max(8, min(d["counts"].shape[0], (seconds - t8) / max(per, 1e-4))))
+    if t8 < seconds / 8:
+        t64, _ = run(64)
+        t256, _ = run(256) if t64 < seconds / 4 else (None, None)
+        if t256 is not None and t256 > t64:
+            per = (t256 - t64) / 192
+        else:
+            per = max(t64 - t8, 1e-4) / 56
+        base = t64
+    else:
+        per, base = t8 / 8, t8
+    n = int(max(8, min(d["counts"].shape[0], (seconds - base) / max(per, 1e-5))))
     n = max(8, (n // 8) * 8)
     t, out = run(n)
     R = d["q"].shape[0]
