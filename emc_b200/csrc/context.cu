@@ -1480,6 +1480,8 @@ struct emc_batch {
   cudaStream_t st = nullptr;
   TileDesc *d_mt = nullptr, *d_ct = nullptr;
   int64_t n_mt = 0, n_ct = 0;
+  bool pair = false;      // the batched maximize on SM pairs
+  bool cmp_pair = false;  // the batched compress on SM pairs
   MaxEpiArgs* d_max = nullptr;  // per-dataset epilogue arguments (fixed per context)
   CmpEpiArgs* d_cmp = nullptr;
   cudaGraph_t graph = nullptr;
@@ -1564,21 +1566,48 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
       for (int64_t w = 0; w < g * inner; ++w) emit(w / g, o0 + w % g);
     }
   };
+  // one form for the batched maximize: SM pairs when the datasets that chose
+  // them on their own hold most of the work
+  double work = 0.0, work_pair = 0.0;
+  for (int32_t i = 0; i < n; ++i) {
+    const double w = (double)ctxs[i]->Npad * ctxs[i]->Rpad * ctxs[i]->Ppad;
+    work += w;
+    if (ctxs[i]->tune.maximize_pair) work_pair += w;
+  }
+  b->pair = work_pair * 2.0 >= work;
   for (int32_t i : order) {
     const emc_context* c = ctxs[i];
-    banded(c->Npad / 128, c->Rpad / 256, c->tune.maximize_raster, [&](int64_t m, int64_t nt) {
-      mt.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
-                            (int32_t)(c->Ppad / kMaximizeBK), (int32_t)nt, (int32_t)m, i});
-    });
+    if (b->pair)
+      banded((c->Npad + 255) / 256, c->Rpad / 256, c->tune.maximize_raster,
+             [&](int64_t m, int64_t nt) {
+               mt.push_back(TileDesc{(int32_t)(m * 256), 0, (int32_t)(nt * 256), 0,
+                                     (int32_t)(c->Ppad / kPairBoxK), (int32_t)nt, (int32_t)m, i});
+             });
+    else
+      banded(c->Npad / 128, c->Rpad / 256, c->tune.maximize_raster, [&](int64_t m, int64_t nt) {
+        mt.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
+                              (int32_t)(c->Ppad / kMaximizeBK), (int32_t)nt, (int32_t)m, i});
+      });
   }
   std::stable_sort(order.begin(), order.end(),
                    [&](int32_t x, int32_t y) { return ctxs[x]->Npad > ctxs[y]->Npad; });
+  double cwork_pair = 0.0;
+  for (int32_t i = 0; i < n; ++i)
+    if (ctxs[i]->tune.compress_pair)
+      cwork_pair += (double)ctxs[i]->Npad * ctxs[i]->Rpad * ctxs[i]->Ppad;
+  b->cmp_pair = cwork_pair * 2.0 >= work;
   for (int32_t i : order) {
     const emc_context* c = ctxs[i];
-    banded(c->Ppad / 256, c->Rpad / 128, c->tune.compress_raster, [&](int64_t nt, int64_t m) {
-      ct.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
-                            (int32_t)(c->Npad / kCompressBK), (int32_t)nt, (int32_t)m, i});
-    });
+    if (b->cmp_pair)
+      banded(c->Ppad / 256, c->Rpad / 256, c->tune.compress_raster, [&](int64_t nt, int64_t m) {
+        ct.push_back(TileDesc{(int32_t)(m * 256), 0, (int32_t)(nt * 256), 0,
+                              (int32_t)(c->Npad / kPairBoxK), (int32_t)nt, (int32_t)m, i});
+      });
+    else
+      banded(c->Ppad / 256, c->Rpad / 128, c->tune.compress_raster, [&](int64_t nt, int64_t m) {
+        ct.push_back(TileDesc{(int32_t)(m * 128), 0, (int32_t)(nt * 256), 0,
+                              (int32_t)(c->Npad / kCompressBK), (int32_t)nt, (int32_t)m, i});
+      });
   }
   b->n_mt = (int64_t)mt.size();
   b->n_ct = (int64_t)ct.size();
@@ -1625,10 +1654,10 @@ emc_status emc_batch_iterate(emc_batch* b) {
     BTRY(b, c, emc_expand(c));
     BCK(b, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * c->N,
                            cudaMemcpyDeviceToDevice, b->st));
-    maps.a0[i] = c->tmKh;
-    maps.a1[i] = c->tmKh;
-    maps.b0[i] = c->tmBhi;
-    maps.b1[i] = c->tmBlo;
+    maps.a0[i] = b->pair ? c->tmKh64 : c->tmKh;
+    maps.a1[i] = maps.a0[i];
+    maps.b0[i] = b->pair ? c->tmBhi64 : c->tmBhi;
+    maps.b1[i] = b->pair ? c->tmBlo64 : c->tmBlo;
   }
   for (int i = n; i < kMaxBatch; ++i) {  // unused sets repeat the first (never indexed)
     maps.a0[i] = maps.a0[0];
@@ -1636,7 +1665,10 @@ emc_status emc_batch_iterate(emc_batch* b) {
     maps.b0[i] = maps.b0[0];
     maps.b1[i] = maps.b1[0];
   }
-  BCK(b, launch_batch_maximize_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
+  if (b->pair)
+    BCK(b, launch_batch_maximize_pair_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
+  else
+    BCK(b, launch_batch_maximize_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];
     BTRY(b, c, mixed_resp_pass(c));
@@ -1646,8 +1678,8 @@ emc_status emc_batch_iterate(emc_batch* b) {
     BCK(b, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, b->st));
     maps.a0[i] = c->tmPhi;
     maps.a1[i] = c->tmPlo;
-    maps.b0[i] = c->tmKt;
-    maps.b1[i] = c->tmKt;
+    maps.b0[i] = b->cmp_pair ? c->tmKt128 : c->tmKt;
+    maps.b1[i] = maps.b0[i];
   }
   for (int i = n; i < kMaxBatch; ++i) {
     maps.a0[i] = maps.a0[0];
@@ -1655,7 +1687,10 @@ emc_status emc_batch_iterate(emc_batch* b) {
     maps.b0[i] = maps.b0[0];
     maps.b1[i] = maps.b1[0];
   }
-  BCK(b, launch_batch_compress_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
+  if (b->cmp_pair)
+    BCK(b, launch_batch_compress_pair_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
+  else
+    BCK(b, launch_batch_compress_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
   c0->launches += 2;
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];

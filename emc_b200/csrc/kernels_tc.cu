@@ -761,6 +761,57 @@ struct EpiBatchCmp {
   __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
 };
 
+// The batched maximize on SM pairs: the tile's local0 is its 256-row pair
+// tile, so this CTA's 128-row block is 2 local0 + rank.
+struct EpiBatchMaxPair {
+  static constexpr bool kListed = true;
+  static constexpr int kSets = kMaxBatch;
+  static constexpr int kEpiWarps = 4;
+  static constexpr int kSmemBytes = EpiMax::kSmemBytes;
+  BatchMaxArgs a;
+  EpiMax inner;
+  int64_t row0;
+
+  __device__ void tile_begin(int64_t t, int64_t, int tid, uint8_t* smem) {
+    const TileDesc d = a.tiles[t];
+    inner.a = a.set[d.set];
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    const int64_t mrow = (int64_t)d.local0 * 2 + rank;
+    row0 = mrow * BM;
+    inner.tile_begin(mrow, d.cell, tid, smem);
+  }
+  __device__ void row_begin(int64_t row) { inner.row_begin(row0 + row); }
+  __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) { inner.consume(c, v, smem); }
+  __device__ void row_end() { inner.row_end(); }
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
+};
+
+// The batched compress on SM pairs (256-rotation pair tiles).
+struct EpiBatchCmpPair {
+  static constexpr bool kListed = true;
+  static constexpr int kSets = kMaxBatch;
+  static constexpr int kEpiWarps = 4;
+  static constexpr int kSmemBytes = EpiCmp::kSmemBytes;
+  BatchCmpArgs a;
+  EpiCmp inner;
+  int64_t row0;
+
+  __device__ void tile_begin(int64_t t, int64_t, int tid, uint8_t* smem) {
+    const TileDesc d = a.tiles[t];
+    inner.a = a.set[d.set];
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    const int64_t mrow = (int64_t)d.local0 * 2 + rank;
+    row0 = mrow * BM;
+    inner.tile_begin(mrow, d.cell, tid, smem);
+  }
+  __device__ void row_begin(int64_t row) { inner.row_begin(row0 + row); }
+  __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) { inner.consume(c, v, smem); }
+  __device__ void row_end() { inner.row_end(); }
+  __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
+};
+
 template <int NA, int NB, int STAGES, bool M_INNER, int BK, class Epi>
 cudaError_t run_gemm(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n_tiles,
                      int64_t k_blocks, const Epi& epi, TcStatus* st, int num_sms,
@@ -841,12 +892,12 @@ constexpr int kPairBK = 64;
 constexpr int kPairStages = 4;
 
 // NA / NB: 1, or 2 for an operand split into FP16 hi + lo (one of them).
+// A listed epilogue (Epi::kListed) supplies the tiles: TileDesc rows of the
+// pair (a_row, b_row: the CTA adds 128 x rank), k-block count and tensor-map
+// set; its row_begin then receives the row inside this CTA's 128 rows.
 template <int NA, int NB, bool M_INNER, class Epi>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
-    tc_pair_kernel(const __grid_constant__ CUtensorMap tmA0,
-                   const __grid_constant__ CUtensorMap tmA1,
-                   const __grid_constant__ CUtensorMap tmB0,
-                   const __grid_constant__ CUtensorMap tmB1, const int64_t m_tiles,
+    tc_pair_kernel(const __grid_constant__ TmapSet<Epi::kSets> maps, const int64_t m_tiles,
                    const int64_t n_tiles, const int64_t k_blocks, const int raster,
                    const Epi epi, TcStatus* status) {
   static_assert(NA * NB == 2, "one hi/lo split per contraction");
@@ -932,10 +983,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       int64_t issued = 0;
       bool ok = true;
       for (int64_t t = cid; t < num_tiles && ok; t += ncl) {
-        int64_t mt, nt;
-        tile_mn(t, mt, nt);
-        const int ar = (int)(mt * 256 + rank * 128), br = (int)(nt * 256 + rank * 128);
-        for (int64_t kb = 0; kb < k_blocks; ++kb) {
+        int ar, br, set = 0;
+        int64_t kbs = k_blocks;
+        if constexpr (Epi::kListed) {
+          const TileDesc d = epi.a.tiles[t];
+          ar = d.a_row + (int)rank * 128;
+          br = d.b_row + (int)rank * 128;
+          kbs = d.k_blocks;
+          set = d.set;
+        } else {
+          int64_t mt, nt;
+          tile_mn(t, mt, nt);
+          ar = (int)(mt * 256 + rank * 128);
+          br = (int)(nt * 256 + rank * 128);
+        }
+        const CUtensorMap* tA0 = &maps.a0[set];
+        const CUtensorMap* tA1 = &maps.a1[set];
+        const CUtensorMap* tB0 = &maps.b0[set];
+        const CUtensorMap* tB1 = &maps.b1[set];
+        for (int64_t kb = 0; kb < kbs; ++kb) {
           if (!bounded_wait(smem_u32(&empty_bar[s]), ph ^ 1, ctl, 1)) {
             ok = false;
             break;
@@ -945,11 +1011,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           const uint32_t fb_leader = peer_addr(fb, 0);
           const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
           const int kc = (int)(kb * kPairBK);
-          tma_load_2d_pair(base, &tmA0, kc, ar, fb_leader);
-          if (NA == 2) tma_load_2d_pair(base + A_BYTES, &tmA1, kc, ar, fb_leader);
+          tma_load_2d_pair(base, tA0, kc, ar, fb_leader);
+          if (NA == 2) tma_load_2d_pair(base + A_BYTES, tA1, kc, ar, fb_leader);
           const uint32_t bbase = base + NA * A_BYTES;
-          tma_load_2d_pair(bbase, &tmB0, kc, br, fb_leader);
-          if (NB == 2) tma_load_2d_pair(bbase + B_BYTES, &tmB1, kc, br, fb_leader);
+          tma_load_2d_pair(bbase, tB0, kc, br, fb_leader);
+          if (NB == 2) tma_load_2d_pair(bbase + B_BYTES, tB1, kc, br, fb_leader);
           ++issued;
           if (++s == STAGES) {
             s = 0;
@@ -998,7 +1064,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         }
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
-        for (int64_t kb = 0; kb < k_blocks; ++kb) {
+        int64_t kbs = k_blocks;
+        if constexpr (Epi::kListed) kbs = epi.a.tiles[t].k_blocks;
+        for (int64_t kb = 0; kb < kbs; ++kb) {
           if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3)) {
             ok = false;
             abort_pair();
@@ -1052,11 +1120,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       epi_bar();
       if (epi_abort) break;
       tc_fence_after();
-      int64_t mt, nt;
-      tile_mn(t, mt, nt);
-      const int64_t mrow = mt * 2 + rank;  // this CTA's 128-pattern block
-      e.tile_begin(mrow, nt, ep_tid, epi_smem);
-      e.row_begin(mrow * BM + quarter * 32 + lane);
+      int64_t mt = t, nt = 0;
+      if constexpr (Epi::kListed) {
+        e.tile_begin(t, 0, ep_tid, epi_smem);
+        e.row_begin(quarter * 32 + lane);
+      } else {
+        tile_mn(t, mt, nt);
+        const int64_t mrow = mt * 2 + rank;  // this CTA's 128-row block
+        e.tile_begin(mrow, nt, ep_tid, epi_smem);
+        e.row_begin(mrow * BM + quarter * 32 + lane);
+      }
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
       for (int c = 0; c < BN; c += 16) {
@@ -1084,9 +1157,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 }
 
 template <int NA, int NB, bool M_INNER, class Epi>
-cudaError_t run_pair(const CUtensorMap& a0, const CUtensorMap& a1, const CUtensorMap& b0,
-                     const CUtensorMap& b1, int64_t m_tiles, int64_t n_tiles, int64_t k_blocks,
-                     const Epi& epi, TcStatus* st, int num_sms, cudaStream_t stream, int raster) {
+cudaError_t run_pair(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n_tiles,
+                     int64_t k_blocks, const Epi& epi, TcStatus* st, int num_sms,
+                     cudaStream_t stream, int raster) {
   constexpr uint32_t stage = 128 * kPairBK * 2 * (NA + NB);
   const size_t dyn = (size_t)kPairStages * stage + 1024;
   auto kern = tc_pair_kernel<NA, NB, M_INNER, Epi>;
@@ -1096,7 +1169,7 @@ cudaError_t run_pair(const CUtensorMap& a0, const CUtensorMap& a1, const CUtenso
   if (tiles == 0) return cudaSuccess;
   const int64_t pairs = num_sms / 2;
   const int grid = 2 * (int)(tiles < pairs ? tiles : pairs);
-  kern<<<grid, kThreads, dyn, stream>>>(a0, a1, b0, b1, m_tiles, n_tiles, k_blocks,
+  kern<<<grid, kThreads, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks,
                                         raster < 1 ? 1 : raster, epi, st);
   return cudaGetLastError();
 }
@@ -1458,7 +1531,7 @@ cudaError_t launch_maximize_pair_tc(const CUtensorMap& tmK, const CUtensorMap& t
   epi.a = e;
   // 256-pattern pair tiles (the last may reach past Mpad: zero-filled by TMA,
   // masked by the epilogue), 64-wide K-steps
-  return run_pair<1, 2, true>(tmK, tmK, tmBhi, tmBlo, (Mpad + 255) / 256, Rpad / BN,
+  return run_pair<1, 2, true>(one_set(tmK, tmK, tmBhi, tmBlo), (Mpad + 255) / 256, Rpad / BN,
                              Kpad / kPairBK, epi, status, num_sms, st, raster);
 }
 
@@ -1469,8 +1542,8 @@ cudaError_t launch_compress_pair_tc(const CUtensorMap& tmPhi, const CUtensorMap&
   EpiCmp epi;
   epi.a = e;
   // 256-rotation pair tiles (Rpad is a multiple of 256), pixel tiles inner
-  return run_pair<2, 1, false>(tmPhi, tmPlo, tmKt, tmKt, Rpad / 256, Ppad / BN, Npad / kPairBK,
-                               epi, status, num_sms, st, raster);
+  return run_pair<2, 1, false>(one_set(tmPhi, tmPlo, tmKt, tmKt), Rpad / 256, Ppad / BN,
+                               Npad / kPairBK, epi, status, num_sms, st, raster);
 }
 
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
@@ -1511,6 +1584,22 @@ cudaError_t launch_batch_maximize_tc(const TmapSet<kMaxBatch>& maps, int64_t n_t
   EpiBatchMax epi;
   epi.a = e;
   return run_gemm<1, 2, 5, true, kMaximizeBK>(maps, n_tiles, 1, 0, epi, status, num_sms, st);
+}
+
+cudaError_t launch_batch_maximize_pair_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                          const BatchMaxArgs& e, TcStatus* status, int num_sms,
+                                          cudaStream_t st) {
+  EpiBatchMaxPair epi;
+  epi.a = e;
+  return run_pair<1, 2, true>(maps, n_tiles, 1, 0, epi, status, num_sms, st, 1);
+}
+
+cudaError_t launch_batch_compress_pair_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                          const BatchCmpArgs& e, TcStatus* status, int num_sms,
+                                          cudaStream_t st) {
+  EpiBatchCmpPair epi;
+  epi.a = e;
+  return run_pair<2, 1, false>(maps, n_tiles, 1, 0, epi, status, num_sms, st, 1);
 }
 
 cudaError_t launch_batch_compress_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,

@@ -159,6 +159,14 @@ struct BatchCmpArgs {
 cudaError_t launch_batch_maximize_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
                                      const BatchMaxArgs& e, TcStatus* status, int num_sms,
                                      cudaStream_t st);
+// The same on SM pairs: tiles of 256 rows (local0 = pair row tile), tensor
+// maps with boxes of 128 rows x kPairBoxK.
+cudaError_t launch_batch_maximize_pair_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                          const BatchMaxArgs& e, TcStatus* status, int num_sms,
+                                          cudaStream_t st);
+cudaError_t launch_batch_compress_pair_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
+                                          const BatchCmpArgs& e, TcStatus* status, int num_sms,
+                                          cudaStream_t st);
 cudaError_t launch_batch_compress_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,
                                      const BatchCmpArgs& e, TcStatus* status, int num_sms,
                                      cudaStream_t st);

@@ -80,3 +80,29 @@ def test_batch_rejects_fp32_contexts():
     with make_ctx(d, "poisson", "nearest", "fp32") as c:
         with pytest.raises(E.EmcError):
             E.Batch([c])
+
+
+def test_batched_pair_maximize_matches_separate_iterations():
+    """Both batched contractions on SM pairs (chosen when the datasets that
+    use pairs on their own hold most of the work) against one-by-one
+    iterations."""
+    import emc_b200 as E
+    ds = _datasets()
+    solo = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
+    for c in solo:
+        c.iterate()
+    refs = [c.get_model() for c in solo]
+    for c in solo:
+        c.close()
+    ctxs = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
+    try:
+        for c in ctxs:
+            c.set_tuning(1, 2, 1, 1)
+        with E.Batch(ctxs) as b:
+            b.iterate()
+            b.synchronize()
+            for c, m in zip(ctxs, refs):
+                assert rel(c.get_model(), m) < 1e-5, rel(c.get_model(), m)
+    finally:
+        for c in ctxs:
+            c.close()
