@@ -49,7 +49,8 @@ class IterStats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("maximize_raster", C.c_int32), ("compress_raster", C.c_int32),
-                ("maximize_pair", C.c_int32), ("compress_pair", C.c_int32)]
+                ("maximize_pair", C.c_int32), ("compress_pair", C.c_int32),
+                ("maximize_sparse", C.c_int32)]
 
 
 class SynthConfig(C.Structure):
@@ -390,11 +391,26 @@ class Context:
         self._c(lib().emc_get_tuning(self._h, C.byref(t)))
         return t.maximize_raster, t.compress_raster, t.maximize_pair, t.compress_pair
 
-    def set_tuning(self, maximize_raster, compress_raster, maximize_pair=None, compress_pair=None):
-        cur = self.get_tuning()
-        maximize_pair = cur[2] if maximize_pair is None else maximize_pair
-        compress_pair = cur[3] if compress_pair is None else compress_pair
-        t = Tuning(maximize_raster, compress_raster, int(maximize_pair), int(compress_pair))
+    def set_tuning(self, maximize_raster, compress_raster, maximize_pair=None, compress_pair=None,
+                   maximize_sparse=None):
+        t = Tuning()
+        self._c(lib().emc_get_tuning(self._h, C.byref(t)))
+        t.maximize_raster, t.compress_raster = int(maximize_raster), int(compress_raster)
+        if maximize_pair is not None:
+            t.maximize_pair = int(maximize_pair)
+        if compress_pair is not None:
+            t.compress_pair = int(compress_pair)
+        if maximize_sparse is not None:
+            t.maximize_sparse = int(maximize_sparse)
+        self._c(lib().emc_set_tuning(self._h, C.byref(t)))
+
+    def set_sparse_maximize(self, on: bool):
+        """FP32 poisson contexts: evaluate the log-likelihood as a gather over
+        each pattern's photon list (its non-zero pixels) instead of the dense
+        rotation x pixel contraction."""
+        t = Tuning()
+        self._c(lib().emc_get_tuning(self._h, C.byref(t)))
+        t.maximize_sparse = int(bool(on))
         self._c(lib().emc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, candidates=(1, 2, 4, 8, 16)):

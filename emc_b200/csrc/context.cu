@@ -145,7 +145,14 @@ struct emc_context {
   // raster bands of the maximize / compress tile orders and the SM-pair forms
   // (defaults from measurements at 64^3 and 128^3, set per shape in
   // alloc_work; emc_autotune re-measures)
-  emc_tuning tune{1, 6, 0, 0};
+  emc_tuning tune{1, 6, 0, 0, 0};
+  // photon-list log-likelihood (FP32 poisson): counts as CSR, log W pixel-major
+  int64_t* d_csr_row = nullptr;
+  int32_t* d_csr_col = nullptr;
+  float* d_csr_val = nullptr;
+  int64_t csr_cap = 0;
+  bool csr_valid = false;
+  float* d_ST = nullptr;
   bool prof = false;
   cudaEvent_t ev[2][6] = {{nullptr}};
   int cur = 0;
@@ -475,6 +482,7 @@ static emc_status finish_patterns(emc_context* c) {
                    "%d counts are not integers in [0, 2048]; the mixed path needs them exact in FP16",
                    bad);
   c->have_pat = true;
+  c->csr_valid = false;
   return EMC_OK;
 }
 
@@ -659,6 +667,54 @@ static emc_status mixed_resp_pass(emc_context* c) {
   return EMC_OK;
 }
 
+// The poisson log-likelihood as a gather over each pattern's photon list:
+// the counts' CSR (built once per pattern upload) and log W transposed to
+// pixel-major rows so a block of rotations reads one coalesced row per photon.
+static emc_status sparse_loglik(emc_context* c) {
+  const int64_t N = c->N, R = c->R, npa = c->npa;
+  if (!c->csr_valid) {
+    if (!c->d_csr_row) TRY(c->alloc(&c->d_csr_row, N + 1));
+    std::vector<int64_t> cnt(N), row(N + 1, 0);
+    int64_t* d_cnt = c->d_csr_row + 1;  // counts land where row_ptr[1..N] goes
+    CK(c, launch_csr_count(c->d_K, N, npa, d_cnt, c->st));
+    CK(c, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int64_t) * N, cudaMemcpyDeviceToHost, c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    for (int64_t p = 0; p < N; ++p) row[p + 1] = row[p] + cnt[p];
+    const int64_t nnz = row[N];
+    if (nnz > c->csr_cap) {
+      for (void* q : {(void*)c->d_csr_col, (void*)c->d_csr_val})
+        if (q) c->release(q);
+      c->d_csr_col = nullptr;
+      c->d_csr_val = nullptr;
+      c->csr_cap = 0;
+      TRY(c->alloc(&c->d_csr_col, nnz + 1));
+      TRY(c->alloc(&c->d_csr_val, nnz + 1));
+      c->csr_cap = nnz + 1;
+    }
+    CK(c, cudaMemcpyAsync(c->d_csr_row, row.data(), sizeof(int64_t) * (N + 1),
+                          cudaMemcpyHostToDevice, c->st));
+    CK(c, launch_csr_fill(c->d_K, N, npa, c->d_csr_row, c->d_csr_col, c->d_csr_val, c->st));
+    c->csr_valid = true;
+  }
+  const int64_t ldT = (R + 3) / 4 * 4;
+  if (!c->d_ST) TRY(c->alloc(&c->d_ST, npa * ldT));
+  CK(c, launch_transpose(c->d_S, R, npa, c->d_ST, ldT, c->st));
+  SparseLLArgs a{};
+  a.row_ptr = c->d_csr_row;
+  a.col = c->d_csr_col;
+  a.val = c->d_csr_val;
+  a.logWT = c->d_ST;
+  a.ldT = ldT;
+  a.scaling = c->d_scaling;
+  a.rowstat = c->d_rowstat;
+  a.R = R;
+  a.N = N;
+  a.LL = c->d_LL;
+  CK(c, launch_ll_sparse(a, c->st));
+  c->launches += 2;
+  return EMC_OK;
+}
+
 extern "C" {
 
 emc_status emc_maximize(emc_context* c) {
@@ -667,7 +723,9 @@ emc_status emc_maximize(emc_context* c) {
   const int64_t R = c->R, N = c->N;
   CK(c, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * N,
                         cudaMemcpyDeviceToDevice, c->st));
-  if (!c->mixed) {
+  if (!c->mixed && c->tune.maximize_sparse) {
+    TRY(sparse_loglik(c));
+  } else if (!c->mixed) {
     LLArgs l{};
     l.A = c->d_S;
     l.K = c->d_K;
@@ -683,6 +741,8 @@ emc_status emc_maximize(emc_context* c) {
     l.poisson = c->gauss ? 0 : 1;
     l.LL = c->d_LL;
     CK(c, launch_ll_fp32(l, c->st));
+  }
+  if (!c->mixed) {
     c->mark(2);
     int nparts = 0;
     CK(c, launch_softmax_fp32(c->d_LL, R, N, c->d_plogp_part, &nparts, c->d_lse32, c->st));
@@ -854,8 +914,11 @@ emc_status emc_get_tuning(const emc_context* c, emc_tuning* t) {
 emc_status emc_set_tuning(emc_context* c, const emc_tuning* t) {
   if (!c || !t || t->maximize_raster < 1 || t->compress_raster < 1 ||
       (t->maximize_pair != 0 && t->maximize_pair != 1) ||
-      (t->compress_pair != 0 && t->compress_pair != 1))
+      (t->compress_pair != 0 && t->compress_pair != 1) ||
+      (t->maximize_sparse != 0 && t->maximize_sparse != 1))
     return EMC_ERR_ARG;
+  if (t->maximize_sparse && (c->mixed || c->gauss))
+    return c->fail(EMC_ERR_UNSUPPORTED, "the photon-list log-likelihood is an FP32 poisson form");
   c->tune = *t;
   return EMC_OK;
 }
@@ -896,7 +959,7 @@ emc_status emc_autotune(emc_context* c, const int32_t* cand, int32_t n, float* m
     for (int32_t i = 0; i < n && s == EMC_OK; ++i) {
       float tmax = 1e30f;
       for (int32_t pair = 0; pair < 2 && s == EMC_OK; ++pair) {
-        c->tune = emc_tuning{cand[i], cand[i], pair, pair};
+        c->tune = emc_tuning{cand[i], cand[i], pair, pair, keep.maximize_sparse};
         if ((s = restore()) != EMC_OK || (s = emc_iterate(c, nullptr)) != EMC_OK) break;
         float t[5];
         if ((s = c->cuda(cudaEventSynchronize(c->ev[c->cur][5]), "autotune")) != EMC_OK) break;

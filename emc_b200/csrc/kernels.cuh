@@ -44,6 +44,34 @@ struct LLArgs {
 };
 cudaError_t launch_ll_fp32(const LLArgs& a, cudaStream_t st);
 
+// Photon-list form of the poisson log-likelihood (FP32 path):
+// LL[r][p] = sum over the non-zero pixels e of pattern p of K_e log W[r][j_e]
+//            - phi_p sum W_r,
+// from the counts in CSR (row_ptr [N+1], col = compact pixel, val = count)
+// and log W pixel-major (logWT [npa][ldT], ldT >= R).
+struct SparseLLArgs {
+  const int64_t* row_ptr;
+  const int32_t* col;
+  const float* val;
+  const float* logWT;
+  int64_t ldT;
+  const float* scaling;
+  const double* rowstat;  // sum W_r
+  int64_t R, N;
+  float* LL;              // [R][N]
+};
+// ldT % 4 == 0 and logWT 16-byte aligned (each thread gathers 4 rotations).
+cudaError_t launch_ll_sparse(const SparseLLArgs& a, cudaStream_t st);
+// logWT[j][r] = S[r][j] (tiled transpose, [R][npa] -> [npa][ldT]).
+cudaError_t launch_transpose(const float* S, int64_t R, int64_t npa, float* ST, int64_t ldT,
+                             cudaStream_t st);
+// CSR of the non-zero entries of K [N][npa]: nnz per row (pass 1), then the
+// entries in pixel order (pass 2, row_ptr given).
+cudaError_t launch_csr_count(const float* K, int64_t N, int64_t npa, int64_t* count,
+                             cudaStream_t st);
+cudaError_t launch_csr_fill(const float* K, int64_t N, int64_t npa, const int64_t* row_ptr,
+                            int32_t* col, float* val, cudaStream_t st);
+
 // Per-pattern softmax over r of X[r][p] (in place), FP32 arithmetic as the
 // reference; plogp_part[blockIdx] receives sum P log P partials (FP64) and
 // lse[p] (optional) the pattern's log-sum-exp.

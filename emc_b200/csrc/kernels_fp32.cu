@@ -532,6 +532,150 @@ cudaError_t launch_expand(const ExpandArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------ photon lists --
+// 128 threads x 4 rotations = 512 rotations per block, 16 patterns per block:
+// for each pattern the block walks its non-zero pixels (uniform loads of the
+// CSR entry) and every thread gathers 16 bytes of log W (its 4 rotations) at
+// that pixel, so one entry reads one coalesced 2 KB row of logWT.  Pattern
+// blocks vary fastest in the grid, so the blocks resident at one time share
+// one rotation block's columns of logWT (npa x 2 KB) in L2.  FP32 partial
+// sums over chunks of 32 photons are folded into FP64 totals, as the dense
+// contraction folds each 32-pixel K-step.  The 16 x 512 results leave through
+// shared memory as rows of LL.
+constexpr int kSparseRot = 512, kSparsePat = 16;
+__global__ void __launch_bounds__(128) sparse_ll_kernel(const SparseLLArgs a) {
+  __shared__ float tile[kSparsePat][kSparseRot + 1];
+  const int64_t r0 = (int64_t)blockIdx.y * kSparseRot + 4 * threadIdx.x;
+  const int64_t p0 = (int64_t)blockIdx.x * kSparsePat;
+  const bool rv = r0 < a.R;  // ldT >= R rounded up to 4: the whole float4 is in bounds
+  double sw[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) sw[u] = r0 + u < a.R ? a.rowstat[r0 + u] : 0.0;
+  for (int i = 0; i < kSparsePat; ++i) {
+    const int64_t p = p0 + i;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (p < a.N && rv) {
+      const int64_t e0 = a.row_ptr[p], e1 = a.row_ptr[p + 1];
+      double tot[4] = {0.0, 0.0, 0.0, 0.0};
+      int64_t e = e0;
+      while (e < e1) {
+        const int64_t ce = e + 32 < e1 ? e + 32 : e1;
+        float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+        for (; e + 2 <= ce; e += 2) {
+          const int32_t j0 = __ldg(a.col + e), j1 = __ldg(a.col + e + 1);
+          const float k0 = __ldg(a.val + e), k1 = __ldg(a.val + e + 1);
+          const float4 w0 = __ldg(reinterpret_cast<const float4*>(a.logWT + (int64_t)j0 * a.ldT + r0));
+          const float4 w1 = __ldg(reinterpret_cast<const float4*>(a.logWT + (int64_t)j1 * a.ldT + r0));
+          s0.x = fmaf(k0, w0.x, s0.x); s0.y = fmaf(k0, w0.y, s0.y);
+          s0.z = fmaf(k0, w0.z, s0.z); s0.w = fmaf(k0, w0.w, s0.w);
+          s1.x = fmaf(k1, w1.x, s1.x); s1.y = fmaf(k1, w1.y, s1.y);
+          s1.z = fmaf(k1, w1.z, s1.z); s1.w = fmaf(k1, w1.w, s1.w);
+        }
+        if (e < ce) {
+          const float k0 = __ldg(a.val + e);
+          const float4 w0 =
+              __ldg(reinterpret_cast<const float4*>(a.logWT + (int64_t)__ldg(a.col + e) * a.ldT + r0));
+          s0.x = fmaf(k0, w0.x, s0.x); s0.y = fmaf(k0, w0.y, s0.y);
+          s0.z = fmaf(k0, w0.z, s0.z); s0.w = fmaf(k0, w0.w, s0.w);
+          ++e;
+        }
+        tot[0] += (double)(s0.x + s1.x);
+        tot[1] += (double)(s0.y + s1.y);
+        tot[2] += (double)(s0.z + s1.z);
+        tot[3] += (double)(s0.w + s1.w);
+      }
+      const double ph = (double)a.scaling[p];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = (float)(tot[u] - ph * sw[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) tile[i][4 * threadIdx.x + u] = v[u];
+  }
+  __syncthreads();
+  // half a warp per LL row: lane & 15 = pattern
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t p = p0 + (lane & 15);
+  for (int rr = 2 * w + (lane >> 4); rr < kSparseRot; rr += 8) {
+    const int64_t ro = (int64_t)blockIdx.y * kSparseRot + rr;
+    if (ro < a.R && p < a.N) a.LL[ro * a.N + p] = tile[lane & 15][rr];
+  }
+}
+
+cudaError_t launch_ll_sparse(const SparseLLArgs& a, cudaStream_t st) {
+  if (a.R <= 0 || a.N <= 0) return cudaSuccess;
+  if (a.ldT % 4 != 0 || a.ldT < a.R || (reinterpret_cast<uintptr_t>(a.logWT) & 15u))
+    return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((a.N + kSparsePat - 1) / kSparsePat),
+            (unsigned)((a.R + kSparseRot - 1) / kSparseRot));
+  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  sparse_ll_kernel<<<grid, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+__global__ void transpose_kernel(const float* S, int64_t R, int64_t npa, float* ST, int64_t ldT) {
+  __shared__ float t[32][33];
+  const int64_t j0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int64_t r = r0 + i, j = j0 + threadIdx.x;
+    t[i][threadIdx.x] = (r < R && j < npa) ? S[r * npa + j] : 0.0f;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int64_t j = j0 + i, r = r0 + threadIdx.x;
+    if (j < npa && r < R) ST[j * ldT + r] = t[threadIdx.x][i];
+  }
+}
+
+cudaError_t launch_transpose(const float* S, int64_t R, int64_t npa, float* ST, int64_t ldT,
+                             cudaStream_t st) {
+  dim3 grid((unsigned)((npa + 31) / 32), (unsigned)((R + 31) / 32));
+  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(S, R, npa, ST, ldT);
+  return cudaGetLastError();
+}
+
+// one warp per pattern
+__global__ void csr_count_kernel(const float* K, int64_t N, int64_t npa, int64_t* count) {
+  const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= N) return;
+  int64_t n = 0;
+  for (int64_t j = lane; j < npa; j += 32) n += K[p * npa + j] != 0.0f;
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if (lane == 0) count[p] = n;
+}
+
+__global__ void csr_fill_kernel(const float* K, int64_t N, int64_t npa, const int64_t* row_ptr,
+                                int32_t* col, float* val) {
+  const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= N) return;
+  int64_t out = row_ptr[p];
+  for (int64_t j0 = 0; j0 < npa; j0 += 32) {
+    const int64_t j = j0 + lane;
+    const float k = j < npa ? K[p * npa + j] : 0.0f;
+    const unsigned nz = __ballot_sync(0xffffffffu, k != 0.0f);
+    if (k != 0.0f) {
+      const int64_t o = out + __popc(nz & ((1u << lane) - 1u));
+      col[o] = (int32_t)j;
+      val[o] = k;
+    }
+    out += __popc(nz);
+  }
+}
+
+cudaError_t launch_csr_count(const float* K, int64_t N, int64_t npa, int64_t* count,
+                             cudaStream_t st) {
+  csr_count_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(K, N, npa, count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_csr_fill(const float* K, int64_t N, int64_t npa, const int64_t* row_ptr,
+                            int32_t* col, float* val, cudaStream_t st) {
+  csr_fill_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(K, N, npa, row_ptr, col, val);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ll_fp32(const LLArgs& a, cudaStream_t st) {
   if (a.R <= 0 || a.N <= 0) return cudaSuccess;
   dim3 grid((unsigned)((a.N + TN - 1) / TN), (unsigned)((a.R + TM - 1) / TM));

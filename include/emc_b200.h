@@ -177,6 +177,9 @@ typedef struct {
   int32_t maximize_raster, compress_raster;
   int32_t maximize_pair; /* 1: the maximize contraction on SM pairs (cta_group::2) */
   int32_t compress_pair; /* 1: the compress contraction on SM pairs */
+  int32_t maximize_sparse; /* FP32 poisson contexts: 1 = the log-likelihood as a
+                              photon-list gather over each pattern's non-zero pixels
+                              instead of the dense contraction */
 } emc_tuning;
 emc_status emc_get_tuning(const emc_context *ctx, emc_tuning *t);
 emc_status emc_set_tuning(emc_context *ctx, const emc_tuning *t);
