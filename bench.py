@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--train-iters", type=int, default=5,
                     help="dense iterations whose responsibilities train the proposal network")
     ap.add_argument("--train-epochs", type=int, default=12)
+    ap.add_argument("--min-cells", type=int, default=4,
+                    help="cells of each pattern's previous responsibility kept in a proposed iteration")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -252,11 +254,11 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     """The learned orientation proposal on the same data: rotations sorted by
     their coarse cell (the 420 rotations of the n=2 sampling), --train-iters
     dense iterations whose responsibilities train the BF16 network, then
-    --learned-steps proposed iterations.  Each proposed iteration selects, per
-    pattern, the cells of the blended posterior (network prediction and the
-    previous iteration's cell responsibilities) up to a predicted mass of
-    0.999 (at most 16 cells); the dense iteration runs instead when the mean
-    predicted mass falls below 0.99."""
+    --learned-steps proposed iterations.  Each proposed iteration evaluates,
+    per pattern, the --min-cells cells holding most of its responsibility in
+    the previous iteration, then the network's most probable cells up to a
+    predicted mass of 0.999 (at most 16 cells in all); the dense iteration
+    runs instead when the mean predicted mass falls below 0.99."""
     import torch
     from emc_b200.proposal import LearnedProposal, sorted_rotations
     w = d["workload"]
@@ -278,7 +280,20 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     probs = lp.predict(x)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
-    max_cells, target, threshold = 16, 0.999, 0.99
+    max_cells, target, threshold, min_cells = 16, 0.999, 0.99, a.min_cells
+
+    def captured_by(scores):
+        """True next-iteration mass on the cells a network alone selects (in
+        order of its probabilities up to `target`, at most max_cells)."""
+        srt = torch.sort(scores, dim=1, descending=True)
+        k = torch.clamp((torch.cumsum(srt.values, 1) < target).sum(1) + 1, max=max_cells)
+        sel = torch.arange(n_cells, device=scores.device)[None, :] < k[:, None]
+        return (torch.gather(t_next, 1, srt.indices) * sel).sum(1)
+
+    def rel_err(m, ref, where=None):
+        if where is None:
+            return float(np.linalg.norm(m - ref) / np.linalg.norm(ref))
+        return float(np.linalg.norm((m - ref)[where]) / np.linalg.norm(ref[where]))
 
     # accuracy of one proposed iteration against the dense iteration from the
     # same state, and the true responsibility mass its candidate cells hold
@@ -286,38 +301,38 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     ctx.iterate(stats=False)
     m_dense, w_dense = ctx.get_model(), ctx.get_buffer(E.BUF_WEIGHT).copy()
     t_next = lp.targets()
+    # the network's cells alone
     ctx.set_model(m0)
     ctx.set_scaling(s0)
-    sel_probs = LearnedProposal.blend(probs, t_dense)
-    st = lp.iterate(sel_probs, max_cells, target, threshold)
+    lp.iterate(probs, max_cells, target, threshold)
+    m_net = ctx.get_model()
+    # the selection rule used below: the previous posterior's top cells, then the network's
+    ctx.set_model(m0)
+    ctx.set_scaling(s0)
+    st = lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=t_dense)
     m_prop = ctx.get_model()
-    srt = torch.sort(sel_probs, dim=1, descending=True)
-    k = torch.clamp((torch.cumsum(srt.values, 1) < target).sum(1) + 1, max=max_cells)
-    keep = torch.arange(n_cells, device=sel_probs.device)[None, :] < k[:, None]
-    captured = (torch.gather(t_next, 1, srt.indices) * keep).sum(1)
+    cand = lp.targets() > 0  # candidate cells (one whose responsibilities all underflow reads as 0)
+    captured = (t_next * cand).sum(1)
     heavy = w_dense > np.quantile(w_dense[w_dense > 0], 0.1)
+    untrained = LearnedProposal(ctx, cell, n_cells, bf16=True, seed=2).predict(x)
     acc = {"captured_mass_mean": float(captured.mean()), "captured_mass_min": float(captured.min()),
            "patterns_below_0.99": float((captured < 0.99).float().mean()),
-           "model_rel_err_vs_dense": float(np.linalg.norm(m_prop - m_dense) /
-                                           np.linalg.norm(m_dense)),
-           "model_rel_err_vs_dense_weight_gt_p10": float(
-               np.linalg.norm((m_prop - m_dense)[heavy]) / np.linalg.norm(m_dense[heavy])),
-           "predicted_mass_mean": st["mean_mass"]}
-    untrained = LearnedProposal(ctx, cell, n_cells, bf16=True, seed=2).predict(x)
-    srt_u = torch.sort(untrained, dim=1, descending=True)
-    ku = torch.clamp((torch.cumsum(srt_u.values, 1) < target).sum(1) + 1, max=max_cells)
-    keep_u = torch.arange(n_cells, device=x.device)[None, :] < ku[:, None]
-    acc["untrained_network_captured_mass_mean"] = float(
-        (torch.gather(t_next, 1, srt_u.indices) * keep_u).sum(1).mean())
+           "model_rel_err_vs_dense": rel_err(m_prop, m_dense),
+           "model_rel_err_vs_dense_weight_gt_p10": rel_err(m_prop, m_dense, heavy),
+           "cells_per_pattern": st["pairs"] / N,
+           "predicted_mass_mean": st["mean_mass"],
+           "network_cells_only": {"model_rel_err_vs_dense": rel_err(m_net, m_dense),
+                                  "captured_mass_mean": float(captured_by(probs).mean())},
+           "untrained_network_cells_only_captured_mass_mean": float(captured_by(untrained).mean())}
 
-    # timed: proposed iterations, each selecting from the blend of the network
-    # and the previous iteration's cell responsibilities
+    # timed: proposed iterations, each keeping the top cells of the previous
+    # iteration's cell responsibilities and adding the network's
     ctx.set_model(m0)
     ctx.set_scaling(s0)
     prev = t_dense
     ext = torch.cuda.ExternalStream(ctx.stream)
     for _ in range(2):
-        lp.iterate(LearnedProposal.blend(probs, prev), max_cells, target, threshold)
+        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
         prev = lp.targets()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -326,7 +341,7 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     evals = fallbacks = 0
     t0 = time.perf_counter()
     for _ in range(a.learned_steps):
-        st = lp.iterate(LearnedProposal.blend(probs, prev), max_cells, target, threshold)
+        st = lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
         prev = lp.targets()
         evals += st["evaluations"]
         fallbacks += st["fallback"]
@@ -338,7 +353,7 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     ctx.set_profiling(True)
     stage = np.zeros(5)
     for i in range(3):
-        lp.iterate(LearnedProposal.blend(probs, prev), max_cells, target, threshold)
+        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
         if i >= 1:
             stage += ctx.stage_times()
     ctx.set_profiling(False)
@@ -354,7 +369,8 @@ def learned_proposal(a, E, W, d, device, dense_ms):
                                "grouped_compress_insert", "normalise"],
                               [round(float(v) / 2, 3) for v in stage])),
         "accuracy": acc,
-        "selection": f"per pattern, cells of the blended posterior up to predicted mass {target} "
+        "selection": f"per pattern, the {min_cells} cells with the most responsibility in the "
+                     f"previous iteration, then the network's cells up to predicted mass {target} "
                      f"(at most {max_cells} of {n_cells}); dense fallback below mean mass {threshold}",
         "network": "BF16 CNN: 3 conv 3x3 stride 2 (16/32/64) + FC -> 420-way softmax on "
                    f"{w.side // 2}^2 log(1+K) (2x2 binned); trained {a.train_epochs} epochs on "

@@ -72,10 +72,36 @@ __global__ void __launch_bounds__(256) targets_kernel(const TargetArgs a) {
     for (int c = w; c < a.n_cells; c += 8) a.t[p * a.n_cells + c] = tc[c * 32 + lane];
 }
 
-// One warp per pattern: its most probable cells in order, until their total
-// probability reaches mass_target or m cells are taken; unused slots -1.
-__global__ void select_kernel(const float* probs, int64_t N, int C, int m, float mass_target,
-                              int32_t* cand, float* mass) {
+// Most probable cell of a row among those not yet taken (lane owns cells
+// lane + 32 i, bit i of `taken`), the lowest index among equals; bi = -1 when
+// every remaining value is NaN.
+__device__ __forceinline__ void warp_argmax(const float* row, int C, uint32_t taken, int lane,
+                                            float& best, int& bi) {
+  best = -INFINITY;
+  bi = -1;
+  for (int i = 0; lane + 32 * i < C; ++i) {
+    const float v = row[lane + 32 * i];
+    if (!((taken >> i) & 1u) && (v > best || (bi < 0 && v == v))) {
+      best = v;
+      bi = lane + 32 * i;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) {
+      best = ov;
+      bi = oi;
+    }
+  }
+}
+
+// One warp per pattern.  With `keep`: first its min_m most probable cells
+// under keep (those with keep > 0).  Then cells in order of probs until at
+// least min_m are taken and their probs total reaches mass_target, at most m;
+// unused slots -1.  mass[p] = the probs total of the taken cells.
+__global__ void select_kernel(const float* probs, const float* keep, int64_t N, int C, int min_m,
+                              int m, float mass_target, int32_t* cand, float* mass) {
   const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (p >= N) return;
@@ -84,24 +110,23 @@ __global__ void select_kernel(const float* probs, int64_t N, int C, int m, float
   float tot = 0.0f;
   const bool adaptive = mass_target < 1.0f;  // else always m cells
   int s = 0;
-  for (; s < m && !(adaptive && tot >= mass_target); ++s) {
-    float best = -INFINITY;
-    int bi = -1;
-    for (int i = 0; lane + 32 * i < C; ++i) {
-      const float v = row[lane + 32 * i];
-      if (!((taken >> i) & 1u) && (v > best || (bi < 0 && v == v))) {
-        best = v;
-        bi = lane + 32 * i;
-      }
+  if (keep) {
+    const float* krow = keep + p * C;
+    for (; s < min_m && s < m; ++s) {
+      float best;
+      int bi;
+      warp_argmax(krow, C, taken, lane, best, bi);
+      if (bi < 0 || !(best > 0.0f)) break;
+      if ((bi & 31) == lane) taken |= 1u << (bi >> 5);
+      if (lane == 0) cand[p * m + s] = bi;
+      const float v = row[bi];
+      tot += v > 0.0f ? v : 0.0f;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      const float ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) {
-        best = ov;
-        bi = oi;
-      }
-    }
+  }
+  for (; s < m && !(adaptive && s >= min_m && tot >= mass_target); ++s) {
+    float best;
+    int bi;
+    warp_argmax(row, C, taken, lane, best, bi);
     if (bi >= 0 && (bi & 31) == lane) taken |= 1u << (bi >> 5);
     if (lane == 0) cand[p * m + s] = bi;
     tot += best > 0.0f ? best : 0.0f;
@@ -435,9 +460,10 @@ cudaError_t launch_scatter_targets(const int32_t* cand, const float* cmass, int6
   return cudaGetLastError();
 }
 
-cudaError_t launch_select(const float* probs, int64_t N, int C, int m, float mass_target,
-                          int32_t* cand, float* mass, cudaStream_t st) {
-  select_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(probs, N, C, m, mass_target, cand, mass);
+cudaError_t launch_select(const float* probs, const float* keep, int64_t N, int C, int min_m,
+                          int m, float mass_target, int32_t* cand, float* mass, cudaStream_t st) {
+  select_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(probs, keep, N, C, min_m, m, mass_target,
+                                                         cand, mass);
   return cudaGetLastError();
 }
 

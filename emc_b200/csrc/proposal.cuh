@@ -32,11 +32,12 @@ cudaError_t launch_targets(const TargetArgs& a, cudaStream_t st);
 cudaError_t launch_scatter_targets(const int32_t* cand, const float* cmass, int64_t N, int m,
                                    int n_cells, float* t, cudaStream_t st);
 
-// cand[p][0..m): the most probable cells of probs[p][0..C) in order, until
-// their total reaches mass_target or m cells are taken (then -1);
-// mass[p] = their total.
-cudaError_t launch_select(const float* probs, int64_t N, int C, int m, float mass_target,
-                          int32_t* cand, float* mass, cudaStream_t st);
+// cand[p][0..m): with keep (optional, [N][C]) first the min_m most probable
+// cells of keep[p] that have keep > 0; then the most probable remaining cells
+// of probs[p] in order until at least min_m are taken and their probs total
+// reaches mass_target, at most m (the rest -1); mass[p] = that total.
+cudaError_t launch_select(const float* probs, const float* keep, int64_t N, int C, int min_m,
+                          int m, float mass_target, int32_t* cand, float* mass, cudaStream_t st);
 
 // Pairs (pattern, selected cell) grouped by cell: group c holds pairs
 // gbeg[c] .. gbeg[c]+gcnt[c]-1, pair q belongs to pattern gpair[q]; pattern

@@ -117,11 +117,37 @@ def test_learned_proposal_end_to_end():
         assert rel(ctx.get_model(), m_dense) < 1e-5
 
 
-def _proposal_case(d, max_cells, mass_target=1.0, seed=0):
+def _select(probs, max_cells, mass_target, min_cells=1, keep=None):
+    """The candidate cells emc_iterate_proposed takes: with keep, first the
+    min_cells most probable cells under keep that hold keep > 0; then cells in
+    order of probs until at least min_cells are taken and their (FP32) probs
+    sum reaches mass_target, at most max_cells."""
+    N, n_cells = probs.shape
+    sel = np.zeros((N, n_cells), bool)
+    for p in range(N):
+        tot, n = np.float32(0), 0
+        if keep is not None:
+            for k in np.argsort(-keep[p], kind="stable")[:min(min_cells, max_cells)]:
+                if not keep[p, k] > 0:
+                    break
+                sel[p, k] = True
+                n += 1
+                tot = np.float32(tot + max(probs[p, k], np.float32(0)))
+        for k in np.argsort(-probs[p], kind="stable"):
+            if n >= max_cells or (mass_target < 1.0 and n >= min_cells and tot >= mass_target):
+                break
+            if sel[p, k]:
+                continue
+            sel[p, k] = True
+            n += 1
+            tot = np.float32(tot + probs[p, k])
+    return sel
+
+
+def _proposal_case(d, max_cells, mass_target=1.0, seed=0, min_cells=1, keep=False):
     """Rotations sorted by coarse cell (n=1: 60 uneven cells), distinct random
-    cell probabilities, and the allowed[r][p] mask of the selected cells: in
-    order of probability until their (FP32) sum reaches mass_target, at most
-    max_cells."""
+    cell probabilities (and, with keep, a second random posterior with half
+    of each row zero), and the allowed[r][p] mask of the selected cells."""
     from emc_b200.proposal import sorted_rotations
     q, w, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=1)
     d = dict(d, q=q, w=w)
@@ -130,37 +156,43 @@ def _proposal_case(d, max_cells, mass_target=1.0, seed=0):
     z = rng.standard_normal((N, n_cells)) * 2.0
     probs = np.exp(z - z.max(1, keepdims=True))
     probs = (probs / probs.sum(1, keepdims=True)).astype(np.float32)
-    sel = np.zeros((N, n_cells), bool)
-    for p in range(N):
-        tot = np.float32(0)
-        for k in np.argsort(-probs[p], kind="stable")[:max_cells]:
-            if mass_target < 1.0 and tot >= mass_target:
-                break
-            sel[p, k] = True
-            tot = np.float32(tot + probs[p, k])
+    kp = None
+    if keep:
+        z = rng.standard_normal((N, n_cells)) * 3.0
+        kp = np.exp(z - z.max(1, keepdims=True)) * (rng.random((N, n_cells)) < 0.5)
+        kp[:3] = 0.0  # patterns with no kept cell at all
+        kp = kp.astype(np.float32)
+    sel = _select(probs, max_cells, mass_target, min_cells, kp)
     allowed = sel[:, cell].T.astype(np.uint8)  # [R][N]
+    if keep:
+        return d, cell, n_cells, probs, allowed, kp
     return d, cell, n_cells, probs, allowed
 
 
-@pytest.mark.parametrize("lik,interp,prec,tol,max_cells,mass_target", [
-    ("poisson", "nearest", "fp32", 1e-5, 7, 1.0),
-    ("gauss", "nearest", "fp32", 1e-4, 7, 1.0),
-    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0),
-    ("gauss", "nearest", "mixed", 1e-4, 7, 1.0),
-    ("poisson", "trilinear", "mixed", 1e-4, 7, 1.0),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.6),
+@pytest.mark.parametrize("lik,interp,prec,tol,max_cells,mass_target,min_cells,keep", [
+    ("poisson", "nearest", "fp32", 1e-5, 7, 1.0, 1, False),
+    ("gauss", "nearest", "fp32", 1e-4, 7, 1.0, 1, False),
+    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0, 1, False),
+    ("gauss", "nearest", "mixed", 1e-4, 7, 1.0, 1, False),
+    ("poisson", "trilinear", "mixed", 1e-4, 7, 1.0, 1, False),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.6, 1, False),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, False),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, True),
 ])
 def test_proposed_iteration_matches_restricted_oracle(lik, interp, prec, tol, max_cells,
-                                                      mass_target):
+                                                      mass_target, min_cells, keep):
     """One proposed iteration (the top cells of 60 uneven cells per pattern:
-    a fixed 7, or adaptive up to a predicted mass of 0.6) against the FP64
+    a fixed 7, adaptive up to a predicted mass of 0.6, at least 3 and then up
+    to 0.7, or the 3 top cells of a second posterior first) against the FP64
     oracle's iteration restricted to the same candidate rotations."""
     import torch
     from emc_b200 import workloads as W
     from emc_b200.proposal import LearnedProposal
     from oracle import oracle as O
     from parity import oracle_cfg
-    d, cell, n_cells, probs, allowed = _proposal_case(W.make("tiny16"), max_cells, mass_target)
+    case = _proposal_case(W.make("tiny16"), max_cells, mass_target, min_cells=min_cells, keep=keep)
+    d, cell, n_cells, probs, allowed = case[:5]
+    kp = torch.from_numpy(case[5]).cuda() if keep else None
     cfg = oracle_cfg(d, lik, interp)
     m_ref, s_ref, P_ref, st_ref = O.iterate(cfg, d["counts"], d["mask"], d["q"], d["w"], d["x"],
                                             d["y"], d["z"], d["model0"].astype(np.float64),
@@ -170,7 +202,8 @@ def test_proposed_iteration_matches_restricted_oracle(lik, interp, prec, tol, ma
     np.add.at(t_ref.T, cell, P_ref)  # responsibility mass per (pattern, cell)
     with make_ctx(d, lik, interp, prec) as ctx:
         lp = LearnedProposal(ctx, cell, n_cells, bf16=True)
-        st = lp.iterate(torch.from_numpy(probs).cuda(), max_cells, mass_target, threshold=0.0)
+        st = lp.iterate(torch.from_numpy(probs).cuda(), max_cells, mass_target, threshold=0.0,
+                        min_cells=min_cells, keep=kp)
         assert st["fallback"] == 0
         assert st["evaluations"] == int(allowed.sum())
         assert rel(ctx.get_scaling(), s_ref) <= tol, rel(ctx.get_scaling(), s_ref)
