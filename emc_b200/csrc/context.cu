@@ -135,10 +135,10 @@ struct emc_context {
   float *d_mass = nullptr, *d_Yc = nullptr, *d_Pt = nullptr;
   int4 *d_mtiles = nullptr, *d_ctiles = nullptr;
   TileDesc *d_gmt = nullptr, *d_gct = nullptr;   // tcgen05 grouped tile lists
-  __half *d_Kg = nullptr, *d_KgT = nullptr, *d_Ahi = nullptr, *d_Alo = nullptr;
+  __half *d_Kg = nullptr, *d_Ahi = nullptr, *d_Alo = nullptr;
   // capacities (elements) of the per-iteration proposal buffers
   int64_t mtiles_cap = 0, ctiles_cap = 0, gmt_cap = 0, gct_cap = 0, pairs_cap = 0, slots_cap = 0,
-          yc_cap = 0, pt_cap = 0, kg_cap = 0, kgt_ld = 0, a_ld = 0;
+          yc_cap = 0, pt_cap = 0, kg_cap = 0, a_ld = 0;
   double *d_lse_c = nullptr, *d_plogp_c = nullptr;
   // Two event sets alternate between iterations, so the times of iteration
   // i-1 can be read while iteration i is still queued.
@@ -1292,8 +1292,8 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   }
   // Group the (pattern, cell) pairs by cell (stable counting sort on the
   // host).  Pairs live in slots: cell c owns slots gbeg[c] .. gbeg[c]+gcnt[c]-1,
-  // its first slot a multiple of 8 (16-byte aligned FP16 columns of KgT);
-  // the slots between cells are padding (pattern -1).
+  // its first slot a multiple of 8; the slots between cells are padding
+  // (pattern -1).
   const int n_cells = c->n_cells;
   std::vector<int32_t> gcnt(n_cells, 0);
   int64_t npairs = 0;
@@ -1365,14 +1365,6 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
     TRY(grow(c, &c->d_gmt, c->gmt_cap, n_gmt));
     TRY(grow(c, &c->d_gct, c->gct_cap, n_gct));
     TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
-    if (S > c->kgt_ld) {
-      if (c->d_KgT) c->release(c->d_KgT);
-      c->d_KgT = nullptr;
-      c->kgt_ld = 0;
-      const int64_t ld = (S + S / 4 + 63) / 64 * 64;
-      TRY(c->alloc(&c->d_KgT, ld * c->Ppad));
-      c->kgt_ld = ld;
-    }
     if (kw > c->a_ld) {
       for (__half** q : {&c->d_Ahi, &c->d_Alo})
         if (*q) {
@@ -1459,13 +1451,13 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   g.acc = c->d_acc;
   int launches = 0;
   if (tc) {
-    CUtensorMap tmKg, tmKgT, tmAhi, tmAlo;
+    CUtensorMap tmKg, tmKg64, tmAhi, tmAlo;
     if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, kMaximizeBK) ||
-        !tc_encode_2d_strided(&tmKgT, c->d_KgT, S, c->Ppad, c->kgt_ld, 256, kCompressBK) ||
+        !tc_encode_2d(&tmKg64, c->d_Kg, c->Ppad, S, kCompressBK, 64) ||
         !tc_encode_2d_strided(&tmAhi, c->d_Ahi, c->a_ld, R, c->a_ld, 128, kCompressBK) ||
         !tc_encode_2d_strided(&tmAlo, c->d_Alo, c->a_ld, R, c->a_ld, 128, kCompressBK))
       return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
-    CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->kgt_ld, c->d_KgT, c->st));
+    CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->st));
     c->mark(1);
     GMaxEpiArgs ge{};
     ge.tiles = c->d_gmt;
@@ -1498,7 +1490,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
     ce.cz = c->d_cz;
     ce.ins = c->d_ins;
     ce.acc = c->d_acc;
-    CK(c, launch_group_compress_tc(tmAhi, tmAlo, tmKgT, n_gct, ce, c->d_status,
+    CK(c, launch_group_compress_tc(tmAhi, tmAlo, tmKg64, n_gct, ce, c->d_status,
                                    c->num_sms, c->st));
     launches = 6;  // gather (2), contraction, softmax, split, contraction
   } else {

@@ -15,6 +15,7 @@
 // site in TcStatus, drains its copies and MMAs, frees TMEM and returns.
 #include <cfloat>
 #include <cstdint>
+#include <type_traits>
 
 #include "tc.cuh"
 #include "voxel.h"
@@ -115,9 +116,31 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
   d |= (uint64_t)(BKT == 64 ? 2 : 4) << 61;
   return d;
 }
+// Shared-memory descriptor of an MN-major B operand, 128B swizzle: blocks of
+// 64 N-elements (128-byte rows), one row per K index, rows 128 bytes apart so
+// 8-row core groups are 1024 bytes apart (SBO), the BN / 64 blocks BKT rows
+// of 128 bytes apart (LBO) -- the layout TMA writes for boxes of 64 x BKT.
+template <int BKT>
+__device__ __forceinline__ uint64_t sdesc_mn(uint32_t addr) {
+  uint64_t d = (uint64_t)((addr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)((BKT * 128) >> 4) << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
 // Instruction descriptor, kind::f16: D = F32, A = B = F16, both K-major.
 constexpr uint32_t kIdesc = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(BN >> 3) << 17) |
                             ((uint32_t)(BM >> 4) << 24);
+// The same with B MN-major (bit 16).
+constexpr uint32_t kIdescBMN = kIdesc | (1u << 16);
+
+// Epilogues whose B operand is stored MN-major in global memory ([K][N], N
+// contiguous) declare kBMajorMN = true.
+template <class E, class = void>
+struct b_major_mn : std::false_type {};
+template <class E>
+struct b_major_mn<E, std::void_t<decltype(E::kBMajorMN)>> : std::bool_constant<E::kBMajorMN> {};
 
 struct Ctl {
   volatile int* abort;
@@ -150,6 +173,8 @@ __global__ void __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
                    const int64_t m_tiles, const int64_t n_tiles, const int64_t k_blocks,
                    const int raster, const Epi epi, TcStatus* status) {
   static_assert(NA * NB == 2, "one hi/lo split per contraction");
+  constexpr bool BMN = b_major_mn<Epi>::value;
+  static_assert(!BMN || (NB == 1 && BK == 64 && BN % 64 == 0), "MN-major B: one 64-row operand");
   constexpr uint32_t A_BYTES = BM * BK * 2;
   constexpr uint32_t B_BYTES = BN * BK * 2;
   constexpr uint32_t STAGE_BYTES = NA * A_BYTES + NB * B_BYTES;
@@ -266,8 +291,15 @@ __global__ void __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
           tma_load_2d(base, tA0, ak + kc, ar, fb);
           if (NA == 2) tma_load_2d(base + A_BYTES, tA1, ak + kc, ar, fb);
           const uint32_t bbase = base + NA * A_BYTES;
-          tma_load_2d(bbase, tB0, bk + kc, br, fb);
-          if (NB == 2) tma_load_2d(bbase + B_BYTES, tB1, bk + kc, br, fb);
+          if constexpr (BMN) {
+            // BN / 64 boxes of 64 N-elements x BK K-rows
+#pragma unroll
+            for (int i = 0; i < BN / 64; ++i)
+              tma_load_2d(bbase + (uint32_t)i * BK * 128, tB0, br + 64 * i, bk + kc, fb);
+          } else {
+            tma_load_2d(bbase, tB0, bk + kc, br, fb);
+            if (NB == 2) tma_load_2d(bbase + B_BYTES, tB1, bk + kc, br, fb);
+          }
           ++issued;
           if (++s == STAGES) {
             s = 0;
@@ -320,8 +352,14 @@ __global__ void __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
               const uint32_t ao = base + (NA == 2 ? q : 0) * A_BYTES + k * 32;
-              const uint32_t bo = bbase + (NB == 2 ? q : 0) * B_BYTES + k * 32;
-              mma_f16(d, sdesc<BK>(ao), sdesc<BK>(bo), kIdesc, (kb | k | q) != 0);
+              if constexpr (BMN) {
+                // 16 K-rows of 128 bytes per step
+                mma_f16(d, sdesc<BK>(ao), sdesc_mn<BK>(bbase + k * 2048), kIdescBMN,
+                        (kb | k | q) != 0);
+              } else {
+                const uint32_t bo = bbase + (NB == 2 ? q : 0) * B_BYTES + k * 32;
+                mma_f16(d, sdesc<BK>(ao), sdesc<BK>(bo), kIdesc, (kb | k | q) != 0);
+              }
             }
           }
           mma_commit(smem_u32(&empty_bar[s]));
@@ -639,6 +677,7 @@ struct EpiGMax {
 struct EpiGCmp {
   static constexpr bool kListed = true;
   static constexpr int kSets = 1;
+  static constexpr bool kBMajorMN = true;  // B = Kg [slot][pixel] read as it lies
   // insertion-heavy epilogue behind short K loops: 16 warps (four per TMEM
   // lane quarter, a quarter of the columns each) keep more reductions in flight
   static constexpr int kEpiWarps = 16;
@@ -1569,13 +1608,13 @@ cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap&
 }
 
 cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap& tmAlo,
-                                     const CUtensorMap& tmKgT, int64_t n_tiles,
+                                     const CUtensorMap& tmKg64, int64_t n_tiles,
                                      const GCmpEpiArgs& e, TcStatus* status, int num_sms,
                                      cudaStream_t st) {
   EpiGCmp epi;
   epi.a = e;
-  return run_gemm<2, 1, 3, false, kCompressBK>(one_set(tmAhi, tmAlo, tmKgT, tmKgT), n_tiles, 1, 0, epi,
-                                               status, num_sms, st);
+  return run_gemm<2, 1, 3, false, kCompressBK>(one_set(tmAhi, tmAlo, tmKg64, tmKg64), n_tiles, 1,
+                                               0, epi, status, num_sms, st);
 }
 
 cudaError_t launch_batch_maximize_tc(const TmapSet<kMaxBatch>& maps, int64_t n_tiles,

@@ -368,42 +368,6 @@ __global__ void gather_rows_kernel(const __half* Kh, int64_t Ppad, const int32_t
     dst[i] = p < 0 ? make_uint4(0, 0, 0, 0) : src[i];
 }
 
-// KgT[j][slot] = Kh[pattern of slot][j] for j < Ppad, slot < S (zero for the
-// padding slots): 64 slots x 64 pixels per block, read and written as half2
-// (pairs of pixels in, pairs of slots out) through a shared-memory tile of
-// 32-bit words.
-__global__ void __launch_bounds__(256) gather_transpose_kernel(const __half* Kh, int64_t Ppad,
-                                                               const int32_t* slot_pat, int64_t S,
-                                                               int64_t ldT, __half* KgT) {
-  __shared__ uint32_t tile[64][33];  // [slot][pixel pair]
-  const int64_t j0 = (int64_t)blockIdx.x * 64, s0 = (int64_t)blockIdx.y * 64;
-  const int t = threadIdx.x;
-  // load: 64 slot rows x 32 pixel pairs
-  for (int e = t; e < 64 * 32; e += 256) {
-    const int sr = e >> 5, jp = e & 31;
-    const int64_t s = s0 + sr, j = j0 + 2 * jp;
-    const int p = s < S ? slot_pat[s] : -1;
-    uint32_t v = 0;
-    if (p >= 0 && j + 1 < Ppad + 1)
-      v = *reinterpret_cast<const uint32_t*>(Kh + (int64_t)p * Ppad + j);
-    tile[sr][jp] = v;
-  }
-  __syncthreads();
-  // store: 64 pixel rows x 32 slot pairs
-  for (int e = t; e < 64 * 32; e += 256) {
-    const int jr = e >> 5, sp = e & 31;
-    const int64_t j = j0 + jr, s = s0 + 2 * sp;
-    if (j >= Ppad || s >= S) continue;
-    const uint32_t a = tile[2 * sp][jr >> 1], b = tile[2 * sp + 1][jr >> 1];
-    const uint32_t lo = (jr & 1) ? (a >> 16) : (a & 0xFFFFu);
-    const uint32_t hi = (jr & 1) ? (b >> 16) : (b & 0xFFFFu);
-    if (s + 1 < S)
-      *reinterpret_cast<uint32_t*>(KgT + j * ldT + s) = lo | (hi << 16);
-    else
-      KgT[j * ldT + s] = __ushort_as_half((unsigned short)lo);
-  }
-}
-
 // The grouped compress operand: A[r][q] = P / (T_r phi) of rotation r and the
 // q-th slot of its cell as FP16 hi + lo, zero from the cell's slot count up to
 // the next multiple of 64 (the contraction's k-blocks), and zero rows for
@@ -484,13 +448,9 @@ cudaError_t launch_group_softmax(const GroupArgs& g, cudaStream_t st) {
 }
 
 cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* slot_pat, int64_t S,
-                                __half* Kg, int64_t ldT, __half* KgT, cudaStream_t st) {
+                                __half* Kg, cudaStream_t st) {
   if (S == 0) return cudaSuccess;
-  if (Kg) gather_rows_kernel<<<(unsigned)S, 256, 0, st>>>(Kh, Ppad, slot_pat, S, Kg);
-  if (KgT) {
-    dim3 grid((unsigned)((Ppad + 63) / 64), (unsigned)((S + 63) / 64));
-    gather_transpose_kernel<<<grid, 256, 0, st>>>(Kh, Ppad, slot_pat, S, ldT, KgT);
-  }
+  gather_rows_kernel<<<(unsigned)S, 256, 0, st>>>(Kh, Ppad, slot_pat, S, Kg);
   return cudaGetLastError();
 }
 

@@ -89,11 +89,11 @@ struct GroupArgs {
 cudaError_t launch_group_maximize(const GroupArgs& g, int64_t n_mtiles, cudaStream_t st);
 // The per-pattern softmax of the grouped maximize alone (after the tcgen05 contraction).
 cudaError_t launch_group_softmax(const GroupArgs& g, cudaStream_t st);
-// Gathered FP16 count operands of the tcgen05 grouped contractions:
-// Kg[slot][Ppad] (if Kg) and KgT[Ppad][ldT] (if KgT), from Kh[Npad][Ppad];
+// Gathered FP16 counts of the tcgen05 grouped contractions (A of the
+// maximize, MN-major B of the compress): Kg[slot][Ppad] from Kh[Npad][Ppad];
 // slot_pat[slot] = pattern, -1 for padding (zero).
 cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* slot_pat, int64_t S,
-                                __half* Kg, int64_t ldT, __half* KgT, cudaStream_t st);
+                                __half* Kg, cudaStream_t st);
 // A[r][q] = P / (T_r phi) of the grouped compress as FP16 hi + lo ([R][ldA]).
 cudaError_t launch_p_split(const GroupArgs& g, const int32_t* cell_of, int64_t R, const float* T,
                            int64_t ldA, __half* Ahi, __half* Alo, cudaStream_t st);

@@ -122,9 +122,12 @@ cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap&
                                      const GMaxEpiArgs& e, TcStatus* status, int num_sms,
                                      cudaStream_t st);
 
-// Grouped compress: acc[member][j] = sum_q A[mbeg_c + member][q] KgT[j][slot0_c + q]
+// Grouped compress: acc[member][j] = sum_q A[mbeg_c + member][q] Kg[slot0_c + q][j]
 // with A = P / (T_r phi) as FP16 hi + lo (zero beyond the cell's slots);
-// 128 members x 256 pixels per tile, inserted in the epilogue.
+// 128 members x 256 pixels per tile, inserted in the epilogue.  Kg is the B
+// operand in its own [slot][pixel] layout (MN-major): its tensor map has
+// boxes of 64 slot rows x 64 pixels; a tile's b_row is its first pixel and
+// b_k0 its cell's first slot.
 struct GCmpEpiArgs {
   const TileDesc* tiles;
   const int32_t* mcnt;
@@ -140,7 +143,7 @@ struct GCmpEpiArgs {
   float2* acc;
 };
 cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap& tmAlo,
-                                     const CUtensorMap& tmKgT, int64_t n_tiles,
+                                     const CUtensorMap& tmKg64, int64_t n_tiles,
                                      const GCmpEpiArgs& e, TcStatus* status, int num_sms,
                                      cudaStream_t st);
 
