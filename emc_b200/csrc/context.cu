@@ -96,6 +96,7 @@ struct emc_context {
   float* d_T = nullptr;
   float* d_Tskip = nullptr;  // T_r for the insertion skip: this context's T, or all shards' sum
   double* d_rowstat = nullptr;
+  uint2* d_vtab = nullptr;  // mixed + nearest: per-voxel (W, split operand) table of the expand
   double* d_scratch = nullptr;  // reductions
   double* d_stats = nullptr;    // [0] mean [1] max [2] plogp [3] loglik
   // FP32 path
@@ -588,6 +589,12 @@ emc_status emc_expand(emc_context* c) {
     a.out_lo = c->d_Blo;
   }
   c->mark(0);
+  if (c->mixed && c->cfg.interp == EMC_INTERP_NEAREST) {
+    if (!c->d_vtab) TRY(c->alloc(&c->d_vtab, c->M + 1));
+    CK(c, launch_expand_table(c->d_model, c->M, a.floor_, a.log_split, c->d_vtab, c->st));
+    a.tab = c->d_vtab;
+    c->launches += 1;
+  }
   CK(c, launch_expand(a, c->st));
   c->launches += 1;
   c->mark(1);

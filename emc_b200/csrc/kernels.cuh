@@ -26,8 +26,16 @@ struct ExpandArgs {
   __half* out_hi;
   __half* out_lo;
   double* rowstat;      // [R] or nullptr
+  // optional, nearest + EXP_F16_SPLIT: per-voxel table from launch_expand_table
+  // ([side^3 + 1], the last entry for pixels that fall outside the grid)
+  const uint2* tab;
 };
 cudaError_t launch_expand(const ExpandArgs& a, cudaStream_t st);
+// tab[v] = (bits of model[v], FP16 hi | lo << 16 of the split operand value:
+// log(max(model[v], floor)) when log_split, else model[v]) for v < M, and
+// tab[M] the same for a pixel outside the grid (value 0).
+cudaError_t launch_expand_table(const float* model, int64_t M, float floor_, int log_split,
+                                uint2* tab, cudaStream_t st);
 
 // LL[r][p] (ld = ldLL) from slices A[R][ldA] and counts K[N][ldK] over npa
 // active pixels (pix: optional column indirection into A and K).

@@ -121,6 +121,75 @@ __global__ void __launch_bounds__(kBlock) expand_kernel(const ExpandArgs a) {
   }
 }
 
+// The operand value of the split expansion and its FP16 hi / lo halves,
+// packed hi | lo << 16.
+__device__ __forceinline__ uint32_t split_bits(float w, float floor_, int log_split) {
+  const float x = log_split ? logf(fmaxf(w, floor_)) : w;
+  const __half hi = __float2half_rn(x);
+  const __half lo = __float2half_rn(x - __half2float(hi));
+  return (uint32_t)__half_as_ushort(hi) | ((uint32_t)__half_as_ushort(lo) << 16);
+}
+
+__global__ void expand_table_kernel(const float* model, int64_t M, float floor_, int log_split,
+                                    uint2* tab) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v > M) return;
+  const float w = v < M ? model[v] : 0.0f;
+  tab[v] = make_uint2(__float_as_uint(w), split_bits(w, floor_, log_split));
+}
+
+// Nearest-voxel expansion into the FP16 hi + lo operands through the voxel
+// table: one 8-byte gather per pixel gives the slice value (for the row
+// statistic) and its split operand, so no logarithm or split runs per
+// element; each thread takes pixel pairs and writes them as half2.  Outputs
+// are those of expand_kernel<0, EXP_F16_SPLIT> bit for bit.
+__global__ void __launch_bounds__(kBlock) expand_tab_kernel(const ExpandArgs a) {
+  __shared__ double red[32];
+  const int64_t r = blockIdx.x;
+  float m[9];
+  emc_voxel::rotation_matrix(a.quat + 4 * r, m);
+  const int64_t M = (int64_t)a.side * a.side * a.side;
+  const int npix = (int)a.npix, npairs = (int)(a.ld / 2);
+  __half2* hi_row = reinterpret_cast<__half2*>(a.out_hi + r * a.ld);
+  __half2* lo_row = reinterpret_cast<__half2*>(a.out_lo + r * a.ld);
+  double stat = 0.0;
+  for (int p0 = threadIdx.x; p0 < npairs; p0 += 2 * kBlock) {
+    uint2 t[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = 2 * (p0 + (u >> 1) * kBlock) + (u & 1);
+      t[u] = make_uint2(0u, 0u);  // padding columns: zero
+      if (i < npix) {
+        float pos[3];
+        emc_voxel::position(m, a.side, __ldg(a.cx + i), __ldg(a.cy + i), __ldg(a.cz + i), pos);
+        int64_t v;
+        if (!emc_voxel::nearest(pos, a.side, 1, &v)) v = M;
+        t[u] = __ldg(a.tab + v);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int pp = p0 + h * kBlock;
+      if (pp >= npairs) continue;
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        if (2 * pp + e < npix && a.stat != STAT_NONE) {
+          const float w = __uint_as_float(t[2 * h + e].x);
+          stat += a.stat == STAT_SUMSQ ? (double)w * w : (double)w;
+        }
+      const uint32_t b0 = t[2 * h].y, b1 = t[2 * h + 1].y;
+      hi_row[pp] = __halves2half2(__ushort_as_half((unsigned short)(b0 & 0xFFFFu)),
+                                  __ushort_as_half((unsigned short)(b1 & 0xFFFFu)));
+      lo_row[pp] = __halves2half2(__ushort_as_half((unsigned short)(b0 >> 16)),
+                                  __ushort_as_half((unsigned short)(b1 >> 16)));
+    }
+  }
+  if (a.rowstat) {
+    const double s = block_sum(stat, red);
+    if (threadIdx.x == 0) a.rowstat[r] = s;
+  }
+}
+
 __device__ __forceinline__ int64_t col_of(const int32_t* pix, int64_t j) { return pix ? pix[j] : j; }
 
 // Likelihood: rows = rotations, columns = patterns, reduction over pixels.
@@ -525,10 +594,23 @@ void expand_dispatch(const ExpandArgs& a, cudaStream_t st) {
 
 cudaError_t launch_expand(const ExpandArgs& a, cudaStream_t st) {
   if (a.R <= 0) return cudaSuccess;
+  if (a.tab && a.interp == 0 && a.out == EXP_F16_SPLIT) {
+    if (a.ld % 2 != 0 || a.npix > a.ld || a.ld > (int64_t)1 << 30 || a.stat_mask)
+      return cudaErrorInvalidValue;
+    expand_tab_kernel<<<(unsigned)a.R, kBlock, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   if (a.interp == 0)
     expand_dispatch<0>(a, st);
   else
     expand_dispatch<1>(a, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_expand_table(const float* model, int64_t M, float floor_, int log_split,
+                                uint2* tab, cudaStream_t st) {
+  expand_table_kernel<<<(unsigned)((M + 1 + 255) / 256), 256, 0, st>>>(model, M, floor_, log_split,
+                                                                      tab);
   return cudaGetLastError();
 }
 
