@@ -325,6 +325,29 @@ def learned_proposal(a, E, W, d, device, dense_ms):
                                   "captured_mass_mean": float(captured_by(probs).mean())},
            "untrained_network_cells_only_captured_mass_mean": float(captured_by(untrained).mean())}
 
+    # drift over chained iterations: three proposed iterations, each keeping the
+    # previous one's top cells, against three dense iterations from the same state
+    ctx.set_model(m0)
+    ctx.set_scaling(s0)
+    for _ in range(3):
+        ctx.iterate(stats=False)
+    m_dense3 = ctx.get_model()
+    ctx.set_model(m0)
+    ctx.set_scaling(s0)
+    prev = t_dense
+    for _ in range(3):
+        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
+        prev = lp.targets()
+    acc["model_rel_err_vs_dense_after_3_iterations"] = rel_err(ctx.get_model(), m_dense3)
+    # the same divergence when only the first of the three is proposed: how
+    # much of it the dense iterations themselves amplify
+    ctx.set_model(m0)
+    ctx.set_scaling(s0)
+    lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=t_dense)
+    for _ in range(2):
+        ctx.iterate(stats=False)
+    acc["model_rel_err_vs_dense_after_1_proposed_2_dense"] = rel_err(ctx.get_model(), m_dense3)
+
     # timed: proposed iterations, each keeping the top cells of the previous
     # iteration's cell responsibilities and adding the network's
     ctx.set_model(m0)
