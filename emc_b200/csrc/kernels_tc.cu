@@ -408,15 +408,12 @@ __global__ void __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
       e.tile_begin(mt, nt, ep_tid, epi_smem);
       e.row_begin(mt * BM + quarter * 32 + lane);
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
-      static_assert(COLS % 32 == 0, "two 16-column TMEM loads per wait");
 #pragma unroll 1
-      for (int c = col0; c < col0 + COLS; c += 32) {
-        uint32_t v0[16], v1[16];
-        tmem_ld16(taddr + c, v0);
-        tmem_ld16(taddr + c + 16, v1);
+      for (int c = col0; c < col0 + COLS; c += 16) {
+        uint32_t v[16];
+        tmem_ld16(taddr + c, v);
         tmem_ld_wait();
-        e.consume(c, v0, epi_smem);
-        e.consume(c + 16, v1, epi_smem);
+        e.consume(c, v, epi_smem);
       }
       e.row_end();
       tc_fence_before();
