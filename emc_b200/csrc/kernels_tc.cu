@@ -581,18 +581,27 @@ struct EpiCmp {
   __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) {
     if (!active) return;
     const float4* cs = reinterpret_cast<const float4*>(smem);
-#pragma unroll 4
-    for (int k = 0; k < 16; ++k) {
-      const float4 q = cs[c + k];
-      if (q.w == 0.0f) continue;
-      float u[3];
-      emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
-      const float val = __uint_as_float(v[k]) * wU;
-      if (a.interp == 0) {
+    // fully unrolled: v[k] stays in registers (a runtime index would put the
+    // 16 accumulator words in local memory)
+    if (a.interp == 0) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const float4 q = cs[c + k];
+        if (q.w == 0.0f) continue;
+        float u[3];
+        emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
         int64_t vox;
         if (!emc_voxel::nearest(u, a.side, 0, &vox)) continue;
-        red_add_v2(a.acc + vox, val, wT);
-      } else {
+        red_add_v2(a.acc + vox, __uint_as_float(v[k]) * wU, wT);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const float4 q = cs[c + k];
+        if (q.w == 0.0f) continue;
+        float u[3];
+        emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
+        const float val = __uint_as_float(v[k]) * wU;
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
           int64_t vox;
@@ -718,18 +727,26 @@ struct EpiGCmp {
   __device__ void consume(int c, const uint32_t (&v)[16], uint8_t* smem) {
     if (!active) return;
     const float4* cs = reinterpret_cast<const float4*>(smem);
-#pragma unroll 4
-    for (int k = 0; k < 16; ++k) {
-      const float4 q = cs[c + k];
-      if (q.w == 0.0f) continue;
-      float u[3];
-      emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
-      const float val = __uint_as_float(v[k]) * wT;
-      if (a.interp == 0) {
+    // fully unrolled: v[k] stays in registers
+    if (a.interp == 0) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const float4 q = cs[c + k];
+        if (q.w == 0.0f) continue;
+        float u[3];
+        emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
         int64_t vox;
         if (!emc_voxel::nearest(u, a.side, 0, &vox)) continue;
-        red_add_v2(a.acc + vox, val, wT);
-      } else {
+        red_add_v2(a.acc + vox, __uint_as_float(v[k]) * wT, wT);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const float4 q = cs[c + k];
+        if (q.w == 0.0f) continue;
+        float u[3];
+        emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
+        const float val = __uint_as_float(v[k]) * wT;
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
           int64_t vox;
