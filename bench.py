@@ -75,6 +75,12 @@ def parse():
     ap.add_argument("--min-cells", type=int, default=4,
                     help="cells of each pattern's previous responsibility kept in a proposed iteration")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--profile-case", choices=["proposed", "expand", "grouped"], default=None,
+                    help="run one small fixed case for a profiler and exit (no JSON line): "
+                         "proposed = two dense and three proposed iterations of the default "
+                         "workload; expand = three dense iterations at 128^3 with 25,680 "
+                         "rotations and 2,000 patterns; grouped = one dense and two proposed "
+                         "iterations at 128^3 with 25,680 rotations and 20,000 patterns")
     return ap.parse_args()
 
 
@@ -467,10 +473,55 @@ def batched_datasets(a, E, W, device, workloads):
 
 # ------------------------------------------------------------------ ours --
 
+def profile_case(a):
+    """Small fixed cases whose kernels the summaries under profiles/ come from
+    (run once plainly, then under ncu).  Prints wall-clock times per
+    iteration, nothing else."""
+    import torch
+    import emc_b200 as E
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    if a.profile_case == "proposed":
+        wl, dense, proposed = W.WORKLOADS["large128"], 2, 3
+    elif a.profile_case == "expand":
+        wl, dense, proposed = W.Workload("prof128", 128, 8, 2000, 500.0, 0.5, 6.0, 1), 3, 0
+    else:
+        wl, dense, proposed = W.Workload("prof128", 128, 8, 20000, 500.0, 0.5, 6.0, 1), 1, 2
+    d = W.make(wl)
+    q, w = d["q"], d["w"]
+    if proposed:
+        q, w, cell, n_cells = sorted_rotations(q, w)
+    N, R = d["counts"].shape[0], q.shape[0]
+    ctx = E.Context(wl.side, N, R, likelihood="poisson", precision="mixed")
+    ctx.set_geometry(d["x"], d["y"], d["z"], d["mask"])
+    ctx.set_rotations(q, w)
+    ctx.set_patterns(d["counts"])
+    ctx.set_model(d["model0"])
+    ctx.set_scaling(d["scaling0"])
+    for i in range(dense):
+        t0 = time.perf_counter()
+        ctx.iterate(stats=False)
+        ctx.synchronize()
+        print(f"dense {i}: {(time.perf_counter() - t0) * 1e3:.2f} ms", flush=True)
+    if proposed:
+        lp = LearnedProposal(ctx, cell, n_cells)
+        t = lp.targets()  # the dense cell posterior serves as the proposal
+        for i in range(proposed):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = lp.iterate(t, 16, 0.999, 0.0, min_cells=4, keep=t)
+            ctx.synchronize()
+            print(f"proposed {i}: {(time.perf_counter() - t0) * 1e3:.2f} ms, "
+                  f"{st['pairs'] / N:.2f} cells per pattern", flush=True)
+    ctx.close()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return reference_arm(a)
+    if a.profile_case:
+        return profile_case(a)
     import torch
     import emc_b200 as E
     from emc_b200 import workloads as W
