@@ -72,8 +72,10 @@ def parse():
     ap.add_argument("--train-iters", type=int, default=5,
                     help="dense iterations whose responsibilities train the proposal network")
     ap.add_argument("--train-epochs", type=int, default=12)
-    ap.add_argument("--min-cells", type=int, default=4,
+    ap.add_argument("--min-cells", type=int, default=8,
                     help="cells of each pattern's previous responsibility kept in a proposed iteration")
+    ap.add_argument("--keep-mass", type=float, default=0.99999,
+                    help="more of those cells until they hold this much of the previous responsibility")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--profile-case", choices=["proposed", "expand", "grouped"], default=None,
                     help="run one small fixed case for a profiler and exit (no JSON line): "
@@ -262,9 +264,10 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     dense iterations whose responsibilities train the BF16 network, then
     --learned-steps proposed iterations.  Each proposed iteration evaluates,
     per pattern, the --min-cells cells holding most of its responsibility in
-    the previous iteration, then the network's most probable cells up to a
-    predicted mass of 0.999 (at most 16 cells in all); the dense iteration
-    runs instead when the mean predicted mass falls below 0.99."""
+    the previous iteration (more until they hold --keep-mass of it), then the
+    network's most probable cells up to a predicted mass of 0.999 (at most 16
+    cells in all); the dense iteration runs instead when the mean predicted
+    mass falls below 0.99."""
     import torch
     from emc_b200.proposal import LearnedProposal, sorted_rotations
     w = d["workload"]
@@ -286,7 +289,7 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     probs = lp.predict(x)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
-    max_cells, target, threshold, min_cells = 16, 0.999, 0.99, a.min_cells
+    max_cells, target, threshold, min_cells, keep_mass = 16, 0.999, 0.99, a.min_cells, a.keep_mass
 
     def captured_by(scores):
         """True next-iteration mass on the cells a network alone selects (in
@@ -315,7 +318,8 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     # the selection rule used below: the previous posterior's top cells, then the network's
     ctx.set_model(m0)
     ctx.set_scaling(s0)
-    st = lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=t_dense)
+    st = lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=t_dense,
+                    keep_mass=keep_mass)
     m_prop = ctx.get_model()
     cand = lp.targets() > 0  # candidate cells (one whose responsibilities all underflow reads as 0)
     captured = (t_next * cand).sum(1)
@@ -342,14 +346,16 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     ctx.set_scaling(s0)
     prev = t_dense
     for _ in range(3):
-        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
+        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev,
+                   keep_mass=keep_mass)
         prev = lp.targets()
     acc["model_rel_err_vs_dense_after_3_iterations"] = rel_err(ctx.get_model(), m_dense3)
     # the same divergence when only the first of the three is proposed: how
     # much of it the dense iterations themselves amplify
     ctx.set_model(m0)
     ctx.set_scaling(s0)
-    lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=t_dense)
+    lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=t_dense,
+                    keep_mass=keep_mass)
     for _ in range(2):
         ctx.iterate(stats=False)
     acc["model_rel_err_vs_dense_after_1_proposed_2_dense"] = rel_err(ctx.get_model(), m_dense3)
@@ -361,7 +367,8 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     prev = t_dense
     ext = torch.cuda.ExternalStream(ctx.stream)
     for _ in range(2):
-        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
+        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev,
+                   keep_mass=keep_mass)
         prev = lp.targets()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -370,7 +377,8 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     evals = fallbacks = 0
     t0 = time.perf_counter()
     for _ in range(a.learned_steps):
-        st = lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
+        st = lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev,
+                   keep_mass=keep_mass)
         prev = lp.targets()
         evals += st["evaluations"]
         fallbacks += st["fallback"]
@@ -382,7 +390,8 @@ def learned_proposal(a, E, W, d, device, dense_ms):
     ctx.set_profiling(True)
     stage = np.zeros(5)
     for i in range(3):
-        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev)
+        lp.iterate(probs, max_cells, target, threshold, min_cells=min_cells, keep=prev,
+                   keep_mass=keep_mass)
         if i >= 1:
             stage += ctx.stage_times()
     ctx.set_profiling(False)
@@ -399,8 +408,9 @@ def learned_proposal(a, E, W, d, device, dense_ms):
                               [round(float(v) / 2, 3) for v in stage])),
         "accuracy": acc,
         "selection": f"per pattern, the {min_cells} cells with the most responsibility in the "
-                     f"previous iteration, then the network's cells up to predicted mass {target} "
-                     f"(at most {max_cells} of {n_cells}); dense fallback below mean mass {threshold}",
+                     f"previous iteration (more up to {keep_mass} of it), then the network's cells "
+                     f"up to predicted mass {target} (at most {max_cells} of {n_cells}); dense "
+                     f"fallback below mean mass {threshold}",
         "network": "BF16 CNN: 3 conv 3x3 stride 2 (16/32/64) + FC -> 420-way softmax on "
                    f"{w.side // 2}^2 log(1+K) (2x2 binned); trained {a.train_epochs} epochs on "
                    f"the responsibilities of {a.train_iters} dense iterations "
@@ -509,7 +519,7 @@ def profile_case(a):
         for i in range(proposed):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            st = lp.iterate(t, 16, 0.999, 0.0, min_cells=4, keep=t)
+            st = lp.iterate(t, 16, 0.999, 0.0, min_cells=8, keep=t, keep_mass=0.99999)
             ctx.synchronize()
             print(f"proposed {i}: {(time.perf_counter() - t0) * 1e3:.2f} ms, "
                   f"{st['pairs'] / N:.2f} cells per pattern", flush=True)

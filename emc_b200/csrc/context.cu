@@ -1237,8 +1237,8 @@ static emc_status grow(emc_context* c, T** p, int64_t& cap, int64_t need) {
 extern "C" {
 
 emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float* keep,
-                                int32_t min_m, int32_t m, float mass_target, float threshold,
-                                emc_proposal_stats* stats) {
+                                int32_t min_m, int32_t m, float mass_target, float keep_mass,
+                                float threshold, emc_proposal_stats* stats) {
   if (!c || !probs || m < 1 || min_m < 1 || min_m > m) return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
   if (m > c->n_cells) return c->fail(EMC_ERR_ARG, "more cells per pattern than cells");
@@ -1266,8 +1266,8 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   if (c->stage != 0) return c->fail(EMC_ERR_STATE, "proposed iteration between stages");
   // candidate cells of every pattern and the proposal's mass on them; their
   // copy to the host is waited for while the expansion runs behind it
-  CK(c, launch_select(probs, keep, N, c->n_cells, min_m, m, mass_target, c->d_cand, c->d_mass,
-                      c->st));
+  CK(c, launch_select(probs, keep, N, c->n_cells, min_m, m, mass_target, keep_mass, c->d_cand,
+                      c->d_mass, c->st));
   int32_t* cand = c->pinned<int32_t>(0, pairs);
   float* mass = c->pinned<float>(1, N);
   if (!cand || !mass) return c->fail(EMC_ERR_OOM, "pinned host staging");

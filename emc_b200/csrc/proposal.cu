@@ -96,12 +96,14 @@ __device__ __forceinline__ void warp_argmax(const float* row, int C, uint32_t ta
   }
 }
 
-// One warp per pattern.  With `keep`: first its min_m most probable cells
-// under keep (those with keep > 0).  Then cells in order of probs until at
-// least min_m are taken and their probs total reaches mass_target, at most m;
-// unused slots -1.  mass[p] = the probs total of the taken cells.
+// One warp per pattern.  With `keep`: first its most probable cells under
+// keep (those with keep > 0) until at least min_m are taken and their keep
+// total reaches keep_mass.  Then cells in order of probs until at least min_m
+// are taken and their probs total reaches mass_target, at most m; unused
+// slots -1.  mass[p] = the probs total of the taken cells.
 __global__ void select_kernel(const float* probs, const float* keep, int64_t N, int C, int min_m,
-                              int m, float mass_target, int32_t* cand, float* mass) {
+                              int m, float mass_target, float keep_mass, int32_t* cand,
+                              float* mass) {
   const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (p >= N) return;
@@ -112,11 +114,13 @@ __global__ void select_kernel(const float* probs, const float* keep, int64_t N, 
   int s = 0;
   if (keep) {
     const float* krow = keep + p * C;
-    for (; s < min_m && s < m; ++s) {
+    float ktot = 0.0f;
+    for (; s < m && (s < min_m || ktot < keep_mass); ++s) {
       float best;
       int bi;
       warp_argmax(krow, C, taken, lane, best, bi);
       if (bi < 0 || !(best > 0.0f)) break;
+      ktot += best;
       if ((bi & 31) == lane) taken |= 1u << (bi >> 5);
       if (lane == 0) cand[p * m + s] = bi;
       const float v = row[bi];
@@ -425,9 +429,10 @@ cudaError_t launch_scatter_targets(const int32_t* cand, const float* cmass, int6
 }
 
 cudaError_t launch_select(const float* probs, const float* keep, int64_t N, int C, int min_m,
-                          int m, float mass_target, int32_t* cand, float* mass, cudaStream_t st) {
+                          int m, float mass_target, float keep_mass, int32_t* cand, float* mass,
+                          cudaStream_t st) {
   select_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(probs, keep, N, C, min_m, m, mass_target,
-                                                         cand, mass);
+                                                         keep_mass, cand, mass);
   return cudaGetLastError();
 }
 

@@ -32,12 +32,14 @@ cudaError_t launch_targets(const TargetArgs& a, cudaStream_t st);
 cudaError_t launch_scatter_targets(const int32_t* cand, const float* cmass, int64_t N, int m,
                                    int n_cells, float* t, cudaStream_t st);
 
-// cand[p][0..m): with keep (optional, [N][C]) first the min_m most probable
-// cells of keep[p] that have keep > 0; then the most probable remaining cells
-// of probs[p] in order until at least min_m are taken and their probs total
-// reaches mass_target, at most m (the rest -1); mass[p] = that total.
+// cand[p][0..m): with keep (optional, [N][C]) first the most probable cells
+// of keep[p] that have keep > 0, until at least min_m are taken and their keep
+// total reaches keep_mass; then the most probable remaining cells of probs[p]
+// in order until at least min_m are taken and their probs total reaches
+// mass_target, at most m (the rest -1); mass[p] = that total.
 cudaError_t launch_select(const float* probs, const float* keep, int64_t N, int C, int min_m,
-                          int m, float mass_target, int32_t* cand, float* mass, cudaStream_t st);
+                          int m, float mass_target, float keep_mass, int32_t* cand, float* mass,
+                          cudaStream_t st);
 
 // Pairs (pattern, selected cell) grouped by cell: group c holds pairs
 // gbeg[c] .. gbeg[c]+gcnt[c]-1, pair q belongs to pattern gpair[q]; pattern

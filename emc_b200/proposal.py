@@ -29,8 +29,8 @@ def _bind():
         ("emc_set_cells", [P, P, C.c_int32], C.c_int),
         ("emc_pattern_features", [P, C.c_int32, P], C.c_int),
         ("emc_cell_targets", [P, P], C.c_int),
-        ("emc_iterate_proposed", [P, P, P, C.c_int32, C.c_int32, C.c_float, C.c_float, P],
-         C.c_int),
+        ("emc_iterate_proposed",
+         [P, P, P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, P], C.c_int),
         ("emc_net_create", [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, P], C.c_int),
         ("emc_net_destroy", [P], C.c_int),
         ("emc_net_num_params", [P], I64),
@@ -198,10 +198,12 @@ class LearnedProposal:
             return probs
         return (1.0 - weight) * probs + weight * previous
 
-    def iterate(self, probs, max_cells, mass_target=1.0, threshold=0.99, min_cells=1, keep=None):
+    def iterate(self, probs, max_cells, mass_target=1.0, threshold=0.99, min_cells=1, keep=None,
+                keep_mass=0.0):
         """One proposed iteration (emc_iterate_proposed).  Per pattern: with
-        `keep` (e.g. the previous iteration's `targets()`) first its min_cells
-        most probable cells under keep; then the most probable cells under
+        `keep` (e.g. the previous iteration's `targets()`) first its most
+        probable cells under keep until at least min_cells are taken and their
+        keep mass reaches keep_mass; then the most probable cells under
         `probs` until at least min_cells are taken and their predicted mass
         reaches mass_target, at most max_cells.  The dense iteration runs
         instead when the mean predicted mass is below threshold.  Returns the
@@ -216,5 +218,5 @@ class LearnedProposal:
         self.ctx._c(lib().emc_iterate_proposed(self.ctx._h, probs.data_ptr(),
                                                None if keep is None else keep.data_ptr(),
                                                int(min_cells), int(max_cells), mass_target,
-                                               threshold, C.byref(st)))
+                                               keep_mass, threshold, C.byref(st)))
         return {k: getattr(st, k) for k, _ in ProposalStats._fields_ if k != "pad_"}

@@ -220,16 +220,18 @@ emc_status emc_pattern_features(emc_context *ctx, int32_t in_side, float *x_devi
 emc_status emc_cell_targets(emc_context *ctx, float *t_device);
 /* One iteration restricted, per pattern, to candidate cells: with
  * keep_device (optional, [N][n_cells], e.g. the previous iteration's
- * emc_cell_targets) first the min_cells most probable cells under keep that
- * hold keep > 0; then cells in order of cell_probs (the proposal) until at
- * least min_cells are taken and their cell_probs mass reaches mass_target
- * (>= 1: always max_cells cells), at most max_cells in all
+ * emc_cell_targets) first the most probable cells under keep that hold
+ * keep > 0, until at least min_cells are taken and their keep mass reaches
+ * keep_mass; then cells in order of cell_probs (the proposal) until at least
+ * min_cells are taken and their cell_probs mass reaches mass_target (>= 1:
+ * always max_cells cells), at most max_cells in all
  * (1 <= min_cells <= max_cells).  The dense iteration runs instead when the
  * mean cell_probs mass of the candidates is below `threshold`.
  * cell_probs: device [N][n_cells]. */
 emc_status emc_iterate_proposed(emc_context *ctx, const float *cell_probs_device,
                                 const float *keep_device, int32_t min_cells, int32_t max_cells,
-                                float mass_target, float threshold, emc_proposal_stats *stats);
+                                float mass_target, float keep_mass, float threshold,
+                                emc_proposal_stats *stats);
 
 /* Proposal network: three 3x3 stride-2 convolutions (16, 32, 64 channels,
  * ReLU) and a fully connected layer to n_out logits, softmax.  BF16 weights

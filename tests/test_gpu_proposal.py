@@ -117,21 +117,26 @@ def test_learned_proposal_end_to_end():
         assert rel(ctx.get_model(), m_dense) < 1e-5
 
 
-def _select(probs, max_cells, mass_target, min_cells=1, keep=None):
+def _select(probs, max_cells, mass_target, min_cells=1, keep=None, keep_mass=0.0):
     """The candidate cells emc_iterate_proposed takes: with keep, first the
-    min_cells most probable cells under keep that hold keep > 0; then cells in
-    order of probs until at least min_cells are taken and their (FP32) probs
-    sum reaches mass_target, at most max_cells."""
+    most probable cells under keep that hold keep > 0 until at least
+    min_cells are taken and their (FP32) keep sum reaches keep_mass; then
+    cells in order of probs until at least min_cells are taken and their
+    (FP32) probs sum reaches mass_target, at most max_cells."""
     N, n_cells = probs.shape
     sel = np.zeros((N, n_cells), bool)
     for p in range(N):
         tot, n = np.float32(0), 0
         if keep is not None:
-            for k in np.argsort(-keep[p], kind="stable")[:min(min_cells, max_cells)]:
+            ktot = np.float32(0)
+            for k in np.argsort(-keep[p], kind="stable"):
+                if n >= max_cells or (n >= min_cells and not ktot < np.float32(keep_mass)):
+                    break
                 if not keep[p, k] > 0:
                     break
                 sel[p, k] = True
                 n += 1
+                ktot = np.float32(ktot + keep[p, k])
                 tot = np.float32(tot + max(probs[p, k], np.float32(0)))
         for k in np.argsort(-probs[p], kind="stable"):
             if n >= max_cells or (mass_target < 1.0 and n >= min_cells and tot >= mass_target):
@@ -144,7 +149,7 @@ def _select(probs, max_cells, mass_target, min_cells=1, keep=None):
     return sel
 
 
-def _proposal_case(d, max_cells, mass_target=1.0, seed=0, min_cells=1, keep=False):
+def _proposal_case(d, max_cells, mass_target=1.0, seed=0, min_cells=1, keep=False, keep_mass=0.0):
     """Rotations sorted by coarse cell (n=1: 60 uneven cells), distinct random
     cell probabilities (and, with keep, a second random posterior with half
     of each row zero), and the allowed[r][p] mask of the selected cells."""
@@ -162,35 +167,38 @@ def _proposal_case(d, max_cells, mass_target=1.0, seed=0, min_cells=1, keep=Fals
         kp = np.exp(z - z.max(1, keepdims=True)) * (rng.random((N, n_cells)) < 0.5)
         kp[:3] = 0.0  # patterns with no kept cell at all
         kp = kp.astype(np.float32)
-    sel = _select(probs, max_cells, mass_target, min_cells, kp)
+    sel = _select(probs, max_cells, mass_target, min_cells, kp, keep_mass)
     allowed = sel[:, cell].T.astype(np.uint8)  # [R][N]
     if keep:
         return d, cell, n_cells, probs, allowed, kp
     return d, cell, n_cells, probs, allowed
 
 
-@pytest.mark.parametrize("lik,interp,prec,tol,max_cells,mass_target,min_cells,keep", [
-    ("poisson", "nearest", "fp32", 1e-5, 7, 1.0, 1, False),
-    ("gauss", "nearest", "fp32", 1e-4, 7, 1.0, 1, False),
-    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0, 1, False),
-    ("gauss", "nearest", "mixed", 1e-4, 7, 1.0, 1, False),
-    ("poisson", "trilinear", "mixed", 1e-4, 7, 1.0, 1, False),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.6, 1, False),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, False),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, True),
+@pytest.mark.parametrize("lik,interp,prec,tol,max_cells,mass_target,min_cells,keep,keep_mass", [
+    ("poisson", "nearest", "fp32", 1e-5, 7, 1.0, 1, False, 0.0),
+    ("gauss", "nearest", "fp32", 1e-4, 7, 1.0, 1, False, 0.0),
+    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0, 1, False, 0.0),
+    ("gauss", "nearest", "mixed", 1e-4, 7, 1.0, 1, False, 0.0),
+    ("poisson", "trilinear", "mixed", 1e-4, 7, 1.0, 1, False, 0.0),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.6, 1, False, 0.0),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, False, 0.0),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, True, 0.0),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.5, 2, True, 1.1),
 ])
 def test_proposed_iteration_matches_restricted_oracle(lik, interp, prec, tol, max_cells,
-                                                      mass_target, min_cells, keep):
+                                                      mass_target, min_cells, keep, keep_mass):
     """One proposed iteration (the top cells of 60 uneven cells per pattern:
     a fixed 7, adaptive up to a predicted mass of 0.6, at least 3 and then up
-    to 0.7, or the 3 top cells of a second posterior first) against the FP64
-    oracle's iteration restricted to the same candidate rotations."""
+    to 0.7, the 3 top cells of a second posterior first, or that posterior's
+    cells up to a mass of 1.1 first) against the FP64 oracle's iteration
+    restricted to the same candidate rotations."""
     import torch
     from emc_b200 import workloads as W
     from emc_b200.proposal import LearnedProposal
     from oracle import oracle as O
     from parity import oracle_cfg
-    case = _proposal_case(W.make("tiny16"), max_cells, mass_target, min_cells=min_cells, keep=keep)
+    case = _proposal_case(W.make("tiny16"), max_cells, mass_target, min_cells=min_cells, keep=keep,
+                          keep_mass=keep_mass)
     d, cell, n_cells, probs, allowed = case[:5]
     kp = torch.from_numpy(case[5]).cuda() if keep else None
     cfg = oracle_cfg(d, lik, interp)
@@ -203,7 +211,7 @@ def test_proposed_iteration_matches_restricted_oracle(lik, interp, prec, tol, ma
     with make_ctx(d, lik, interp, prec) as ctx:
         lp = LearnedProposal(ctx, cell, n_cells, bf16=True)
         st = lp.iterate(torch.from_numpy(probs).cuda(), max_cells, mass_target, threshold=0.0,
-                        min_cells=min_cells, keep=kp)
+                        min_cells=min_cells, keep=kp, keep_mass=keep_mass)
         assert st["fallback"] == 0
         assert st["evaluations"] == int(allowed.sum())
         assert rel(ctx.get_scaling(), s_ref) <= tol, rel(ctx.get_scaling(), s_ref)
