@@ -1348,11 +1348,14 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   std::vector<int4> mt, ct;
   int64_t n_gmt = 0, n_gct = 0;
   TileDesc *gmt = nullptr, *gct = nullptr;
+  // the grouped maximize on SM pairs (256-slot tiles) where the dense one is
+  const bool gpair_form = tc && c->tune.maximize_pair;
+  const int32_t gm_rows = gpair_form ? 256 : 128;
   if (tc) {
     const int64_t ptiles = (c->npa + 255) / 256;
     for (int32_t k = 0; k < n_cells; ++k)
       if (gcnt[k] > 0) {
-        n_gmt += (gcnt[k] + 127) / 128;
+        n_gmt += (gcnt[k] + gm_rows - 1) / gm_rows;
         n_gct += (int64_t)((c->h_mcnt[k] + 127) / 128) * ptiles;
       }
     gmt = c->pinned<TileDesc>(4, n_gmt);
@@ -1361,9 +1364,10 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
     int64_t im = 0, ic = 0;
     for (int32_t k = 0; k < n_cells; ++k) {
       if (gcnt[k] == 0) continue;
-      for (int32_t q0 = 0; q0 < gcnt[k]; q0 += 128)
+      for (int32_t q0 = 0; q0 < gcnt[k]; q0 += gm_rows)
         gmt[im++] = TileDesc{(int32_t)(gbeg[k] + q0), 0, (int32_t)c->h_mbeg[k], 0,
-                             (int32_t)(c->Ppad / kMaximizeBK), k, q0, 0};
+                             (int32_t)(c->Ppad / (gpair_form ? kPairBoxK : kMaximizeBK)), k, q0,
+                             0};
       for (int32_t r0 = 0; r0 < c->h_mcnt[k]; r0 += 128)
         for (int64_t nt = 0; nt < ptiles; ++nt)
           gct[ic++] = TileDesc{(int32_t)(c->h_mbeg[k] + r0), 0, (int32_t)(nt * 256),
@@ -1459,7 +1463,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   int launches = 0;
   if (tc) {
     CUtensorMap tmKg, tmKg64, tmAhi, tmAlo;
-    if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, kMaximizeBK) ||
+    if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, gpair_form ? kPairBoxK : kMaximizeBK) ||
         !tc_encode_2d(&tmKg64, c->d_Kg, c->Ppad, S, kCompressBK, 64) ||
         !tc_encode_2d_strided(&tmAhi, c->d_Ahi, c->a_ld, R, c->a_ld, 128, kCompressBK) ||
         !tc_encode_2d_strided(&tmAlo, c->d_Alo, c->a_ld, R, c->a_ld, 128, kCompressBK))
@@ -1476,8 +1480,12 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
     ge.rowstat = c->d_rowstat;
     ge.Y = c->d_Yc;
     ge.ldY = MM;
-    CK(c, launch_group_maximize_tc(tmKg, c->tmBhi, c->tmBlo, n_gmt, ge, c->d_status,
-                                   c->num_sms, c->st));
+    if (gpair_form)
+      CK(c, launch_group_maximize_pair_tc(tmKg, c->tmBhi64, c->tmBlo64, n_gmt, ge, c->d_status,
+                                          c->num_sms, c->st));
+    else
+      CK(c, launch_group_maximize_tc(tmKg, c->tmBhi, c->tmBlo, n_gmt, ge, c->d_status,
+                                     c->num_sms, c->st));
     c->mark(2);
     CK(c, launch_group_softmax(g, c->st));
     CK(c, launch_p_split(g, c->d_cell, R, c->d_T, c->a_ld, c->d_Ahi, c->d_Alo, c->st));

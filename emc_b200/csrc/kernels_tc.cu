@@ -680,6 +680,19 @@ struct EpiGMax {
   __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
 };
 
+// The grouped maximize on SM pairs: tiles of 256 slots (a_row, local0 = the
+// pair tile's first slot), this CTA's accumulator holds slots 128 rank ..
+// 128 rank + 127 of it against all the tile's member columns.
+struct EpiGMaxPair : EpiGMax {
+  __device__ void tile_begin(int64_t t, int64_t x, int tid, uint8_t* smem) {
+    EpiGMax::tile_begin(t, x, tid, smem);
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    d.a_row += (int32_t)rank * 128;
+    d.local0 += (int32_t)rank * 128;
+  }
+};
+
 // Grouped compress: row = member rotation r of the tile's cell, column =
 // active pixel; acc = U_r (the operand rows are P / (T_r phi)), inserted with
 // weight rotw T_r as in EpiCmp.
@@ -1622,6 +1635,16 @@ cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap&
   epi.a = e;
   return run_gemm<1, 2, 5, true, kMaximizeBK>(one_set(tmKg, tmKg, tmBhi, tmBlo), n_tiles, 1, 0, epi,
                                               status, num_sms, st);
+}
+
+cudaError_t launch_group_maximize_pair_tc(const CUtensorMap& tmKg, const CUtensorMap& tmBhi,
+                                          const CUtensorMap& tmBlo, int64_t n_tiles,
+                                          const GMaxEpiArgs& e, TcStatus* status, int num_sms,
+                                          cudaStream_t st) {
+  EpiGMaxPair epi;
+  epi.a = e;
+  return run_pair<1, 2, true>(one_set(tmKg, tmKg, tmBhi, tmBlo), n_tiles, 1, 0, epi, status,
+                              num_sms, st, 1);
 }
 
 cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap& tmAlo,

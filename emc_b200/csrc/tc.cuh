@@ -122,6 +122,14 @@ cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap&
                                      const GMaxEpiArgs& e, TcStatus* status, int num_sms,
                                      cudaStream_t st);
 
+// The same on SM pairs (cta_group::2): tiles of 256 slots (a_row and local0
+// the pair tile's first slot) x 256 members, 64-wide K-steps; tensor maps with
+// boxes of 128 rows x kPairBoxK (Kg, and each half of the slice operand).
+cudaError_t launch_group_maximize_pair_tc(const CUtensorMap& tmKg, const CUtensorMap& tmBhi,
+                                          const CUtensorMap& tmBlo, int64_t n_tiles,
+                                          const GMaxEpiArgs& e, TcStatus* status, int num_sms,
+                                          cudaStream_t st);
+
 // Grouped compress: acc[member][j] = sum_q A[mbeg_c + member][q] Kg[slot0_c + q][j]
 // with A = P / (T_r phi) as FP16 hi + lo (zero beyond the cell's slots);
 // 128 members x 256 pixels per tile, inserted in the epilogue.  Kg is the B

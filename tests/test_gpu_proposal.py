@@ -174,24 +174,28 @@ def _proposal_case(d, max_cells, mass_target=1.0, seed=0, min_cells=1, keep=Fals
     return d, cell, n_cells, probs, allowed
 
 
-@pytest.mark.parametrize("lik,interp,prec,tol,max_cells,mass_target,min_cells,keep,keep_mass", [
-    ("poisson", "nearest", "fp32", 1e-5, 7, 1.0, 1, False, 0.0),
-    ("gauss", "nearest", "fp32", 1e-4, 7, 1.0, 1, False, 0.0),
-    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0, 1, False, 0.0),
-    ("gauss", "nearest", "mixed", 1e-4, 7, 1.0, 1, False, 0.0),
-    ("poisson", "trilinear", "mixed", 1e-4, 7, 1.0, 1, False, 0.0),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.6, 1, False, 0.0),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, False, 0.0),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, True, 0.0),
-    ("poisson", "nearest", "mixed", 1e-4, 12, 0.5, 2, True, 1.1),
+@pytest.mark.parametrize("lik,interp,prec,tol,max_cells,mass_target,min_cells,keep,keep_mass,pair", [
+    ("poisson", "nearest", "fp32", 1e-5, 7, 1.0, 1, False, 0.0, False),
+    ("gauss", "nearest", "fp32", 1e-4, 7, 1.0, 1, False, 0.0, False),
+    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0, 1, False, 0.0, False),
+    ("gauss", "nearest", "mixed", 1e-4, 7, 1.0, 1, False, 0.0, False),
+    ("poisson", "trilinear", "mixed", 1e-4, 7, 1.0, 1, False, 0.0, False),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.6, 1, False, 0.0, False),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, False, 0.0, False),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.7, 3, True, 0.0, False),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.5, 2, True, 1.1, False),
+    ("poisson", "nearest", "mixed", 1e-4, 7, 1.0, 1, False, 0.0, True),
+    ("poisson", "nearest", "mixed", 1e-4, 12, 0.5, 2, True, 1.1, True),
 ])
 def test_proposed_iteration_matches_restricted_oracle(lik, interp, prec, tol, max_cells,
-                                                      mass_target, min_cells, keep, keep_mass):
+                                                      mass_target, min_cells, keep, keep_mass,
+                                                      pair):
     """One proposed iteration (the top cells of 60 uneven cells per pattern:
     a fixed 7, adaptive up to a predicted mass of 0.6, at least 3 and then up
     to 0.7, the 3 top cells of a second posterior first, or that posterior's
-    cells up to a mass of 1.1 first) against the FP64 oracle's iteration
-    restricted to the same candidate rotations."""
+    cells up to a mass of 1.1 first; pair: the grouped maximize on SM pairs)
+    against the FP64 oracle's iteration restricted to the same candidate
+    rotations."""
     import torch
     from emc_b200 import workloads as W
     from emc_b200.proposal import LearnedProposal
@@ -209,6 +213,8 @@ def test_proposed_iteration_matches_restricted_oracle(lik, interp, prec, tol, ma
     t_ref = np.zeros((P_ref.shape[1], n_cells))
     np.add.at(t_ref.T, cell, P_ref)  # responsibility mass per (pattern, cell)
     with make_ctx(d, lik, interp, prec) as ctx:
+        if pair:
+            ctx.set_tuning(1, 6, 1, 0)
         lp = LearnedProposal(ctx, cell, n_cells, bf16=True)
         st = lp.iterate(torch.from_numpy(probs).cuda(), max_cells, mass_target, threshold=0.0,
                         min_cells=min_cells, keep=kp, keep_mass=keep_mass)
