@@ -753,6 +753,27 @@ def main():
                 "speedup_of_mixed": ms32 / ms_step}
         if learned:
             learned["speedup_vs_plain_fp32"] = ms32 / learned["ms_per_step"]
+        if a.likelihood == "poisson":
+            # the same FP32 iteration with both contractions as gathers over
+            # the non-zero counts (photon lists)
+            c32 = make_ctx("fp32")
+            c32.set_sparse_maximize(True)
+            c32.set_sparse_compress(True)
+            mss, sts, _ = timed(c32, a.fp32_steps, 1)
+            c32.set_model(d["model0"])
+            c32.set_scaling(d["scaling0"])
+            c32.iterate(stats=False)
+            m_sparse = c32.get_model()
+            c32.close()
+            c32 = make_ctx("fp32")
+            c32.iterate(stats=False)
+            m_plain = c32.get_model()
+            c32.close()
+            fp32["photon_lists"] = {
+                "ms_per_step": mss, "stages_ms": [round(float(x), 3) for x in sts],
+                "speedup_vs_dense_fp32": ms32 / mss,
+                "model_rel_err_vs_dense_fp32": float(np.linalg.norm(m_sparse - m_plain) /
+                                                     np.linalg.norm(m_plain))}
 
     if dist:
         dist.barrier()

@@ -50,7 +50,7 @@ class IterStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("maximize_raster", C.c_int32), ("compress_raster", C.c_int32),
                 ("maximize_pair", C.c_int32), ("compress_pair", C.c_int32),
-                ("maximize_sparse", C.c_int32)]
+                ("maximize_sparse", C.c_int32), ("compress_sparse", C.c_int32)]
 
 
 class SynthConfig(C.Structure):
@@ -411,6 +411,15 @@ class Context:
         t = Tuning()
         self._c(lib().emc_get_tuning(self._h, C.byref(t)))
         t.maximize_sparse = int(bool(on))
+        self._c(lib().emc_set_tuning(self._h, C.byref(t)))
+
+    def set_sparse_compress(self, on: bool):
+        """FP32 contexts: form the slice sums as a gather over each active
+        pixel's non-zero counts instead of the dense rotation x pattern
+        contraction."""
+        t = Tuning()
+        self._c(lib().emc_get_tuning(self._h, C.byref(t)))
+        t.compress_sparse = int(bool(on))
         self._c(lib().emc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, candidates=(1, 2, 4, 8, 16)):

@@ -146,7 +146,7 @@ struct emc_context {
   // raster bands of the maximize / compress tile orders and the SM-pair forms
   // (defaults from measurements at 64^3 and 128^3, set per shape in
   // alloc_work; emc_autotune re-measures)
-  emc_tuning tune{1, 6, 0, 0, 0};
+  emc_tuning tune{1, 6, 0, 0, 0, 0};
   // photon-list log-likelihood (FP32 poisson): counts as CSR, log W pixel-major
   int64_t* d_csr_row = nullptr;
   int32_t* d_csr_col = nullptr;
@@ -154,6 +154,16 @@ struct emc_context {
   int64_t csr_cap = 0;
   bool csr_valid = false;
   float* d_ST = nullptr;
+  // photon-list slice sums (FP32): counts as CSC over active pixels, the
+  // entries divided by their pattern's scaling, responsibilities pattern-major
+  int64_t* d_csc_ptr = nullptr;
+  int32_t* d_csc_row = nullptr;
+  float* d_csc_val = nullptr;
+  float* d_csc_sval = nullptr;
+  int64_t csc_cap = 0;
+  bool csc_valid = false;
+  int64_t csc_nnz = 0;
+  float* d_PT = nullptr;
   bool prof = false;
   cudaEvent_t ev[2][6] = {{nullptr}};
   int cur = 0;
@@ -484,6 +494,7 @@ static emc_status finish_patterns(emc_context* c) {
                    bad);
   c->have_pat = true;
   c->csr_valid = false;
+  c->csc_valid = false;
   return EMC_OK;
 }
 
@@ -722,6 +733,64 @@ static emc_status sparse_loglik(emc_context* c) {
   return EMC_OK;
 }
 
+// The slice sums U[r][j] = sum_p P_rp K_pj / phi_p / T_r as a gather over
+// each active pixel's non-zero counts: the counts' CSC (built once per
+// pattern upload through a transposed copy of K), its entries divided by the
+// current scaling, and P transposed to pattern-major rows.
+static emc_status sparse_slicesums(emc_context* c) {
+  const int64_t N = c->N, R = c->R, npa = c->npa;
+  if (!c->csc_valid) {
+    if (!c->d_csc_ptr) TRY(c->alloc(&c->d_csc_ptr, npa + 1));
+    float* KT = nullptr;
+    TRY(c->alloc(&KT, npa * N));
+    CK(c, launch_transpose(c->d_K, N, npa, KT, N, c->st));
+    std::vector<int64_t> cnt(npa), ptr(npa + 1, 0);
+    int64_t* d_cnt = c->d_csc_ptr + 1;
+    CK(c, launch_csr_count(KT, npa, N, d_cnt, c->st));
+    CK(c, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int64_t) * npa, cudaMemcpyDeviceToHost, c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    for (int64_t j = 0; j < npa; ++j) ptr[j + 1] = ptr[j] + cnt[j];
+    const int64_t nnz = ptr[npa];
+    if (nnz + 1 > c->csc_cap) {
+      for (void* q : {(void*)c->d_csc_row, (void*)c->d_csc_val, (void*)c->d_csc_sval})
+        if (q) c->release(q);
+      c->d_csc_row = nullptr;
+      c->d_csc_val = nullptr;
+      c->d_csc_sval = nullptr;
+      c->csc_cap = 0;
+      TRY(c->alloc(&c->d_csc_row, nnz + 1));
+      TRY(c->alloc(&c->d_csc_val, nnz + 1));
+      TRY(c->alloc(&c->d_csc_sval, nnz + 1));
+      c->csc_cap = nnz + 1;
+    }
+    CK(c, cudaMemcpyAsync(c->d_csc_ptr, ptr.data(), sizeof(int64_t) * (npa + 1),
+                          cudaMemcpyHostToDevice, c->st));
+    CK(c, launch_csr_fill(KT, npa, N, c->d_csc_ptr, c->d_csc_row, c->d_csc_val, c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    c->release(KT);
+    c->csc_nnz = nnz;
+    c->csc_valid = true;
+  }
+  const int64_t ldT = (R + 3) / 4 * 4;
+  if (!c->d_PT) TRY(c->alloc(&c->d_PT, N * ldT));
+  CK(c, launch_transpose(c->d_LL, R, N, c->d_PT, ldT, c->st));
+  CK(c, launch_scale_entries(c->d_csc_val, c->d_csc_row, c->d_scaling, c->csc_nnz, c->d_csc_sval,
+                             c->st));
+  SparseCmpArgs a{};
+  a.col_ptr = c->d_csc_ptr;
+  a.row = c->d_csc_row;
+  a.val = c->d_csc_sval;
+  a.PT = c->d_PT;
+  a.ldT = ldT;
+  a.T = c->d_T;
+  a.R = R;
+  a.npa = npa;
+  a.U = c->d_S;
+  CK(c, launch_compress_sparse(a, c->st));
+  c->launches += 3;
+  return EMC_OK;
+}
+
 extern "C" {
 
 emc_status emc_maximize(emc_context* c) {
@@ -808,18 +877,22 @@ emc_status emc_compress_insert(emc_context* c) {
     CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
   }
   if (!c->mixed) {
-    CompressArgs a{};
-    a.P = c->d_LL;
-    a.K = c->d_K;
-    a.scaling = c->d_scaling;
-    a.T = c->d_T;
-    a.R = c->R;
-    a.N = c->N;
-    a.npa = c->npa;
-    a.ldK = c->npa;
-    a.ldU = c->npa;
-    a.U = c->d_S;  // the averaged slices replace the expanded ones (emc_atomic.cu:96)
-    CK(c, launch_compress_fp32(a, c->st));
+    if (c->tune.compress_sparse) {
+      TRY(sparse_slicesums(c));
+    } else {
+      CompressArgs a{};
+      a.P = c->d_LL;
+      a.K = c->d_K;
+      a.scaling = c->d_scaling;
+      a.T = c->d_T;
+      a.R = c->R;
+      a.N = c->N;
+      a.npa = c->npa;
+      a.ldK = c->npa;
+      a.ldU = c->npa;
+      a.U = c->d_S;  // the averaged slices replace the expanded ones (emc_atomic.cu:96)
+      CK(c, launch_compress_fp32(a, c->st));
+    }
     InsertArgs in{};
     in.U = c->d_S;
     in.T = c->d_T;
@@ -922,8 +995,11 @@ emc_status emc_set_tuning(emc_context* c, const emc_tuning* t) {
   if (!c || !t || t->maximize_raster < 1 || t->compress_raster < 1 ||
       (t->maximize_pair != 0 && t->maximize_pair != 1) ||
       (t->compress_pair != 0 && t->compress_pair != 1) ||
-      (t->maximize_sparse != 0 && t->maximize_sparse != 1))
+      (t->maximize_sparse != 0 && t->maximize_sparse != 1) ||
+      (t->compress_sparse != 0 && t->compress_sparse != 1))
     return EMC_ERR_ARG;
+  if (t->compress_sparse && c->mixed)
+    return c->fail(EMC_ERR_UNSUPPORTED, "the photon-list slice sums are an FP32 form");
   if (t->maximize_sparse && (c->mixed || c->gauss))
     return c->fail(EMC_ERR_UNSUPPORTED, "the photon-list log-likelihood is an FP32 poisson form");
   c->tune = *t;
@@ -966,7 +1042,8 @@ emc_status emc_autotune(emc_context* c, const int32_t* cand, int32_t n, float* m
     for (int32_t i = 0; i < n && s == EMC_OK; ++i) {
       float tmax = 1e30f;
       for (int32_t pair = 0; pair < 2 && s == EMC_OK; ++pair) {
-        c->tune = emc_tuning{cand[i], cand[i], pair, pair, keep.maximize_sparse};
+        c->tune = emc_tuning{cand[i], cand[i], pair, pair, keep.maximize_sparse,
+                             keep.compress_sparse};
         if ((s = restore()) != EMC_OK || (s = emc_iterate(c, nullptr)) != EMC_OK) break;
         float t[5];
         if ((s = c->cuda(cudaEventSynchronize(c->ev[c->cur][5]), "autotune")) != EMC_OK) break;

@@ -70,6 +70,24 @@ struct SparseLLArgs {
 };
 // ldT % 4 == 0 and logWT 16-byte aligned (each thread gathers 4 rotations).
 cudaError_t launch_ll_sparse(const SparseLLArgs& a, cudaStream_t st);
+// Slice sums from the counts in CSC (col_ptr [npa+1] over active pixels, row
+// = pattern, val = K / phi of that pattern) and the responsibilities
+// pattern-major (PT [N][ldT], ldT >= R, % 4 == 0):
+//   U[r][j] = (sum over the pixel's entries val * PT[p][r]) / T_r   (T_r > 1e-30)
+struct SparseCmpArgs {
+  const int64_t* col_ptr;
+  const int32_t* row;
+  const float* val;
+  const float* PT;
+  int64_t ldT;
+  const float* T;
+  int64_t R, npa;
+  float* U;               // [R][npa]
+};
+cudaError_t launch_compress_sparse(const SparseCmpArgs& a, cudaStream_t st);
+// val_out[e] = val[e] / scaling[row[e]] over nnz entries.
+cudaError_t launch_scale_entries(const float* val, const int32_t* row, const float* scaling,
+                                 int64_t nnz, float* val_out, cudaStream_t st);
 // logWT[j][r] = S[r][j] (tiled transpose, [R][npa] -> [npa][ldT]).
 cudaError_t launch_transpose(const float* S, int64_t R, int64_t npa, float* ST, int64_t ldT,
                              cudaStream_t st);

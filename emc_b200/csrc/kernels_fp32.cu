@@ -615,48 +615,61 @@ cudaError_t launch_expand_table(const float* model, int64_t M, float floor_, int
 }
 
 // ------------------------------------------------------------ photon lists --
-// 128 threads x 4 rotations = 512 rotations per block, 16 patterns per block:
-// for each pattern the block walks its non-zero pixels (uniform loads of the
-// CSR entry) and every thread gathers 16 bytes of log W (its 4 rotations) at
-// that pixel, so one entry reads one coalesced 2 KB row of logWT.  Pattern
-// blocks vary fastest in the grid, so the blocks resident at one time share
-// one rotation block's columns of logWT (npa x 2 KB) in L2.  FP32 partial
-// sums over chunks of 32 photons are folded into FP64 totals, as the dense
-// contraction folds each 32-pixel K-step.  The 16 x 512 results leave through
-// shared memory as rows of LL.
+// Gathers over the non-zero counts.  One block: 128 threads x 4 rotations =
+// 512 rotations by 16 output columns (patterns of the log-likelihood, pixels
+// of the slice sums).  For each column the block walks its entries (uniform
+// loads of the sparse entry) and every thread gathers 16 bytes of the
+// transposed operand row at that entry (logWT[pixel] for the log-likelihood,
+// PT[pattern] for the slice sums), so one entry reads one coalesced 2 KB row.
+// Column blocks vary fastest in the grid, so the blocks resident at one time
+// share one rotation block's columns of the operand in L2.  FP32 partial sums
+// over chunks of 32 entries are folded into FP64 totals, as the dense
+// contraction folds each 32-wide K-step.  The 16 x 512 results leave through
+// shared memory as rows of the output.
+//   MODE 0: LL[r][p] = total - phi_p sum W_r      MODE 1: U[r][j] = total / T_r
 constexpr int kSparseRot = 512, kSparsePat = 16;
-__global__ void __launch_bounds__(128) sparse_ll_kernel(const SparseLLArgs a) {
+template <int MODE>
+__global__ void __launch_bounds__(128)
+    sparse_gather_kernel(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                         const float* __restrict__ val, const float* __restrict__ XT,
+                         int64_t ldT, int64_t R, int64_t ncol, const float* scaling,
+                         const double* rowstat, const float* T, float* out) {
   __shared__ float tile[kSparsePat][kSparseRot + 1];
   const int64_t r0 = (int64_t)blockIdx.y * kSparseRot + 4 * threadIdx.x;
   const int64_t p0 = (int64_t)blockIdx.x * kSparsePat;
-  const bool rv = r0 < a.R;  // ldT >= R rounded up to 4: the whole float4 is in bounds
+  const bool rv = r0 < R;  // ldT >= R rounded up to 4: the whole float4 is in bounds
   double sw[4];
 #pragma unroll
-  for (int u = 0; u < 4; ++u) sw[u] = r0 + u < a.R ? a.rowstat[r0 + u] : 0.0;
+  for (int u = 0; u < 4; ++u) {
+    if (MODE == 0)
+      sw[u] = r0 + u < R ? rowstat[r0 + u] : 0.0;
+    else
+      sw[u] = r0 + u < R ? (double)T[r0 + u] : 0.0;
+  }
   for (int i = 0; i < kSparsePat; ++i) {
     const int64_t p = p0 + i;
     float v[4] = {0.f, 0.f, 0.f, 0.f};
-    if (p < a.N && rv) {
-      const int64_t e0 = a.row_ptr[p], e1 = a.row_ptr[p + 1];
+    if (p < ncol && rv) {
+      const int64_t e0 = ptr[p], e1 = ptr[p + 1];
       double tot[4] = {0.0, 0.0, 0.0, 0.0};
       int64_t e = e0;
       while (e < e1) {
         const int64_t ce = e + 32 < e1 ? e + 32 : e1;
         float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
         for (; e + 2 <= ce; e += 2) {
-          const int32_t j0 = __ldg(a.col + e), j1 = __ldg(a.col + e + 1);
-          const float k0 = __ldg(a.val + e), k1 = __ldg(a.val + e + 1);
-          const float4 w0 = __ldg(reinterpret_cast<const float4*>(a.logWT + (int64_t)j0 * a.ldT + r0));
-          const float4 w1 = __ldg(reinterpret_cast<const float4*>(a.logWT + (int64_t)j1 * a.ldT + r0));
+          const int32_t j0 = __ldg(idx + e), j1 = __ldg(idx + e + 1);
+          const float k0 = __ldg(val + e), k1 = __ldg(val + e + 1);
+          const float4 w0 = __ldg(reinterpret_cast<const float4*>(XT + (int64_t)j0 * ldT + r0));
+          const float4 w1 = __ldg(reinterpret_cast<const float4*>(XT + (int64_t)j1 * ldT + r0));
           s0.x = fmaf(k0, w0.x, s0.x); s0.y = fmaf(k0, w0.y, s0.y);
           s0.z = fmaf(k0, w0.z, s0.z); s0.w = fmaf(k0, w0.w, s0.w);
           s1.x = fmaf(k1, w1.x, s1.x); s1.y = fmaf(k1, w1.y, s1.y);
           s1.z = fmaf(k1, w1.z, s1.z); s1.w = fmaf(k1, w1.w, s1.w);
         }
         if (e < ce) {
-          const float k0 = __ldg(a.val + e);
+          const float k0 = __ldg(val + e);
           const float4 w0 =
-              __ldg(reinterpret_cast<const float4*>(a.logWT + (int64_t)__ldg(a.col + e) * a.ldT + r0));
+              __ldg(reinterpret_cast<const float4*>(XT + (int64_t)__ldg(idx + e) * ldT + r0));
           s0.x = fmaf(k0, w0.x, s0.x); s0.y = fmaf(k0, w0.y, s0.y);
           s0.z = fmaf(k0, w0.z, s0.z); s0.w = fmaf(k0, w0.w, s0.w);
           ++e;
@@ -666,21 +679,36 @@ __global__ void __launch_bounds__(128) sparse_ll_kernel(const SparseLLArgs a) {
         tot[2] += (double)(s0.z + s1.z);
         tot[3] += (double)(s0.w + s1.w);
       }
-      const double ph = (double)a.scaling[p];
+      if (MODE == 0) {
+        const double ph = (double)scaling[p];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = (float)(tot[u] - ph * sw[u]);
+        for (int u = 0; u < 4; ++u) v[u] = (float)(tot[u] - ph * sw[u]);
+      } else {
+        // emc_atomic.cu:105-111: divide by the slice's total responsibility
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float Tr = (float)sw[u];
+          v[u] = Tr > 1e-30f ? (float)tot[u] / Tr : (float)tot[u];
+        }
+      }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) tile[i][4 * threadIdx.x + u] = v[u];
   }
   __syncthreads();
-  // half a warp per LL row: lane & 15 = pattern
+  // half a warp per output row: lane & 15 = column
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t p = p0 + (lane & 15);
   for (int rr = 2 * w + (lane >> 4); rr < kSparseRot; rr += 8) {
     const int64_t ro = (int64_t)blockIdx.y * kSparseRot + rr;
-    if (ro < a.R && p < a.N) a.LL[ro * a.N + p] = tile[lane & 15][rr];
+    if (ro < R && p < ncol) out[ro * ncol + p] = tile[lane & 15][rr];
   }
+}
+
+__global__ void scale_entries_kernel(const float* val, const int32_t* row, const float* scaling,
+                                     int64_t nnz, float* out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < nnz) out[e] = val[e] / scaling[row[e]];
 }
 
 cudaError_t launch_ll_sparse(const SparseLLArgs& a, cudaStream_t st) {
@@ -690,7 +718,28 @@ cudaError_t launch_ll_sparse(const SparseLLArgs& a, cudaStream_t st) {
   dim3 grid((unsigned)((a.N + kSparsePat - 1) / kSparsePat),
             (unsigned)((a.R + kSparseRot - 1) / kSparseRot));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-  sparse_ll_kernel<<<grid, 128, 0, st>>>(a);
+  sparse_gather_kernel<0><<<grid, 128, 0, st>>>(a.row_ptr, a.col, a.val, a.logWT, a.ldT, a.R, a.N,
+                                                a.scaling, a.rowstat, nullptr, a.LL);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compress_sparse(const SparseCmpArgs& a, cudaStream_t st) {
+  if (a.R <= 0 || a.npa <= 0) return cudaSuccess;
+  if (a.ldT % 4 != 0 || a.ldT < a.R || (reinterpret_cast<uintptr_t>(a.PT) & 15u))
+    return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((a.npa + kSparsePat - 1) / kSparsePat),
+            (unsigned)((a.R + kSparseRot - 1) / kSparseRot));
+  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  sparse_gather_kernel<1><<<grid, 128, 0, st>>>(a.col_ptr, a.row, a.val, a.PT, a.ldT, a.R, a.npa,
+                                                nullptr, nullptr, a.T, a.U);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale_entries(const float* val, const int32_t* row, const float* scaling,
+                                 int64_t nnz, float* val_out, cudaStream_t st) {
+  if (nnz <= 0) return cudaSuccess;
+  scale_entries_kernel<<<(unsigned)((nnz + 255) / 256), 256, 0, st>>>(val, row, scaling, nnz,
+                                                                     val_out);
   return cudaGetLastError();
 }
 

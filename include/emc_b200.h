@@ -180,6 +180,8 @@ typedef struct {
   int32_t maximize_sparse; /* FP32 poisson contexts: 1 = the log-likelihood as a
                               photon-list gather over each pattern's non-zero pixels
                               instead of the dense contraction */
+  int32_t compress_sparse; /* FP32 contexts: 1 = the slice sums as a gather over each
+                              pixel's non-zero counts instead of the dense contraction */
 } emc_tuning;
 emc_status emc_get_tuning(const emc_context *ctx, emc_tuning *t);
 emc_status emc_set_tuning(emc_context *ctx, const emc_tuning *t);

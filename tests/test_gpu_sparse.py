@@ -1,6 +1,7 @@
-"""Photon-list maximize (FP32 poisson): the log-likelihood gathered over each
-pattern's non-zero pixels gives the responsibilities, scaling and model of
-the dense FP32 contraction and of the FP64 oracle.
+"""Photon-list forms of the FP32 path: the poisson log-likelihood gathered
+over each pattern's non-zero pixels, and the slice sums gathered over each
+pixel's non-zero counts, give the responsibilities, scaling and model of the
+dense FP32 contractions and of the FP64 oracle.
 
 Tolerances: against the oracle, the FP32 bars of the dense path
 (responsibilities within 1e-4 per-pattern L1, models within 1e-5 relative);
@@ -99,3 +100,51 @@ def test_sparse_rejected_outside_fp32_poisson(small, lik, prec):
         with pytest.raises(E.EmcError) as ei:
             ctx.set_sparse_maximize(True)
         assert ei.value.status == 7
+        if prec == "mixed":
+            with pytest.raises(E.EmcError) as ei:
+                ctx.set_sparse_compress(True)
+            assert ei.value.status == 7
+
+
+@pytest.mark.parametrize("lik", ["poisson", "gauss"])
+def test_sparse_slice_sums_match_dense_and_oracle(small, lik):
+    """Slice sums gathered over each pixel's non-zero counts (FP32, both
+    likelihoods): the model of the dense FP32 compress and of the oracle's
+    insertion from the engine's own responsibilities."""
+    import emc_b200 as E
+    d = small
+    with make_ctx(d, lik, "nearest", "fp32") as ctx:
+        P0, phi0, m0 = _stage(ctx)
+    with make_ctx(d, lik, "nearest", "fp32") as ctx:
+        ctx.set_sparse_compress(True)
+        P1, phi1, m1 = _stage(ctx)
+        T1 = ctx.get_buffer(E.BUF_TOTALRESP)
+    np.testing.assert_array_equal(P1, P0)  # the maximize is unchanged
+    assert rel(m1, m0) <= 1e-5, rel(m1, m0)
+    cfg = oracle_cfg(d, lik, "nearest")
+    acc, wacc, T = O.compress(cfg, P1.astype(np.float64), d["counts"], d["mask"],
+                              phi1.astype(np.float64), d["q"], d["w"], d["x"], d["y"], d["z"])
+    assert rel(m1, O.normalize_model(acc, wacc)) <= 1e-5
+    np.testing.assert_allclose(T1, T, rtol=1e-4, atol=1e-6)
+
+
+def test_sparse_iteration_both_gathers_ragged():
+    """Photon-list maximize and slice sums together over three iterations
+    with empty patterns and ragged sizes, against the oracle."""
+    from emc_b200 import workloads as W
+    d = dict(W.make("tiny16"))
+    counts = d["counts"][:45].copy()
+    counts[[0, 17, 44]] = 0.0
+    d["counts"], d["scaling0"] = counts, d["scaling0"][:45]
+    d["q"], d["w"] = d["q"][:301], d["w"][:301]
+    cfg = oracle_cfg(d, "poisson", "nearest")
+    m_ref, s_ref = d["model0"].astype(np.float64), d["scaling0"].astype(np.float64)
+    with make_ctx(d, "poisson", "nearest", "fp32") as ctx:
+        ctx.set_sparse_maximize(True)
+        ctx.set_sparse_compress(True)
+        for _ in range(3):
+            ctx.iterate()
+            m_ref, s_ref, _, _ = O.iterate(cfg, d["counts"], d["mask"], d["q"], d["w"], d["x"],
+                                           d["y"], d["z"], m_ref, s_ref)
+        model = ctx.get_model()
+    assert rel(model, m_ref) <= 1e-4, rel(model, m_ref)
