@@ -422,8 +422,16 @@ class Context:
         t.compress_sparse = int(bool(on))
         self._c(lib().emc_set_tuning(self._h, C.byref(t)))
 
+    def tuning(self):
+        """Every field of emc_tuning as a dict."""
+        t = Tuning()
+        self._c(lib().emc_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+
     def autotune(self, candidates=(1, 2, 4, 8, 16)):
-        """emc_autotune: returns (best (maximize, compress), ms[2][n])."""
+        """emc_autotune: returns (best (maximize, compress) band sizes, ms[2][n]);
+        for FP32 contexts the choice is the dense or photon-list form of each
+        contraction (see tuning())."""
         cand = np.ascontiguousarray(candidates, np.int32)
         ms = np.zeros((2, len(cand)), np.float32)
         t = Tuning()

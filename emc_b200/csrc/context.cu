@@ -1014,10 +1014,6 @@ emc_status emc_autotune(emc_context* c, const int32_t* cand, int32_t n, float* m
   if (!c->have_geom || !c->have_rot || !c->have_pat || !c->have_model)
     return c->fail(EMC_ERR_STATE, "set geometry, rotations, patterns and model first");
   if (c->stage != 0) return c->fail(EMC_ERR_STATE, "autotune between iterations");
-  if (!c->mixed) {  // the CUDA-core path has no tile order to tune
-    if (best) *best = c->tune;
-    return EMC_OK;
-  }
   // every trial iterates from the current model and scaling, restored after
   float* save = nullptr;
   CK(c, cudaMalloc(&save, sizeof(float) * (c->M + c->N)));
@@ -1039,7 +1035,31 @@ emc_status emc_autotune(emc_context* c, const int32_t* cand, int32_t n, float* m
       (s = emc_set_profiling(c, 1)) == EMC_OK) {
     // one untimed iteration first (first-launch costs)
     s = emc_iterate(c, nullptr);
-    for (int32_t i = 0; i < n && s == EMC_OK; ++i) {
+    // FP32 contexts: the dense and the photon-list form of each contraction
+    // (the maximize's only for poisson); the candidates do not apply
+    for (int32_t form = 0; form < 2 && s == EMC_OK && !c->mixed; ++form) {
+      c->tune = keep;
+      c->tune.maximize_sparse = form && !c->gauss ? 1 : 0;
+      c->tune.compress_sparse = form;
+      if ((s = restore()) != EMC_OK || (s = emc_iterate(c, nullptr)) != EMC_OK) break;
+      float t[5];
+      if ((s = c->cuda(cudaEventSynchronize(c->ev[c->cur][5]), "autotune")) != EMC_OK) break;
+      for (int k = 0; k < 5; ++k)
+        cudaEventElapsedTime(&t[k], c->ev[c->cur][k], c->ev[c->cur][k + 1]);
+      if (t[1] < bmax) {
+        bmax = t[1];
+        win.maximize_sparse = c->tune.maximize_sparse;
+      }
+      if (t[3] < bcmp) {
+        bcmp = t[3];
+        win.compress_sparse = c->tune.compress_sparse;
+      }
+      if (ms) {
+        ms[0] = bmax;
+        ms[n] = bcmp;
+      }
+    }
+    for (int32_t i = 0; i < n && s == EMC_OK && c->mixed; ++i) {
       float tmax = 1e30f;
       for (int32_t pair = 0; pair < 2 && s == EMC_OK; ++pair) {
         c->tune = emc_tuning{cand[i], cand[i], pair, pair, keep.maximize_sparse,

@@ -190,7 +190,10 @@ emc_status emc_set_tuning(emc_context *ctx, const emc_tuning *t);
  * model and scaling, which are restored afterwards; keeps the fastest band
  * size of each contraction and the faster maximize form.  ms (optional):
  * [2][n], the best maximize then compress time per candidate.  FP32
- * contexts: no-op. */
+ * contexts: one iteration with the dense contractions and one with the
+ * photon-list forms (maximize_sparse for poisson, compress_sparse), keeping
+ * the faster form of each; the candidates are not used and ms[0] / ms[n]
+ * receive the chosen maximize / compress times. */
 emc_status emc_autotune(emc_context *ctx, const int32_t *candidates, int32_t n, float *ms,
                         emc_tuning *best);
 

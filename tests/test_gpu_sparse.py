@@ -148,3 +148,22 @@ def test_sparse_iteration_both_gathers_ragged():
                                            d["y"], d["z"], m_ref, s_ref)
         model = ctx.get_model()
     assert rel(model, m_ref) <= 1e-4, rel(model, m_ref)
+
+
+def test_fp32_autotune_picks_forms_and_restores_state(small):
+    """emc_autotune on an FP32 context times the dense and the photon-list
+    forms, keeps the faster of each, and leaves model and scaling as they
+    were; the chosen forms give the dense iteration's model."""
+    d = small
+    with make_ctx(d, "poisson", "nearest", "fp32") as ctx:
+        ctx.iterate()
+        m_dense = ctx.get_model()
+    with make_ctx(d, "poisson", "nearest", "fp32") as ctx:
+        m0 = ctx.get_model()
+        _, ms = ctx.autotune((1,))
+        assert ms[0, 0] > 0 and ms[1, 0] > 0
+        t = ctx.tuning()
+        assert t["maximize_sparse"] in (0, 1) and t["compress_sparse"] in (0, 1)
+        np.testing.assert_array_equal(ctx.get_model(), m0)
+        ctx.iterate()
+        assert rel(ctx.get_model(), m_dense) <= 1e-5
