@@ -64,6 +64,16 @@ __global__ void split_sum_kernel(const __half* hi, const __half* lo, int64_t R, 
 
 }  // namespace
 
+// Non-zero entries of a dense matrix as compressed rows (see build_rows).
+struct SparseRows {
+  int64_t* ptr = nullptr;   // [rows + 1]
+  int32_t* idx = nullptr;   // column of each entry, ascending within a row
+  float* val = nullptr;     // the entry
+  float* aux = nullptr;     // optional second value per entry
+  int64_t cap = 0, nnz = 0;
+  bool valid = false;
+};
+
 struct emc_context {
   emc_config cfg{};
   std::string err;
@@ -147,22 +157,12 @@ struct emc_context {
   // (defaults from measurements at 64^3 and 128^3, set per shape in
   // alloc_work; emc_autotune re-measures)
   emc_tuning tune{1, 6, 0, 0, 0, 0};
-  // photon-list log-likelihood (FP32 poisson): counts as CSR, log W pixel-major
-  int64_t* d_csr_row = nullptr;
-  int32_t* d_csr_col = nullptr;
-  float* d_csr_val = nullptr;
-  int64_t csr_cap = 0;
-  bool csr_valid = false;
+  // photon-list forms (FP32): the counts' non-zero entries by pattern (csr,
+  // for the log-likelihood, with log W pixel-major in d_ST) and by active pixel
+  // (csc, for the slice sums, with its entries divided by the scaling in aux
+  // and the responsibilities pattern-major in d_PT); rebuilt after an upload
+  SparseRows csr, csc;
   float* d_ST = nullptr;
-  // photon-list slice sums (FP32): counts as CSC over active pixels, the
-  // entries divided by their pattern's scaling, responsibilities pattern-major
-  int64_t* d_csc_ptr = nullptr;
-  int32_t* d_csc_row = nullptr;
-  float* d_csc_val = nullptr;
-  float* d_csc_sval = nullptr;
-  int64_t csc_cap = 0;
-  bool csc_valid = false;
-  int64_t csc_nnz = 0;
   float* d_PT = nullptr;
   bool prof = false;
   cudaEvent_t ev[2][6] = {{nullptr}};
@@ -493,8 +493,8 @@ static emc_status finish_patterns(emc_context* c) {
                    "%d counts are not integers in [0, 2048]; the mixed path needs them exact in FP16",
                    bad);
   c->have_pat = true;
-  c->csr_valid = false;
-  c->csc_valid = false;
+  c->csr.valid = false;
+  c->csc.valid = false;
   return EMC_OK;
 }
 
@@ -685,42 +685,54 @@ static emc_status mixed_resp_pass(emc_context* c) {
   return EMC_OK;
 }
 
+// The non-zero entries of M [rows][cols] (device, FP32) into s: one warp per
+// row counts them, the host scans the counts, a second pass writes each row's
+// entries in column order (ballot compaction), so sums over them run in a
+// fixed order.  with_aux allocates a second value array of the same length.
+static emc_status build_rows(emc_context* c, const float* M, int64_t rows, int64_t cols,
+                             SparseRows& s, bool with_aux) {
+  if (!s.ptr) TRY(c->alloc(&s.ptr, rows + 1));
+  std::vector<int64_t> cnt(rows), ptr(rows + 1, 0);
+  int64_t* d_cnt = s.ptr + 1;  // counts land where ptr[1..rows] goes
+  CK(c, launch_csr_count(M, rows, cols, d_cnt, c->st));
+  CK(c, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int64_t) * rows, cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  for (int64_t r = 0; r < rows; ++r) ptr[r + 1] = ptr[r] + cnt[r];
+  const int64_t nnz = ptr[rows];
+  if (nnz + 1 > s.cap || (with_aux && !s.aux)) {
+    for (void* q : {(void*)s.idx, (void*)s.val, (void*)s.aux})
+      if (q) c->release(q);
+    s.idx = nullptr;
+    s.val = nullptr;
+    s.aux = nullptr;
+    s.cap = 0;
+    TRY(c->alloc(&s.idx, nnz + 1));
+    TRY(c->alloc(&s.val, nnz + 1));
+    if (with_aux) TRY(c->alloc(&s.aux, nnz + 1));
+    s.cap = nnz + 1;
+  }
+  CK(c, cudaMemcpyAsync(s.ptr, ptr.data(), sizeof(int64_t) * (rows + 1), cudaMemcpyHostToDevice,
+                        c->st));
+  CK(c, launch_csr_fill(M, rows, cols, s.ptr, s.idx, s.val, c->st));
+  s.nnz = nnz;
+  s.valid = true;
+  return EMC_OK;
+}
+
 // The poisson log-likelihood as a gather over each pattern's photon list:
-// the counts' CSR (built once per pattern upload) and log W transposed to
-// pixel-major rows so a block of rotations reads one coalesced row per photon.
+// the counts' entries by pattern (built once per pattern upload) and log W
+// transposed to pixel-major rows so a block of rotations reads one coalesced
+// row per photon.
 static emc_status sparse_loglik(emc_context* c) {
   const int64_t N = c->N, R = c->R, npa = c->npa;
-  if (!c->csr_valid) {
-    if (!c->d_csr_row) TRY(c->alloc(&c->d_csr_row, N + 1));
-    std::vector<int64_t> cnt(N), row(N + 1, 0);
-    int64_t* d_cnt = c->d_csr_row + 1;  // counts land where row_ptr[1..N] goes
-    CK(c, launch_csr_count(c->d_K, N, npa, d_cnt, c->st));
-    CK(c, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int64_t) * N, cudaMemcpyDeviceToHost, c->st));
-    CK(c, cudaStreamSynchronize(c->st));
-    for (int64_t p = 0; p < N; ++p) row[p + 1] = row[p] + cnt[p];
-    const int64_t nnz = row[N];
-    if (nnz > c->csr_cap) {
-      for (void* q : {(void*)c->d_csr_col, (void*)c->d_csr_val})
-        if (q) c->release(q);
-      c->d_csr_col = nullptr;
-      c->d_csr_val = nullptr;
-      c->csr_cap = 0;
-      TRY(c->alloc(&c->d_csr_col, nnz + 1));
-      TRY(c->alloc(&c->d_csr_val, nnz + 1));
-      c->csr_cap = nnz + 1;
-    }
-    CK(c, cudaMemcpyAsync(c->d_csr_row, row.data(), sizeof(int64_t) * (N + 1),
-                          cudaMemcpyHostToDevice, c->st));
-    CK(c, launch_csr_fill(c->d_K, N, npa, c->d_csr_row, c->d_csr_col, c->d_csr_val, c->st));
-    c->csr_valid = true;
-  }
+  if (!c->csr.valid) TRY(build_rows(c, c->d_K, N, npa, c->csr, false));
   const int64_t ldT = (R + 3) / 4 * 4;
   if (!c->d_ST) TRY(c->alloc(&c->d_ST, npa * ldT));
   CK(c, launch_transpose(c->d_S, R, npa, c->d_ST, ldT, c->st));
   SparseLLArgs a{};
-  a.row_ptr = c->d_csr_row;
-  a.col = c->d_csr_col;
-  a.val = c->d_csr_val;
+  a.row_ptr = c->csr.ptr;
+  a.col = c->csr.idx;
+  a.val = c->csr.val;
   a.logWT = c->d_ST;
   a.ldT = ldT;
   a.scaling = c->d_scaling;
@@ -734,52 +746,29 @@ static emc_status sparse_loglik(emc_context* c) {
 }
 
 // The slice sums U[r][j] = sum_p P_rp K_pj / phi_p / T_r as a gather over
-// each active pixel's non-zero counts: the counts' CSC (built once per
-// pattern upload through a transposed copy of K), its entries divided by the
+// each active pixel's non-zero counts: the counts' entries by pixel (built
+// once per pattern upload from a transposed copy of K), divided by the
 // current scaling, and P transposed to pattern-major rows.
 static emc_status sparse_slicesums(emc_context* c) {
   const int64_t N = c->N, R = c->R, npa = c->npa;
-  if (!c->csc_valid) {
-    if (!c->d_csc_ptr) TRY(c->alloc(&c->d_csc_ptr, npa + 1));
+  if (!c->csc.valid) {
     float* KT = nullptr;
     TRY(c->alloc(&KT, npa * N));
     CK(c, launch_transpose(c->d_K, N, npa, KT, N, c->st));
-    std::vector<int64_t> cnt(npa), ptr(npa + 1, 0);
-    int64_t* d_cnt = c->d_csc_ptr + 1;
-    CK(c, launch_csr_count(KT, npa, N, d_cnt, c->st));
-    CK(c, cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int64_t) * npa, cudaMemcpyDeviceToHost, c->st));
-    CK(c, cudaStreamSynchronize(c->st));
-    for (int64_t j = 0; j < npa; ++j) ptr[j + 1] = ptr[j] + cnt[j];
-    const int64_t nnz = ptr[npa];
-    if (nnz + 1 > c->csc_cap) {
-      for (void* q : {(void*)c->d_csc_row, (void*)c->d_csc_val, (void*)c->d_csc_sval})
-        if (q) c->release(q);
-      c->d_csc_row = nullptr;
-      c->d_csc_val = nullptr;
-      c->d_csc_sval = nullptr;
-      c->csc_cap = 0;
-      TRY(c->alloc(&c->d_csc_row, nnz + 1));
-      TRY(c->alloc(&c->d_csc_val, nnz + 1));
-      TRY(c->alloc(&c->d_csc_sval, nnz + 1));
-      c->csc_cap = nnz + 1;
-    }
-    CK(c, cudaMemcpyAsync(c->d_csc_ptr, ptr.data(), sizeof(int64_t) * (npa + 1),
-                          cudaMemcpyHostToDevice, c->st));
-    CK(c, launch_csr_fill(KT, npa, N, c->d_csc_ptr, c->d_csc_row, c->d_csc_val, c->st));
-    CK(c, cudaStreamSynchronize(c->st));
+    const emc_status s = build_rows(c, KT, npa, N, c->csc, true);
+    cudaStreamSynchronize(c->st);
     c->release(KT);
-    c->csc_nnz = nnz;
-    c->csc_valid = true;
+    if (s != EMC_OK) return s;
   }
   const int64_t ldT = (R + 3) / 4 * 4;
   if (!c->d_PT) TRY(c->alloc(&c->d_PT, N * ldT));
   CK(c, launch_transpose(c->d_LL, R, N, c->d_PT, ldT, c->st));
-  CK(c, launch_scale_entries(c->d_csc_val, c->d_csc_row, c->d_scaling, c->csc_nnz, c->d_csc_sval,
+  CK(c, launch_scale_entries(c->csc.val, c->csc.idx, c->d_scaling, c->csc.nnz, c->csc.aux,
                              c->st));
   SparseCmpArgs a{};
-  a.col_ptr = c->d_csc_ptr;
-  a.row = c->d_csc_row;
-  a.val = c->d_csc_sval;
+  a.col_ptr = c->csc.ptr;
+  a.row = c->csc.idx;
+  a.val = c->csc.aux;
   a.PT = c->d_PT;
   a.ldT = ldT;
   a.T = c->d_T;
