@@ -24,7 +24,6 @@ namespace emc {
 namespace {
 
 constexpr int BM = 128, BN = 256;
-constexpr int kThreads = 192;
 constexpr int kTmemCols = 512;
 constexpr uint64_t kWaitLimitNs = 10ull * 1000ull * 1000ull * 1000ull;
 
@@ -439,14 +438,20 @@ __global__ void __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
 //   s_k = sum e^(LL-m_k),  d_k = sum e^(LL-m_k) X,  q_k = sum e^(LL-m_k) (LL-m_k)
 // with X the scaling denominator term (gaussian: C_rp, poisson: sum W_r).  The
 // combine kernel turns them into lse_p, the new scaling and sum P log P.
-struct EpiMax {
+// EW = 8 (SM pairs): two warps per TMEM lane quarter, each with half of the
+// 256 columns; at the end of a row the second half's running partials are
+// merged into the first's through shared memory.
+template <int EW>
+struct EpiMaxT {
   static constexpr bool kListed = false;
   static constexpr int kSets = 1;
-  static constexpr int kEpiWarps = 4;
-  static constexpr int kSmemBytes = BN * 8;
+  static constexpr int kEpiWarps = EW;
+  static constexpr int kSmemBytes = BN * 8 + (EW == 8 ? BM * 16 : 0);
   MaxEpiArgs a;
   int64_t n0, ntile, p;
   bool pv;
+  int half;
+  uint8_t* sbuf;
   float phi, mx, sm, sd, sq;
   double c1, c0;
 
@@ -457,8 +462,10 @@ struct EpiMax {
     float2* rs2 = reinterpret_cast<float2*>(smem);
     n0 = nt * BN;
     ntile = nt;
-    epi_bar();
-    for (int c = tid; c < BN; c += 128) {
+    half = tid >> 7;
+    sbuf = smem;
+    epi_bar(32 * EW);
+    for (int c = tid; c < BN; c += 32 * EW) {
       const int64_t r = n0 + c;
       const double w = r < a.R ? a.rowstat[r] : 0.0;
       if (a.poisson) {
@@ -468,7 +475,7 @@ struct EpiMax {
         rs[c] = w * a.gauss_inv;
       }
     }
-    epi_bar();
+    epi_bar(32 * EW);
     (void)mt;
   }
   __device__ void row_begin(int64_t p_) {
@@ -529,10 +536,36 @@ struct EpiMax {
     }
   }
   __device__ void row_end() {
+    if constexpr (EW == 8) {
+      // merge the two column halves' partials of this row (log-sum-exp
+      // relative to the larger maximum)
+      float4* other = reinterpret_cast<float4*>(sbuf + BN * 8);
+      const int lr = (int)(p % BM);
+      if (half == 1) other[lr] = make_float4(mx, sm, sd, sq);
+      epi_bar(32 * EW);
+      if (half == 1) return;
+      const float4 o = other[lr];
+      if (o.x > -FLT_MAX) {
+        if (mx > -FLT_MAX) {
+          const float m = fmaxf(mx, o.x);
+          const float f1 = __expf(mx - m), f2 = __expf(o.x - m);
+          sq = f1 * (sq + (mx - m) * sm) + f2 * (o.w + (o.x - m) * o.y);
+          sm = f1 * sm + f2 * o.y;
+          sd = f1 * sd + f2 * o.z;
+          mx = m;
+        } else {
+          mx = o.x;
+          sm = o.y;
+          sd = o.z;
+          sq = o.w;
+        }
+      }
+    }
     if (pv) a.part[ntile * a.N + p] = make_float4(mx, sm, sd, sq);
   }
   __device__ void tile_end(int64_t, int64_t, int, uint8_t*) {}
 };
+using EpiMax = EpiMaxT<4>;
 
 // (model, weight) += (x, y) at one voxel as a single vector reduction.
 __device__ __forceinline__ void red_add_v2(float2* p, float x, float y) {
@@ -965,7 +998,7 @@ constexpr int kPairStages = 4;
 // pair (a_row, b_row: the CTA adds 128 x rank), k-block count and tensor-map
 // set; its row_begin then receives the row inside this CTA's 128 rows.
 template <int NA, int NB, bool M_INNER, class Epi>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
     tc_pair_kernel(const __grid_constant__ TmapSet<Epi::kSets> maps, const int64_t m_tiles,
                    const int64_t n_tiles, const int64_t k_blocks, const int raster,
                    const Epi epi, TcStatus* status) {
@@ -1174,8 +1207,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     }
   } else {
     // -------------------------------------------------- epilogue warps (both CTAs)
+    // TMEM lane quarter = warp % 4; with 8 epilogue warps two share a quarter
+    // and take one half of the columns each
+    constexpr int EW = Epi::kEpiWarps;
+    static_assert(EW == 4 || EW == 8, "4 or 8 epilogue warps");
+    constexpr int COLS = BN / (EW / 4);
     const int quarter = warp & 3;
     const int ep_tid = threadIdx.x - 64;
+    const int col0 = ((warp - 2) / 4) * COLS;
     Epi e = epi;
     int64_t i = 0;
     const uint32_t tempty_leader0 = peer_addr(smem_u32(&tempty_bar[0]), 0);
@@ -1184,9 +1223,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       const int acc = (int)(i & 1);
       const uint32_t aph = (uint32_t)((i >> 1) & 1);
       bounded_wait(smem_u32(&tfull_bar[acc]), aph, ctl, 4);
-      epi_bar();
+      epi_bar(32 * EW);
       if (ep_tid == 0) epi_abort = abort_flag;
-      epi_bar();
+      epi_bar(32 * EW);
       if (epi_abort) break;
       tc_fence_after();
       int64_t mt = t, nt = 0;
@@ -1201,7 +1240,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       }
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
-      for (int c = 0; c < BN; c += 16) {
+      for (int c = col0; c < col0 + COLS; c += 16) {
         uint32_t v[16];
         tmem_ld16(taddr + c, v);
         tmem_ld_wait();
@@ -1209,7 +1248,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       }
       e.row_end();
       tc_fence_before();
-      epi_bar();  // the whole accumulator of this CTA has been read
+      epi_bar(32 * EW);  // the whole accumulator of this CTA has been read
       if (ep_tid == 0) mbar_arrive_cluster(acc ? tempty_leader1 : tempty_leader0);
       e.tile_end(mt, nt, ep_tid, epi_smem);
     }
@@ -1238,7 +1277,7 @@ cudaError_t run_pair(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n
   if (tiles == 0) return cudaSuccess;
   const int64_t pairs = num_sms / 2;
   const int grid = 2 * (int)(tiles < pairs ? tiles : pairs);
-  kern<<<grid, kThreads, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks,
+  kern<<<grid, 64 + 32 * Epi::kEpiWarps, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks,
                                         raster < 1 ? 1 : raster, epi, st);
   return cudaGetLastError();
 }
@@ -1596,7 +1635,7 @@ cudaError_t launch_maximize_pair_tc(const CUtensorMap& tmK, const CUtensorMap& t
                                     const CUtensorMap& tmBlo, int64_t Mpad, int64_t Rpad,
                                     int64_t Kpad, const MaxEpiArgs& e, TcStatus* status,
                                     int num_sms, cudaStream_t st, int raster) {
-  EpiMax epi;
+  EpiMaxT<8> epi;  // two epilogue warps per TMEM lane quarter
   epi.a = e;
   // 256-pattern pair tiles (the last may reach past Mpad: zero-filled by TMA,
   // masked by the epilogue), 64-wide K-steps
