@@ -495,8 +495,9 @@ struct EpiMaxT {
     const float2* rs2 = reinterpret_cast<const float2*>(smem);
     float ll[16], xs[16];
     float cmax = -FLT_MAX;
+    float* yp = a.Y + (n0 + c) * a.ldY + p;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
+    for (int k = 0; k < 16; ++k, yp += a.ldY) {
       const float x = __uint_as_float(v[k]);
       const int64_t r = n0 + c + k;
       if (a.poisson) {
@@ -509,8 +510,8 @@ struct EpiMaxT {
       }
       const bool ok = pv && r < a.R;
       if (ok) {
-        // streamed (evict-first): Y is 1 GB and must not push operand tiles out of L2
-        __stcs(a.Y + r * a.ldY + p, a.poisson ? ll[k] : x);
+        // a plain store: measured faster than an evict-first (.cs) store here
+        *yp = a.poisson ? ll[k] : x;
         cmax = fmaxf(cmax, ll[k]);
       } else {
         ll[k] = -FLT_MAX;
