@@ -5,8 +5,10 @@ Fine rotations are grouped into coarse cells (nearest rotation of a coarse
 CUDA kernels in emc_b200/csrc/net.cu) learns to predict, from a pattern's
 2x-downsampled log(1 + K), the posterior over cells that dense EMC
 iterations produce; emc_iterate_proposed then evaluates each pattern only
-against the fine rotations of its most probable cells, with the dense
-iteration as the fallback.  torch provides device buffers only.
+against the fine rotations of its candidate cells (those holding most of its
+responsibility in the previous iteration, then the network's most probable
+ones), with the dense iteration as the fallback.  torch provides device
+buffers only.
 """
 from __future__ import annotations
 
@@ -188,15 +190,6 @@ class LearnedProposal:
             out[i:i + batch] = self.net.forward(x[i:i + batch].contiguous())
         torch.cuda.synchronize()
         return out
-
-    @staticmethod
-    def blend(probs, previous=None, weight=0.5):
-        """Cell probabilities to select from: the network's prediction mixed
-        with the previous iteration's cell posterior (emc_cell_targets), so
-        the cells holding a pattern's last responsibilities stay candidates."""
-        if previous is None:
-            return probs
-        return (1.0 - weight) * probs + weight * previous
 
     def iterate(self, probs, max_cells, mass_target=1.0, threshold=0.99, min_cells=1, keep=None,
                 keep_mass=0.0):
