@@ -78,6 +78,7 @@ def lib():
             ("emc_set_scaling", [P, P], C.c_int), ("emc_iterate", [P, P], C.c_int),
             ("emc_expand", [P], C.c_int), ("emc_maximize", [P], C.c_int),
             ("emc_compress", [P], C.c_int), ("emc_synchronize", [P], C.c_int),
+            ("emc_wait_probe", [P, C.c_uint32], C.c_int),
             ("emc_get_model", [P, P], C.c_int), ("emc_get_scaling", [P, P], C.c_int),
             ("emc_get_buffer", [P, C.c_int, P, C.c_size_t], C.c_int),
             ("emc_device_buffer", [P, C.c_int, P, P], C.c_int),
@@ -336,6 +337,12 @@ class Context:
 
     def synchronize(self):
         self._c(lib().emc_synchronize(self._h))
+
+    def wait_probe(self, limit_us=2000):
+        """emc_wait_probe: one device wait that cannot succeed, given up after
+        limit_us; raises EmcError with status EMC_ERR_TIMEOUT, after which the
+        context is usable again."""
+        self._c(lib().emc_wait_probe(self._h, int(limit_us)))
 
     @property
     def active_pixels(self):

@@ -954,6 +954,14 @@ emc_status emc_synchronize(emc_context* c) {
   return check_status(c);
 }
 
+emc_status emc_wait_probe(emc_context* c, uint32_t limit_us) {
+  if (!c || limit_us < 1 || limit_us > 1000000) return EMC_ERR_ARG;
+  if (c->stage != 0) return c->fail(EMC_ERR_STATE, "wait probe between iterations");
+  TRY(check_status(c));
+  CK(c, launch_wait_probe(c->d_status, (uint64_t)limit_us * 1000ull, c->st));
+  return check_status(c);
+}
+
 emc_status emc_iterate(emc_context* c, emc_iter_stats* stats) {
   TRY(emc_expand(c));
   TRY(emc_maximize(c));

@@ -146,14 +146,15 @@ struct Ctl {
   TcStatus* st;
 };
 
-__device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int site) {
+__device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int site,
+                             uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_test(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
     if (mbar_test(bar, parity)) return true;
     if ((it & 31) == 0) {
       if (*c.abort) return false;
-      if (globaltimer() - t0 > kWaitLimitNs) {
+      if (globaltimer() - t0 > limit_ns) {
         *c.abort = 1;
         if (atomicCAS(&c.st->code, 0, TC_TIMEOUT) == 0) {
           c.st->where = site;
@@ -163,6 +164,20 @@ __device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int si
       }
     }
   }
+}
+
+// One bounded wait, with a short limit, on an mbarrier that nothing completes:
+// the time-out path of bounded_wait (status word, site, early return) that
+// every contraction's waits share.  Site 90.
+__global__ void wait_probe_kernel(TcStatus* status, uint64_t limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x != 0) return;
+  mbar_init(smem_u32(&bar), 1);
+  abort_flag = 0;
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  Ctl ctl{&abort_flag, status};
+  bounded_wait(smem_u32(&bar), 0, ctl, 90, limit_ns);
 }
 
 // ---------------------------------------------------------------- kernel --
@@ -1583,6 +1598,11 @@ __global__ void pack_kernel(const float* K, int64_t N, int64_t npa, int64_t Npad
 }  // namespace
 
 // ------------------------------------------------------------- host side --
+
+cudaError_t launch_wait_probe(TcStatus* status, uint64_t limit_ns, cudaStream_t st) {
+  wait_probe_kernel<<<1, 32, 0, st>>>(status, limit_ns);
+  return cudaGetLastError();
+}
 
 bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
                   uint32_t box_rows, uint32_t box_inner) {

@@ -24,6 +24,9 @@ constexpr int kCompressBK = 64;
 
 bool tc_encode_2d(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,
                   uint32_t box_rows, uint32_t box_inner);
+// One bounded wait that cannot succeed, given up after limit_ns: records
+// TC_TIMEOUT (site 90) in *status the way the contractions do.
+cudaError_t launch_wait_probe(TcStatus* status, uint64_t limit_ns, cudaStream_t st);
 // The same for a matrix whose rows are ld >= inner elements apart (reads past
 // `inner` are zero-filled).
 bool tc_encode_2d_strided(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows,

@@ -183,6 +183,12 @@ typedef struct {
   int32_t compress_sparse; /* FP32 contexts: 1 = the slice sums as a gather over each
                               pixel's non-zero counts instead of the dense contraction */
 } emc_tuning;
+/* Time-out check (no counterpart in the reference): runs one bounded device
+ * wait on an mbarrier that nothing completes, given up after limit_us
+ * microseconds (1 .. 1,000,000), through the same wait routine as every
+ * tensor-core kernel.  Returns EMC_ERR_TIMEOUT with the wait site (90) in
+ * emc_last_error; the status word is cleared and the context stays usable. */
+emc_status emc_wait_probe(emc_context *ctx, uint32_t limit_us);
 emc_status emc_get_tuning(const emc_context *ctx, emc_tuning *t);
 emc_status emc_set_tuning(emc_context *ctx, const emc_tuning *t);
 /* Autotuner: two iterations per candidate band size (the maximize on one SM
