@@ -109,3 +109,57 @@ def test_sharded_iteration_equals_single_process(tmp_path):
     np.testing.assert_allclose(got[:M], m, rtol=1e-12, atol=1e-12)
     assert abs(got[M] - st["sum_plogp"]) < 1e-9 * max(1.0, abs(st["sum_plogp"]))
     assert abs(got[M + 1] - st["total_loglik"]) < 1e-9 * max(1.0, abs(st["total_loglik"]))
+
+
+class FailingShard(OracleShard):
+    """A shard whose maximize raises: a rank that fails between collectives."""
+
+    def maximize(self):
+        raise RuntimeError("shard failed before the exchange")
+
+
+def _failing_worker(rank, world, port, out_dir):
+    import datetime
+    import time
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=10))
+    from emc_b200 import workloads as W
+    from emc_b200.parallel import ShardedIteration, shard_range
+    d = W.make("tiny16")
+    first, n = shard_range(d["counts"].shape[0], rank, world)
+    cls = FailingShard if rank == 1 else OracleShard
+    it = ShardedIteration(cls(d, d["counts"][first:first + n], d["scaling0"][first:first + n]))
+    t0 = time.monotonic()
+    try:
+        it()
+        status = "completed"
+    except Exception as e:  # noqa: BLE001 - the failure is what is recorded
+        status = type(e).__name__
+    with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as f:
+        f.write(f"{status} {time.monotonic() - t0:.2f}")
+    # the failed rank leaves without joining any further collective
+    os._exit(0)
+
+
+def test_failed_rank_ends_the_others_collective_with_an_error(tmp_path):
+    """Rank 1 raises before the responsibility-total all-reduce and leaves;
+    rank 0's all-reduce must end with an error (the peer's exit or the
+    10 s process-group timeout), not wait for ever."""
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, str(tmp_path)))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    alive = [p for p in procs if p.is_alive()]
+    for p in alive:
+        p.kill()
+    assert not alive, "a rank did not finish"
+    st0, t0 = open(tmp_path / "rank0.txt").read().split()
+    st1, _ = open(tmp_path / "rank1.txt").read().split()
+    assert st1 == "RuntimeError"
+    assert st0 != "completed", st0
+    assert float(t0) < 60.0
