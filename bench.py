@@ -166,7 +166,10 @@ def cpu_oracle_rate(d, likelihood, interp, seconds, rot=None):
     rot = sample_indices(d) if rot is None else rot
     r = len(rot)
 
+    n_all = d["counts"].shape[0]
+
     def run(n):
+        n = min(n, n_all)
         cfg = O.make_config(w.side, n, r, likelihood=O.LL_POISSON if likelihood == "poisson"
                             else O.LL_GAUSS, interp=O.NEAREST if interp == "nearest"
                             else O.TRILINEAR)
@@ -175,20 +178,21 @@ def cpu_oracle_rate(d, likelihood, interp, seconds, rot=None):
                         d["y"], d["z"], d["model0"], d["scaling0"][:n], want_resp=True)
         return time.perf_counter() - t, out
 
+    n1, n2 = min(64, n_all), min(256, n_all)
     t8, _ = run(8)
     # per-pattern cost from two sizes (the fixed expand / insert cost cancels)
-    if t8 < seconds / 8:
-        t64, _ = run(64)
-        t256, _ = run(256) if t64 < seconds / 4 else (None, None)
-        if t256 is not None and t256 > t64:
-            per = (t256 - t64) / 192
+    if t8 < seconds / 8 and n1 > 8:
+        t1, _ = run(n1)
+        t2, _ = run(n2) if t1 < seconds / 4 and n2 > n1 else (None, None)
+        if t2 is not None and t2 > t1:
+            per = (t2 - t1) / (n2 - n1)
         else:
-            per = max(t64 - t8, 1e-4) / 56
-        base = t64
+            per = max(t1 - t8, 1e-4) / (n1 - 8)
+        base = t1
     else:
         per, base = t8 / 8, t8
-    n = int(max(8, min(d["counts"].shape[0], (seconds - base) / max(per, 1e-5))))
-    n = max(8, (n // 8) * 8)
+    n = int(max(8, min(n_all, (seconds - base) / max(per, 1e-5))))
+    n = min(n_all, max(8, (n // 8) * 8))
     t, out = run(n)
     R = d["q"].shape[0]
     return (n * r / t, f"1 FP64 iteration, {n} patterns x {r} rotations (every "
@@ -208,10 +212,12 @@ def reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from emc_b200 import workloads as W
+    from emc_b200 import workloads as W  # workload shapes only; the engine is not loaded
     from oracle import oracle as O
     O.build() if not os.path.isfile(O.LIB_PATH) else None
-    d = W.make(workload_of(a))
+    w = workload_of(a)
+    d = O.make_workload(w, wavelength=W.WAVELENGTH, distance=W.DISTANCE,
+                        pixel_size=W.pixel_size(w.side))
     w = d["workload"]
     N, R = d["counts"].shape[0], d["q"].shape[0]
     for _ in range(max(0, min(a.warmup, 1))):

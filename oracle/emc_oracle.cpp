@@ -307,28 +307,82 @@ void orc_expand(const orc_config* c, const double* model, const float* rot, cons
 
 // -------------------------------------------------------- log-likelihood --
 
-// C[r][p] = sum_{active j} A[r][j] * B[p][j], plain blocked FP64.
+// One dot product in a fixed order: four partial sums over j = 0, 1, 2, 3
+// (mod 4), the tail added to the first, combined as (s0 + s1) + (s2 + s3).
+static inline double dot4(const double* a, const double* b, int64_t P) {
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  int64_t j = 0;
+  for (; j + 4 <= P; j += 4) {
+    s0 += a[j] * b[j];
+    s1 += a[j + 1] * b[j + 1];
+    s2 += a[j + 2] * b[j + 2];
+    s3 += a[j + 3] * b[j + 3];
+  }
+  for (; j < P; ++j) s0 += a[j] * b[j];
+  return (s0 + s1) + (s2 + s3);
+}
+
+typedef double v4d __attribute__((vector_size(32)));
+
+static inline v4d load4(const double* p) {
+  v4d v;
+  std::memcpy(&v, p, sizeof(v));
+  return v;
+}
+
+// C[r][p] = sum_{active j} A[r][j] * B[p][j] in FP64.  Blocks of 16 r x 64 p
+// walk j in chunks of 256 (the block's rows of a chunk stay in L1/L2); 2 x 4
+// sub-blocks share their loads.  Lane k of each vector accumulator is dot4's
+// partial sum k, carried across the chunks in j order, so every element is
+// summed exactly as dot4 sums it.
 static void cross(int64_t R, int64_t N, int64_t P, const double* A, const double* B, double* C) {
-  const int64_t RB = 16, NB = 64;
+  const int64_t RB = 16, NB = 64, JB = 256;
 #pragma omp parallel for collapse(2) schedule(dynamic)
   for (int64_t r0 = 0; r0 < R; r0 += RB)
     for (int64_t p0 = 0; p0 < N; p0 += NB) {
       const int64_t r1 = std::min(R, r0 + RB), p1 = std::min(N, p0 + NB);
-      for (int64_t r = r0; r < r1; ++r)
-        for (int64_t p = p0; p < p1; ++p) {
-          const double* a = A + r * P;
-          const double* b = B + p * P;
-          double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-          int64_t j = 0;
-          for (; j + 4 <= P; j += 4) {
-            s0 += a[j] * b[j];
-            s1 += a[j + 1] * b[j + 1];
-            s2 += a[j + 2] * b[j + 2];
-            s3 += a[j + 3] * b[j + 3];
+      const int64_t P4 = P / 4 * 4;
+      const int64_t rq = r0 + (r1 - r0) / 2 * 2, pq = p0 + (p1 - p0) / 4 * 4;
+      v4d acc[RB][NB];
+      for (int64_t r = r0; r < rq; ++r)
+        for (int64_t p = p0; p < pq; ++p) acc[r - r0][p - p0] = v4d{0, 0, 0, 0};
+      for (int64_t j0 = 0; j0 < P4; j0 += JB) {
+        const int64_t j1 = std::min(P4, j0 + JB);
+        for (int64_t r = r0; r < rq; r += 2) {
+          const double* a0 = A + r * P;
+          const double* a1 = a0 + P;
+          for (int64_t p = p0; p < pq; p += 4) {
+            const double* b0 = B + p * P;
+            const double* b1 = b0 + P;
+            const double* b2 = b1 + P;
+            const double* b3 = b2 + P;
+            v4d* s0 = &acc[r - r0][p - p0];
+            v4d* s1 = &acc[r + 1 - r0][p - p0];
+            v4d t00 = s0[0], t01 = s0[1], t02 = s0[2], t03 = s0[3];
+            v4d t10 = s1[0], t11 = s1[1], t12 = s1[2], t13 = s1[3];
+            for (int64_t j = j0; j < j1; j += 4) {
+              const v4d x0 = load4(a0 + j), x1 = load4(a1 + j);
+              const v4d y0 = load4(b0 + j), y1 = load4(b1 + j), y2 = load4(b2 + j),
+                        y3 = load4(b3 + j);
+              t00 += x0 * y0; t01 += x0 * y1; t02 += x0 * y2; t03 += x0 * y3;
+              t10 += x1 * y0; t11 += x1 * y1; t12 += x1 * y2; t13 += x1 * y3;
+            }
+            s0[0] = t00; s0[1] = t01; s0[2] = t02; s0[3] = t03;
+            s1[0] = t10; s1[1] = t11; s1[2] = t12; s1[3] = t13;
           }
-          for (; j < P; ++j) s0 += a[j] * b[j];
-          C[r * N + p] = (s0 + s1) + (s2 + s3);
         }
+      }
+      for (int64_t r = r0; r < rq; ++r)
+        for (int64_t p = p0; p < pq; ++p) {
+          const v4d s = acc[r - r0][p - p0];
+          double l0 = s[0];
+          for (int64_t j = P4; j < P; ++j) l0 += A[r * P + j] * B[p * P + j];
+          C[r * N + p] = (l0 + s[1]) + (s[2] + s[3]);
+        }
+      // the ragged edges of the block, one element at a time
+      for (int64_t r = r0; r < r1; ++r)
+        for (int64_t p = (r < rq ? pq : p0); p < p1; ++p)
+          C[r * N + p] = dot4(A + r * P, B + p * P, P);
     }
 }
 
@@ -502,26 +556,47 @@ void orc_insert_shard(const orc_config* c, const double* U, const double* total_
   // model += w * U/T, weight += w with w = rotw_r * T_r, for mask == 1 pixels.
   // For a shard of the patterns the skip test reads the total over all
   // shards (all_total_resp), so the shards' sums add up to the unsharded one.
-  // Serial, so the accumulation order is fixed.
+  // The rotations are split into a number of contiguous chunks fixed by the
+  // shape alone (not by the thread count); each chunk is accumulated serially
+  // into its own grids and the chunks are added in order, so the result is
+  // the same on every machine.
   const int side = c->side;
   const int64_t npix = (int64_t)side * side;
+  const int64_t M = npix * side, R = c->n_rotations;
   const std::vector<int64_t> ins = active_pixels(mask, npix, true);
-  for (int64_t r = 0; r < c->n_rotations; ++r) {
-    const double T = total_resp[r];
-    if (!(all_total_resp[r] > 1e-10) || !(T > 0.0)) continue;
-    const double w = (double)rotw[r] * T;
-    float m[9];
-    orc_rotation_matrix_f32(rot + 4 * r, m);
-    for (int64_t i : ins) {
-      VoxelPos pos = voxel_pos(m, side, cx[i], cy[i], cz[i]);
-      Stencil st;
-      stencil(pos, side, c->interp, 0, &st);
-      const double s = U[r * npix + i] / T;
-      for (int k = 0; k < st.n; ++k) {
-        model_acc[st.v[k]] += st.w[k] * w * s;
-        weight_acc[st.v[k]] += st.w[k] * w;
+  const int64_t budget = (int64_t)1 << 29;  // bytes of per-chunk grids
+  int64_t nch = std::min<int64_t>(32, std::max<int64_t>(1, budget / (16 * M)));
+  nch = std::max<int64_t>(1, std::min<int64_t>(nch, R));
+  std::vector<double> part(nch > 1 ? (size_t)(2 * M * nch) : 0, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t ch = 0; ch < nch; ++ch) {
+    double* ma = nch > 1 ? part.data() + 2 * M * ch : model_acc;
+    double* wa = nch > 1 ? ma + M : weight_acc;
+    for (int64_t r = R * ch / nch; r < R * (ch + 1) / nch; ++r) {
+      const double T = total_resp[r];
+      if (!(all_total_resp[r] > 1e-10) || !(T > 0.0)) continue;
+      const double w = (double)rotw[r] * T;
+      float m[9];
+      orc_rotation_matrix_f32(rot + 4 * r, m);
+      for (int64_t i : ins) {
+        VoxelPos pos = voxel_pos(m, side, cx[i], cy[i], cz[i]);
+        Stencil st;
+        stencil(pos, side, c->interp, 0, &st);
+        const double s = U[r * npix + i] / T;
+        for (int k = 0; k < st.n; ++k) {
+          ma[st.v[k]] += st.w[k] * w * s;
+          wa[st.v[k]] += st.w[k] * w;
+        }
       }
     }
+  }
+  if (nch > 1) {
+#pragma omp parallel for
+    for (int64_t v = 0; v < M; ++v)
+      for (int64_t ch = 0; ch < nch; ++ch) {
+        model_acc[v] += part[2 * M * ch + v];
+        weight_acc[v] += part[2 * M * ch + M + v];
+      }
   }
 }
 
@@ -544,6 +619,164 @@ void orc_normalize_model(int64_t M, double* model, const double* weight) {
   const double mean = sum / (double)M;
   if (mean != 0.0)
     for (int64_t i = 0; i < M; ++i) model[i] /= mean;
+}
+
+// ------------------------------------------------- synthetic inputs --
+// The seeded synthetic datasets of the benchmark configurations, restated
+// here so that a CPU-only run (the timed CPU baseline) needs nothing but this
+// library.  Same counter-based streams, Poisson sampler and FP32 trilinear
+// weights as the engine's host generator, so both produce identical data.
+
+namespace {
+
+inline uint64_t syn_mix(uint64_t z) {  // splitmix64 finaliser
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Draw i of stream (seed, a, b) is a pure function of (seed, a, b, i).
+struct SynStream {
+  uint64_t key, ctr = 0;
+  SynStream(uint64_t seed, uint64_t a, uint64_t b) : key(syn_mix(syn_mix(seed ^ syn_mix(a)) + b)) {}
+  double uniform() { return (double)(syn_mix(key + syn_mix(ctr++)) >> 11) * 0x1.0p-53; }
+  double normal() {  // Box-Muller, first output
+    double u1 = uniform(), u2 = uniform();
+    if (u1 < 1e-300) u1 = 1e-300;
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+  }
+  // Inversion for means below 12, else Hormann's PTRS transformed rejection.
+  double poisson(double lam) {
+    if (!(lam > 0)) return 0.0;
+    if (lam < 12.0) {
+      double p = std::exp(-lam), s = p, u = uniform();
+      int k = 0;
+      while (u > s && k < 1000) {
+        ++k;
+        p *= lam / k;
+        s += p;
+      }
+      return k;
+    }
+    const double slam = std::sqrt(lam), loglam = std::log(lam);
+    const double b = 0.931 + 2.53 * slam, a = -0.059 + 0.02483 * b;
+    const double invalpha = 1.1239 + 1.1328 / (b - 3.4), vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (;;) {
+      const double U = uniform() - 0.5, V = uniform();
+      const double us = 0.5 - std::fabs(U);
+      const double k = std::floor((2.0 * a / us + b) * U + lam + 0.43);
+      if (us >= 0.07 && V <= vr) return k;
+      if (k < 0 || (us < 0.013 && V > us)) continue;
+      if (std::log(V) + std::log(invalpha) - std::log(a / (us * us) + b) <=
+          -lam + k * loglam - std::lgamma(k + 1.0))
+        return k;
+    }
+  }
+};
+
+// Trilinear sample of the model at continuous voxel position u: FP32 corner
+// weights (x, y, z factors multiplied in that order), corners in bit order,
+// zero-weight and out-of-grid corners skipped, FP64 sum.
+double syn_trilinear(const float* model, int side, const float* u) {
+  const float fx = std::floor(u[0]), fy = std::floor(u[1]), fz = std::floor(u[2]);
+  const float ax = u[0] - fx, ay = u[1] - fy, az = u[2] - fz;
+  double acc = 0;
+  for (int c = 0; c < 8; ++c) {
+    const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
+    const int kx = (int)fx + bx, ky = (int)fy + by, kz = (int)fz + bz;
+    if (kx < 0 || kx >= side || ky < 0 || ky >= side || kz < 0 || kz >= side) continue;
+    const float w = (bx ? ax : 1.0f - ax) * (by ? ay : 1.0f - ay) * (bz ? az : 1.0f - az);
+    if (w == 0.0f) continue;
+    acc += (double)w * model[((int64_t)kz * side + ky) * side + kx];
+  }
+  return acc;
+}
+
+}  // namespace
+
+void orc_random_model(int side, uint64_t seed, float* model) {
+  const int64_t M = (int64_t)side * side * side;
+#pragma omp parallel for
+  for (int64_t i = 0; i < M; ++i) {
+    SynStream s(seed, 0x6d6f64656cull, (uint64_t)i);
+    model[i] = (float)s.uniform();
+  }
+}
+
+int orc_synthesize(int side, int n_scatterers, double object_radius, int64_t n_patterns,
+                   double mean_photons, double scale_sigma, double beamstop_radius,
+                   uint64_t seed, int64_t first_pattern, const float* x, const float* y,
+                   const float* z, float* true_model, float* counts, int32_t* mask) {
+  if (side < 2 || n_patterns < 1 || n_scatterers < 1 || first_pattern < 0 || !x || !y || !z ||
+      !counts || !mask)
+    return 1;
+  const int64_t npix = (int64_t)side * side, M = npix * side;
+  // unit point scatterers uniform in a sphere of radius object_radius * side
+  std::vector<std::array<double, 3>> pos(n_scatterers);
+  {
+    SynStream s(seed, 0x73636174ull, 0);
+    const double rad = object_radius * side;
+    for (auto& p : pos) {
+      double a, b, c;
+      do {
+        a = 2 * s.uniform() - 1;
+        b = 2 * s.uniform() - 1;
+        c = 2 * s.uniform() - 1;
+      } while (a * a + b * b + c * c > 1.0);
+      p = {a * rad, b * rad, c * rad};
+    }
+  }
+  // |F|^2 at every voxel centre (voxel k at pixel-unit position k - side/2 - 0.5)
+  std::vector<float> model(M);
+#pragma omp parallel for
+  for (int64_t v = 0; v < M; ++v) {
+    const int kx = (int)(v % side), ky = (int)((v / side) % side), kz = (int)(v / npix);
+    const double qx = kx - side / 2.0 - 0.5, qy = ky - side / 2.0 - 0.5, qz = kz - side / 2.0 - 0.5;
+    double re = 0, im = 0;
+    for (const auto& p : pos) {
+      const double ph = 2.0 * M_PI * (qx * p[0] + qy * p[1] + qz * p[2]) / side;
+      re += std::cos(ph);
+      im += std::sin(ph);
+    }
+    model[v] = (float)(re * re + im * im);
+  }
+  if (true_model) std::memcpy(true_model, model.data(), sizeof(float) * M);
+  int64_t active = 0;  // beamstop: pixel centres within the radius are masked
+  for (int iy = 0; iy < side; ++iy)
+    for (int ix = 0; ix < side; ++ix) {
+      const double dx = ix - side / 2.0 + 0.5, dy = iy - side / 2.0 + 0.5;
+      const int on = std::sqrt(dx * dx + dy * dy) > beamstop_radius ? 1 : 0;
+      mask[(int64_t)iy * side + ix] = on;
+      active += on;
+    }
+  if (active == 0) return 1;
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int64_t p = 0; p < n_patterns; ++p) {
+    const uint64_t gp = (uint64_t)(p + first_pattern);
+    SynStream s(seed, 0x70617474ull, gp);
+    // uniform random rotation (Shoemake), lognormal scale of mean 1
+    const double u1 = s.uniform(), u2 = s.uniform(), u3 = s.uniform();
+    const float q[4] = {(float)(std::sqrt(1 - u1) * std::sin(2 * M_PI * u2)),
+                        (float)(std::sqrt(1 - u1) * std::cos(2 * M_PI * u2)),
+                        (float)(std::sqrt(u1) * std::sin(2 * M_PI * u3)),
+                        (float)(std::sqrt(u1) * std::cos(2 * M_PI * u3))};
+    const double scale = std::exp(scale_sigma * s.normal() - 0.5 * scale_sigma * scale_sigma);
+    float m[9];
+    orc_rotation_matrix_f32(q, m);
+    std::vector<double> sl(npix);
+    double tot = 0;
+    for (int64_t i = 0; i < npix; ++i) {
+      const VoxelPos vp = voxel_pos(m, side, x[i], y[i], z[i]);
+      sl[i] = syn_trilinear(model.data(), side, vp.u);
+      if (mask[i]) tot += sl[i];
+    }
+    const double f = tot > 0 ? mean_photons * scale / tot : 0.0;
+    SynStream d(seed, 0x636f756eull, gp);
+    float* out = counts + p * npix;
+    for (int64_t i = 0; i < npix; ++i) out[i] = (float)d.poisson(sl[i] * f);
+  }
+  return 0;
 }
 
 void orc_iterate(const orc_config* c, const float* images, const int32_t* mask, const float* rot,

@@ -115,6 +115,18 @@ void orc_iterate_restricted(const orc_config* c, const float* images, const int3
                             const float* cz, const uint8_t* allowed, double* model,
                             double* scaling, double* resp_out, orc_stats* stats);
 
+/* Seeded synthetic inputs (the benchmark configurations' data): a uniform
+ * [0,1) model, and a dataset of point-scatterer |F|^2 (true_model, optional),
+ * beamstop mask [side^2] and Poisson counts [n_patterns][side^2] drawn at
+ * uniform random rotations with lognormal scales; patterns first_pattern ..
+ * first_pattern + n_patterns - 1 of the seeded sequence.  Returns 0, or 1 for
+ * invalid arguments. */
+void orc_random_model(int side, uint64_t seed, float* model);
+int orc_synthesize(int side, int n_scatterers, double object_radius, int64_t n_patterns,
+                   double mean_photons, double scale_sigma, double beamstop_radius,
+                   uint64_t seed, int64_t first_pattern, const float* x, const float* y,
+                   const float* z, float* true_model, float* counts, int32_t* mask);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,11 +41,18 @@ class Stats(C.Structure):
     ]
 
 
+def reference_dir() -> str:
+    """The reference checkout: $EMC_REFERENCE_DIR, else a sibling directory
+    `reference` of the repository (absent on machines that only run tests)."""
+    return os.environ.get("EMC_REFERENCE_DIR") or os.path.abspath(
+        os.path.join(HERE, os.pardir, os.pardir, "reference"))
+
+
 def build() -> None:
     """Compile liboracle.so (and oracle/_ref when the reference sources exist)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if os.path.isfile("/root/reference/emc.c"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if os.path.isfile(os.path.join(reference_dir(), "emc.c")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={reference_dir()}"], check=True)
 
 
 _lib = None
@@ -76,6 +83,11 @@ def lib():
         _lib.orc_iterate.argtypes = [P] * 12
         _lib.orc_iterate_restricted.argtypes = [P] * 13
         _lib.orc_insert_shard.argtypes = [P] * 12
+        _lib.orc_random_model.argtypes = [C.c_int, C.c_uint64, P]
+        _lib.orc_synthesize.restype = C.c_int
+        _lib.orc_synthesize.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int64, C.c_double,
+                                        C.c_double, C.c_double, C.c_uint64, C.c_int64,
+                                        P, P, P, P, P, P]
     return _lib
 
 
@@ -236,6 +248,11 @@ def iterate(cfg, images, mask, rot, rotw, cx, cy, cz, model, scaling, want_resp=
     candidate set of rotations (orc_iterate_restricted).
     Returns (model, scaling, P or None, stats dict)."""
     k = _Keep()
+    npix = cfg.side * cfg.side
+    if (np.asarray(images).size != cfg.n_patterns * npix or np.asarray(mask).size != npix
+            or np.asarray(rot).shape != (cfg.n_rotations, 4) or np.asarray(rotw).size != cfg.n_rotations
+            or np.asarray(scaling).size != cfg.n_patterns or np.asarray(model).size != npix * cfg.side):
+        raise ValueError("oracle.iterate: array shapes do not match the configuration")
     m = _f64(model).copy()
     sc = _f64(scaling).copy()
     P = np.zeros((cfg.n_rotations, cfg.n_patterns), np.float64) if want_resp else None
@@ -252,3 +269,44 @@ def iterate(cfg, images, mask, rot, rotw, cx, cy, cz, model, scaling, want_resp=
                                      _p(m), _p(sc), _p(P), C.byref(st))
     stats = {k: getattr(st, k) for k, _ in Stats._fields_}
     return m, sc, P, stats
+
+
+# ------------------------------------------------------- synthetic inputs --
+
+def random_model(side, seed=0):
+    """Uniform [0, 1) model from the seeded counter-based stream."""
+    m = np.zeros(side ** 3, np.float32)
+    lib().orc_random_model(side, seed, _p(m))
+    return m
+
+
+def synthesize(side, n_patterns, x, y, z, mean_photons=1000.0, scale_sigma=0.3,
+               beamstop_radius=0.0, n_scatterers=40, object_radius=0.3, seed=0, first_pattern=0):
+    """Seeded synthetic dataset: dict(model, counts [N][side^2], mask)."""
+    npix = side * side
+    model = np.zeros(side ** 3, np.float32)
+    counts = np.zeros((n_patterns, npix), np.float32)
+    mask = np.zeros(npix, np.int32)
+    k = _Keep()
+    rc = lib().orc_synthesize(side, n_scatterers, object_radius, n_patterns, mean_photons,
+                              scale_sigma, beamstop_radius, seed, first_pattern, k(_f32(x)),
+                              k(_f32(y)), k(_f32(z)), _p(model), _p(counts), _p(mask))
+    if rc != 0:
+        raise ValueError("orc_synthesize: invalid arguments")
+    return dict(model=model, counts=counts, mask=mask)
+
+
+def make_workload(w, n_patterns=None, first_pattern=0, wavelength=1e-10, distance=1.0,
+                  pixel_size=None):
+    """A benchmark workload (an object with side, rot_n, n_patterns,
+    mean_photons, scale_sigma, beamstop, seed) built with this library alone:
+    the same arrays as the engine's own workload builder, in the same dict."""
+    N = n_patterns or w.n_patterns
+    x, y, z = (a.astype(np.float32) for a in coordinates(w.side, wavelength, pixel_size, distance))
+    d = synthesize(w.side, N, x, y, z, mean_photons=w.mean_photons, scale_sigma=w.scale_sigma,
+                   beamstop_radius=w.beamstop, seed=w.seed, first_pattern=first_pattern)
+    q, wt = generate_rotations(w.rot_n, halve=True)
+    return dict(workload=w, x=x, y=y, z=z, mask=d["mask"], counts=d["counts"],
+                q=q.astype(np.float32), w=wt.astype(np.float32),
+                model0=random_model(w.side, w.seed), true_model=d["model"],
+                scaling0=np.ones(N, np.float32))
