@@ -111,7 +111,8 @@ struct emc_context {
   double* d_stats = nullptr;    // [0] mean [1] max [2] plogp [3] loglik
   // FP32 path
   float* d_S = nullptr;   // [R][npa]
-  float* d_LL = nullptr;  // [R][N]
+  float* d_LL = nullptr;  // [R][N] responsibilities (FP32)
+  double* d_LL64 = nullptr;  // [R][N] log-likelihood (FP64) the softmax reads
   double* d_den = nullptr;
   double* d_lse32 = nullptr;
   double* d_plogp_part = nullptr;
@@ -363,6 +364,10 @@ static emc_status alloc_work(emc_context* c) {
   if (!c->mixed) {
     TRY(c->alloc(&c->d_S, R * npa));
     TRY(c->alloc(&c->d_LL, R * N));
+    // the log-likelihood is kept in FP64: its values reach 10^3 - 10^4 (poisson),
+    // where an FP32 ulp (1e-4 - 1e-3) would move the responsibilities by more
+    // than the contraction's own error
+    TRY(c->alloc(&c->d_LL64, R * N));
     TRY(c->alloc(&c->d_K, N * npa));
     TRY(c->alloc(&c->d_den, ((R + 127) / 128) * N));
     TRY(c->alloc(&c->d_plogp_part, (N + 31) / 32 + 1));
@@ -740,6 +745,7 @@ static emc_status sparse_loglik(emc_context* c) {
   a.R = R;
   a.N = N;
   a.LL = c->d_LL;
+  a.LL64 = c->d_LL64;
   CK(c, launch_ll_sparse(a, c->st));
   c->launches += 2;
   return EMC_OK;
@@ -805,12 +811,14 @@ emc_status emc_maximize(emc_context* c) {
     l.gauss_inv = gauss_inv(c);
     l.poisson = c->gauss ? 0 : 1;
     l.LL = c->d_LL;
+    l.LL64 = c->d_LL64;
     CK(c, launch_ll_fp32(l, c->st));
   }
   if (!c->mixed) {
     c->mark(2);
     int nparts = 0;
-    CK(c, launch_softmax_fp32(c->d_LL, R, N, c->d_plogp_part, &nparts, c->d_lse32, c->st));
+    CK(c, launch_softmax_from_f64(c->d_LL64, c->d_LL, R, N, c->d_plogp_part, &nparts,
+                                  c->d_lse32, c->st));
     CK(c, launch_sum_f64(c->d_plogp_part, nparts, c->d_stats + 2, c->st));
     CK(c, launch_sum_f64(c->d_lse32, N, c->d_stats + 3, c->st));
     int64_t nden = 0;

@@ -49,6 +49,7 @@ struct LLArgs {
   double gauss_inv;      // 1 / (2 cnt sigma^2)
   int poisson;
   float* LL;
+  double* LL64;          // when set, LL is written here in FP64 instead (LL unused)
 };
 cudaError_t launch_ll_fp32(const LLArgs& a, cudaStream_t st);
 
@@ -67,6 +68,7 @@ struct SparseLLArgs {
   const double* rowstat;  // sum W_r
   int64_t R, N;
   float* LL;              // [R][N]
+  double* LL64;           // when set, [R][N] in FP64 instead of LL
 };
 // ldT % 4 == 0 and logWT 16-byte aligned (each thread gathers 4 rotations).
 cudaError_t launch_ll_sparse(const SparseLLArgs& a, cudaStream_t st);
@@ -101,6 +103,11 @@ cudaError_t launch_csr_fill(const float* K, int64_t N, int64_t npa, const int64_
 // Per-pattern softmax over r of X[r][p] (in place), FP32 arithmetic as the
 // reference; plogp_part[blockIdx] receives sum P log P partials (FP64) and
 // lse[p] (optional) the pattern's log-sum-exp.
+// The same per-pattern softmax from an FP64 log-likelihood L [R][N] into the
+// FP32 responsibilities P [R][N].
+cudaError_t launch_softmax_from_f64(const double* L, float* P, int64_t R, int64_t N,
+                                    double* plogp_part, int* nparts, double* lse,
+                                    cudaStream_t st);
 cudaError_t launch_softmax_fp32(float* X, int64_t R, int64_t N, double* plogp_part,
                                 int* nparts, double* lse, cudaStream_t st);
 // sum of x log x over n floats into *out (FP64).

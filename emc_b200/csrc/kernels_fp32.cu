@@ -218,7 +218,10 @@ struct OpLL {
         if (n >= p.N) continue;
         const double v = p.poisson ? acc[i][j] - (double)p.scaling[n] * p.rowstat[r]
                                    : -acc[i][j] * p.gauss_inv;
-        p.LL[r * p.ldLL + n] = (float)v;
+        if (p.LL64)
+          p.LL64[r * p.ldLL + n] = v;
+        else
+          p.LL[r * p.ldLL + n] = (float)v;
       }
     }
   }
@@ -304,26 +307,29 @@ struct OpCompress {
 };
 
 // ----------------------------------------------------------------- softmax --
-// 32 patterns per block (lane == pattern), 8 warps share the rotations.
-__global__ void __launch_bounds__(kBlock) softmax_kernel(float* X, int64_t R, int64_t N,
-                                                         double* plogp_part, double* lse) {
-  __shared__ float smax[8][32];
+// 32 patterns per block (lane == pattern), 8 warps share the rotations.  The
+// log-likelihood is read from X (FP32, then overwritten by P in place) or, for
+// an FP64 log-likelihood, from X64 with P written to X.
+template <class T>
+__device__ __forceinline__ void softmax_body(const T* L, float* X, int64_t R, int64_t N,
+                                             double* plogp_part, double* lse) {
+  __shared__ T smax[8][32];
   __shared__ float ssum[8][32];
   __shared__ double sred[8][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t p = (int64_t)blockIdx.x * 32 + lane;
   const bool ok = p < N;
-  float mx = -FLT_MAX;
+  T mx = -FLT_MAX;
   if (ok)
-    for (int64_t r = w; r < R; r += 8) mx = fmaxf(mx, X[r * N + p]);
+    for (int64_t r = w; r < R; r += 8) mx = L[r * N + p] > mx ? L[r * N + p] : mx;
   smax[w][lane] = mx;
   __syncthreads();
   mx = smax[0][lane];
-  for (int k = 1; k < 8; ++k) mx = fmaxf(mx, smax[k][lane]);
+  for (int k = 1; k < 8; ++k) mx = smax[k][lane] > mx ? smax[k][lane] : mx;
   float s = 0.0f;
   if (ok)
     for (int64_t r = w; r < R; r += 8) {
-      const float d = X[r * N + p] - mx;
+      const float d = (float)(L[r * N + p] - mx);
       if (d > -1.0e10f) s += expf(d);  // emc_cuda.cu:463-468
     }
   ssum[w][lane] = s;
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(kBlock) softmax_kernel(float* X, int64_t R, in
   double pl = 0.0;
   if (ok)
     for (int64_t r = w; r < R; r += 8) {
-      const float d = X[r * N + p] - mx;
+      const float d = (float)(L[r * N + p] - mx);
       const float P = d > -1.0e10f ? expf(d) * inv : 0.0f;
       X[r * N + p] = P;
       if (P > 0.0f) pl += (double)P * log((double)P);
@@ -348,6 +354,17 @@ __global__ void __launch_bounds__(kBlock) softmax_kernel(float* X, int64_t R, in
     t = warp_sum(t);
     if (lane == 0 && plogp_part) plogp_part[blockIdx.x] = t;
   }
+}
+
+__global__ void __launch_bounds__(kBlock) softmax_kernel(float* X, int64_t R, int64_t N,
+                                                         double* plogp_part, double* lse) {
+  softmax_body<float>(X, X, R, N, plogp_part, lse);
+}
+
+__global__ void __launch_bounds__(kBlock) softmax64_kernel(const double* L, float* X, int64_t R,
+                                                           int64_t N, double* plogp_part,
+                                                           double* lse) {
+  softmax_body<double>(L, X, R, N, plogp_part, lse);
 }
 
 __global__ void xlogx_partial(const float* x, int64_t n, double* part) {
@@ -633,7 +650,7 @@ __global__ void __launch_bounds__(128)
     sparse_gather_kernel(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                          const float* __restrict__ val, const float* __restrict__ XT,
                          int64_t ldT, int64_t R, int64_t ncol, const float* scaling,
-                         const double* rowstat, const float* T, float* out) {
+                         const double* rowstat, const float* T, float* out, double* out64) {
   __shared__ float tile[kSparsePat][kSparseRot + 1];
   const int64_t r0 = (int64_t)blockIdx.y * kSparseRot + 4 * threadIdx.x;
   const int64_t p0 = (int64_t)blockIdx.x * kSparsePat;
@@ -681,6 +698,12 @@ __global__ void __launch_bounds__(128)
       }
       if (MODE == 0) {
         const double ph = (double)scaling[p];
+        if (out64) {
+          // FP64 results leave from registers (one column of 4 rows each)
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (r0 + u < R) out64[(r0 + u) * ncol + p] = tot[u] - ph * sw[u];
+        }
 #pragma unroll
         for (int u = 0; u < 4; ++u) v[u] = (float)(tot[u] - ph * sw[u]);
       } else {
@@ -695,6 +718,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
     for (int u = 0; u < 4; ++u) tile[i][4 * threadIdx.x + u] = v[u];
   }
+  if (out64) return;  // uniform over the block
   __syncthreads();
   // half a warp per output row: lane & 15 = column
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -719,7 +743,7 @@ cudaError_t launch_ll_sparse(const SparseLLArgs& a, cudaStream_t st) {
             (unsigned)((a.R + kSparseRot - 1) / kSparseRot));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
   sparse_gather_kernel<0><<<grid, 128, 0, st>>>(a.row_ptr, a.col, a.val, a.logWT, a.ldT, a.R, a.N,
-                                                a.scaling, a.rowstat, nullptr, a.LL);
+                                                a.scaling, a.rowstat, nullptr, a.LL, a.LL64);
   return cudaGetLastError();
 }
 
@@ -731,7 +755,7 @@ cudaError_t launch_compress_sparse(const SparseCmpArgs& a, cudaStream_t st) {
             (unsigned)((a.R + kSparseRot - 1) / kSparseRot));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
   sparse_gather_kernel<1><<<grid, 128, 0, st>>>(a.col_ptr, a.row, a.val, a.PT, a.ldT, a.R, a.npa,
-                                                nullptr, nullptr, a.T, a.U);
+                                                nullptr, nullptr, a.T, a.U, nullptr);
   return cudaGetLastError();
 }
 
@@ -819,6 +843,15 @@ cudaError_t launch_ll_fp32(const LLArgs& a, cudaStream_t st) {
     op.p = a;
     tile_kernel<<<grid, kBlock, 0, st>>>(op);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_softmax_from_f64(const double* L, float* P, int64_t R, int64_t N,
+                                    double* plogp_part, int* nparts, double* lse,
+                                    cudaStream_t st) {
+  const int64_t nb = (N + 31) / 32;
+  if (nparts) *nparts = (int)nb;
+  softmax64_kernel<<<(unsigned)nb, kBlock, 0, st>>>(L, P, R, N, plogp_part, lse);
   return cudaGetLastError();
 }
 

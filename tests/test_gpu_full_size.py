@@ -57,3 +57,39 @@ def test_full_size_properties(workload, n_patterns):
         for P in (Pm, Pf):
             err = np.abs(P.astype(np.float64) - P_ref).sum(axis=0).max()
             assert err < 2e-3, err
+
+
+# Bars of the benchmark geometry against the FP64 oracle: the mixed path must
+# hold the north-star bar (responsibility L1 <= 1e-2 per pattern, model <= 1e-3
+# relative); the FP32 path the FP32 bars of the parity tests.
+LARGE_BARS = {"mixed": (1e-2, 1e-3), "fp32": (1e-4, 1e-5)}
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp32"])
+def test_large128_sample_vs_oracle(precision):
+    """The 128^3 benchmark geometry (128x128 detector, radius-6 beamstop,
+    16,272 active pixels, 500 photons on average, ~3% non-zero pixels) on
+    every 43rd of its 86,520 rotations and its first 384 patterns: one
+    iteration of the engine against the oracle's from the same model."""
+    import emc_b200 as E
+    from emc_b200 import workloads as W
+    d = W.make("large128", n_patterns=384)
+    rot = np.arange(0, d["q"].shape[0], 43)
+    d = dict(d, q=d["q"][rot], w=d["w"][rot])
+    cfg = oracle_cfg(d, "poisson")
+    m_ref, s_ref, P_ref, _ = O.iterate(cfg, d["counts"], d["mask"], d["q"], d["w"], d["x"],
+                                       d["y"], d["z"], d["model0"], d["scaling0"],
+                                       want_resp=True)
+    with make_ctx(d, "poisson", "nearest", precision) as ctx:
+        ctx.expand()
+        ctx.maximize()
+        P = ctx.get_buffer(E.BUF_RESP)
+        ctx.compress()
+        model, scaling = ctx.get_model(), ctx.get_scaling()
+    err_p = float(np.abs(P.astype(np.float64) - P_ref).sum(axis=0).max())
+    err_m, err_s = rel(model, m_ref), rel(scaling, s_ref)
+    print(f"large128 sample ({precision}): responsibility L1 {err_p:.3g}, scaling {err_s:.3g}, "
+          f"model {err_m:.3g}")
+    bar_p, bar_m = LARGE_BARS[precision]
+    assert err_p <= bar_p, f"responsibility L1 {err_p:.3g}"
+    assert err_m <= bar_m, f"model error {err_m:.3g}"
