@@ -26,7 +26,9 @@ std::mutex g_setup_mutex;
 
 // Device address of the scratch array for the current device.  In host code
 // g_noalloc_scratch names a host-side stand-in, not device memory, so the
-// address is looked up once per device with that device current.
+// address is looked up once per device with that device current and kept for
+// the life of the process (a cudaDeviceReset of that device would leave it
+// pointing into the destroyed context: the header forbids calls after one).
 int scratch_for_current_device(double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 2;
@@ -48,16 +50,34 @@ extern "C" int cuda_normalize_responsabilities_noalloc(real* d_respons, int N_sl
                                                        double* sum_plogp) {
   if (!d_respons || N_slices < 1 || N_images < 1) return 1;
   if ((int64_t)N_images > kMaxPartials * kPatternsPerPartial) return 1;  // scratch too small
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // where the sum goes: device (or managed) memory receives it on the stream;
+  // host memory needs a copy and a wait, which a capturing stream cannot take
+  bool sum_on_device = false;
+  if (sum_plogp) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, sum_plogp) != cudaSuccess) {
+      cudaGetLastError();
+      return 1;
+    }
+    sum_on_device = attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+    if (!sum_on_device) {
+      cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return 2;
+      if (cap != cudaStreamCaptureStatusNone) return 1;  // refused before any stream work
+    }
+  }
   double* scratch = nullptr;
   if (scratch_for_current_device(&scratch) != 0) return 2;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   // every partial the sum reads is written by this call's softmax launch, so
   // nothing left in the array by an earlier call is read
   int nparts = 0;
   cudaError_t e = emc::launch_softmax_fp32(d_respons, N_slices, N_images, scratch, &nparts,
                                            nullptr, st);
-  if (e == cudaSuccess) e = emc::launch_sum_f64(scratch, nparts, scratch + kMaxPartials, st);
-  if (e == cudaSuccess && sum_plogp) {
+  if (e == cudaSuccess)
+    e = emc::launch_sum_f64(scratch, nparts, sum_on_device ? sum_plogp : scratch + kMaxPartials,
+                            st);
+  if (e == cudaSuccess && sum_plogp && !sum_on_device) {
     e = cudaMemcpyAsync(sum_plogp, scratch + kMaxPartials, sizeof(double),
                         cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -101,12 +101,22 @@ real cuda_total_respons(real *d_respons, real *respons, int n);
  * nothing; every GPU that loads the library holds that array until exit.
  * Limit: N_images <= 2,097,152; larger calls are rejected with status 1.
  * d_respons [N_slices][N_images] is normalised in place on `stream` (a
- * cudaStream_t, NULL for the default stream); if sum_plogp is not NULL it
- * receives sum P log P and the call waits for the stream.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the one array:
- * calls that overlap on the GPU (other streams, other host threads) race.
- * Returns 0 on success, 1 for invalid or too large sizes, 2 for a CUDA error. */
+ * cudaStream_t, NULL for the default stream).  sum_plogp (optional)
+ * receives sum P log P:
+ *   - a device (or managed) pointer: written by a kernel on `stream`; the call
+ *     does not wait, so it can be recorded into a CUDA graph with the rest;
+ *   - a host pointer: copied back, and the call waits for the stream.  A
+ *     capturing stream cannot wait, so while `stream` is being captured a
+ *     host sum_plogp is refused with status 1 before any work is enqueued
+ *     (the capture stays valid); pass NULL or a device pointer there.
+ * The first call on a device looks up the array's device address and keeps
+ * it for the life of the process; make that first call before any stream
+ * capture, and make no call on a device after cudaDeviceReset of it (the
+ * kept address would belong to the destroyed context).  All calls share the
+ * one array: calls that overlap on the GPU (other streams, other host
+ * threads) race.
+ * Returns 0 on success, 1 for invalid or too large sizes (or a host
+ * sum_plogp during capture), 2 for a CUDA error. */
 int cuda_normalize_responsabilities_noalloc(real *d_respons, int N_slices, int N_images,
                                             void *stream, double *sum_plogp);
 
