@@ -107,6 +107,10 @@ def lib():
             ("emc_model_load", [C.c_char_p, C.c_int, P], C.c_int),
             ("emc_model_save", [C.c_char_p, C.c_int, P], C.c_int),
             ("emc_autotune", [P, P, C.c_int32, P, P], C.c_int),
+            ("emc_set_memory_limit", [P, C.c_size_t], C.c_int),
+            ("emc_memory_used", [P], C.c_size_t),
+            ("emc_save_state", [P, C.c_char_p, I64], C.c_int),
+            ("emc_load_state", [P, C.c_char_p, P], C.c_int),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -444,6 +448,24 @@ class Context:
         t = Tuning()
         self._c(lib().emc_autotune(self._h, _ptr(cand), len(cand), _ptr(ms), C.byref(t)))
         return (t.maximize_raster, t.compress_raster), ms
+
+    def set_memory_limit(self, nbytes):
+        """emc_set_memory_limit: cap on the device memory this context allocates."""
+        self._c(lib().emc_set_memory_limit(self._h, int(nbytes)))
+
+    @property
+    def memory_used(self):
+        return int(lib().emc_memory_used(self._h))
+
+    def save_state(self, path, iteration=0):
+        """emc_save_state: model, weight grid, scaling and the iteration number."""
+        self._c(lib().emc_save_state(self._h, os.fsencode(path), int(iteration)))
+
+    def load_state(self, path):
+        """emc_load_state; returns the saved iteration number."""
+        it = C.c_int64()
+        self._c(lib().emc_load_state(self._h, os.fsencode(path), C.byref(it)))
+        return it.value
 
     def device_buffer(self, which):
         p, n = C.c_void_p(), C.c_size_t()

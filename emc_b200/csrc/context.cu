@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -84,6 +85,8 @@ struct emc_context {
   bool have_geom = false, have_rot = false, have_pat = false, have_model = false;
   int stage = 0;  // 0 ready to expand, 1 expanded, 2 maximized
   std::vector<void*> allocs;
+  std::vector<size_t> alloc_bytes;  // size of each entry of allocs
+  size_t mem_used = 0, mem_limit = 0;  // device bytes held; limit 0 = none
 
   // geometry (compact active pixels)
   int32_t* d_pix = nullptr;
@@ -152,6 +155,18 @@ struct emc_context {
   int64_t mtiles_cap = 0, ctiles_cap = 0, gmt_cap = 0, gct_cap = 0, pairs_cap = 0, slots_cap = 0,
           yc_cap = 0, pt_cap = 0, kg_cap = 0, a_ld = 0;
   double *d_lse_c = nullptr, *d_plogp_c = nullptr;
+  float* d_lcmass = nullptr;  // [N][m] log responsibility mass of each candidate cell
+  GroupArgs last_group{};     // arguments of the last grouped iteration (responsibility export)
+  // dense audit of sampled patterns in a proposed iteration
+  int64_t* d_aud_pat = nullptr;
+  int32_t* d_aud_slot = nullptr;
+  float *d_aud_scal = nullptr, *d_aud_cap = nullptr, *d_aud_K32 = nullptr, *d_aud_Y = nullptr;
+  double *d_aud_patsq = nullptr, *d_aud_LL = nullptr;
+  __half* d_aud_K16 = nullptr;
+  float4* d_aud_part = nullptr;
+  CUtensorMap tm_aud;
+  int64_t audit_round = 0;
+  cudaEvent_t ev_audit = nullptr;
   // Two event sets alternate between iterations, so the times of iteration
   // i-1 can be read while iteration i is still queued.
   // raster bands of the maximize / compress tile orders and the SM-pair forms
@@ -180,8 +195,8 @@ struct emc_context {
   }
 
   // pinned host staging of the proposed iteration, reused between calls
-  void* hpin[6] = {nullptr};
-  size_t hcap[6] = {0};
+  void* hpin[8] = {nullptr};
+  size_t hcap[8] = {0};
   template <class T>
   T* pinned(int slot, size_t n) {
     const size_t bytes = n * sizeof(T) + 16;
@@ -214,9 +229,14 @@ struct emc_context {
   emc_status alloc(T** p, size_t count, bool zero = false) {
     void* q = nullptr;
     const size_t bytes = count * sizeof(T) ? count * sizeof(T) : 16;
+    if (mem_limit && mem_used + bytes > mem_limit)
+      return fail(EMC_ERR_OOM, "device memory limit of %zu bytes reached (%zu held, %zu requested)",
+                  mem_limit, mem_used, bytes);
     cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return cuda(e, "cudaMalloc");
     allocs.push_back(q);
+    alloc_bytes.push_back(bytes);
+    mem_used += bytes;
     if (zero) {
       e = cudaMemsetAsync(q, 0, bytes, st);
       if (e != cudaSuccess) return cuda(e, "cudaMemset");
@@ -225,10 +245,12 @@ struct emc_context {
     return EMC_OK;
   }
   void release(void* p) {
-    for (auto& a : allocs)
-      if (a == p) {
-        cudaFree(a);
-        a = nullptr;
+    for (size_t k = 0; k < allocs.size(); ++k)
+      if (allocs[k] == p) {
+        cudaFree(allocs[k]);
+        allocs[k] = nullptr;
+        mem_used -= alloc_bytes[k];
+        alloc_bytes[k] = 0;
       }
   }
 };
@@ -241,6 +263,16 @@ struct emc_context {
 #define CK(ctx, x) TRY((ctx)->cuda((x), #x))
 
 static thread_local std::string g_create_err;
+
+// Number of entries of a host array that are NaN or infinite (or negative,
+// when nonneg is set).
+static int64_t count_bad(const float* x, int64_t n, bool nonneg) {
+  int64_t bad = 0;
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(x[i]) || (nonneg && x[i] < 0.0f)) ++bad;
+  return bad;
+}
+
 
 extern "C" {
 
@@ -327,6 +359,7 @@ emc_status emc_destroy(emc_context* ctx) {
   for (void* h : ctx->hpin)
     if (h) cudaFreeHost(h);
   if (ctx->ev_sel) cudaEventDestroy(ctx->ev_sel);
+  if (ctx->ev_audit) cudaEventDestroy(ctx->ev_audit);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
   return EMC_OK;
@@ -334,6 +367,17 @@ emc_status emc_destroy(emc_context* ctx) {
 
 void* emc_stream(emc_context* ctx) { return ctx ? (void*)ctx->st : nullptr; }
 int64_t emc_launch_count(const emc_context* ctx) { return ctx ? ctx->launches : 0; }
+
+emc_status emc_set_memory_limit(emc_context* c, size_t bytes) {
+  if (!c) return EMC_ERR_ARG;
+  if (bytes && bytes < c->mem_used)
+    return c->fail(EMC_ERR_ARG, "limit %zu is below the %zu bytes already held", bytes,
+                   c->mem_used);
+  c->mem_limit = bytes;
+  return EMC_OK;
+}
+
+size_t emc_memory_used(const emc_context* c) { return c ? c->mem_used : 0; }
 
 emc_status emc_set_profiling(emc_context* c, int on) {
   if (!c) return EMC_ERR_ARG;
@@ -414,6 +458,8 @@ emc_status emc_set_geometry(emc_context* c, const float* x, const float* y, cons
                             const int32_t* mask) {
   if (!c || !x || !y || !z || !mask) return EMC_ERR_ARG;
   if (c->have_geom) return c->fail(EMC_ERR_STATE, "geometry is already set");
+  if (count_bad(x, c->npix, false) || count_bad(y, c->npix, false) || count_bad(z, c->npix, false))
+    return c->fail(EMC_ERR_RANGE, "pixel coordinates must be finite");
   std::vector<int32_t> pix, ins;
   std::vector<float> cx, cy, cz;
   for (int64_t i = 0; i < c->npix; ++i)
@@ -444,6 +490,8 @@ emc_status emc_set_geometry(emc_context* c, const float* x, const float* y, cons
 
 emc_status emc_set_rotations(emc_context* c, const float* q, const float* w) {
   if (!c || !q || !w) return EMC_ERR_ARG;
+  if (count_bad(q, 4 * c->R, false) || count_bad(w, c->R, true))
+    return c->fail(EMC_ERR_RANGE, "rotations must be finite and their weights non-negative");
   CK(c, cudaMemcpyAsync(c->d_quat, q, sizeof(float) * 4 * c->R, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_rotw, w, sizeof(float) * c->R, cudaMemcpyHostToDevice, c->st));
   c->have_rot = true;
@@ -484,19 +532,22 @@ static emc_status finish_patterns(emc_context* c) {
   cudaError_t e = launch_pattern_stats(compact, nullptr, N, npa, npa, 1, c->d_patsq, c->st);
   if (e == cudaSuccess) e = launch_pattern_stats(compact, nullptr, N, npa, npa, 0, c->d_patsum, c->st);
   int bad = 0;
-  if (e == cudaSuccess && c->mixed) {
-    int* d_bad = reinterpret_cast<int*>(c->d_scratch);
-    e = cudaMemsetAsync(d_bad, 0, sizeof(int), c->st);
-    if (e == cudaSuccess)
-      e = launch_pack_patterns(compact, N, npa, c->Npad, c->Ppad, c->d_Kh, c->d_Kt, d_bad, c->st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
-  }
+  int* d_bad = reinterpret_cast<int*>(c->d_scratch);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), c->st);
+  if (e == cudaSuccess && c->mixed)
+    e = launch_pack_patterns(compact, N, npa, c->Npad, c->Ppad, c->d_Kh, c->d_Kt, d_bad, c->st);
+  else if (e == cudaSuccess)
+    e = launch_count_invalid(compact, N * npa, d_bad, c->st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return c->cuda(e, "emc_set_patterns");
-  if (bad)
+  c->have_pat = false;
+  if (bad && c->mixed)
     return c->fail(EMC_ERR_RANGE,
                    "%d counts are not integers in [0, 2048]; the mixed path needs them exact in FP16",
                    bad);
+  if (bad)
+    return c->fail(EMC_ERR_RANGE, "%d counts are negative, NaN or infinite", bad);
   c->have_pat = true;
   c->csr.valid = false;
   c->csc.valid = false;
@@ -558,6 +609,8 @@ emc_status emc_set_patterns_sparse(emc_context* c, const int64_t* row_ptr, const
 
 emc_status emc_set_model(emc_context* c, const float* model) {
   if (!c || !model) return EMC_ERR_ARG;
+  if (const int64_t b = count_bad(model, c->M, false))
+    return c->fail(EMC_ERR_RANGE, "%lld model values are NaN or infinite", (long long)b);
   CK(c, cudaMemcpyAsync(c->d_model, model, sizeof(float) * c->M, cudaMemcpyHostToDevice, c->st));
   c->have_model = true;
   c->stage = 0;
@@ -566,6 +619,10 @@ emc_status emc_set_model(emc_context* c, const float* model) {
 
 emc_status emc_set_scaling(emc_context* c, const float* scaling) {
   if (!c || !scaling) return EMC_ERR_ARG;
+  for (int64_t p = 0; p < c->N; ++p)
+    if (!(scaling[p] > 0.0f) || !std::isfinite(scaling[p]))
+      return c->fail(EMC_ERR_RANGE, "scaling of pattern %lld is not a finite positive number",
+                     (long long)p);
   CK(c, cudaMemcpyAsync(c->d_scaling, scaling, sizeof(float) * c->N, cudaMemcpyHostToDevice, c->st));
   return EMC_OK;
 }
@@ -1164,6 +1221,80 @@ emc_status emc_get_scaling(emc_context* c, float* scaling) {
   return emc_get_buffer(c, EMC_BUF_SCALING, scaling, sizeof(float) * (c ? c->N : 0));
 }
 
+// ---------------------------------------------------------- checkpoint --
+// File layout (little-endian): "EMCSTAT1", int32 side, likelihood, interp,
+// precision, int64 patterns, rotations, iteration, then float model [side^3],
+// weight [side^3], scaling [patterns].  The model and the scaling are the
+// whole input of the next iteration (emc.c:989-1084 reads nothing else), so a
+// context loaded from the file continues exactly where the saved one stopped.
+namespace {
+constexpr char kStateMagic[8] = {'E', 'M', 'C', 'S', 'T', 'A', 'T', '1'};
+struct StateHeader {
+  char magic[8];
+  int32_t side, likelihood, interp, precision;
+  int64_t n_patterns, n_rotations, iteration;
+};
+}  // namespace
+
+emc_status emc_save_state(emc_context* c, const char* path, int64_t iteration) {
+  if (!c || !path) return EMC_ERR_ARG;
+  if (!c->have_model) return c->fail(EMC_ERR_STATE, "no model to save");
+  if (c->stage != 0) return c->fail(EMC_ERR_STATE, "save the state between iterations");
+  TRY(check_status(c));
+  std::vector<float> buf(2 * c->M + c->N);
+  CK(c, cudaMemcpyAsync(buf.data(), c->d_model, sizeof(float) * c->M, cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaMemcpyAsync(buf.data() + c->M, c->d_weight, sizeof(float) * c->M,
+                        cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaMemcpyAsync(buf.data() + 2 * c->M, c->d_scaling, sizeof(float) * c->N,
+                        cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  StateHeader h{};
+  std::memcpy(h.magic, kStateMagic, 8);
+  h.side = c->cfg.side;
+  h.likelihood = c->cfg.likelihood;
+  h.interp = c->cfg.interp;
+  h.precision = c->cfg.precision;
+  h.n_patterns = c->N;
+  h.n_rotations = c->R;
+  h.iteration = iteration;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return c->fail(EMC_ERR_ARG, "cannot open %s for writing", path);
+  const bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 &&
+                  std::fwrite(buf.data(), sizeof(float), buf.size(), f) == buf.size();
+  if (std::fclose(f) != 0 || !ok) return c->fail(EMC_ERR_ARG, "short write to %s", path);
+  return EMC_OK;
+}
+
+emc_status emc_load_state(emc_context* c, const char* path, int64_t* iteration) {
+  if (!c || !path) return EMC_ERR_ARG;
+  if (c->stage != 0) return c->fail(EMC_ERR_STATE, "load a state between iterations");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return c->fail(EMC_ERR_ARG, "cannot open %s", path);
+  StateHeader h{};
+  std::vector<float> buf(2 * c->M + c->N);
+  const bool ok = std::fread(&h, sizeof(h), 1, f) == 1 &&
+                  std::fread(buf.data(), sizeof(float), buf.size(), f) == buf.size() &&
+                  std::fgetc(f) == EOF;
+  std::fclose(f);
+  if (!ok || std::memcmp(h.magic, kStateMagic, 8) != 0)
+    return c->fail(EMC_ERR_RANGE, "%s is not a state file of this size", path);
+  if (h.side != c->cfg.side || h.n_patterns != c->N || h.n_rotations != c->R)
+    return c->fail(EMC_ERR_RANGE,
+                   "state of side %d / %lld patterns / %lld rotations does not fit this context",
+                   h.side, (long long)h.n_patterns, (long long)h.n_rotations);
+  if (count_bad(buf.data(), 2 * c->M + c->N, false))
+    return c->fail(EMC_ERR_RANGE, "the state holds NaN or infinite values");
+  CK(c, cudaMemcpyAsync(c->d_model, buf.data(), sizeof(float) * c->M, cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_weight, buf.data() + c->M, sizeof(float) * c->M,
+                        cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaMemcpyAsync(c->d_scaling, buf.data() + 2 * c->M, sizeof(float) * c->N,
+                        cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  c->have_model = true;
+  if (iteration) *iteration = h.iteration;
+  return EMC_OK;
+}
+
 emc_status emc_device_buffer(emc_context* c, emc_buffer which, void** dptr, size_t* bytes) {
   if (!c || !dptr) return EMC_ERR_ARG;
   void* p = nullptr;
@@ -1180,6 +1311,9 @@ emc_status emc_device_buffer(emc_context* c, emc_buffer which, void** dptr, size
       break;
     case EMC_BUF_RESP:
       if (c->mixed) return c->fail(EMC_ERR_UNSUPPORTED, "mixed path keeps no FP32 responsibility matrix");
+      if (c->resp_source == 2)
+        return c->fail(EMC_ERR_STATE, "a proposed iteration's responsibilities are read with "
+                                      "emc_get_buffer");
       p = c->d_LL; n = sizeof(float) * c->R * c->N; break;
     case EMC_BUF_SLICES:
       if (c->mixed) return c->fail(EMC_ERR_UNSUPPORTED, "mixed path keeps FP16 hi/lo slices");
@@ -1194,6 +1328,19 @@ emc_status emc_device_buffer(emc_context* c, emc_buffer which, void** dptr, size
 emc_status emc_get_buffer(emc_context* c, emc_buffer which, void* host, size_t bytes) {
   if (!c || !host) return EMC_ERR_ARG;
   TRY(check_status(c));
+  if (which == EMC_BUF_RESP && c->resp_source == 2) {
+    // a proposed iteration: P over each pattern's candidate cells, 0 elsewhere
+    const size_t n = (size_t)(c->R * c->N);
+    if (bytes != n * sizeof(float)) return c->fail(EMC_ERR_ARG, "buffer size mismatch");
+    if (c->stage != 0) return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+    float* tmp = nullptr;
+    CK(c, cudaMalloc(&tmp, n * sizeof(float)));
+    cudaError_t e = launch_proposed_resp(c->last_group, tmp, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(tmp);
+    return c->cuda(e, "emc_get_buffer");
+  }
   if (c->mixed && (which == EMC_BUF_RESP || which == EMC_BUF_SLICES)) {
     const size_t n = which == EMC_BUF_RESP ? (size_t)(c->R * c->N) : (size_t)(c->R * c->npa);
     if (bytes != n * sizeof(float)) return c->fail(EMC_ERR_ARG, "buffer size mismatch");
@@ -1338,12 +1485,139 @@ static emc_status grow(emc_context* c, T** p, int64_t& cap, int64_t need) {
 
 extern "C" {
 
-emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float* keep,
-                                int32_t min_m, int32_t m, float mass_target, float keep_mass,
-                                float threshold, emc_proposal_stats* stats) {
-  if (!c || !probs || m < 1 || min_m < 1 || min_m > m) return EMC_ERR_ARG;
-  if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
-  if (m > c->n_cells) return c->fail(EMC_ERR_ARG, "more cells per pattern than cells");
+}  // extern "C"
+
+// Parameters of one proposed iteration.
+struct ProposedPlan {
+  int32_t m = 1;              // candidate slots per pattern
+  float threshold = 0.0f;     // dense fallback when the mean predicted mass is below this
+  int32_t audit = 0;          // patterns evaluated against every rotation (0: none)
+  float min_captured = 0.0f;  // dense fallback when an audited pattern keeps less than this
+};
+
+// Gathers what the dense audit of the sampled patterns needs: their scaling,
+// their sum K^2, their pattern index for the FP16 row gather (slots beyond n:
+// -1, zero rows), and for FP32 contexts their compact counts.
+__global__ void gather_audit_kernel(const int64_t* pat, int n, int nslot, const float* scaling,
+                                    const double* patsq, const float* K, int64_t npa,
+                                    float* scal_out, double* patsq_out, int32_t* slot_out,
+                                    float* K_out) {
+  const int a = blockIdx.x;
+  if (a >= nslot) return;
+  const int64_t p = a < n ? pat[a] : -1;
+  if (threadIdx.x == 0) {
+    slot_out[a] = (int32_t)p;
+    if (a < n) {
+      scal_out[a] = scaling[p];
+      patsq_out[a] = patsq[p];
+    }
+  }
+  if (K_out && a < n)
+    for (int64_t j = threadIdx.x; j < npa; j += blockDim.x) K_out[a * npa + j] = K[p * npa + j];
+}
+
+// The dense audit: every rotation's log-likelihood for `audit` sampled
+// patterns (the mixed path's maximize contraction on their gathered counts,
+// or the FP32 contraction), then the share of each one's responsibility on
+// its candidate cells; the result is copied to the host behind ev_audit.
+static emc_status run_audit(emc_context* c, int32_t n_aud, int32_t m, float** host_captured) {
+  const int64_t R = c->R, N = c->N;
+  const int32_t nslot = 128;
+  if (!c->d_aud_pat) {
+    TRY(c->alloc(&c->d_aud_pat, nslot));
+    TRY(c->alloc(&c->d_aud_slot, nslot));
+    TRY(c->alloc(&c->d_aud_scal, nslot));
+    TRY(c->alloc(&c->d_aud_patsq, nslot));
+    TRY(c->alloc(&c->d_aud_cap, nslot));
+    if (c->mixed) {
+      TRY(c->alloc(&c->d_aud_K16, nslot * c->Ppad, true));
+      TRY(c->alloc(&c->d_aud_Y, R * nslot));
+      TRY(c->alloc(&c->d_aud_part, c->nrt * nslot));
+      if (!tc_encode_2d(&c->tm_aud, c->d_aud_K16, c->Ppad, nslot, 128, kMaximizeBK))
+        return c->fail(EMC_ERR_CUDA, "tensor map of the audit counts");
+    } else {
+      TRY(c->alloc(&c->d_aud_K32, nslot * c->npa));
+      TRY(c->alloc(&c->d_aud_LL, R * nslot));
+    }
+  }
+  // an evenly strided sample, shifted every call
+  std::vector<int64_t> pat(n_aud);
+  const int64_t stride = std::max<int64_t>(1, N / n_aud);
+  for (int32_t a = 0; a < n_aud; ++a) pat[a] = (c->audit_round + (int64_t)a * stride) % N;
+  c->audit_round = (c->audit_round + 7919) % N;
+  int64_t* hp = c->pinned<int64_t>(6, n_aud);
+  if (!hp) return c->fail(EMC_ERR_OOM, "pinned host staging");
+  std::copy(pat.begin(), pat.end(), hp);
+  CK(c, cudaMemcpyAsync(c->d_aud_pat, hp, sizeof(int64_t) * n_aud, cudaMemcpyHostToDevice, c->st));
+  gather_audit_kernel<<<nslot, 128, 0, c->st>>>(c->d_aud_pat, n_aud, nslot, c->d_scaling,
+                                                c->d_patsq, c->mixed ? nullptr : c->d_K, c->npa,
+                                                c->d_aud_scal, c->d_aud_patsq, c->d_aud_slot,
+                                                c->mixed ? nullptr : c->d_aud_K32);
+  CK(c, cudaGetLastError());
+  AuditArgs a{};
+  a.R = R;
+  a.ld = nslot;
+  a.m = m;
+  a.poisson = c->gauss ? 0 : 1;
+  a.pat = c->d_aud_pat;
+  a.cand = c->d_cand;
+  a.cell = c->d_cell;
+  a.scaling = c->d_aud_scal;
+  a.rowstat = c->d_rowstat;
+  a.patstat = c->d_aud_patsq;
+  a.gauss_inv = gauss_inv(c);
+  a.captured = c->d_aud_cap;
+  if (c->mixed) {
+    CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_aud_slot, nslot, c->d_aud_K16, c->st));
+    MaxEpiArgs e{};
+    e.N = n_aud;
+    e.R = R;
+    e.ldY = nslot;
+    e.poisson = a.poisson;
+    e.scaling = c->d_aud_scal;
+    e.rowstat = c->d_rowstat;
+    e.patstat = c->d_aud_patsq;
+    e.gauss_inv = a.gauss_inv;
+    e.Y = c->d_aud_Y;
+    e.part = c->d_aud_part;
+    CK(c, launch_maximize_tc(c->tm_aud, c->tmBhi, c->tmBlo, nslot, c->Rpad, c->Ppad, e,
+                             c->d_status, c->num_sms, c->st, 1));
+    a.Y = c->d_aud_Y;
+  } else {
+    LLArgs l{};
+    l.A = c->d_S;
+    l.K = c->d_aud_K32;
+    l.scaling = c->d_aud_scal;
+    l.rowstat = c->d_rowstat;
+    l.R = R;
+    l.N = n_aud;
+    l.npa = c->npa;
+    l.ldA = c->npa;
+    l.ldK = c->npa;
+    l.ldLL = nslot;
+    l.gauss_inv = a.gauss_inv;
+    l.poisson = a.poisson;
+    l.LL64 = c->d_aud_LL;
+    CK(c, launch_ll_fp32(l, c->st));
+    a.LL64 = c->d_aud_LL;
+  }
+  CK(c, launch_audit(a, n_aud, c->st));
+  float* hc = c->pinned<float>(7, n_aud);
+  if (!hc) return c->fail(EMC_ERR_OOM, "pinned host staging");
+  CK(c, cudaMemcpyAsync(hc, c->d_aud_cap, sizeof(float) * n_aud, cudaMemcpyDeviceToHost, c->st));
+  if (!c->ev_audit) CK(c, cudaEventCreateWithFlags(&c->ev_audit, cudaEventDisableTiming));
+  CK(c, cudaEventRecord(c->ev_audit, c->st));
+  c->launches += c->mixed ? 4 : 3;  // gather (2), contraction, audit
+  *host_captured = hc;
+  return EMC_OK;
+}
+
+// One proposed iteration: `select` writes the candidate cells (d_cand,
+// [N][m]) and their predicted mass (d_mass) on the context stream.
+template <class Select>
+static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select select,
+                               emc_proposal_stats* stats) {
+  const int32_t m = pl.m;
   const int64_t N = c->N, R = c->R, pairs = N * m;
   if (!c->d_mass) {
     TRY(c->alloc(&c->d_mass, N));
@@ -1362,14 +1636,15 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
     TRY(grow(c, &c->d_ppos, cap, pairs));
     cap = c->pairs_cap;
     TRY(grow(c, &c->d_cmass, cap, pairs));
+    cap = c->pairs_cap;
+    TRY(grow(c, &c->d_lcmass, cap, pairs));
     c->pairs_cap = cap;
     c->cand_m = m;
   }
   if (c->stage != 0) return c->fail(EMC_ERR_STATE, "proposed iteration between stages");
   // candidate cells of every pattern and the proposal's mass on them; their
   // copy to the host is waited for while the expansion runs behind it
-  CK(c, launch_select(probs, keep, N, c->n_cells, min_m, m, mass_target, keep_mass, c->d_cand,
-                      c->d_mass, c->st));
+  CK(c, select());
   int32_t* cand = c->pinned<int32_t>(0, pairs);
   float* mass = c->pinned<float>(1, N);
   if (!cand || !mass) return c->fail(EMC_ERR_OOM, "pinned host staging");
@@ -1380,6 +1655,9 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   TRY(emc_expand(c));
   if (!c->mixed && c->gauss)  // the grouped gaussian LL uses the expanded form: sum_j S_rj^2
     CK(c, launch_pattern_stats(c->d_S, nullptr, R, c->npa, c->npa, 1, c->d_rowstat, c->st));
+  float* captured = nullptr;
+  const int32_t n_aud = (int32_t)std::min<int64_t>(pl.audit, std::min<int64_t>(N, 128));
+  if (n_aud > 0) TRY(run_audit(c, n_aud, m, &captured));
   CK(c, cudaEventSynchronize(c->ev_sel));
   double msum = 0.0, mmin = 1e300;
   for (int64_t p = 0; p < N; ++p) {
@@ -1389,8 +1667,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   emc_proposal_stats st{};
   st.mean_mass = msum / (double)N;
   st.min_mass = mmin;
-  if (st.mean_mass < threshold) {
-    // the proposal is not confident enough: the dense iteration runs instead
+  auto dense_instead = [&]() -> emc_status {
     TRY(emc_maximize(c));
     TRY(emc_compress(c));
     st.fallback = 1;
@@ -1398,7 +1675,9 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
     st.evaluations = N * R;
     if (stats) *stats = st;
     return EMC_OK;
-  }
+  };
+  // the proposal is not confident enough: the dense iteration runs instead
+  if (st.mean_mass < pl.threshold) return dense_instead();
   // Group the (pattern, cell) pairs by cell (stable counting sort on the
   // host).  Pairs live in slots: cell c owns slots gbeg[c] .. gbeg[c]+gcnt[c]-1,
   // its first slot a multiple of 8; the slots between cells are padding
@@ -1441,6 +1720,20 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
       gpair[q] = (int32_t)p;
       ppos[p * m + i] = q;
     }
+  // the audited patterns' captured responsibility decides between the
+  // grouped stages and the dense iteration
+  if (n_aud > 0) {
+    CK(c, cudaEventSynchronize(c->ev_audit));
+    double csum = 0.0, cmin = 1e300;
+    for (int32_t a = 0; a < n_aud; ++a) {
+      csum += captured[a];
+      cmin = captured[a] < cmin ? captured[a] : cmin;
+    }
+    st.audited = n_aud;
+    st.audit_mean_captured = csum / n_aud;
+    st.audit_min_captured = cmin;
+    if (cmin < pl.min_captured) return dense_instead();
+  }
   // tcgen05 grouped contractions: mixed precision, cells of at most 256 rotations
   const bool tc = c->mixed && c->max_members <= 256 && S > 0 && (S + 31) / 32 <= 65535;
   const int64_t MM = tc ? 256 : c->max_members;
@@ -1515,6 +1808,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   CK(c, cudaMemsetAsync(c->d_T, 0, sizeof(float) * R, c->st));
   GroupArgs g{};
   g.N = N;
+  g.R = R;
   g.npa = c->npa;
   g.MM = MM;
   g.n_cells = n_cells;
@@ -1549,6 +1843,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   g.plogp = c->d_plogp_c;
   g.new_scaling = c->d_scaling;
   g.cmass = c->d_cmass;
+  g.lcmass = c->d_lcmass;
   g.best_rot = c->d_best;
   g.best_p = c->d_bestp;
   g.mtiles = c->d_mtiles;
@@ -1620,6 +1915,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
     launches = 3;  // contraction, softmax, contraction
   }
   c->resp_source = 2;
+  c->last_group = g;
   c->mark(4);
   CK(c, launch_normalize_acc(c->d_acc, c->d_model, c->d_weight, c->M, c->d_scratch, c->d_stats,
                              c->st));
@@ -1640,6 +1936,77 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   if (stats) *stats = st;
   return EMC_OK;
 }
+
+extern "C" {
+
+emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float* keep,
+                                int32_t min_m, int32_t m, float mass_target, float keep_mass,
+                                float threshold, emc_proposal_stats* stats) {
+  if (!c || !probs || m < 1 || min_m < 1 || min_m > m) return EMC_ERR_ARG;
+  if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
+  if (m > c->n_cells) return c->fail(EMC_ERR_ARG, "more cells per pattern than cells");
+  ProposedPlan pl;
+  pl.m = m;
+  pl.threshold = threshold;
+  return run_proposed(c, pl, [&]() {
+    return launch_select(probs, keep, c->N, c->n_cells, min_m, m, mass_target, keep_mass,
+                         c->d_cand, c->d_mass, c->st);
+  }, stats);
+}
+
+emc_status emc_iterate_topk(emc_context* c, const float* probs, const float* log_keep,
+                            const emc_topk_config* cfg, emc_proposal_stats* stats) {
+  if (!c || !cfg || (!probs && !log_keep) || cfg->top_k < 1 || cfg->max_cells < 1 ||
+      cfg->audit_patterns < 0 || cfg->audit_patterns > 128 || !(cfg->min_captured <= 1.0f))
+    return EMC_ERR_ARG;
+  if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
+  const int32_t m = std::min<int32_t>(cfg->max_cells, c->n_cells);
+  ProposedPlan pl;
+  pl.m = m;
+  pl.threshold = 0.0f;
+  pl.audit = cfg->audit_patterns;
+  pl.min_captured = cfg->min_captured;
+  return run_proposed(c, pl, [&]() {
+    return launch_select_topk(probs, log_keep, c->d_mcnt, c->N, c->n_cells, cfg->top_k, m,
+                              cfg->mass_target, c->d_cand, c->d_mass, c->st);
+  }, stats);
+}
+
+emc_status emc_cell_log_mass(emc_context* c, float* t) {
+  if (!c || !t) return EMC_ERR_ARG;
+  if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
+  if (c->resp_source == 0 || c->stage == 1)
+    return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+  if (c->resp_source == 2) {
+    CK(c, launch_scatter_log_targets(c->d_cand, c->d_lcmass, c->N, c->cand_m, c->n_cells, t,
+                                     c->st));
+  } else {
+    TargetArgs a{};
+    a.N = c->N;
+    a.R = c->R;
+    a.n_cells = c->n_cells;
+    a.cell = c->d_cell;
+    if (!c->mixed) {
+      a.L64 = c->d_LL64;
+      a.ldP = c->N;
+      a.lse = c->d_lse32;
+    } else {
+      a.Y = c->d_Y;
+      a.ldY = c->Npad;
+      a.poisson = c->gauss ? 0 : 1;
+      a.lse = c->d_lse;
+      a.scaling = c->d_scaling_prev;
+      a.rowstat = c->d_rowstat;
+      a.patstat = c->d_patsq;
+      a.gauss_inv = gauss_inv(c);
+    }
+    a.t = t;
+    CK(c, launch_log_targets(a, c->st));
+  }
+  CK(c, cudaStreamSynchronize(c->st));
+  return EMC_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------ several datasets at once --

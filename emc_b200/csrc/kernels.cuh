@@ -182,5 +182,7 @@ cudaError_t launch_model_max(const float* model, int64_t M, double* scratch, dou
                              cudaStream_t st);
 cudaError_t launch_fill(float* x, int64_t n, float v, cudaStream_t st);
 cudaError_t launch_sum_f64(const double* x, int64_t n, double* out, cudaStream_t st);
+// bad[0] += number of entries of x that are negative, NaN or infinite.
+cudaError_t launch_count_invalid(const float* x, int64_t n, int* bad, cudaStream_t st);
 
 }  // namespace emc

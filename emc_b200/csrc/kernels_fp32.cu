@@ -962,6 +962,22 @@ cudaError_t launch_fill(float* x, int64_t n, float v, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+__global__ void count_invalid_kernel(const float* x, int64_t n, int* bad) {
+  int nb = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float v = x[i];
+    if (!(v >= 0.0f && v <= FLT_MAX)) nb++;  // negative, NaN or infinite
+  }
+  if (nb) atomicAdd(bad, nb);
+}
+
+cudaError_t launch_count_invalid(const float* x, int64_t n, int* bad, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  count_invalid_kernel<<<grid_for(n), kBlock, 0, st>>>(x, n, bad);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_sum_f64(const double* x, int64_t n, double* out, cudaStream_t st) {
   sum_f64_kernel<<<1, kBlock, 0, st>>>(x, n, out);
   return cudaGetLastError();

@@ -10,6 +10,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -70,6 +71,43 @@ __global__ void __launch_bounds__(256) targets_kernel(const TargetArgs a) {
   __syncthreads();
   if (p < a.N)
     for (int c = w; c < a.n_cells; c += 8) a.t[p * a.n_cells + c] = tc[c * 32 + lane];
+}
+
+// lt[p][c] = log of the responsibility mass of cell c (natural log, -inf when
+// it is 0 in FP64): the same sums as targets_kernel in FP64, so the ranking of
+// cells holding 1e-300 of a pattern's mass is still defined.  16 patterns per
+// block (tid & 15), 16 rotation lanes (tid >> 4), FP64 shared-memory sums.
+__global__ void __launch_bounds__(256) log_targets_kernel(const TargetArgs a) {
+  extern __shared__ double tcd[];  // [n_cells][16]
+  const int pl = threadIdx.x & 15, rl = threadIdx.x >> 4;
+  const int64_t p = (int64_t)blockIdx.x * 16 + pl;
+  for (int i = threadIdx.x; i < a.n_cells * 16; i += blockDim.x) tcd[i] = 0.0;
+  __syncthreads();
+  if (p < a.N)
+    for (int64_t r = rl; r < a.R; r += 16) {
+      double ll;
+      if (a.L64) {
+        ll = a.L64[r * a.ldP + p] - a.lse[p];
+      } else if (a.P) {
+        ll = log((double)a.P[r * a.ldP + p]);
+      } else {
+        const float y = a.Y[r * a.ldY + p];
+        if (a.poisson) {
+          ll = (double)y;
+        } else {
+          const double phi = a.scaling[p];
+          ll = ((double)y * 2.0 / phi - a.rowstat[r] - a.patstat[p] / (phi * phi)) * a.gauss_inv;
+        }
+        ll -= a.lse[p];
+      }
+      atomicAdd(&tcd[a.cell[r] * 16 + pl], exp(ll));
+    }
+  __syncthreads();
+  if (p < a.N)
+    for (int c = rl; c < a.n_cells; c += 16) {
+      const double m = tcd[c * 16 + pl];
+      a.t[p * a.n_cells + c] = m > 0.0 ? (float)log(m) : -INFINITY;
+    }
 }
 
 // Most probable cell of a row among those not yet taken (lane owns cells
@@ -137,6 +175,135 @@ __global__ void select_kernel(const float* probs, const float* keep, int64_t N, 
   }
   for (int k = s + lane; k < m; k += 32) cand[p * m + k] = -1;
   if (lane == 0) mass[p] = tot;
+}
+
+// Top-k selection, one warp per pattern.  With log_keep (the log-posterior
+// mass of every cell in a previous iteration): cells in order of it (finite
+// values only) until they hold at least top_k fine rotations.  Then, with
+// probs (a predicted cell posterior): cells in order of probs until the probs
+// total of everything taken reaches mass_target.  At most m cells; unused
+// slots -1; mass[p] = the probs total of the taken cells (1 without probs).
+__global__ void select_topk_kernel(const float* probs, const float* log_keep, const int32_t* mcnt,
+                                   int64_t N, int C, int top_k, int m, float mass_target,
+                                   int32_t* cand, float* mass) {
+  const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= N) return;
+  uint32_t taken = 0;  // bit i: cell lane + 32 i already selected (C <= 1024)
+  float tot = 0.0f;
+  int s = 0;
+  if (log_keep) {
+    const float* krow = log_keep + p * C;
+    int64_t covered = 0;
+    for (; s < m && covered < top_k; ++s) {
+      float best;
+      int bi;
+      warp_argmax(krow, C, taken, lane, best, bi);
+      if (bi < 0 || !(best > -INFINITY)) break;
+      if ((bi & 31) == lane) taken |= 1u << (bi >> 5);
+      if (lane == 0) cand[p * m + s] = bi;
+      covered += mcnt[bi];
+      if (probs) {
+        const float v = probs[p * C + bi];
+        tot += v > 0.0f ? v : 0.0f;
+      }
+    }
+  }
+  if (probs) {
+    const float* row = probs + p * C;
+    for (; s < m && (s == 0 || tot < mass_target); ++s) {
+      float best;
+      int bi;
+      warp_argmax(row, C, taken, lane, best, bi);
+      if (bi < 0) break;
+      if ((bi & 31) == lane) taken |= 1u << (bi >> 5);
+      if (lane == 0) cand[p * m + s] = bi;
+      tot += best > 0.0f ? best : 0.0f;
+    }
+  }
+  for (int k = s + lane; k < m; k += 32) cand[p * m + k] = -1;
+  if (lane == 0) mass[p] = probs ? tot : 1.0f;
+}
+
+// Dense audit of a sample of patterns: for audited pattern a (global index
+// pat[a]) the share of its responsibility that falls on the fine rotations of
+// its candidate cells, from its log-likelihood against every rotation:
+// LL64 [R][ld] (FP64) or the mixed path's Y [R][ld] (poisson LL, gaussian
+// cross term C).  One block per audited pattern.
+__global__ void __launch_bounds__(256) audit_kernel(const AuditArgs a) {
+  __shared__ uint32_t mask[32];  // candidate cells (n_cells <= 1024)
+  __shared__ double red[8];
+  const int aidx = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int64_t p = a.pat[aidx];
+  if (t < 32) mask[t] = 0u;
+  __syncthreads();
+  for (int i = t; i < a.m; i += blockDim.x) {
+    const int c = a.cand[p * a.m + i];
+    if (c >= 0) atomicOr(&mask[c >> 5], 1u << (c & 31));
+  }
+  __syncthreads();
+  const double phi = a.scaling ? (double)a.scaling[aidx] : 1.0;
+  auto ll_of = [&](int64_t r) -> double {
+    if (a.LL64) return a.LL64[r * a.ld + aidx];
+    const double y = (double)a.Y[r * a.ld + aidx];
+    if (a.poisson) return y;
+    return (y * 2.0 / phi - a.rowstat[r] - a.patstat[aidx] / (phi * phi)) * a.gauss_inv;
+  };
+  double mx = -INFINITY;
+  for (int64_t r = t; r < a.R; r += blockDim.x) mx = fmax(mx, ll_of(r));
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) red[w] = mx;
+  __syncthreads();
+  mx = red[0];
+  for (int k = 1; k < 8; ++k) mx = fmax(mx, red[k]);
+  __syncthreads();
+  double s = 0.0, in = 0.0;
+  for (int64_t r = t; r < a.R; r += blockDim.x) {
+    const double e = exp(ll_of(r) - mx);
+    s += e;
+    const int c = a.cell[r];
+    if ((mask[c >> 5] >> (c & 31)) & 1u) in += e;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    in += __shfl_xor_sync(0xffffffffu, in, o);
+  }
+  __shared__ double red2[8];
+  if (lane == 0) {
+    red[w] = s;
+    red2[w] = in;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double S = 0.0, I = 0.0;
+    for (int k = 0; k < 8; ++k) {
+      S += red[k];
+      I += red2[k];
+    }
+    a.captured[aidx] = (float)(I / S);
+  }
+}
+
+// FP32 responsibilities [R][N] of a proposed iteration (0 outside each
+// pattern's candidate cells; P zeroed by the caller): one warp per pattern.
+__global__ void proposed_resp_kernel(const GroupArgs g, float* P) {
+  const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= g.N) return;
+  const double phi = g.scaling[p];
+  const double c1 = 2.0 * g.gauss_inv / phi,
+               c0 = g.poisson ? 0.0 : -g.patstat[p] / (phi * phi) * g.gauss_inv;
+  const double lse = g.lse[p];
+  for (int i = 0; i < g.m; ++i) {
+    const int c = g.cand[p * g.m + i];
+    if (c < 0) break;
+    const int64_t q = g.ppos[p * g.m + i];
+    for (int k = lane; k < g.mcnt[c]; k += 32) {
+      const double y = (double)g.Y[q * g.MM + k];
+      const double l = g.poisson ? y : fma(y, c1, c0 - g.rowstat[g.mbeg[c] + k] * g.gauss_inv);
+      P[(g.mbeg[c] + k) * g.N + p] = (float)exp(l - lse);
+    }
+  }
 }
 
 // Grouped maximize, one contraction per cell: rows = the cell's fine
@@ -261,15 +428,19 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
     if (c < 0) break;
     const int64_t q = g.ppos[p * g.m + i];
     const int64_t col = q - g.gbeg[c];
-    float cm = 0.0f;
+    double cm = 0.0;  // FP64, so its log ranks cells far down the tail
     for (int k = lane; k < g.mcnt[c]; k += 32) {
-      const float P = (float)exp(ll_of(c, q, k) - lse);
+      const double Pd = exp(ll_of(c, q, k) - lse);
+      const float P = (float)Pd;
       g.Pt[g.goff[c] + (int64_t)k * g.gcnt[c] + col] = (float)(P / phi_new);
       atomicAdd(g.T + g.mbeg[c] + k, P);
-      cm += P;
+      cm += Pd;
     }
     for (int o = 16; o > 0; o >>= 1) cm += __shfl_xor_sync(0xffffffffu, cm, o);
-    if (lane == 0) g.cmass[p * g.m + i] = cm;
+    if (lane == 0) {
+      g.cmass[p * g.m + i] = (float)cm;
+      if (g.lcmass) g.lcmass[p * g.m + i] = cm > 0.0 ? (float)log(cm) : -INFINITY;
+    }
   }
 }
 
@@ -425,6 +596,52 @@ cudaError_t launch_scatter_targets(const int32_t* cand, const float* cmass, int6
   cudaError_t e = cudaMemsetAsync(t, 0, sizeof(float) * N * n_cells, st);
   if (e != cudaSuccess) return e;
   scatter_targets_kernel<<<(unsigned)((N * m + 255) / 256), 256, 0, st>>>(cand, cmass, N, m, n_cells, t);
+  return cudaGetLastError();
+}
+
+__global__ void fill_f32_kernel(float* x, int64_t n, float v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+cudaError_t launch_log_targets(const TargetArgs& a, cudaStream_t st) {
+  const size_t smem = sizeof(double) * 16 * a.n_cells;
+  cudaError_t e = cudaFuncSetAttribute(log_targets_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  log_targets_kernel<<<(unsigned)((a.N + 15) / 16), 256, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_log_targets(const int32_t* cand, const float* lcmass, int64_t N, int m,
+                                      int n_cells, float* t, cudaStream_t st) {
+  const int64_t n = N * n_cells;
+  fill_f32_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(t, n,
+                                                                                     -INFINITY);
+  scatter_targets_kernel<<<(unsigned)((N * m + 255) / 256), 256, 0, st>>>(cand, lcmass, N, m,
+                                                                          n_cells, t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_select_topk(const float* probs, const float* log_keep, const int32_t* mcnt,
+                               int64_t N, int C, int top_k, int m, float mass_target,
+                               int32_t* cand, float* mass, cudaStream_t st) {
+  select_topk_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(probs, log_keep, mcnt, N, C, top_k,
+                                                              m, mass_target, cand, mass);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_audit(const AuditArgs& a, int64_t n_audit, cudaStream_t st) {
+  if (n_audit <= 0) return cudaSuccess;
+  audit_kernel<<<(unsigned)n_audit, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_proposed_resp(const GroupArgs& g, float* P, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(P, 0, sizeof(float) * g.N * g.R, st);
+  if (e != cudaSuccess) return e;
+  proposed_resp_kernel<<<(unsigned)((g.N + 7) / 8), 256, 0, st>>>(g, P);
   return cudaGetLastError();
 }
 

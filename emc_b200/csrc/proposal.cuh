@@ -16,6 +16,7 @@ struct TargetArgs {
   int n_cells;
   const int32_t* cell;     // [R] cell of every fine rotation
   const float* P;          // FP32 responsibilities [R][ldP] (FP32 path) or nullptr
+  const double* L64;       // log targets of FP32 contexts: the FP64 log-likelihood [R][ldP]
   int64_t ldP;
   const float* Y;          // otherwise from the mixed path's Y and lse
   int64_t ldY;
@@ -48,6 +49,7 @@ cudaError_t launch_select(const float* probs, const float* keep, int64_t N, int 
 // fine rotations are mbeg[c] .. mbeg[c]+mcnt[c]-1.
 struct GroupArgs {
   int64_t N, npa, MM;      // MM: row stride of Y (>= largest cell)
+  int64_t R;               // fine rotations (responsibility export)
   int n_cells, m, poisson;
   const int64_t* mbeg;
   const int32_t* mcnt;
@@ -74,6 +76,7 @@ struct GroupArgs {
   double* plogp;           // [N]
   float* new_scaling;      // [N]
   float* cmass;            // [N][m] responsibility mass of each candidate cell
+  float* lcmass;           // optional [N][m]: its natural log in FP64 (-inf when 0)
   int32_t* best_rot;       // [N] most probable rotation among the candidates
   float* best_p;           // [N] its responsibility
   // tile lists: mtiles (cell, member offset, pair offset) of the grouped
@@ -100,5 +103,41 @@ cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* s
 cudaError_t launch_p_split(const GroupArgs& g, const int32_t* cell_of, int64_t R, const float* T,
                            int64_t ldA, __half* Ahi, __half* Alo, cudaStream_t st);
 cudaError_t launch_group_compress(const GroupArgs& g, int64_t n_ctiles, cudaStream_t st);
+
+// lt[p][c] = natural log of cell c's responsibility mass, summed in FP64
+// (-inf when it is 0); t of TargetArgs receives it.
+cudaError_t launch_log_targets(const TargetArgs& a, cudaStream_t st);
+// The same after a proposed iteration from the candidates' log masses
+// (-inf outside the candidate cells).
+cudaError_t launch_scatter_log_targets(const int32_t* cand, const float* lcmass, int64_t N, int m,
+                                      int n_cells, float* t, cudaStream_t st);
+// Top-k selection: cells in order of log_keep (finite values) until they hold
+// at least top_k fine rotations, then cells in order of probs until the
+// probs total reaches mass_target; at most m; either input may be null.
+cudaError_t launch_select_topk(const float* probs, const float* log_keep, const int32_t* mcnt,
+                               int64_t N, int C, int top_k, int m, float mass_target,
+                               int32_t* cand, float* mass, cudaStream_t st);
+
+// Dense audit of sampled patterns (see audit_kernel): captured[a] = share of
+// audited pattern pat[a]'s responsibility on the fine rotations of its
+// candidate cells (cand [N][m]), from LL64 [R][ld] or Y [R][ld].
+struct AuditArgs {
+  int64_t R, ld;
+  int m, poisson;
+  const int64_t* pat;      // [n_audit] global pattern index
+  const int32_t* cand;     // [N][m]
+  const int32_t* cell;     // [R]
+  const double* LL64;      // FP32 contexts: log-likelihood, or nullptr ->
+  const float* Y;          // mixed: Y of the audit contraction
+  const float* scaling;    // [n_audit] phi used for LL (gaussian)
+  const double* rowstat;   // [R]
+  const double* patstat;   // [n_audit] gaussian: sum K^2
+  double gauss_inv;
+  float* captured;         // [n_audit]
+};
+cudaError_t launch_audit(const AuditArgs& a, int64_t n_audit, cudaStream_t st);
+// FP32 responsibilities [R][N] of the last proposed iteration (zero outside
+// each pattern's candidate cells).
+cudaError_t launch_proposed_resp(const GroupArgs& g, float* P, cudaStream_t st);
 
 }  // namespace emc

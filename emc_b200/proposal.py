@@ -42,6 +42,8 @@ def _bind():
         ("emc_net_gradients", [P, P, P, I64, P, P], C.c_int),
         ("emc_net_train_step", [P, P, P, I64, C.c_float, P], C.c_int),
         ("emc_net_last_error", [P], C.c_char_p),
+        ("emc_iterate_topk", [P, P, P, P, P], C.c_int),
+        ("emc_cell_log_mass", [P, P], C.c_int),
     ]:
         f = getattr(L, name)
         f.argtypes = args
@@ -51,8 +53,14 @@ def _bind():
 
 class ProposalStats(C.Structure):
     _fields_ = [("mean_mass", C.c_double), ("min_mass", C.c_double), ("pairs", C.c_int64),
-                ("evaluations", C.c_int64), ("fallback", C.c_int32), ("pad_", C.c_int32),
-                ("sum_plogp", C.c_double), ("total_loglik", C.c_double)]
+                ("evaluations", C.c_int64), ("fallback", C.c_int32), ("audited", C.c_int32),
+                ("sum_plogp", C.c_double), ("total_loglik", C.c_double),
+                ("audit_mean_captured", C.c_double), ("audit_min_captured", C.c_double)]
+
+
+class TopkConfig(C.Structure):
+    _fields_ = [("top_k", C.c_int32), ("max_cells", C.c_int32), ("mass_target", C.c_float),
+                ("audit_patterns", C.c_int32), ("min_captured", C.c_float), ("pad_", C.c_int32)]
 
 
 def assign_cells(q_fine, q_coarse, chunk=8192):
@@ -212,4 +220,37 @@ class LearnedProposal:
                                                None if keep is None else keep.data_ptr(),
                                                int(min_cells), int(max_cells), mass_target,
                                                keep_mass, threshold, C.byref(st)))
-        return {k: getattr(st, k) for k, _ in ProposalStats._fields_ if k != "pad_"}
+        return {k: getattr(st, k) for k, _ in ProposalStats._fields_}
+
+    def log_mass(self):
+        """Log-posterior mass of every cell in the last maximize (dense, or
+        proposed: -inf outside the candidate cells), [N][n_cells]."""
+        import torch
+        t = torch.empty((self.ctx.N, self.n_cells), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        self.ctx._c(lib().emc_cell_log_mass(self.ctx._h, t.data_ptr()))
+        return t
+
+    def iterate_topk(self, probs=None, log_keep=None, top_k=512, max_cells=32, mass_target=0.999,
+                     audit=0, min_captured=0.99):
+        """One proposed iteration of emc_iterate_topk: per pattern the cells
+        holding the best of its previous log-posterior until they hold top_k
+        fine rotations (log_keep, e.g. log_mass() of the previous iteration),
+        then the network's most probable cells up to a predicted mass of
+        mass_target (probs), at most max_cells; `audit` sampled patterns are
+        evaluated against every rotation and the dense iteration runs when one
+        of them holds less than min_captured of its responsibility."""
+        import torch
+        for t in (probs, log_keep):
+            if t is not None and (t.dtype != torch.float32 or tuple(t.shape) !=
+                                  (self.ctx.N, self.n_cells)):
+                raise ValueError("probs / log_keep must be float32 [N][n_cells] tensors")
+        torch.cuda.synchronize()
+        cfg = TopkConfig(int(top_k), int(max_cells), float(mass_target), int(audit),
+                         float(min_captured), 0)
+        st = ProposalStats()
+        self.ctx._c(lib().emc_iterate_topk(
+            self.ctx._h, None if probs is None else probs.contiguous().data_ptr(),
+            None if log_keep is None else log_keep.contiguous().data_ptr(), C.byref(cfg),
+            C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ProposalStats._fields_}

@@ -64,7 +64,8 @@ typedef enum {
   EMC_BUF_MODEL = 0,    /* float [side^3] */
   EMC_BUF_WEIGHT = 1,   /* float [side^3] weight grid of the last compress */
   EMC_BUF_SCALING = 2,  /* float [N] */
-  EMC_BUF_RESP = 3,     /* float [R][N] responsibilities after maximize */
+  EMC_BUF_RESP = 3,     /* float [R][N] responsibilities after maximize (after a proposed
+                           iteration: 0 outside each pattern's candidate cells; host copy only) */
   EMC_BUF_SLICES = 4,   /* float [R][Pa] expanded slices (FP32 path), Pa = active pixels */
   EMC_BUF_TOTALRESP = 5, /* float [R] T_r */
   EMC_BUF_ACCUM = 6,     /* float [2*side^3] insertion accumulators (model and weight sums)
@@ -88,7 +89,12 @@ emc_status emc_set_geometry(emc_context *ctx, const float *x, const float *y, co
                             const int32_t *mask);
 /* Unit quaternions [R][4] and rotation weights [R]. */
 emc_status emc_set_rotations(emc_context *ctx, const float *quaternions, const float *weights);
-/* Photon counts [N][side*side] (non-negative; the mixed path needs integers <= 2048). */
+/* Photon counts [N][side*side]: finite and non-negative (EMC_ERR_RANGE
+ * otherwise); the mixed path needs integers <= 2048.  A rejected upload
+ * leaves the context without patterns.  emc_set_model rejects NaN or
+ * infinite values, emc_set_scaling anything but finite positive numbers,
+ * emc_set_rotations non-finite quaternions or negative weights, and
+ * emc_set_geometry non-finite coordinates (all EMC_ERR_RANGE). */
 emc_status emc_set_patterns(emc_context *ctx, const float *counts);
 /* The same from photon lists (sparse patterns, CSR over patterns): pattern p's
  * entries are row_ptr[p] .. row_ptr[p+1]-1 (row_ptr[0] = 0, row_ptr[N] =
@@ -132,6 +138,22 @@ emc_status emc_device_buffer(emc_context *ctx, emc_buffer which, void **dptr, si
  * it can be called after each emc_iterate without draining the stream. */
 emc_status emc_set_profiling(emc_context *ctx, int on);
 emc_status emc_stage_times(emc_context *ctx, float ms[5]);
+/* Cap on the device memory this context allocates, in bytes (0: no cap; the
+ * default).  A call whose allocations would pass it fails with EMC_ERR_OOM
+ * before allocating; the context is then only good for emc_destroy, which
+ * frees what it holds.  EMC_ERR_ARG when the cap is below what is already
+ * held.  emc_memory_used: device bytes the context holds. */
+emc_status emc_set_memory_limit(emc_context *ctx, size_t bytes);
+size_t emc_memory_used(const emc_context *ctx);
+/* Checkpoint (emc.c:715-716 resumes from a model file at start_iteration;
+ * this keeps the whole state): model, weight grid and per-pattern scaling
+ * with the iteration number, in a raw little-endian file.  The model and the
+ * scaling are everything the next iteration reads, so a context loaded from
+ * the file continues exactly as the saved one would.  Loading needs the same
+ * side, pattern and rotation counts (EMC_ERR_RANGE otherwise); the
+ * likelihood, interpolation and precision may differ. */
+emc_status emc_save_state(emc_context *ctx, const char *path, int64_t iteration);
+emc_status emc_load_state(emc_context *ctx, const char *path, int64_t *iteration);
 /* Number of kernels this context has launched since creation. */
 int64_t emc_launch_count(const emc_context *ctx);
 /* cudaStream_t the context enqueues on. */
@@ -216,8 +238,11 @@ typedef struct {
   int64_t pairs;               /* (pattern, cell) pairs evaluated */
   int64_t evaluations;         /* (pattern, rotation) evaluations */
   int32_t fallback;            /* 1: the dense iteration ran instead */
-  int32_t pad_;
+  int32_t audited;             /* patterns evaluated against every rotation (emc_iterate_topk) */
   double sum_plogp, total_loglik;
+  /* share of each audited pattern's responsibility (against every rotation)
+   * that its candidate cells hold: mean and minimum over the audited patterns */
+  double audit_mean_captured, audit_min_captured;
 } emc_proposal_stats;
 
 /* cell[r] for every rotation (non-decreasing), n_cells cells. */
@@ -243,6 +268,40 @@ emc_status emc_iterate_proposed(emc_context *ctx, const float *cell_probs_device
                                 const float *keep_device, int32_t min_cells, int32_t max_cells,
                                 float mass_target, float keep_mass, float threshold,
                                 emc_proposal_stats *stats);
+
+/* The proposal of the configuration "top-k fine rotations evaluated from the
+ * coarse posterior, dense maximize when the captured responsibility falls
+ * below a bound":
+ *   - log_keep (optional, device [N][n_cells]): the log-posterior mass of
+ *     every cell in a previous iteration (emc_cell_log_mass); each pattern
+ *     takes its cells in that order (finite values only) until they hold at
+ *     least top_k fine rotations;
+ *   - cell_probs (optional, device [N][n_cells]): the proposal network's cell
+ *     posterior; cells are then added in its order until the candidates'
+ *     predicted mass reaches mass_target (every pattern gets at least one);
+ *   - at most max_cells cells per pattern;
+ *   - audit_patterns (0..128) patterns, an evenly strided sample shifted on
+ *     every call, are evaluated against every rotation after the expansion;
+ *     when one of them holds less than min_captured of its responsibility on
+ *     its candidate cells, the dense iteration runs instead (stats->fallback,
+ *     stats->audit_*).
+ * At least one of log_keep and cell_probs is given. */
+typedef struct {
+  int32_t top_k;
+  int32_t max_cells;
+  float mass_target;
+  int32_t audit_patterns;
+  float min_captured;
+  int32_t pad_;
+} emc_topk_config;
+emc_status emc_iterate_topk(emc_context *ctx, const float *cell_probs_device,
+                            const float *log_keep_device, const emc_topk_config *cfg,
+                            emc_proposal_stats *stats);
+/* t [N][n_cells] (device): natural log of each cell's responsibility mass in
+ * the last maximize (dense, or proposed: -inf outside the candidate cells),
+ * summed in FP64 so cells far down the tail are still ordered (-inf only
+ * below about 1e-308). */
+emc_status emc_cell_log_mass(emc_context *ctx, float *t_device);
 
 /* Proposal network: three 3x3 stride-2 convolutions (16, 32, 64 channels,
  * ReLU) and a fully connected layer to n_out logits, softmax.  BF16 weights

@@ -244,3 +244,151 @@ def test_proposed_iteration_with_every_cell_is_the_dense_iteration():
         assert st["evaluations"] == ctx.N * ctx.R
         assert rel(ctx.get_model(), m_dense) <= 1e-4
         assert rel(ctx.get_scaling(), s_dense) <= 1e-4
+
+
+def _select_topk(probs, log_keep, mcnt, top_k, m, mass_target):
+    """The candidate cells emc_iterate_topk takes: cells in order of log_keep
+    (finite values) until they hold at least top_k fine rotations, then
+    cells in order of probs until the (FP32) probs total of all taken cells
+    reaches mass_target (at least one cell), at most m."""
+    N, n_cells = (probs if probs is not None else log_keep).shape
+    sel = np.zeros((N, n_cells), bool)
+    for p in range(N):
+        tot, n, covered = np.float32(0), 0, 0
+        if log_keep is not None:
+            for k in np.argsort(-log_keep[p], kind="stable"):
+                if n >= m or covered >= top_k or not log_keep[p, k] > -np.inf:
+                    break
+                sel[p, k] = True
+                n += 1
+                covered += mcnt[k]
+                if probs is not None:
+                    tot = np.float32(tot + max(probs[p, k], np.float32(0)))
+        if probs is not None:
+            for k in np.argsort(-probs[p], kind="stable"):
+                if n >= m or (n > 0 and tot >= np.float32(mass_target)):
+                    break
+                if sel[p, k]:
+                    continue
+                sel[p, k] = True
+                n += 1
+                tot = np.float32(tot + max(probs[p, k], np.float32(0)))
+    return sel
+
+
+@pytest.mark.parametrize("prec,use_probs,use_keep,tol", [
+    ("fp32", True, True, 1e-5), ("mixed", True, True, 1e-4), ("mixed", False, True, 1e-4),
+    ("mixed", True, False, 1e-4)])
+def test_topk_iteration_matches_restricted_oracle(prec, use_probs, use_keep, tol):
+    """emc_iterate_topk (cells holding each pattern's best previous
+    log-posterior until 20 fine rotations are covered, then network cells up
+    to a predicted mass of 0.6, at most 9 of 60 uneven cells) against the
+    FP64 oracle restricted to the same candidates: model, scaling, the
+    exported responsibilities, and the log cell masses of the iteration."""
+    import torch
+
+    import emc_b200 as E
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    from oracle import oracle as O
+    from parity import oracle_cfg, resp_l1
+    d = W.make("tiny16")
+    q, w, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=1)
+    d = dict(d, q=q, w=w)
+    N = d["counts"].shape[0]
+    mcnt = np.bincount(cell, minlength=n_cells)
+    rng = np.random.default_rng(5)
+    z = rng.standard_normal((N, n_cells)) * 2.0
+    probs = np.exp(z - z.max(1, keepdims=True))
+    probs = (probs / probs.sum(1, keepdims=True)).astype(np.float32)
+    lk = (rng.standard_normal((N, n_cells)) * 30.0).astype(np.float32)
+    lk[rng.random((N, n_cells)) < 0.6] = -np.inf
+    lk[:2] = -np.inf  # patterns with no previous posterior at all
+    if not use_probs:
+        lk[:2, 0] = 0.0
+    sel = _select_topk(probs if use_probs else None, lk if use_keep else None, mcnt, 20, 9, 0.6)
+    allowed = sel[:, cell].T.astype(np.uint8)
+    cfg = oracle_cfg(d, "poisson", "nearest")
+    m_ref, s_ref, P_ref, st_ref = O.iterate(cfg, d["counts"], d["mask"], d["q"], d["w"], d["x"],
+                                            d["y"], d["z"], d["model0"], d["scaling0"],
+                                            want_resp=True, allowed=allowed)
+    t_ref = np.zeros((N, n_cells))
+    np.add.at(t_ref.T, cell, P_ref)
+    with make_ctx(d, "poisson", "nearest", prec) as ctx:
+        lp = LearnedProposal(ctx, cell, n_cells)
+        st = lp.iterate_topk(torch.from_numpy(probs).cuda() if use_probs else None,
+                             torch.from_numpy(lk).cuda() if use_keep else None, top_k=20,
+                             max_cells=9, mass_target=0.6)
+        assert st["fallback"] == 0 and st["audited"] == 0
+        assert st["evaluations"] == int(allowed.sum()) and st["pairs"] == int(sel.sum())
+        assert rel(ctx.get_model(), m_ref) <= tol, rel(ctx.get_model(), m_ref)
+        assert rel(ctx.get_scaling(), s_ref) <= tol
+        P = ctx.get_buffer(E.BUF_RESP)
+        assert resp_l1(P, P_ref) <= 10 * tol, resp_l1(P, P_ref)
+        assert (P[allowed == 0] == 0).all()
+        lm = lp.log_mass().cpu().numpy()
+        assert np.isneginf(lm[~sel]).all()
+        big = t_ref > 1e-30
+        assert np.abs(lm[big] - np.log(t_ref[big])).max() <= 1e-2
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_log_mass_of_a_dense_iteration(prec):
+    """emc_cell_log_mass after a dense maximize: log of the oracle's per-cell
+    responsibility mass, down the tail (cells with mass > 1e-200)."""
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    from oracle import oracle as O
+    from parity import oracle_cfg
+    d = W.make("tiny16")
+    q, w, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=1)
+    d = dict(d, q=q, w=w)
+    cfg = oracle_cfg(d, "poisson", "nearest")
+    _, _, P_ref, _ = O.iterate(cfg, d["counts"], d["mask"], d["q"], d["w"], d["x"], d["y"],
+                               d["z"], d["model0"], d["scaling0"], want_resp=True)
+    t_ref = np.zeros((d["counts"].shape[0], n_cells))
+    np.add.at(t_ref.T, cell, P_ref)
+    with make_ctx(d, "poisson", "nearest", prec) as ctx:
+        lp = LearnedProposal(ctx, cell, n_cells)
+        ctx.iterate()
+        lm = lp.log_mass().cpu().numpy()
+    big = t_ref > 1e-200
+    err = np.abs(lm[big] - np.log(t_ref[big]))
+    # relative errors of tail masses follow the log-likelihood's absolute error
+    assert err.max() <= (2e-3 if prec == "fp32" else 5e-2), err.max()
+    assert big.sum() > 0.5 * big.size
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_audit_triggers_the_dense_fallback(prec):
+    """With candidates drawn from the previous iteration's log-posterior, the
+    audited patterns keep their responsibility and the grouped stages run;
+    with every pattern handed another pattern's cells, the audit sees the
+    responsibility outside the candidates and the dense iteration runs (same
+    model as emc_iterate)."""
+    import torch
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    d = W.make("b200_64", n_patterns=600)
+    q, w, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=2)
+    d = dict(d, q=q, w=w)
+    with make_ctx(d, "poisson", "nearest", prec) as ctx:
+        lp = LearnedProposal(ctx, cell, n_cells)
+        for _ in range(3):
+            ctx.iterate()
+        lk = lp.log_mass()
+        m0, s0 = ctx.get_model(), ctx.get_scaling()
+        ctx.iterate()
+        m_dense = ctx.get_model()
+        ctx.set_model(m0)
+        ctx.set_scaling(s0)
+        st = lp.iterate_topk(None, lk, top_k=512, max_cells=16, audit=64, min_captured=0.99)
+        assert st["fallback"] == 0 and st["audited"] == 64, st
+        assert st["audit_min_captured"] >= 0.99, st
+        assert rel(ctx.get_model(), m_dense) < 1e-3
+        ctx.set_model(m0)
+        ctx.set_scaling(s0)
+        wrong = torch.roll(lk, shifts=1, dims=0)  # pattern p gets pattern p-1's cells
+        st = lp.iterate_topk(None, wrong, top_k=512, max_cells=16, audit=64, min_captured=0.99)
+        assert st["fallback"] == 1 and st["audit_min_captured"] < 0.99, st
+        assert rel(ctx.get_model(), m_dense) < 1e-5
