@@ -108,6 +108,7 @@ def lib():
             ("emc_model_save", [C.c_char_p, C.c_int, P], C.c_int),
             ("emc_autotune", [P, P, C.c_int32, P, P], C.c_int),
             ("emc_set_memory_limit", [P, C.c_size_t], C.c_int),
+            ("emc_get_resp_columns", [P, I64, P, P], C.c_int),
             ("emc_memory_used", [P], C.c_size_t),
             ("emc_save_state", [P, C.c_char_p, I64], C.c_int),
             ("emc_load_state", [P, C.c_char_p, P], C.c_int),
@@ -448,6 +449,14 @@ class Context:
         t = Tuning()
         self._c(lib().emc_autotune(self._h, _ptr(cand), len(cand), _ptr(ms), C.byref(t)))
         return (t.maximize_raster, t.compress_raster), ms
+
+    def resp_columns(self, patterns):
+        """emc_get_resp_columns: responsibilities [R][n] of the given patterns
+        in the last maximize (dense or proposed)."""
+        pat = np.ascontiguousarray(patterns, np.int64)
+        out = np.zeros((self.R, pat.size), np.float32)
+        self._c(lib().emc_get_resp_columns(self._h, pat.size, _ptr(pat), _ptr(out)))
+        return out
 
     def set_memory_limit(self, nbytes):
         """emc_set_memory_limit: cap on the device memory this context allocates."""

@@ -56,14 +56,70 @@ __global__ void scatter_photons_kernel(const int64_t* row_ptr, const int32_t* pi
 }
 
 __global__ void split_sum_kernel(const __half* hi, const __half* lo, int64_t R, int64_t ld,
-                                 int64_t npa, float* out) {
+                                 int64_t npa, const int32_t* rank, float* out) {
   const int64_t r = blockIdx.y;
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < npa;
        j += (int64_t)gridDim.x * blockDim.x)
-    out[r * npa + j] = __half2float(hi[r * ld + j]) + __half2float(lo[r * ld + j]);
+    out[r * npa + (rank ? rank[j] : j)] = __half2float(hi[r * ld + j]) + __half2float(lo[r * ld + j]);
+}
+
+// Responsibility columns of chosen patterns, out [R][n]:
+//   dense FP32 path: P itself ([R][N]);
+//   dense mixed path: exp(LL - lse) from Y (poisson LL, gaussian cross term);
+//   proposed iteration: over each pattern's candidate cells (out zeroed).
+__global__ void resp_cols_dense_kernel(const float* P, const float* Y, int64_t ld, int poisson,
+                                       const float* scaling, const double* rowstat,
+                                       const double* patstat, double gauss_inv, const double* lse,
+                                       int64_t R, const int64_t* cols, int64_t n, float* out) {
+  const int64_t total = R * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / n, a = e - r * n, p = cols[a];
+    if (P) {
+      out[e] = P[r * ld + p];
+      continue;
+    }
+    double ll = (double)Y[r * ld + p];
+    if (!poisson) {
+      const double phi = scaling[p];
+      ll = (ll * 2.0 / phi - rowstat[r] - patstat[p] / (phi * phi)) * gauss_inv;
+    }
+    out[e] = (float)exp(ll - lse[p]);
+  }
+}
+
+__global__ void resp_cols_proposed_kernel(const GroupArgs g, const int64_t* cols, int64_t n,
+                                          float* out) {
+  const int64_t a = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (a >= n) return;
+  const int64_t p = cols[a];
+  const double phi = g.scaling[p];
+  const double c1 = 2.0 * g.gauss_inv / phi,
+               c0 = g.poisson ? 0.0 : -g.patstat[p] / (phi * phi) * g.gauss_inv;
+  for (int i = 0; i < g.m; ++i) {
+    const int c = g.cand[p * g.m + i];
+    if (c < 0) break;
+    const int64_t q = g.ppos[p * g.m + i];
+    for (int k = lane; k < g.mcnt[c]; k += 32) {
+      const double y = (double)g.Y[q * g.MM + k];
+      const double l = g.poisson ? y : fma(y, c1, c0 - g.rowstat[g.mbeg[c] + k] * g.gauss_inv);
+      out[(g.mbeg[c] + k) * n + a] = (float)exp(l - g.lse[p]);
+    }
+  }
 }
 
 }  // namespace
+
+// The compress lists keep the responsibilities P_rp >= kListRel T_r: a
+// dropped entry moves its rotation's slice sum by less than 1e-12 (FP16 P'
+// of the dense contraction rounds entries below 2^-25 of the row to zero).
+// The row-sum sweep compacts P >= kListMinP first (rotations with T_r <=
+// 1e-10 are not inserted, emc_atomic.cu:128, so nothing kept is below it).
+constexpr float kListRel = 1e-12f;
+constexpr float kListMinP = 1e-30f;
+// Shared memory of the list compress: one FP32 per active pixel.
+constexpr int64_t kListMaxPixels = 51200;
 
 // Non-zero entries of a dense matrix as compressed rows (see build_rows).
 struct SparseRows {
@@ -89,7 +145,8 @@ struct emc_context {
   size_t mem_used = 0, mem_limit = 0;  // device bytes held; limit 0 = none
 
   // geometry (compact active pixels)
-  int32_t* d_pix = nullptr;
+  int32_t* d_pix = nullptr;   // detector pixel of every compact (active) pixel
+  int32_t* d_rank = nullptr;  // mixed: ascending position of every compact pixel
   int32_t* d_ins = nullptr;
   float *d_cx = nullptr, *d_cy = nullptr, *d_cz = nullptr;
   // rotations
@@ -156,6 +213,17 @@ struct emc_context {
           yc_cap = 0, pt_cap = 0, kg_cap = 0, a_ld = 0;
   double *d_lse_c = nullptr, *d_plogp_c = nullptr;
   float* d_lcmass = nullptr;  // [N][m] log responsibility mass of each candidate cell
+  // responsibility lists of the mixed compress: per rotation the patterns with
+  // a non-zero compress operand entry (offsets d_lrowoff [R+1]) and the entry
+  unsigned long long* d_lcount = nullptr;  // entries compacted by the row-sum sweep
+  int2* d_lcomp_rp = nullptr;              // their (rotation, pattern)
+  float* d_lcomp_P = nullptr;              // and P
+  int64_t lcomp_cap = 0, lcomp_cap2 = 0;
+  int64_t *d_lrowtot = nullptr, *d_lrowoff = nullptr, *d_lcursor = nullptr;
+  int32_t* d_lpat = nullptr;
+  float* d_lx = nullptr;
+  int64_t lcap = 0, lcap_x = 0, list_nnz = 0;
+  bool list_mode = false;  // this iteration's compress reads the lists
   GroupArgs last_group{};     // arguments of the last grouped iteration (responsibility export)
   // dense audit of sampled patterns in a proposed iteration
   int64_t* d_aud_pat = nullptr;
@@ -425,6 +493,9 @@ static emc_status alloc_work(emc_context* c) {
   c->tune.maximize_pair = c->Ppad >= 8192 ? 1 : 0;
   // the compress on pairs: 5% faster at 128^3 / 50k patterns (raster 2)
   c->tune.compress_pair = (c->Ppad >= 8192 && c->Npad >= 8192) ? 1 : 0;
+  // the compress from responsibility lists (a handful of non-zero entries
+  // per pattern once the posteriors are sharp) where its shared-memory slice fits
+  c->tune.compress_sparse = npa <= kListMaxPixels ? 1 : 0;
   if (c->tune.compress_pair) c->tune.compress_raster = 2;
   c->Rpad = round_up(R, 256);
   c->nrt = c->Rpad / 256;
@@ -472,6 +543,38 @@ emc_status emc_set_geometry(emc_context* c, const float* x, const float* y, cons
     }
   if (pix.empty()) return c->fail(EMC_ERR_ARG, "mask has no active pixel");
   c->npa = (int64_t)pix.size();
+  std::vector<int32_t> rank;
+  if (c->mixed) {
+    // The mixed path's operands list the active pixels along a Morton
+    // (Z-order) curve of the detector: consecutive pixels then form compact
+    // patches, whose voxels under any rotation lie close together, so the
+    // expansion's gathers and the insertion's atomics of a warp touch fewer
+    // cache sectors.  The pixel order of a contraction is free; rank[j] is
+    // pixel j's position in the ascending order, which the slice export uses.
+    auto morton = [](uint32_t x, uint32_t y) {
+      uint64_t k = 0;
+      for (int b = 0; b < 16; ++b)
+        k |= ((uint64_t)((x >> b) & 1u) << (2 * b)) | ((uint64_t)((y >> b) & 1u) << (2 * b + 1));
+      return k;
+    };
+    std::vector<int32_t> ord(pix.size());
+    for (size_t j = 0; j < ord.size(); ++j) ord[j] = (int32_t)j;
+    const int side = c->cfg.side;
+    std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
+      return morton(pix[a] % side, pix[a] / side) < morton(pix[b] % side, pix[b] / side);
+    });
+    auto permute = [&](auto& v) {
+      auto w = v;
+      for (size_t j = 0; j < ord.size(); ++j) w[j] = v[ord[j]];
+      v.swap(w);
+    };
+    permute(pix);
+    permute(ins);
+    permute(cx);
+    permute(cy);
+    permute(cz);
+    rank = ord;
+  }
   TRY(c->alloc(&c->d_pix, c->npa));
   TRY(c->alloc(&c->d_ins, c->npa));
   TRY(c->alloc(&c->d_cx, c->npa));
@@ -482,6 +585,10 @@ emc_status emc_set_geometry(emc_context* c, const float* x, const float* y, cons
   CK(c, cudaMemcpyAsync(c->d_cx, cx.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_cy, cy.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_cz, cz.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
+  if (!rank.empty()) {
+    TRY(c->alloc(&c->d_rank, c->npa));
+    CK(c, cudaMemcpyAsync(c->d_rank, rank.data(), 4 * c->npa, cudaMemcpyHostToDevice, c->st));
+  }
   TRY(alloc_work(c));
   CK(c, cudaStreamSynchronize(c->st));
   c->have_geom = true;
@@ -715,7 +822,24 @@ static CmpEpiArgs cmp_args(emc_context* c) {
 
 // After the maximize contraction: lse, new scaling and sum P log P per
 // pattern, T_r, the compress operand P / (T_r phi), and the stats sums.
-static emc_status mixed_resp_pass(emc_context* c) {
+// Grows a work buffer to hold at least `need` elements (contents not kept).
+template <class T>
+static emc_status grow(emc_context* c, T** p, int64_t& cap, int64_t need) {
+  if (need <= cap && *p) return EMC_OK;
+  if (*p) c->release(*p);
+  *p = nullptr;
+  cap = 0;
+  const int64_t n = need + need / 4 + 64;
+  TRY(c->alloc(p, n));
+  cap = n;
+  return EMC_OK;
+}
+
+
+static emc_status build_rows(emc_context* c, const float* M, int64_t rows, int64_t cols,
+                             SparseRows& s, bool with_aux);
+
+static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
   const int64_t N = c->N;
   RespArgs a{};
   a.N = N;
@@ -740,10 +864,67 @@ static emc_status mixed_resp_pass(emc_context* c) {
   a.Tpart = c->d_Tpart;
   a.T = c->d_T;
   a.P32 = nullptr;
-  CK(c, launch_resp_pass(a, c->st));
+  c->list_mode = false;
+  if (allow_lists && c->tune.compress_sparse && c->npa <= kListMaxPixels) {
+    // the compress operand as per-rotation lists of its non-zero entries:
+    // entries P >= kListMinP are compacted during the row-sum sweep, the host
+    // reads their count (one wait), a counting sort orders them by rotation
+    const int64_t R = c->R;
+    if (!c->d_lcount) {
+      TRY(c->alloc(&c->d_lcount, 1));
+      TRY(c->alloc(&c->d_lrowtot, R));
+      TRY(c->alloc(&c->d_lrowoff, R + 1));
+      TRY(c->alloc(&c->d_lcursor, R));
+    }
+    if (c->lcomp_cap < std::max<int64_t>(64 * N, (int64_t)1 << 20)) {
+      int64_t cap = c->lcomp_cap;
+      TRY(grow(c, &c->d_lcomp_rp, cap, std::max<int64_t>(64 * N, (int64_t)1 << 20)));
+      int64_t cap2 = c->lcomp_cap2;
+      TRY(grow(c, &c->d_lcomp_P, cap2, cap));
+      c->lcomp_cap = cap;
+      c->lcomp_cap2 = cap2;
+    }
+    CK(c, cudaMemsetAsync(c->d_lcount, 0, sizeof(unsigned long long), c->st));
+    a.list_count = c->d_lcount;
+    a.list_cap = c->lcomp_cap;
+    a.list_rp = c->d_lcomp_rp;
+    a.list_P = c->d_lcomp_P;
+    a.list_min = kListMinP;
+    CK(c, launch_resp_rowsums(a, c->st));
+    unsigned long long* hn = c->pinned<unsigned long long>(7, 1);
+    if (!hn) return c->fail(EMC_ERR_OOM, "pinned host staging");
+    CK(c, cudaMemcpyAsync(hn, c->d_lcount, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    c->list_nnz = (int64_t)*hn;
+    if (c->list_nnz <= c->lcomp_cap) {
+      TRY(grow(c, &c->d_lpat, c->lcap, c->list_nnz + 1));
+      int64_t cap = c->lcap_x;
+      TRY(grow(c, &c->d_lx, cap, c->list_nnz + 1));
+      c->lcap_x = cap;
+      CK(c, launch_list_from_compact(a, c->list_nnz, kListRel, c->d_lrowtot, c->d_lcursor,
+                                     c->d_lrowoff, c->d_lpat, c->d_lx, c->st));
+      c->list_mode = true;
+      c->launches += 6;  // combine, row sums, T, count, scan, fill
+    } else {
+      // more entries than the compaction holds: the dense operand this time,
+      // room for them next time
+      CK(c, launch_resp_write(a, c->st));
+      int64_t cap = c->lcomp_cap;
+      TRY(grow(c, &c->d_lcomp_rp, cap, c->list_nnz));
+      int64_t cap2 = c->lcomp_cap2;
+      TRY(grow(c, &c->d_lcomp_P, cap2, cap));
+      c->lcomp_cap = cap;
+      c->lcomp_cap2 = cap2;
+      c->launches += 3;
+    }
+  } else {
+    CK(c, launch_resp_pass(a, c->st));
+    c->launches += 3;  // combine, 2 sweeps
+  }
   CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
   CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
-  c->launches += 5;  // combine, 2 sweeps, 2 sums
+  c->launches += 2;
   return EMC_OK;
 }
 
@@ -968,12 +1149,25 @@ emc_status emc_compress_insert(emc_context* c) {
     c->launches += 2;
   } else {
     CmpEpiArgs e = cmp_args(c);
-    if (c->tune.compress_pair)
+    if (c->list_mode) {
+      // responsibility lists x the counts' photon lists (built once per upload)
+      if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
+      ListCmpArgs la{};
+      la.rowoff = c->d_lrowoff;
+      la.pat = c->d_lpat;
+      la.xv = c->d_lx;
+      la.kptr = c->csr.ptr;
+      la.kidx = c->csr.idx;
+      la.kval = c->csr.val;
+      la.e = e;
+      CK(c, launch_list_compress(la, c->st));
+    } else if (c->tune.compress_pair) {
       CK(c, launch_compress_pair_tc(c->tmPhi, c->tmPlo, c->tmKt128, c->Rpad, c->Ppad, c->Npad, e,
                                     c->d_status, c->num_sms, c->st, c->tune.compress_raster));
-    else
-    CK(c, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
-                             c->d_status, c->num_sms, c->st, c->tune.compress_raster));
+    } else {
+      CK(c, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
+                               c->d_status, c->num_sms, c->st, c->tune.compress_raster));
+    }
     c->launches += 1;
   }
   c->mark(4);
@@ -1060,8 +1254,9 @@ emc_status emc_set_tuning(emc_context* c, const emc_tuning* t) {
       (t->maximize_sparse != 0 && t->maximize_sparse != 1) ||
       (t->compress_sparse != 0 && t->compress_sparse != 1))
     return EMC_ERR_ARG;
-  if (t->compress_sparse && c->mixed)
-    return c->fail(EMC_ERR_UNSUPPORTED, "the photon-list slice sums are an FP32 form");
+  if (t->compress_sparse && c->mixed && c->npa > kListMaxPixels)
+    return c->fail(EMC_ERR_UNSUPPORTED, "responsibility lists need at most %lld active pixels",
+                   (long long)kListMaxPixels);
   if (t->maximize_sparse && (c->mixed || c->gauss))
     return c->fail(EMC_ERR_UNSUPPORTED, "the photon-list log-likelihood is an FP32 poisson form");
   c->tune = *t;
@@ -1295,6 +1490,47 @@ emc_status emc_load_state(emc_context* c, const char* path, int64_t* iteration) 
   return EMC_OK;
 }
 
+emc_status emc_get_resp_columns(emc_context* c, int64_t n, const int64_t* patterns, float* out) {
+  if (!c || n < 1 || !patterns || !out) return EMC_ERR_ARG;
+  for (int64_t a = 0; a < n; ++a)
+    if (patterns[a] < 0 || patterns[a] >= c->N) return c->fail(EMC_ERR_ARG, "pattern out of range");
+  if (c->resp_source == 0 || c->stage == 1) return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+  if (c->mixed && c->resp_source == 1 && c->stage != 2 && c->stage != 0)
+    return c->fail(EMC_ERR_STATE, "no responsibilities yet");
+  TRY(check_status(c));
+  const int64_t R = c->R;
+  int64_t* d_cols = nullptr;
+  float* d_out = nullptr;
+  cudaError_t e = cudaMalloc(&d_cols, sizeof(int64_t) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(float) * R * n);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_cols, patterns, sizeof(int64_t) * n, cudaMemcpyHostToDevice, c->st);
+  if (e == cudaSuccess && c->resp_source == 2) {
+    e = cudaMemsetAsync(d_out, 0, sizeof(float) * R * n, c->st);
+    if (e == cudaSuccess) {
+      resp_cols_proposed_kernel<<<(unsigned)((n + 7) / 8), 256, 0, c->st>>>(c->last_group, d_cols,
+                                                                            n, d_out);
+      e = cudaGetLastError();
+    }
+  } else if (e == cudaSuccess) {
+    const unsigned grid = (unsigned)std::min<int64_t>((R * n + 255) / 256, 8192);
+    if (!c->mixed)
+      resp_cols_dense_kernel<<<grid, 256, 0, c->st>>>(c->d_LL, nullptr, c->N, 0, nullptr, nullptr,
+                                                      nullptr, 0.0, nullptr, R, d_cols, n, d_out);
+    else
+      resp_cols_dense_kernel<<<grid, 256, 0, c->st>>>(
+          nullptr, c->d_Y, c->Npad, c->gauss ? 0 : 1, c->d_scaling_prev, c->d_rowstat, c->d_patsq,
+          gauss_inv(c), c->d_lse, R, d_cols, n, d_out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, d_out, sizeof(float) * R * n, cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  cudaFree(d_cols);
+  cudaFree(d_out);
+  return c->cuda(e, "emc_get_resp_columns");
+}
+
 emc_status emc_device_buffer(emc_context* c, emc_buffer which, void** dptr, size_t* bytes) {
   if (!c || !dptr) return EMC_ERR_ARG;
   void* p = nullptr;
@@ -1364,12 +1600,12 @@ emc_status emc_get_buffer(emc_context* c, emc_buffer which, void* host, size_t b
       e = launch_resp_export(a, tmp, c->st);
     } else {
       split_sum_kernel<<<dim3(8, (unsigned)(c->R < 65535 ? c->R : 65535)), 256, 0, c->st>>>(
-          c->d_Bhi, c->d_Blo, c->R, c->Ppad, c->npa, tmp);
+          c->d_Bhi, c->d_Blo, c->R, c->Ppad, c->npa, c->d_rank, tmp);
       e = cudaGetLastError();
       for (int64_t r0 = 65535; r0 < c->R && e == cudaSuccess; r0 += 65535) {
         const int64_t rows = c->R - r0 < 65535 ? c->R - r0 : 65535;
         split_sum_kernel<<<dim3(8, (unsigned)rows), 256, 0, c->st>>>(
-            c->d_Bhi + r0 * c->Ppad, c->d_Blo + r0 * c->Ppad, rows, c->Ppad, c->npa,
+            c->d_Bhi + r0 * c->Ppad, c->d_Blo + r0 * c->Ppad, rows, c->Ppad, c->npa, c->d_rank,
             tmp + r0 * c->npa);
         e = cudaGetLastError();
       }
@@ -1470,18 +1706,6 @@ emc_status emc_cell_targets(emc_context* c, float* t) {
 
 }  // extern "C"
 
-// Grows a proposal buffer to hold at least `need` elements (contents not kept).
-template <class T>
-static emc_status grow(emc_context* c, T** p, int64_t& cap, int64_t need) {
-  if (need <= cap && *p) return EMC_OK;
-  if (*p) c->release(*p);
-  *p = nullptr;
-  cap = 0;
-  const int64_t n = need + need / 4 + 64;
-  TRY(c->alloc(p, n));
-  cap = n;
-  return EMC_OK;
-}
 
 extern "C" {
 
@@ -1885,6 +2109,41 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
                                      c->num_sms, c->st));
     c->mark(2);
     CK(c, launch_group_softmax(g, c->st));
+    if (c->tune.compress_sparse && c->npa <= kListMaxPixels) {
+      // compress from responsibility lists, as the dense mixed iteration does
+      if (!c->d_lrowoff) {
+        TRY(c->alloc(&c->d_lrowtot, R));
+        TRY(c->alloc(&c->d_lrowoff, R + 1));
+      }
+      if (!c->d_lcursor) TRY(c->alloc(&c->d_lcursor, R));
+      CK(c, launch_group_list_count(g, kListRel, c->d_lrowtot, c->st));
+      CK(c, launch_list_rowscan(c->d_lrowtot, R, c->d_lrowoff, c->st));
+      int64_t* hn = c->pinned<int64_t>(7, 1);
+      if (!hn) return c->fail(EMC_ERR_OOM, "pinned host staging");
+      CK(c, cudaMemcpyAsync(hn, c->d_lrowoff + R, sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
+      CK(c, cudaStreamSynchronize(c->st));
+      c->list_nnz = *hn;
+      TRY(grow(c, &c->d_lpat, c->lcap, c->list_nnz + 1));
+      int64_t cap = c->lcap_x;
+      TRY(grow(c, &c->d_lx, cap, c->list_nnz + 1));
+      c->lcap_x = cap;
+      CK(c, launch_group_list_fill(g, kListRel, c->d_lcursor, c->d_lrowoff, c->d_lpat, c->d_lx,
+                                   c->st));
+      if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
+      c->mark(3);
+      CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
+      ListCmpArgs la{};
+      la.rowoff = c->d_lrowoff;
+      la.pat = c->d_lpat;
+      la.xv = c->d_lx;
+      la.kptr = c->csr.ptr;
+      la.kidx = c->csr.idx;
+      la.kval = c->csr.val;
+      la.e = cmp_args(c);
+      la.e.Tskip = nullptr;  // the proposed iteration's own T_r
+      CK(c, launch_list_compress(la, c->st));
+      launches = 7;  // gather (2), contraction, softmax, count + scan, fill, compress
+    } else {
     CK(c, launch_p_split(g, c->d_cell, R, c->d_T, c->a_ld, c->d_Ahi, c->d_Alo, c->st));
     c->mark(3);
     CK(c, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, c->st));
@@ -1905,6 +2164,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     CK(c, launch_group_compress_tc(tmAhi, tmAlo, tmKg64, n_gct, ce, c->d_status,
                                    c->num_sms, c->st));
     launches = 6;  // gather (2), contraction, softmax, split, contraction
+    }
   } else {
     c->mark(1);
     CK(c, launch_group_maximize(g, (int64_t)mt.size(), c->st));
@@ -1957,7 +2217,8 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
 emc_status emc_iterate_topk(emc_context* c, const float* probs, const float* log_keep,
                             const emc_topk_config* cfg, emc_proposal_stats* stats) {
   if (!c || !cfg || (!probs && !log_keep) || cfg->top_k < 1 || cfg->max_cells < 1 ||
-      cfg->audit_patterns < 0 || cfg->audit_patterns > 128 || !(cfg->min_captured <= 1.0f))
+      cfg->audit_patterns < 0 || cfg->audit_patterns > 128 || !(cfg->min_captured <= 1.0f) ||
+      !(cfg->keep_tail >= 0.0f && cfg->keep_tail < 1.0f))
     return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
   const int32_t m = std::min<int32_t>(cfg->max_cells, c->n_cells);
@@ -1968,7 +2229,7 @@ emc_status emc_iterate_topk(emc_context* c, const float* probs, const float* log
   pl.min_captured = cfg->min_captured;
   return run_proposed(c, pl, [&]() {
     return launch_select_topk(probs, log_keep, c->d_mcnt, c->N, c->n_cells, cfg->top_k, m,
-                              cfg->mass_target, c->d_cand, c->d_mass, c->st);
+                              cfg->mass_target, cfg->keep_tail, c->d_cand, c->d_mass, c->st);
   }, stats);
 }
 
@@ -2212,7 +2473,7 @@ emc_status emc_batch_iterate(emc_batch* b) {
     BCK(b, launch_batch_maximize_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];
-    BTRY(b, c, mixed_resp_pass(c));
+    BTRY(b, c, mixed_resp_pass(c, false));
     BCK(b, cudaMemcpyAsync(c->d_Tskip, c->d_T, sizeof(float) * c->R, cudaMemcpyDeviceToDevice, b->st));
     c->resp_source = 1;
     c->stage = 2;

@@ -13,6 +13,7 @@
 // FP32 accumulators in TMEM let the epilogue of tile i overlap the MMAs of
 // tile i+1.  Every mbarrier wait is bounded; on expiry the kernel records the
 // site in TcStatus, drains its copies and MMAs, frees TMEM and returns.
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 #include <type_traits>
@@ -1434,11 +1435,37 @@ __global__ void __launch_bounds__(kSweepThreads, 4) rowsum_kernel(const RespArgs
     for (int u = 0; u < 4; ++u) {
       const int64_t r = r0 + i0 + u;
       t[u] = 0.0f;
+      float P[4] = {0.f, 0.f, 0.f, 0.f};
       if (r < a.R && any) {
         const double rs = POISSON ? 0.0 : a.rowstat[r] * a.gauss_inv;
-        float P[4];
         probs_from<POISSON>(k, y[u], rs, P);
         t[u] = (P[0] + P[1]) + (P[2] + P[3]);
+      }
+      if (a.list_count) {
+        // append the entries >= list_min: one atomic per warp and row
+        int n = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) n += (k.ok[j] && P[j] >= a.list_min) ? 1 : 0;
+        int inc = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += v;
+        }
+        const int tot = __shfl_sync(0xffffffffu, inc, 31);
+        unsigned long long base = 0;
+        if (lane == 31 && tot > 0) base = atomicAdd(a.list_count, (unsigned long long)tot);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        int64_t pos = (int64_t)base + inc - n;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (k.ok[j] && P[j] >= a.list_min) {
+            if (pos < a.list_cap) {
+              a.list_rp[pos] = make_int2((int)r, (int)(p0 + j));
+              a.list_P[pos] = P[j];
+            }
+            ++pos;
+          }
       }
     }
 #pragma unroll
@@ -1521,6 +1548,115 @@ __global__ void __launch_bounds__(kSweepThreads, 4) write_kernel(const RespArgs 
       for (int j = 0; j < 4; ++j)
         if (k.ok[j]) a.P32[r * a.N + p0 + j] = P[j];
     }
+    }
+  }
+}
+
+// ------------------------------------------------ responsibility lists --
+// The compress operand as lists: for every rotation r the patterns p with
+// P_rp >= list_min and x_rp = P_rp / (T_r phi_p) (the value write_kernel
+// stores in P').  Posteriors are sharp, so there are a few per pattern
+// against R per pattern in P'.  rowsum_kernel compacts the entries while it
+// sums the rows; a counting sort orders them by rotation.
+
+// rowoff[0..R] = exclusive prefix sums of rowtot; one block of 1024 threads,
+// each with a contiguous run of rows.
+__global__ void __launch_bounds__(1024) list_rowscan_kernel(const int64_t* rowtot, int64_t R,
+                                                            int64_t* rowoff) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t chunk = (R + 1023) / 1024, beg = t * chunk, end = beg + chunk < R ? beg + chunk : R;
+  int64_t s = 0;
+  for (int64_t r = beg; r < end; ++r) s += rowtot[r];
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int64_t v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int64_t run = part[t] - s;
+  for (int64_t r = beg; r < end; ++r) {
+    rowoff[r] = run;
+    run += rowtot[r];
+  }
+  if (t == 1023) rowoff[R] = part[1023];
+}
+
+// T_r from the row-sum partials (FP64 sum in pattern-block order, as
+// write_kernel forms it).
+__global__ void finish_T_kernel(const float* Tpart, int64_t nblk, int64_t R, float* T) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  double t = 0.0;
+  for (int64_t b = 0; b < nblk; ++b) t += Tpart[b * R + r];
+  T[r] = (float)t;
+}
+
+// Counting sort of the compacted entries by rotation: STEP 0 counts per
+// rotation, STEP 1 writes (pattern, x) at rowoff[r] + cursor.
+// Entries below rel_min T_r are dropped: each moves its rotation's slice sum
+// by less than rel_min.
+template <int STEP>
+__global__ void compact_sort_kernel(const int2* rp, const float* Pv, int64_t n, const float* T,
+                                    const float* new_scaling, float rel_min,
+                                    unsigned long long* cnt, const int64_t* rowoff, int32_t* pat,
+                                    float* xv) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int2 v = rp[e];
+    const float Tr = T[v.x], P = Pv[e];
+    if (!(Tr > 0.0f) || !(P >= rel_min * Tr)) continue;
+    if (STEP == 0) {
+      atomicAdd(cnt + v.x, 1ull);
+    } else {
+      const int64_t pos = rowoff[v.x] + (int64_t)atomicAdd(cnt + v.x, 1ull);
+      pat[pos] = v.y;
+      xv[pos] = P / Tr / new_scaling[v.y];
+    }
+  }
+}
+
+// Compress from the lists: one block per rotation.  U_r / T_r over the active
+// pixels is accumulated in shared memory from the listed patterns' photon
+// lists (x times each non-zero count), then inserted exactly as the dense
+// contraction's epilogue does (EpiCmp).
+__global__ void __launch_bounds__(256) list_compress_kernel(const ListCmpArgs a) {
+  extern __shared__ float Us[];  // [npa]
+  const int64_t r = blockIdx.x;
+  const CmpEpiArgs& e = a.e;
+  const float T = e.T[r];
+  if (!((e.Tskip ? e.Tskip[r] : T) > 1e-10f) || !(T > 0.0f)) return;  // emc_atomic.cu:128
+  for (int64_t j = threadIdx.x; j < e.npa; j += blockDim.x) Us[j] = 0.0f;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int64_t q = a.rowoff[r] + w; q < a.rowoff[r + 1]; q += blockDim.x >> 5) {
+    const int64_t p = a.pat[q];
+    const float x = a.xv[q];
+    for (int64_t t = a.kptr[p] + lane; t < a.kptr[p + 1]; t += 32)
+      atomicAdd(&Us[a.kidx[t]], x * a.kval[t]);
+  }
+  __syncthreads();
+  const float wT = e.rotw[r] * T;
+  float m[9];
+  emc_voxel::rotation_matrix(e.quat + 4 * r, m);
+  for (int64_t j = threadIdx.x; j < e.npa; j += blockDim.x) {
+    if (e.ins[j] != 1) continue;
+    float u[3];
+    emc_voxel::position(m, e.side, e.cx[j], e.cy[j], e.cz[j], u);
+    const float val = Us[j] * wT;
+    if (e.interp == 0) {
+      int64_t vox;
+      if (emc_voxel::nearest(u, e.side, 0, &vox)) red_add_v2(e.acc + vox, val, wT);
+    } else {
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) {
+        int64_t vox;
+        float wc;
+        if (!emc_voxel::trilinear_corner(u, e.side, cc, &vox, &wc) || wc == 0.0f) continue;
+        red_add_v2(e.acc + vox, wc * val, wc * wT);
+      }
     }
   }
 }
@@ -1749,7 +1885,7 @@ cudaError_t launch_batch_compress_tc(const TmapSet<kMaxBatch>& maps, int64_t n_t
   return run_gemm<2, 1, 3, false, kCompressBK>(maps, n_tiles, 1, 0, epi, status, num_sms, st);
 }
 
-cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {
+cudaError_t launch_resp_rowsums(RespArgs& a, cudaStream_t st) {
   combine_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, st>>>(a);
   const int64_t nblk = (a.N + kSweepPatterns - 1) / kSweepPatterns;
   const int64_t rblk = (a.R + kSweepRows - 1) / kSweepRows;
@@ -1757,11 +1893,58 @@ cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {
     rowsum_kernel<true><<<dim3((unsigned)nblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a);
   else
     rowsum_kernel<false><<<dim3((unsigned)nblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_resp_write(RespArgs& a, cudaStream_t st) {
+  const int64_t nblk = (a.N + kSweepPatterns - 1) / kSweepPatterns;
+  const int64_t rblk = (a.R + kSweepRows - 1) / kSweepRows;
   const int64_t wblk = (a.ldP + kSweepPatterns - 1) / kSweepPatterns;
   if (a.poisson)
     write_kernel<true><<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
   else
     write_kernel<false><<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st) {
+  cudaError_t e = launch_resp_rowsums(a, st);
+  return e == cudaSuccess ? launch_resp_write(a, st) : e;
+}
+
+int64_t resp_list_blocks(int64_t N) { return (N + kSweepPatterns - 1) / kSweepPatterns; }
+
+cudaError_t launch_list_rowscan(const int64_t* rowtot, int64_t R, int64_t* rowoff,
+                                cudaStream_t st) {
+  list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, R, rowoff);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int64_t* rowtot,
+                                     int64_t* cursor, int64_t* rowoff, int32_t* pat, float* xv,
+                                     cudaStream_t st) {
+  const int64_t nblk = resp_list_blocks(a.N);
+  finish_T_kernel<<<(unsigned)((a.R + 255) / 256), 256, 0, st>>>(a.Tpart, nblk, a.R, a.T);
+  cudaError_t e = cudaMemsetAsync(rowtot, 0, sizeof(int64_t) * a.R, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, sizeof(int64_t) * a.R, st);
+  if (e != cudaSuccess) return e;
+  const unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256 + 1, 4096);
+  compact_sort_kernel<0><<<g, 256, 0, st>>>(a.list_rp, a.list_P, n, a.T, a.new_scaling, rel_min,
+                                            reinterpret_cast<unsigned long long*>(rowtot),
+                                            nullptr, nullptr, nullptr);
+  list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, a.R, rowoff);
+  compact_sort_kernel<1><<<g, 256, 0, st>>>(a.list_rp, a.list_P, n, a.T, a.new_scaling, rel_min,
+                                            reinterpret_cast<unsigned long long*>(cursor), rowoff,
+                                            pat, xv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_list_compress(const ListCmpArgs& a, cudaStream_t st) {
+  const size_t smem = sizeof(float) * (size_t)a.e.npa;
+  cudaError_t e = cudaFuncSetAttribute(list_compress_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (a.e.R > 0) list_compress_kernel<<<(unsigned)a.e.R, 256, smem, st>>>(a);
   return cudaGetLastError();
 }
 

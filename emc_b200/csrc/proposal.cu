@@ -73,40 +73,55 @@ __global__ void __launch_bounds__(256) targets_kernel(const TargetArgs a) {
     for (int c = w; c < a.n_cells; c += 8) a.t[p * a.n_cells + c] = tc[c * 32 + lane];
 }
 
-// lt[p][c] = log of the responsibility mass of cell c (natural log, -inf when
-// it is 0 in FP64): the same sums as targets_kernel in FP64, so the ranking of
-// cells holding 1e-300 of a pattern's mass is still defined.  16 patterns per
-// block (tid & 15), 16 rotation lanes (tid >> 4), FP64 shared-memory sums.
+// Largest of *addr and v for floats (ordered through their bit patterns:
+// atomicMax on the signed bits of non-negative values, atomicMin on the
+// unsigned bits of negative ones).
+__device__ __forceinline__ void atomic_max_f32(float* addr, float v) {
+  if (__float_as_int(v) >= 0)
+    atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
+  else
+    atomicMin(reinterpret_cast<unsigned int*>(addr), __float_as_uint(v));
+}
+
+// lt[p][c] = natural log of the responsibility mass of cell c, in the log
+// domain (cell maximum, then a FP64 sum of exponentials relative to it), so
+// every cell is ranked however far down the tail it lies.  16 patterns per
+// block (tid & 15), 16 rotation lanes (tid >> 4); two passes over the
+// rotations (maximum, then sums) through shared memory.
 __global__ void __launch_bounds__(256) log_targets_kernel(const TargetArgs a) {
-  extern __shared__ double tcd[];  // [n_cells][16]
+  extern __shared__ double tcd[];  // [n_cells][16] sums, then [n_cells][16] float maxima
+  float* tcm = reinterpret_cast<float*>(tcd + a.n_cells * 16);
   const int pl = threadIdx.x & 15, rl = threadIdx.x >> 4;
   const int64_t p = (int64_t)blockIdx.x * 16 + pl;
-  for (int i = threadIdx.x; i < a.n_cells * 16; i += blockDim.x) tcd[i] = 0.0;
+  for (int i = threadIdx.x; i < a.n_cells * 16; i += blockDim.x) {
+    tcd[i] = 0.0;
+    tcm[i] = -INFINITY;
+  }
+  __syncthreads();
+  auto ll_of = [&](int64_t r) -> double {  // log-likelihood (FP32 path: minus lse)
+    if (a.L64) return a.L64[r * a.ldP + p];
+    if (a.P) return log((double)a.P[r * a.ldP + p]);
+    const float y = a.Y[r * a.ldY + p];
+    if (a.poisson) return (double)y;
+    const double phi = a.scaling[p];
+    return ((double)y * 2.0 / phi - a.rowstat[r] - a.patstat[p] / (phi * phi)) * a.gauss_inv;
+  };
+  const double lse = a.P ? 0.0 : a.lse[p < a.N ? p : 0];
+  if (p < a.N)
+    for (int64_t r = rl; r < a.R; r += 16) atomic_max_f32(&tcm[a.cell[r] * 16 + pl], (float)ll_of(r));
   __syncthreads();
   if (p < a.N)
     for (int64_t r = rl; r < a.R; r += 16) {
-      double ll;
-      if (a.L64) {
-        ll = a.L64[r * a.ldP + p] - a.lse[p];
-      } else if (a.P) {
-        ll = log((double)a.P[r * a.ldP + p]);
-      } else {
-        const float y = a.Y[r * a.ldY + p];
-        if (a.poisson) {
-          ll = (double)y;
-        } else {
-          const double phi = a.scaling[p];
-          ll = ((double)y * 2.0 / phi - a.rowstat[r] - a.patstat[p] / (phi * phi)) * a.gauss_inv;
-        }
-        ll -= a.lse[p];
-      }
-      atomicAdd(&tcd[a.cell[r] * 16 + pl], exp(ll));
+      const int k = a.cell[r] * 16 + pl;
+      atomicAdd(&tcd[k], exp(ll_of(r) - (double)tcm[k]));
     }
   __syncthreads();
   if (p < a.N)
     for (int c = rl; c < a.n_cells; c += 16) {
-      const double m = tcd[c * 16 + pl];
-      a.t[p * a.n_cells + c] = m > 0.0 ? (float)log(m) : -INFINITY;
+      const double sum = tcd[c * 16 + pl];
+      const float mx = tcm[c * 16 + pl];
+      a.t[p * a.n_cells + c] =
+          (sum > 0.0 && mx > -INFINITY) ? (float)((double)mx + log(sum) - lse) : -INFINITY;
     }
 }
 
@@ -179,13 +194,14 @@ __global__ void select_kernel(const float* probs, const float* keep, int64_t N, 
 
 // Top-k selection, one warp per pattern.  With log_keep (the log-posterior
 // mass of every cell in a previous iteration): cells in order of it (finite
-// values only) until they hold at least top_k fine rotations.  Then, with
+// values only) until they hold at least top_k fine rotations and, with
+// keep_tail > 0, all but keep_tail of that posterior.  Then, with
 // probs (a predicted cell posterior): cells in order of probs until the probs
 // total of everything taken reaches mass_target.  At most m cells; unused
 // slots -1; mass[p] = the probs total of the taken cells (1 without probs).
 __global__ void select_topk_kernel(const float* probs, const float* log_keep, const int32_t* mcnt,
                                    int64_t N, int C, int top_k, int m, float mass_target,
-                                   int32_t* cand, float* mass) {
+                                   float keep_tail, int32_t* cand, float* mass) {
   const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (p >= N) return;
@@ -195,7 +211,8 @@ __global__ void select_topk_kernel(const float* probs, const float* log_keep, co
   if (log_keep) {
     const float* krow = log_keep + p * C;
     int64_t covered = 0;
-    for (; s < m && covered < top_k; ++s) {
+    double held = 0.0;  // previous posterior mass of the taken cells
+    for (; s < m && (covered < top_k || (keep_tail > 0.0f && held < 1.0 - keep_tail)); ++s) {
       float best;
       int bi;
       warp_argmax(krow, C, taken, lane, best, bi);
@@ -203,6 +220,7 @@ __global__ void select_topk_kernel(const float* probs, const float* log_keep, co
       if ((bi & 31) == lane) taken |= 1u << (bi >> 5);
       if (lane == 0) cand[p * m + s] = bi;
       covered += mcnt[bi];
+      held += exp((double)best);
       if (probs) {
         const float v = probs[p * C + bi];
         tot += v > 0.0f ? v : 0.0f;
@@ -428,18 +446,73 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
     if (c < 0) break;
     const int64_t q = g.ppos[p * g.m + i];
     const int64_t col = q - g.gbeg[c];
-    double cm = 0.0;  // FP64, so its log ranks cells far down the tail
+    // the cell's mass in the log domain (its largest LL, then the sum
+    // relative to it), so cells far down the tail are still ranked
+    double cmx = -INFINITY;
+    if (g.lcmass) {
+      for (int k = lane; k < g.mcnt[c]; k += 32) cmx = fmax(cmx, ll_of(c, q, k));
+      for (int o = 16; o > 0; o >>= 1) cmx = fmax(cmx, __shfl_xor_sync(0xffffffffu, cmx, o));
+    }
+    float cm = 0.0f;
+    double crel = 0.0;
     for (int k = lane; k < g.mcnt[c]; k += 32) {
-      const double Pd = exp(ll_of(c, q, k) - lse);
-      const float P = (float)Pd;
+      const double l = ll_of(c, q, k);
+      const float P = (float)exp(l - lse);
       g.Pt[g.goff[c] + (int64_t)k * g.gcnt[c] + col] = (float)(P / phi_new);
       atomicAdd(g.T + g.mbeg[c] + k, P);
-      cm += Pd;
+      cm += P;
+      if (g.lcmass) crel += exp(l - cmx);
     }
-    for (int o = 16; o > 0; o >>= 1) cm += __shfl_xor_sync(0xffffffffu, cm, o);
+    for (int o = 16; o > 0; o >>= 1) {
+      cm += __shfl_xor_sync(0xffffffffu, cm, o);
+      crel += __shfl_xor_sync(0xffffffffu, crel, o);
+    }
     if (lane == 0) {
-      g.cmass[p * g.m + i] = (float)cm;
-      if (g.lcmass) g.lcmass[p * g.m + i] = cm > 0.0 ? (float)log(cm) : -INFINITY;
+      g.cmass[p * g.m + i] = cm;
+      if (g.lcmass)
+        g.lcmass[p * g.m + i] =
+            (crel > 0.0 && cmx > -INFINITY) ? (float)(cmx + log(crel) - lse) : -INFINITY;
+    }
+  }
+}
+
+// Responsibility lists of a proposed iteration (after the grouped softmax,
+// with T_r and the new scaling final): per rotation the patterns whose P is
+// at least theta T_r, with x = P / (T_r phi_new).  FILL = 0 counts per rotation
+// (cnt [R], zeroed by the caller); FILL = 1 writes the entries at rowoff[r]
+// plus a per-rotation cursor (zeroed), in no fixed order within a row.  One
+// warp per pattern.
+template <int FILL>
+__global__ void group_list_kernel(const GroupArgs g, float theta, unsigned long long* cnt,
+                                  const int64_t* rowoff, int32_t* pat, float* xv) {
+  const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= g.N) return;
+  const double phi = g.scaling[p];
+  const double c1 = 2.0 * g.gauss_inv / phi,
+               c0 = g.poisson ? 0.0 : -g.patstat[p] / (phi * phi) * g.gauss_inv;
+  const double lse = g.lse[p];
+  const float inv_phi = 1.0f / g.new_scaling[p];
+  for (int i = 0; i < g.m; ++i) {
+    const int c = g.cand[p * g.m + i];
+    if (c < 0) break;
+    const int64_t q = g.ppos[p * g.m + i];
+    for (int k = lane; k < g.mcnt[c]; k += 32) {
+      const int64_t r = g.mbeg[c] + k;
+      const float T = g.T[r];
+      if (!(T > 0.0f)) continue;
+      const double y = (double)g.Y[q * g.MM + k];
+      const double l = g.poisson ? y : fma(y, c1, c0 - g.rowstat[r] * g.gauss_inv);
+      const float P = (float)exp(l - lse);
+      if (!(P >= theta * T)) continue;
+      const float x = P / T * inv_phi;
+      if (FILL == 0) {
+        atomicAdd(cnt + r, 1ull);
+      } else {
+        const int64_t pos = rowoff[r] + (int64_t)atomicAdd(cnt + r, 1ull);
+        pat[pos] = (int32_t)p;
+        xv[pos] = x;
+      }
     }
   }
 }
@@ -606,7 +679,7 @@ __global__ void fill_f32_kernel(float* x, int64_t n, float v) {
 }
 
 cudaError_t launch_log_targets(const TargetArgs& a, cudaStream_t st) {
-  const size_t smem = sizeof(double) * 16 * a.n_cells;
+  const size_t smem = (sizeof(double) + sizeof(float)) * 16 * a.n_cells;
   cudaError_t e = cudaFuncSetAttribute(log_targets_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -626,15 +699,35 @@ cudaError_t launch_scatter_log_targets(const int32_t* cand, const float* lcmass,
 
 cudaError_t launch_select_topk(const float* probs, const float* log_keep, const int32_t* mcnt,
                                int64_t N, int C, int top_k, int m, float mass_target,
-                               int32_t* cand, float* mass, cudaStream_t st) {
+                               float keep_tail, int32_t* cand, float* mass, cudaStream_t st) {
   select_topk_kernel<<<(unsigned)((N + 7) / 8), 256, 0, st>>>(probs, log_keep, mcnt, N, C, top_k,
-                                                              m, mass_target, cand, mass);
+                                                              m, mass_target, keep_tail, cand,
+                                                              mass);
   return cudaGetLastError();
 }
 
 cudaError_t launch_audit(const AuditArgs& a, int64_t n_audit, cudaStream_t st) {
   if (n_audit <= 0) return cudaSuccess;
   audit_kernel<<<(unsigned)n_audit, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_list_count(const GroupArgs& g, float theta, int64_t* cnt,
+                                    cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(int64_t) * g.R, st);
+  if (e != cudaSuccess) return e;
+  group_list_kernel<0><<<(unsigned)((g.N + 7) / 8), 256, 0, st>>>(
+      g, theta, reinterpret_cast<unsigned long long*>(cnt), nullptr, nullptr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_list_fill(const GroupArgs& g, float theta, int64_t* cursor,
+                                   const int64_t* rowoff, int32_t* pat, float* xv,
+                                   cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(int64_t) * g.R, st);
+  if (e != cudaSuccess) return e;
+  group_list_kernel<1><<<(unsigned)((g.N + 7) / 8), 256, 0, st>>>(
+      g, theta, reinterpret_cast<unsigned long long*>(cursor), rowoff, pat, xv);
   return cudaGetLastError();
 }
 

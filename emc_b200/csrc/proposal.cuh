@@ -112,11 +112,12 @@ cudaError_t launch_log_targets(const TargetArgs& a, cudaStream_t st);
 cudaError_t launch_scatter_log_targets(const int32_t* cand, const float* lcmass, int64_t N, int m,
                                       int n_cells, float* t, cudaStream_t st);
 // Top-k selection: cells in order of log_keep (finite values) until they hold
-// at least top_k fine rotations, then cells in order of probs until the
-// probs total reaches mass_target; at most m; either input may be null.
+// at least top_k fine rotations and (keep_tail > 0) all but keep_tail of the
+// previous posterior, then cells in order of probs until the probs total
+// reaches mass_target; at most m; either input may be null.
 cudaError_t launch_select_topk(const float* probs, const float* log_keep, const int32_t* mcnt,
                                int64_t N, int C, int top_k, int m, float mass_target,
-                               int32_t* cand, float* mass, cudaStream_t st);
+                               float keep_tail, int32_t* cand, float* mass, cudaStream_t st);
 
 // Dense audit of sampled patterns (see audit_kernel): captured[a] = share of
 // audited pattern pat[a]'s responsibility on the fine rotations of its
@@ -136,6 +137,14 @@ struct AuditArgs {
   float* captured;         // [n_audit]
 };
 cudaError_t launch_audit(const AuditArgs& a, int64_t n_audit, cudaStream_t st);
+// Responsibility lists of a proposed iteration (after the grouped softmax):
+// count[r] of the patterns with P >= theta T_r, then the entries
+// (pattern, value) at rowoff[r] (cursor [R] scratch); for launch_list_compress.
+cudaError_t launch_group_list_count(const GroupArgs& g, float theta, int64_t* cnt,
+                                    cudaStream_t st);
+cudaError_t launch_group_list_fill(const GroupArgs& g, float theta, int64_t* cursor,
+                                   const int64_t* rowoff, int32_t* pat, float* xv,
+                                   cudaStream_t st);
 // FP32 responsibilities [R][N] of the last proposed iteration (zero outside
 // each pattern's candidate cells).
 cudaError_t launch_proposed_resp(const GroupArgs& g, float* P, cudaStream_t st);

@@ -207,8 +207,49 @@ struct RespArgs {
   float* Tpart;            // [ceil(N/1024)][R] partial sums of T_r
   float* T;                // [R]
   float* P32;              // optional [R][N] FP32 responsibilities
+  // optional compaction during the row sums: every P_rp >= list_min is
+  // appended as (r, p, P) at list_count[0]++ (capacity list_cap; entries past
+  // it are counted, not written)
+  unsigned long long* list_count;
+  int64_t list_cap;
+  int2* list_rp;
+  float* list_P;
+  float list_min;
 };
 cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st);
+// The pass in two parts: combine + row sums (partials of T_r), then the
+// FP16 compress operand (which also finishes T_r).
+cudaError_t launch_resp_rowsums(RespArgs& a, cudaStream_t st);
+cudaError_t launch_resp_write(RespArgs& a, cudaStream_t st);
+
+// Responsibility lists (the compress operand as lists instead of P'):
+// launch_resp_rowsums with RespArgs.list_* set compacts the entries, then
+// launch_list_from_compact sorts them by rotation.
+int64_t resp_list_blocks(int64_t N);
+// rowoff[0..R] = exclusive prefix sums of rowtot (rowoff[R] = total).
+cudaError_t launch_list_rowscan(const int64_t* rowtot, int64_t R, int64_t* rowoff,
+                                cudaStream_t st);
+// From the entries compacted by launch_resp_rowsums (n of them): T_r, then
+// the lists sorted by rotation with x = P / (T_r phi_new), keeping entries
+// with P >= rel_min T_r (rowtot, cursor: [R] scratch; rowoff [R+1]).  Order
+// within a row is not fixed.
+cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int64_t* rowtot,
+                                     int64_t* cursor, int64_t* rowoff, int32_t* pat, float* xv,
+                                     cudaStream_t st);
+// Compress from the lists with the counts' photon lists (kptr [N+1], kidx =
+// active pixel, kval = count): one block per rotation accumulates its slice
+// in shared memory (npa floats) and inserts it as the contraction's epilogue
+// does (e.inv_c0 unused).
+struct ListCmpArgs {
+  const int64_t* rowoff;
+  const int32_t* pat;
+  const float* xv;
+  const int64_t* kptr;
+  const int32_t* kidx;
+  const float* kval;
+  CmpEpiArgs e;
+};
+cudaError_t launch_list_compress(const ListCmpArgs& a, cudaStream_t st);
 // FP32 responsibilities [R][N] from Y and lse (readback / tests).
 cudaError_t launch_resp_export(const RespArgs& a, float* P, cudaStream_t st);
 // Most probable rotation of every pattern and its responsibility, from Y and lse.

@@ -60,7 +60,8 @@ class ProposalStats(C.Structure):
 
 class TopkConfig(C.Structure):
     _fields_ = [("top_k", C.c_int32), ("max_cells", C.c_int32), ("mass_target", C.c_float),
-                ("audit_patterns", C.c_int32), ("min_captured", C.c_float), ("pad_", C.c_int32)]
+                ("audit_patterns", C.c_int32), ("min_captured", C.c_float),
+                ("keep_tail", C.c_float)]
 
 
 def assign_cells(q_fine, q_coarse, chunk=8192):
@@ -232,12 +233,14 @@ class LearnedProposal:
         return t
 
     def iterate_topk(self, probs=None, log_keep=None, top_k=512, max_cells=32, mass_target=0.999,
-                     audit=0, min_captured=0.99):
+                     audit=0, min_captured=0.99, keep_tail=0.0):
         """One proposed iteration of emc_iterate_topk: per pattern the cells
         holding the best of its previous log-posterior until they hold top_k
         fine rotations (log_keep, e.g. log_mass() of the previous iteration),
         then the network's most probable cells up to a predicted mass of
-        mass_target (probs), at most max_cells; `audit` sampled patterns are
+        mass_target (probs), at most max_cells (with keep_tail > 0 the
+        log_keep cells continue until they hold all but keep_tail of the
+        previous posterior); `audit` sampled patterns are
         evaluated against every rotation and the dense iteration runs when one
         of them holds less than min_captured of its responsibility."""
         import torch
@@ -247,7 +250,7 @@ class LearnedProposal:
                 raise ValueError("probs / log_keep must be float32 [N][n_cells] tensors")
         torch.cuda.synchronize()
         cfg = TopkConfig(int(top_k), int(max_cells), float(mass_target), int(audit),
-                         float(min_captured), 0)
+                         float(min_captured), float(keep_tail))
         st = ProposalStats()
         self.ctx._c(lib().emc_iterate_topk(
             self.ctx._h, None if probs is None else probs.contiguous().data_ptr(),

@@ -128,6 +128,10 @@ emc_status emc_synchronize(emc_context *ctx);
 emc_status emc_get_model(emc_context *ctx, float *model);
 emc_status emc_get_scaling(emc_context *ctx, float *scaling);
 emc_status emc_get_buffer(emc_context *ctx, emc_buffer which, void *host, size_t bytes);
+/* The responsibilities of n chosen patterns (indices patterns[n]) from the
+ * last maximize, dense or proposed, into the host array out [R][n] (column a
+ * is pattern patterns[a]; 0 outside a proposed iteration's candidates). */
+emc_status emc_get_resp_columns(emc_context *ctx, int64_t n, const int64_t *patterns, float *out);
 /* Device pointer of a buffer (valid until emc_destroy). */
 emc_status emc_device_buffer(emc_context *ctx, emc_buffer which, void **dptr, size_t *bytes);
 /* Per-stage device timing.  With profiling on, every iteration records CUDA
@@ -275,7 +279,8 @@ emc_status emc_iterate_proposed(emc_context *ctx, const float *cell_probs_device
  *   - log_keep (optional, device [N][n_cells]): the log-posterior mass of
  *     every cell in a previous iteration (emc_cell_log_mass); each pattern
  *     takes its cells in that order (finite values only) until they hold at
- *     least top_k fine rotations;
+ *     least top_k fine rotations and, with keep_tail > 0, all but keep_tail
+ *     of that posterior;
  *   - cell_probs (optional, device [N][n_cells]): the proposal network's cell
  *     posterior; cells are then added in its order until the candidates'
  *     predicted mass reaches mass_target (every pattern gets at least one);
@@ -292,15 +297,17 @@ typedef struct {
   float mass_target;
   int32_t audit_patterns;
   float min_captured;
-  int32_t pad_;
+  float keep_tail;  /* > 0: also keep taking log_keep cells until they hold all but this much
+                       of the previous posterior (e.g. 1e-6); 0: top_k alone */
 } emc_topk_config;
 emc_status emc_iterate_topk(emc_context *ctx, const float *cell_probs_device,
                             const float *log_keep_device, const emc_topk_config *cfg,
                             emc_proposal_stats *stats);
 /* t [N][n_cells] (device): natural log of each cell's responsibility mass in
  * the last maximize (dense, or proposed: -inf outside the candidate cells),
- * summed in FP64 so cells far down the tail are still ordered (-inf only
- * below about 1e-308). */
+ * formed in the log domain (the cell's largest log-likelihood plus the log of
+ * an FP64 sum relative to it), so every evaluated cell is ranked however far
+ * down the tail it lies. */
 emc_status emc_cell_log_mass(emc_context *ctx, float *t_device);
 
 /* Proposal network: three 3x3 stride-2 convolutions (16, 32, 64 channels,

@@ -228,3 +228,36 @@ def test_pair_maximize_at_size():
     assert resp_l1(out[1][0], out[0][0]) <= 1e-4
     assert rel(out[1][1], out[0][1]) <= 1e-5
     assert rel(out[1][2], out[0][2]) <= 1e-6
+
+
+@pytest.mark.parametrize("lik,interp", [("poisson", "nearest"), ("gauss", "nearest"),
+                                        ("poisson", "trilinear")])
+def test_list_compress_matches_dense_contraction(small, lik, interp):
+    """The mixed compress from responsibility lists (per rotation, the
+    patterns with a non-zero operand entry, times their photon lists; the
+    default) gives the model of the dense tensor-core compress on one SM and
+    on SM pairs, and the oracle's compress of the engine's responsibilities."""
+    import emc_b200 as E
+    d = small
+    cfg = oracle_cfg(d, lik, interp)
+    out = {}
+    for mode in ("lists", "dense", "dense_pairs"):
+        with make_ctx(d, lik, interp, "mixed") as ctx:
+            assert ctx.tuning()["compress_sparse"] == 1
+            if mode != "lists":
+                ctx.set_sparse_compress(False)
+                ctx.set_tuning(1, 2, 0, 1 if mode == "dense_pairs" else 0)
+            ctx.expand()
+            ctx.maximize()
+            P, phi = ctx.get_buffer(E.BUF_RESP), ctx.get_scaling()
+            ctx.compress()
+            out[mode] = (ctx.get_model(), ctx.get_buffer(E.BUF_TOTALRESP), P, phi)
+    m, T, P, phi = out["lists"]
+    acc, wacc, T_ref = O.compress(cfg, P.astype(np.float64), d["counts"], d["mask"],
+                                  phi.astype(np.float64), d["q"], d["w"], d["x"], d["y"], d["z"])
+    assert rel(m, O.normalize_model(acc, wacc)) <= 1e-5, rel(m, O.normalize_model(acc, wacc))
+    np.testing.assert_allclose(T, T_ref, rtol=1e-4, atol=1e-6)
+    # the dense contraction rounds the operand to FP16 hi + lo: within the
+    # mixed path's model tolerance of the lists
+    for mode in ("dense", "dense_pairs"):
+        assert rel(out[mode][0], m) <= TOL["mixed"]["model"], (mode, rel(out[mode][0], m))
