@@ -404,9 +404,7 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
     # responsibilities of sampled patterns against the FP64 oracle's dense ones
     cols = np.arange(0, N, max(1, N // a.oracle_patterns))[: a.oracle_patterns]
     P_prop = ctx.resp_columns(cols)
-    t1 = time.perf_counter()
     P_orc = oracle_columns(dict(d, q=q), m0, s0, q, cols)
-    oracle_s = time.perf_counter() - t1
     l1 = np.abs(P_prop.astype(np.float64) - P_orc).sum(0)
     st_f, _, forced = one_step(None, torch.roll(lk, shifts=1, dims=0))
 
@@ -475,16 +473,15 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
         "fallback_iterations": fallbacks, "forced_fallback_iterations": st_f["fallback"],
         "cells_per_pattern": round(pairs / a.learned_steps / N, 2),
         "evaluated_fraction": evals / a.learned_steps / (N * R),
-        "value_dense_equivalent": N * R / (ms / 1e3), "speedup_vs_dense_mixed": dense_ms / ms,
+        "speedup_vs_dense_mixed": dense_ms / ms,
         "stages_ms": [round(float(v) / 2, 2) for v in stage],
         "one_step": variants, "held_out_captured": held_out,
         "model_err_vs_dense_after_12": drift, "chain_fallbacks": chain_fb, "spec_top_k": spec,
         "vs_fp64_oracle": {
-            "resp_l1_max": float(l1.max()), "resp_l1_mean": float(l1.mean()),
-            "patterns": len(cols), "oracle_s": round(oracle_s, 1),
+            "resp_l1_max": float(l1.max()), "patterns": len(cols),
             "model_bound": variants["with_network"]["model_err_vs_dense"]
             + (dense_err or {}).get("model_rel_err", float("nan"))},
-        "train_s": round(train_s, 1), "loss": [round(losses[0], 3), round(losses[-1], 4)],
+        "train_s": round(train_s, 1),
     }
 
 
@@ -542,8 +539,8 @@ def batched_datasets(a, E, W, device, workloads):
     b.close()
     for c in ctxs:
         c.close()
-    return {"evals": evals, "separate_ms": round(sep, 2), "graph_ms": round(ms, 2),
-            "speedup": round(sep / ms, 3), "finite": ok}
+    assert ok, "batched iteration gave a non-finite model"
+    return {"separate_ms": round(sep, 2), "graph_ms": round(ms, 2), "speedup": round(sep / ms, 3)}
 
 
 # ------------------------------------------------------------------ ours --
@@ -584,7 +581,7 @@ def profile_case(a):
         for i in range(proposed):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            st = lp.iterate_topk(None, keep, 512, 32, audit=64)
+            st = lp.iterate_topk(None, keep, 2048, 32, audit=64)
             keep = lp.log_mass()
             ctx.synchronize()
             print(f"proposed {i}: {(time.perf_counter() - t0) * 1e3:.2f} ms, "

@@ -110,6 +110,8 @@ def lib():
             ("emc_set_memory_limit", [P, C.c_size_t], C.c_int),
             ("emc_get_resp_columns", [P, I64, P, P], C.c_int),
             ("emc_memory_used", [P], C.c_size_t),
+            ("emc_set_rotation_chunk", [P, C.c_int64, C.c_int64], C.c_int),
+            ("emc_rotation_chunk", [P], C.c_int64),
             ("emc_save_state", [P, C.c_char_p, I64], C.c_int),
             ("emc_load_state", [P, C.c_char_p, P], C.c_int),
         ]:
@@ -465,6 +467,17 @@ class Context:
     @property
     def memory_used(self):
         return int(lib().emc_memory_used(self._h))
+
+    def set_rotation_chunk(self, rows, capacity=0):
+        """emc_set_rotation_chunk: the log-likelihood held for `rows`
+        rotations at a time (a multiple of 256; 0 = all, -1 = what fits the
+        memory limit); capacity = initial kept-entry capacity (0: default)."""
+        self._c(lib().emc_set_rotation_chunk(self._h, int(rows), int(capacity)))
+
+    @property
+    def rotation_chunk(self):
+        """Rotations the log-likelihood buffer holds (R when unchunked)."""
+        return int(lib().emc_rotation_chunk(self._h))
 
     def save_state(self, path, iteration=0):
         """emc_save_state: model, weight grid, scaling and the iteration number."""

@@ -181,6 +181,14 @@ struct emc_context {
   __half *d_Kh = nullptr, *d_Kt = nullptr, *d_Bhi = nullptr, *d_Blo = nullptr;
   __half *d_Phi = nullptr, *d_Plo = nullptr;
   float* d_Y = nullptr;
+  // rotation chunks: Y holds y_rows rotations (R: one chunk); a chunked
+  // maximize keeps its candidates (d_lcomp_rp / d_lcomp_P: rotation, pattern,
+  // y) and their final P (d_cand_P) until the next maximize
+  int64_t y_rows = 0, cand_n = 0, cand_cap_min = 0, cand_P_cap = 0;
+  bool batched = false;  // a member of an emc_batch
+  float* d_cand_P = nullptr;
+  double* d_T64 = nullptr;
+  unsigned long long* d_cand_key = nullptr;
   float4* d_part = nullptr;
   float2* d_acc = nullptr;  // interleaved (model, weight) accumulators
   double *d_lse = nullptr, *d_plogp = nullptr;
@@ -191,7 +199,9 @@ struct emc_context {
   // profiling: events at stage boundaries, kernel launch count
   // learned proposal: rotation cells and the candidate-iteration buffers
   int32_t n_cells = 0, cand_m = 0;
-  int resp_source = 0;  // responsibilities of the last maximize: 1 dense, 2 proposed
+  // responsibilities of the last maximize: 1 dense, 2 proposed, 3 dense over
+  // rotation chunks (kept as candidates)
+  int resp_source = 0;
   float* d_cmass = nullptr;
   cudaEvent_t ev_sel = nullptr;  // the proposed iteration's selection has reached the host
   int32_t* d_best = nullptr;  // orientation diagnostics: most probable rotation per pattern
@@ -344,6 +354,10 @@ static int64_t count_bad(const float* x, int64_t n, bool nonneg) {
 
 extern "C" {
 
+static size_t avail_bytes(emc_context* c, size_t held);
+static int64_t fit_rows(const emc_context* c, size_t bytes);
+static emc_status set_y_rows(emc_context* c, int64_t rows);
+
 const char* emc_status_string(emc_status s) {
   switch (s) {
     case EMC_OK: return "ok";
@@ -447,6 +461,35 @@ emc_status emc_set_memory_limit(emc_context* c, size_t bytes) {
 
 size_t emc_memory_used(const emc_context* c) { return c ? c->mem_used : 0; }
 
+emc_status emc_set_rotation_chunk(emc_context* c, int64_t rows, int64_t capacity) {
+  if (!c || rows < -1 || capacity < 0) return EMC_ERR_ARG;
+  if (!c->mixed) return c->fail(EMC_ERR_UNSUPPORTED, "rotation chunks are a form of the mixed path");
+  if (!c->have_geom) return c->fail(EMC_ERR_STATE, "set the geometry first");
+  if (c->stage != 0 || c->batched)
+    return c->fail(EMC_ERR_STATE, "rotation chunks change between iterations, outside a batch");
+  const int64_t R = c->R;
+  if (rows == -1) {
+    // what Y and P' hold now is given back first
+    size_t held = sizeof(float) * (size_t)(c->y_rows * c->Npad);
+    if (c->d_Phi) held += 4 * (size_t)(c->Rpad * c->Npad);
+    rows = fit_rows(c, avail_bytes(c, held) / 2);
+  } else if (rows == 0) {
+    rows = R;
+  } else if (rows < R && rows % 256) {
+    return c->fail(EMC_ERR_ARG, "a rotation chunk is a multiple of 256 rotations");
+  }
+  if (rows < R && c->npa > kListMaxPixels)
+    return c->fail(EMC_ERR_UNSUPPORTED,
+                   "rotation chunks need the responsibility lists (at most %d active pixels)",
+                   kListMaxPixels);
+  c->cand_cap_min = capacity;
+  TRY(set_y_rows(c, rows));
+  if (rows < R) c->tune.compress_sparse = 1;
+  return EMC_OK;
+}
+
+int64_t emc_rotation_chunk(const emc_context* c) { return c ? c->y_rows : 0; }
+
 emc_status emc_set_profiling(emc_context* c, int on) {
   if (!c) return EMC_ERR_ARG;
   if (on && !c->ev[0][0])
@@ -469,6 +512,56 @@ emc_status emc_stage_times(emc_context* c, float* ms) {
   return EMC_OK;
 }
 int64_t emc_active_pixels(const emc_context* ctx) { return ctx ? ctx->npa : 0; }
+
+// Device bytes this context may still allocate, after `held` bytes it holds
+// are given back, less a reserve for the pattern staging, the photon and
+// responsibility lists and scratch.
+static size_t avail_bytes(emc_context* c, size_t held) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+  size_t a = fr + held;
+  if (c->mem_limit) {
+    const size_t used = c->mem_used - held;
+    a = std::min(a, c->mem_limit > used ? c->mem_limit - used : 0);
+  }
+  const size_t reserve =
+      sizeof(float) * (size_t)c->N * (size_t)(c->npix + c->npa) + ((size_t)1 << 30);
+  return a > reserve ? a - reserve : 0;
+}
+
+// The most rotations (a multiple of 256, at least 256) whose Y fits in `bytes`.
+static int64_t fit_rows(const emc_context* c, size_t bytes) {
+  const int64_t rows = (int64_t)(bytes / (sizeof(float) * (size_t)c->Npad)) / 256 * 256;
+  return rows < 256 ? 256 : rows;
+}
+
+// Y for `rows` rotations (a multiple of 256, or R and more: every rotation).
+// Chunks drop the dense compress operand P', which only the unchunked
+// maximize writes; one chunk of every rotation allocates it again.
+static emc_status set_y_rows(emc_context* c, int64_t rows) {
+  if (rows >= c->R) rows = c->R;
+  if (c->d_Y && rows == c->y_rows) return EMC_OK;
+  if (c->d_Y) c->release(c->d_Y);
+  c->d_Y = nullptr;
+  c->y_rows = 0;
+  c->resp_source = 0;  // the last iteration's responsibilities are gone with Y
+  if (rows < c->R)
+    for (__half** q : {&c->d_Phi, &c->d_Plo})
+      if (*q) {
+        c->release(*q);
+        *q = nullptr;
+      }
+  TRY(c->alloc(&c->d_Y, rows * c->Npad));
+  if (rows == c->R && !c->d_Phi) {
+    TRY(c->alloc(&c->d_Phi, c->Rpad * c->Npad, true));
+    TRY(c->alloc(&c->d_Plo, c->Rpad * c->Npad, true));
+    if (!tc_encode_2d(&c->tmPhi, c->d_Phi, c->Npad, c->Rpad, 128, kCompressBK) ||
+        !tc_encode_2d(&c->tmPlo, c->d_Plo, c->Npad, c->Rpad, 128, kCompressBK))
+      return c->fail(EMC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  }
+  c->y_rows = rows;
+  return EMC_OK;
+}
 
 static emc_status alloc_work(emc_context* c) {
   // called once geometry is known (npa fixes every pixel dimension)
@@ -504,18 +597,22 @@ static emc_status alloc_work(emc_context* c) {
   TRY(c->alloc(&c->d_Kt, c->Ppad * c->Npad, true));
   TRY(c->alloc(&c->d_Bhi, c->Rpad * c->Ppad, true));
   TRY(c->alloc(&c->d_Blo, c->Rpad * c->Ppad, true));
-  TRY(c->alloc(&c->d_Phi, c->Rpad * c->Npad, true));
-  TRY(c->alloc(&c->d_Plo, c->Rpad * c->Npad, true));
-  TRY(c->alloc(&c->d_Y, R * c->Npad));
   TRY(c->alloc(&c->d_part, c->nrt * N));
   TRY(c->alloc(&c->d_lse, N));
   TRY(c->alloc(&c->d_plogp, N));
   TRY(c->alloc(&c->d_Tpart, ((N + 1023) / 1024) * R));
+  // Y (R x Npad FP32) and the dense compress operand P' (2 x Rpad x Npad
+  // FP16) are the large buffers.  Where they do not fit the memory limit or
+  // the free device memory, Y holds rotation chunks (half of what is left)
+  // and P' is not kept: the compress reads responsibility lists.
+  const size_t full = sizeof(float) * (size_t)(R * c->Npad) + 4 * (size_t)(c->Rpad * c->Npad);
+  const size_t avail = avail_bytes(c, 0);
+  int64_t rows = R;
+  if (full > avail && c->tune.compress_sparse) rows = fit_rows(c, avail / 2);
+  TRY(set_y_rows(c, rows));
   bool ok = tc_encode_2d(&c->tmKh, c->d_Kh, c->Ppad, c->Npad, 128, kMaximizeBK) &&
             tc_encode_2d(&c->tmBhi, c->d_Bhi, c->Ppad, c->Rpad, 256, kMaximizeBK) &&
             tc_encode_2d(&c->tmBlo, c->d_Blo, c->Ppad, c->Rpad, 256, kMaximizeBK) &&
-            tc_encode_2d(&c->tmPhi, c->d_Phi, c->Npad, c->Rpad, 128, kCompressBK) &&
-            tc_encode_2d(&c->tmPlo, c->d_Plo, c->Npad, c->Rpad, 128, kCompressBK) &&
             tc_encode_2d(&c->tmKt, c->d_Kt, c->Npad, c->Ppad, 256, kCompressBK) &&
             tc_encode_2d(&c->tmKh64, c->d_Kh, c->Ppad, c->Npad, 128, kPairBoxK) &&
             tc_encode_2d(&c->tmBhi64, c->d_Bhi, c->Ppad, c->Rpad, 128, kPairBoxK) &&
@@ -839,10 +936,10 @@ static emc_status grow(emc_context* c, T** p, int64_t& cap, int64_t need) {
 static emc_status build_rows(emc_context* c, const float* M, int64_t rows, int64_t cols,
                              SparseRows& s, bool with_aux);
 
-static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
-  const int64_t N = c->N;
+// Arguments of the responsibility pass over every rotation.
+static RespArgs resp_args(emc_context* c) {
   RespArgs a{};
-  a.N = N;
+  a.N = c->N;
   a.R = c->R;
   a.ldY = c->Npad;
   a.ldP = c->Npad;
@@ -864,26 +961,42 @@ static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
   a.Tpart = c->d_Tpart;
   a.T = c->d_T;
   a.P32 = nullptr;
+  return a;
+}
+
+static emc_status list_buffers(emc_context* c) {
+  if (!c->d_lcount) {
+    const int64_t R = c->R;
+    TRY(c->alloc(&c->d_lcount, 1));
+    TRY(c->alloc(&c->d_lrowtot, R));
+    TRY(c->alloc(&c->d_lrowoff, R + 1));
+    TRY(c->alloc(&c->d_lcursor, R));
+  }
+  return EMC_OK;
+}
+
+// Room for `n` compacted (rotation, pattern, value) entries.
+static emc_status compact_capacity(emc_context* c, int64_t n) {
+  if (c->lcomp_cap >= n && c->d_lcomp_rp) return EMC_OK;
+  int64_t cap = c->lcomp_cap;
+  TRY(grow(c, &c->d_lcomp_rp, cap, n));
+  int64_t cap2 = c->lcomp_cap2;
+  TRY(grow(c, &c->d_lcomp_P, cap2, cap));
+  c->lcomp_cap = cap;
+  c->lcomp_cap2 = cap2;
+  return EMC_OK;
+}
+
+static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
+  const int64_t N = c->N;
+  RespArgs a = resp_args(c);
   c->list_mode = false;
   if (allow_lists && c->tune.compress_sparse && c->npa <= kListMaxPixels) {
     // the compress operand as per-rotation lists of its non-zero entries:
     // entries P >= kListMinP are compacted during the row-sum sweep, the host
     // reads their count (one wait), a counting sort orders them by rotation
-    const int64_t R = c->R;
-    if (!c->d_lcount) {
-      TRY(c->alloc(&c->d_lcount, 1));
-      TRY(c->alloc(&c->d_lrowtot, R));
-      TRY(c->alloc(&c->d_lrowoff, R + 1));
-      TRY(c->alloc(&c->d_lcursor, R));
-    }
-    if (c->lcomp_cap < std::max<int64_t>(64 * N, (int64_t)1 << 20)) {
-      int64_t cap = c->lcomp_cap;
-      TRY(grow(c, &c->d_lcomp_rp, cap, std::max<int64_t>(64 * N, (int64_t)1 << 20)));
-      int64_t cap2 = c->lcomp_cap2;
-      TRY(grow(c, &c->d_lcomp_P, cap2, cap));
-      c->lcomp_cap = cap;
-      c->lcomp_cap2 = cap2;
-    }
+    TRY(list_buffers(c));
+    TRY(compact_capacity(c, std::max<int64_t>(64 * N, (int64_t)1 << 20)));
     CK(c, cudaMemsetAsync(c->d_lcount, 0, sizeof(unsigned long long), c->st));
     a.list_count = c->d_lcount;
     a.list_cap = c->lcomp_cap;
@@ -910,12 +1023,7 @@ static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
       // more entries than the compaction holds: the dense operand this time,
       // room for them next time
       CK(c, launch_resp_write(a, c->st));
-      int64_t cap = c->lcomp_cap;
-      TRY(grow(c, &c->d_lcomp_rp, cap, c->list_nnz));
-      int64_t cap2 = c->lcomp_cap2;
-      TRY(grow(c, &c->d_lcomp_P, cap2, cap));
-      c->lcomp_cap = cap;
-      c->lcomp_cap2 = cap2;
+      TRY(compact_capacity(c, c->list_nnz));
       c->launches += 3;
     }
   } else {
@@ -925,6 +1033,89 @@ static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
   CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
   CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
   c->launches += 2;
+  return EMC_OK;
+}
+
+// The maximize over rotation chunks of y_rows rotations, Y holding one chunk
+// at a time.  Per chunk: the contraction into Y and the chunk's tile
+// partials; the combine over the partials of the chunks so far (the running
+// lse, a lower bound of the final one); the row-sum sweep keeping the
+// candidates, the entries with P >= kListMinP under the running lse, which
+// include every entry the unchunked pass compacts.  After the last chunk,
+// whose combine covers every tile, lse, scaling and sum P log P are those of
+// the unchunked pass; P of the candidates under it gives T_r and the
+// responsibility lists.  More candidates than the arrays hold: they grow and
+// the chunks run again (the contraction is deterministic).
+static emc_status chunked_maximize(emc_context* c) {
+  const int64_t R = c->R, N = c->N, rows = c->y_rows;
+  if (!(c->tune.compress_sparse && c->npa <= kListMaxPixels))
+    return c->fail(EMC_ERR_STATE, "rotation chunks need the compress from responsibility lists");
+  TRY(list_buffers(c));
+  if (!c->d_T64) TRY(c->alloc(&c->d_T64, R));
+  TRY(compact_capacity(c, c->cand_cap_min > 0 ? c->cand_cap_min
+                                              : std::max<int64_t>(64 * N, (int64_t)1 << 20)));
+  unsigned long long* hn = c->pinned<unsigned long long>(7, 1);
+  if (!hn) return c->fail(EMC_ERR_OOM, "pinned host staging");
+  const bool pair = c->tune.maximize_pair != 0;
+  RespArgs a = resp_args(c);
+  a.Tpart = nullptr;
+  a.list_count = c->d_lcount;
+  a.list_min = kListMinP;
+  a.list_store_y = 1;
+  for (int attempt = 0;; ++attempt) {
+    a.list_cap = c->lcomp_cap;
+    a.list_rp = c->d_lcomp_rp;
+    a.list_P = c->d_lcomp_P;
+    CK(c, cudaMemsetAsync(c->d_lcount, 0, sizeof(unsigned long long), c->st));
+    for (int64_t r0 = 0; r0 < R; r0 += rows) {
+      const int64_t rc = std::min(rows, R - r0), rcp = round_up(rc, 256);
+      // the chunk's rows of the slice operand (r0 is a multiple of 256)
+      CUtensorMap th, tl;
+      if (!tc_encode_2d(&th, c->d_Bhi + r0 * c->Ppad, c->Ppad, rcp, pair ? 128 : 256,
+                        pair ? kPairBoxK : kMaximizeBK) ||
+          !tc_encode_2d(&tl, c->d_Blo + r0 * c->Ppad, c->Ppad, rcp, pair ? 128 : 256,
+                        pair ? kPairBoxK : kMaximizeBK))
+        return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
+      MaxEpiArgs e = max_args(c);
+      e.R = rc;
+      e.rowstat = c->d_rowstat + r0;
+      e.part = c->d_part + (r0 / 256) * N;
+      if (pair)
+        CK(c, launch_maximize_pair_tc(c->tmKh64, th, tl, c->Npad, rcp, c->Ppad, e, c->d_status,
+                                      c->num_sms, c->st, c->tune.maximize_raster));
+      else
+        CK(c, launch_maximize_tc(c->tmKh, th, tl, c->Npad, rcp, c->Ppad, e, c->d_status,
+                                 c->num_sms, c->st, c->tune.maximize_raster));
+      a.R = rc;
+      a.rowstat = c->d_rowstat + r0;
+      a.nparts = (r0 + rcp) / 256;
+      a.list_r0 = r0;
+      CK(c, launch_resp_rowsums(a, c->st));  // combine + candidate sweep
+      c->launches += 3;
+    }
+    CK(c, cudaMemcpyAsync(hn, c->d_lcount, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    c->cand_n = (int64_t)*hn;
+    if (c->cand_n <= c->lcomp_cap) break;
+    if (attempt) return c->fail(EMC_ERR_CUDA, "candidate count changed between identical passes");
+    TRY(compact_capacity(c, c->cand_n));
+  }
+  c->mark(2);
+  TRY(grow(c, &c->d_cand_P, c->cand_P_cap, c->cand_n + 1));
+  TRY(grow(c, &c->d_lpat, c->lcap, c->cand_n + 1));
+  int64_t cap = c->lcap_x;
+  TRY(grow(c, &c->d_lx, cap, c->cand_n + 1));
+  c->lcap_x = cap;
+  a.R = R;
+  a.rowstat = c->d_rowstat;
+  a.list_r0 = 0;
+  CK(c, launch_list_from_candidates(a, c->cand_n, kListRel, c->d_cand_P, c->d_T64, c->d_lrowtot,
+                                    c->d_lcursor, c->d_lrowoff, c->d_lpat, c->d_lx, c->st));
+  c->list_mode = true;
+  CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
+  CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
+  c->launches += 7;  // finish, T, count, scan, fill, 2 sums
   return EMC_OK;
 }
 
@@ -1080,6 +1271,8 @@ emc_status emc_maximize(emc_context* c) {
                                 c->d_scaling, c->st));
     CK(c, launch_row_sums(c->d_LL, R, N, c->d_T, c->st));
     c->launches += 8;
+  } else if (c->y_rows < R) {
+    TRY(chunked_maximize(c));
   } else {
     MaxEpiArgs e = max_args(c);
     if (c->tune.maximize_pair)
@@ -1096,7 +1289,7 @@ emc_status emc_maximize(emc_context* c) {
   // pattern-sharded caller replaces it by the sum over every shard
   CK(c, cudaMemcpyAsync(c->d_Tskip, c->d_T, sizeof(float) * R, cudaMemcpyDeviceToDevice, c->st));
   c->mark(3);
-  c->resp_source = 1;
+  c->resp_source = c->mixed && c->y_rows < R ? 3 : 1;
   c->stage = 2;
   return EMC_OK;
 }
@@ -1259,6 +1452,8 @@ emc_status emc_set_tuning(emc_context* c, const emc_tuning* t) {
                    (long long)kListMaxPixels);
   if (t->maximize_sparse && (c->mixed || c->gauss))
     return c->fail(EMC_ERR_UNSUPPORTED, "the photon-list log-likelihood is an FP32 poisson form");
+  if (!t->compress_sparse && c->mixed && c->y_rows < c->R)
+    return c->fail(EMC_ERR_STATE, "rotation chunks compress from responsibility lists");
   c->tune = *t;
   return EMC_OK;
 }
@@ -1382,6 +1577,13 @@ emc_status emc_orientation_stats(emc_context* c, int32_t* best_rot, float* best_
       CK(c, launch_resp_argmax(a, c->d_best, c->d_bestp, c->st));
     }
     c->launches += 1;
+  } else if (c->resp_source == 3) {
+    if (!c->d_cand_key) TRY(c->alloc(&c->d_cand_key, N));
+    RespArgs a = resp_args(c);
+    a.list_rp = c->d_lcomp_rp;
+    a.list_P = c->d_lcomp_P;
+    CK(c, launch_cand_argmax(a, c->cand_n, c->d_cand_key, c->d_best, c->d_bestp, c->st));
+    c->launches += 3;
   }  // a proposed iteration recorded its best candidates itself
   if (best_rot)
     CK(c, cudaMemcpyAsync(best_rot, c->d_best, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, c->st));
@@ -1512,6 +1714,12 @@ emc_status emc_get_resp_columns(emc_context* c, int64_t n, const int64_t* patter
                                                                             n, d_out);
       e = cudaGetLastError();
     }
+  } else if (e == cudaSuccess && c->resp_source == 3) {
+    // rotation chunks: the candidates' P, 0 elsewhere (every dropped entry is
+    // below kListMinP)
+    e = cudaMemsetAsync(d_out, 0, sizeof(float) * R * n, c->st);
+    if (e == cudaSuccess)
+      e = launch_cand_columns(c->d_lcomp_rp, c->d_cand_P, c->cand_n, d_cols, n, d_out, c->st);
   } else if (e == cudaSuccess) {
     const unsigned grid = (unsigned)std::min<int64_t>((R * n + 255) / 256, 8192);
     if (!c->mixed)
@@ -1585,7 +1793,12 @@ emc_status emc_get_buffer(emc_context* c, emc_buffer which, void* host, size_t b
     float* tmp = nullptr;
     CK(c, cudaMalloc(&tmp, n * sizeof(float)));
     cudaError_t e;
-    if (which == EMC_BUF_RESP) {
+    if (which == EMC_BUF_RESP && c->resp_source == 3) {
+      // rotation chunks: the candidates' P, 0 elsewhere (below kListMinP)
+      e = cudaMemsetAsync(tmp, 0, n * sizeof(float), c->st);
+      if (e == cudaSuccess)
+        e = launch_cand_scatter(c->d_lcomp_rp, c->d_cand_P, c->cand_n, c->N, tmp, c->st);
+    } else if (which == EMC_BUF_RESP) {
       RespArgs a{};
       a.N = c->N;
       a.R = c->R;
@@ -1670,6 +1883,25 @@ emc_status emc_pattern_features(emc_context* c, int32_t in_side, float* x) {
   return EMC_OK;
 }
 
+}  // extern "C"
+
+// Cell masses (take_log: their logs) of a chunked iteration from its
+// candidates, summed in FP64 (a temporary [N][n_cells] accumulator).
+static emc_status cand_cells(emc_context* c, float* t, int take_log) {
+  const int64_t count = c->N * (int64_t)c->n_cells;
+  double* acc = nullptr;
+  cudaError_t e = cudaMalloc(&acc, sizeof(double) * count);
+  if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, sizeof(double) * count, c->st);
+  if (e == cudaSuccess)
+    e = launch_cand_cells(c->d_lcomp_rp, c->d_cand_P, c->cand_n, c->d_cell, c->n_cells, acc, c->st);
+  if (e == cudaSuccess) e = launch_cells_out(acc, count, take_log, t, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  cudaFree(acc);
+  return c->cuda(e, "cell masses of a chunked iteration");
+}
+
+extern "C" {
+
 emc_status emc_cell_targets(emc_context* c, float* t) {
   if (!c || !t) return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
@@ -1677,6 +1909,11 @@ emc_status emc_cell_targets(emc_context* c, float* t) {
     return c->fail(EMC_ERR_STATE, "no responsibilities yet");
   if (c->resp_source == 2) {
     CK(c, launch_scatter_targets(c->d_cand, c->d_cmass, c->N, c->cand_m, c->n_cells, t, c->st));
+    CK(c, cudaStreamSynchronize(c->st));
+    return EMC_OK;
+  }
+  if (c->resp_source == 3) {
+    TRY(cand_cells(c, t, 0));
     CK(c, cudaStreamSynchronize(c->st));
     return EMC_OK;
   }
@@ -1970,6 +2207,8 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
   // the grouped maximize on SM pairs (256-slot tiles) where the dense one is
   const bool gpair_form = tc && c->tune.maximize_pair;
   const int32_t gm_rows = gpair_form ? 256 : 128;
+  // compress from responsibility lists (as the dense mixed iteration does)
+  const bool lists = c->tune.compress_sparse && c->npa <= kListMaxPixels;
   if (tc) {
     const int64_t ptiles = (c->npa + 255) / 256;
     for (int32_t k = 0; k < n_cells; ++k)
@@ -1995,7 +2234,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     TRY(grow(c, &c->d_gmt, c->gmt_cap, n_gmt));
     TRY(grow(c, &c->d_gct, c->gct_cap, n_gct));
     TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
-    if (kw > c->a_ld) {
+    if (!lists && kw > c->a_ld) {
       for (__half** q : {&c->d_Ahi, &c->d_Alo})
         if (*q) {
           c->release(*q);
@@ -2084,12 +2323,14 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
   int launches = 0;
   if (tc) {
     CUtensorMap tmKg, tmKg64, tmAhi, tmAlo;
-    if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, gpair_form ? kPairBoxK : kMaximizeBK) ||
-        !tc_encode_2d(&tmKg64, c->d_Kg, c->Ppad, S, kCompressBK, 64) ||
-        !tc_encode_2d_strided(&tmAhi, c->d_Ahi, c->a_ld, R, c->a_ld, 128, kCompressBK) ||
-        !tc_encode_2d_strided(&tmAlo, c->d_Alo, c->a_ld, R, c->a_ld, 128, kCompressBK))
+    if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, gpair_form ? kPairBoxK : kMaximizeBK))
       return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
     CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->st));
+    if (!lists &&
+        (!tc_encode_2d(&tmKg64, c->d_Kg, c->Ppad, S, kCompressBK, 64) ||
+         !tc_encode_2d_strided(&tmAhi, c->d_Ahi, c->a_ld, R, c->a_ld, 128, kCompressBK) ||
+         !tc_encode_2d_strided(&tmAlo, c->d_Alo, c->a_ld, R, c->a_ld, 128, kCompressBK)))
+      return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
     c->mark(1);
     GMaxEpiArgs ge{};
     ge.tiles = c->d_gmt;
@@ -2109,8 +2350,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
                                      c->num_sms, c->st));
     c->mark(2);
     CK(c, launch_group_softmax(g, c->st));
-    if (c->tune.compress_sparse && c->npa <= kListMaxPixels) {
-      // compress from responsibility lists, as the dense mixed iteration does
+    if (lists) {
       if (!c->d_lrowoff) {
         TRY(c->alloc(&c->d_lrowtot, R));
         TRY(c->alloc(&c->d_lrowoff, R + 1));
@@ -2142,7 +2382,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
       la.e = cmp_args(c);
       la.e.Tskip = nullptr;  // the proposed iteration's own T_r
       CK(c, launch_list_compress(la, c->st));
-      launches = 7;  // gather (2), contraction, softmax, count + scan, fill, compress
+      launches = 7;  // gather, contraction, softmax, count + scan, fill, compress
     } else {
     CK(c, launch_p_split(g, c->d_cell, R, c->d_T, c->a_ld, c->d_Ahi, c->d_Alo, c->st));
     c->mark(3);
@@ -2241,6 +2481,8 @@ emc_status emc_cell_log_mass(emc_context* c, float* t) {
   if (c->resp_source == 2) {
     CK(c, launch_scatter_log_targets(c->d_cand, c->d_lcmass, c->N, c->cand_m, c->n_cells, t,
                                      c->st));
+  } else if (c->resp_source == 3) {
+    TRY(cand_cells(c, t, 1));
   } else {
     TargetArgs a{};
     a.N = c->N;
@@ -2316,7 +2558,10 @@ extern "C" {
 emc_status emc_batch_destroy(emc_batch* b) {
   if (!b) return EMC_OK;
   if (b->st) cudaStreamSynchronize(b->st);
-  for (size_t i = 0; i < b->ctx.size(); ++i) b->ctx[i]->st = b->own[i];
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    b->ctx[i]->st = b->own[i];
+    b->ctx[i]->batched = false;
+  }
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->d_mt) cudaFree(b->d_mt);
@@ -2335,8 +2580,11 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
   for (int32_t i = 0; i < n; ++i) {
     emc_context* c = ctxs[i];
     if (!c || !c->mixed || c->cfg.device != dev) return EMC_ERR_ARG;
-    if (!c->have_geom || !c->have_rot || !c->have_pat || !c->have_model || c->stage != 0)
+    if (!c->have_geom || !c->have_rot || !c->have_pat || !c->have_model || c->stage != 0 ||
+        c->batched)
       return EMC_ERR_STATE;
+    // the batched contractions read every rotation's Y and P'
+    if (c->y_rows < c->R) return EMC_ERR_UNSUPPORTED;
     for (int32_t k = 0; k < i; ++k)
       if (ctxs[k] == c) return EMC_ERR_ARG;
   }
@@ -2351,6 +2599,7 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
     b->ctx.push_back(ctxs[i]);
     b->own.push_back(ctxs[i]->st);
     ctxs[i]->st = b->st;  // every stage of every dataset on the batch's stream
+    ctxs[i]->batched = true;
   }
   // Tile lists, the costliest tiles first (a tile's time grows with its K
   // extent), each dataset's tiles in the order of its own launch.

@@ -1457,12 +1457,13 @@ __global__ void __launch_bounds__(kSweepThreads, 4) rowsum_kernel(const RespArgs
         if (lane == 31 && tot > 0) base = atomicAdd(a.list_count, (unsigned long long)tot);
         base = __shfl_sync(0xffffffffu, base, 31);
         int64_t pos = (int64_t)base + inc - n;
+        const float yy[4] = {y[u].x, y[u].y, y[u].z, y[u].w};
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           if (k.ok[j] && P[j] >= a.list_min) {
             if (pos < a.list_cap) {
-              a.list_rp[pos] = make_int2((int)r, (int)(p0 + j));
-              a.list_P[pos] = P[j];
+              a.list_rp[pos] = make_int2((int)(a.list_r0 + r), (int)(p0 + j));
+              a.list_P[pos] = a.list_store_y ? yy[j] : P[j];
             }
             ++pos;
           }
@@ -1480,7 +1481,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) rowsum_kernel(const RespArgs
     const int64_t r = r0 + threadIdx.x;
     float t = 0.0f;
     for (int i = 0; i < kSweepThreads / 32; ++i) t += red[i][threadIdx.x];
-    if (r < a.R) a.Tpart[(int64_t)blockIdx.x * a.R + r] = t;
+    if (r < a.R && a.Tpart) a.Tpart[(int64_t)blockIdx.x * a.R + r] = t;
   }
 }
 
@@ -1616,6 +1617,111 @@ __global__ void compact_sort_kernel(const int2* rp, const float* Pv, int64_t n, 
       xv[pos] = P / Tr / new_scaling[v.y];
     }
   }
+}
+
+// ------------------------------------------------------ rotation chunks --
+// A maximize over rotation chunks holds Y for one chunk at a time.  After
+// each chunk the running lse (the combine over the tile partials of the
+// chunks so far) is a lower bound of the final one, so an entry whose P under
+// it is below list_min stays below it: the chunk's row-sum sweep keeps the
+// entries at or above it (rotation, pattern and y), and after the last chunk,
+// whose combine covers every tile, the lse is final.
+
+// LL of a candidate from its stored y (poisson: y; gaussian: C), in FP64.
+__device__ __forceinline__ double cand_ll(const RespArgs& a, int64_t r, int64_t p, float y) {
+  if (a.poisson) return (double)y;
+  const double phi = a.scaling[p];
+  return fma((double)y, 2.0 * a.gauss_inv / phi,
+             -a.patstat[p] / (phi * phi) * a.gauss_inv - a.rowstat[r] * a.gauss_inv);
+}
+
+// Pv[e] = exp(LL - lse_p) as probs_from forms it; T64[r] += Pv[e].
+__global__ void cand_finish_kernel(const RespArgs a, int64_t n, float* Pv, double* T64) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int2 v = a.list_rp[e];
+    const double ll = cand_ll(a, v.x, v.y, a.list_P[e]);
+    const float P = expf((float)(ll - a.lse[v.y]));
+    Pv[e] = P;
+    atomicAdd(T64 + v.x, (double)P);
+  }
+}
+
+__global__ void T_from64_kernel(const double* T64, int64_t R, float* T) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < R) T[r] = (float)T64[r];
+}
+
+__global__ void cand_scatter_kernel(const int2* rp, const float* Pv, int64_t n, int64_t N,
+                                    float* P) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int2 v = rp[e];
+    P[(int64_t)v.x * N + v.y] = Pv[e];
+  }
+}
+
+// one block per requested column
+__global__ void cand_columns_kernel(const int2* rp, const float* Pv, int64_t n,
+                                    const int64_t* cols, int64_t ncols, float* out) {
+  const int64_t a = blockIdx.x, p = cols[a];
+  for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+    const int2 v = rp[e];
+    if (v.y == p) out[(int64_t)v.x * ncols + a] = Pv[e];
+  }
+}
+
+// Total order of doubles as unsigned integers.
+__device__ __forceinline__ unsigned long long ordered_bits(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// STEP 0: key[p] = max over the pattern's candidates of LL; STEP 1: best[p]
+// = the lowest rotation whose LL is that maximum.
+template <int STEP>
+__global__ void cand_argmax_kernel(const RespArgs a, int64_t n, unsigned long long* key,
+                                   int32_t* best) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int2 v = a.list_rp[e];
+    const unsigned long long k = ordered_bits(cand_ll(a, v.x, v.y, a.list_P[e]));
+    if (STEP == 0)
+      atomicMax(key + v.y, k);
+    else if (k == key[v.y])
+      atomicMin(best + v.y, v.x);
+  }
+}
+
+// bestp[p] = exp(max LL - lse_p); a pattern without candidates gets -1, 0.
+__global__ void cand_bestp_kernel(const RespArgs a, const unsigned long long* key, int32_t* best,
+                                  float* bestp) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.N) return;
+  const unsigned long long k = key[p];
+  if (k == 0) {
+    best[p] = -1;
+    bestp[p] = 0.0f;
+    return;
+  }
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  bestp[p] = (float)exp(__longlong_as_double((long long)b) - a.lse[p]);
+}
+
+__global__ void cand_cells_kernel(const int2* rp, const float* Pv, int64_t n, const int32_t* cell,
+                                  int C, double* acc) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int2 v = rp[e];
+    atomicAdd(acc + (int64_t)v.y * C + cell[v.x], (double)Pv[e]);
+  }
+}
+
+__global__ void cells_out_kernel(const double* acc, int64_t count, int take_log, float* t) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const double v = acc[i];
+  t[i] = take_log ? (v > 0.0 ? (float)log(v) : -INFINITY) : (float)v;
 }
 
 // Compress from the lists: one block per rotation.  U_r / T_r over the active
@@ -1936,6 +2042,69 @@ cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int6
   compact_sort_kernel<1><<<g, 256, 0, st>>>(a.list_rp, a.list_P, n, a.T, a.new_scaling, rel_min,
                                             reinterpret_cast<unsigned long long*>(cursor), rowoff,
                                             pat, xv);
+  return cudaGetLastError();
+}
+
+static unsigned grid_for(int64_t n) {
+  return (unsigned)std::min<int64_t>((n + 255) / 256 + 1, 4096);
+}
+
+cudaError_t launch_list_from_candidates(RespArgs& a, int64_t n, float rel_min, float* Pv,
+                                        double* T64, int64_t* rowtot, int64_t* cursor,
+                                        int64_t* rowoff, int32_t* pat, float* xv, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(T64, 0, sizeof(double) * a.R, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(rowtot, 0, sizeof(int64_t) * a.R, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, sizeof(int64_t) * a.R, st);
+  if (e != cudaSuccess) return e;
+  const unsigned g = grid_for(n);
+  cand_finish_kernel<<<g, 256, 0, st>>>(a, n, Pv, T64);
+  T_from64_kernel<<<(unsigned)((a.R + 255) / 256), 256, 0, st>>>(T64, a.R, a.T);
+  compact_sort_kernel<0><<<g, 256, 0, st>>>(a.list_rp, Pv, n, a.T, a.new_scaling, rel_min,
+                                            reinterpret_cast<unsigned long long*>(rowtot),
+                                            nullptr, nullptr, nullptr);
+  list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, a.R, rowoff);
+  compact_sort_kernel<1><<<g, 256, 0, st>>>(a.list_rp, Pv, n, a.T, a.new_scaling, rel_min,
+                                            reinterpret_cast<unsigned long long*>(cursor), rowoff,
+                                            pat, xv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cand_scatter(const int2* rp, const float* Pv, int64_t n, int64_t N, float* P,
+                                cudaStream_t st) {
+  if (n > 0) cand_scatter_kernel<<<grid_for(n), 256, 0, st>>>(rp, Pv, n, N, P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cand_columns(const int2* rp, const float* Pv, int64_t n, const int64_t* cols,
+                                int64_t ncols, float* out, cudaStream_t st) {
+  if (n > 0 && ncols > 0)
+    cand_columns_kernel<<<(unsigned)ncols, 256, 0, st>>>(rp, Pv, n, cols, ncols, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cand_argmax(const RespArgs& a, int64_t n, unsigned long long* key,
+                               int32_t* best, float* bestp, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(key, 0, sizeof(unsigned long long) * a.N, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(best, 0x7f, sizeof(int32_t) * a.N, st);
+  if (e != cudaSuccess) return e;
+  if (n > 0) {
+    cand_argmax_kernel<0><<<grid_for(n), 256, 0, st>>>(a, n, key, best);
+    cand_argmax_kernel<1><<<grid_for(n), 256, 0, st>>>(a, n, key, best);
+  }
+  cand_bestp_kernel<<<(unsigned)((a.N + 255) / 256), 256, 0, st>>>(a, key, best, bestp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cand_cells(const int2* rp, const float* Pv, int64_t n, const int32_t* cell,
+                              int C, double* acc, cudaStream_t st) {
+  if (n > 0) cand_cells_kernel<<<grid_for(n), 256, 0, st>>>(rp, Pv, n, cell, C, acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cells_out(const double* acc, int64_t count, int take_log, float* t,
+                             cudaStream_t st) {
+  if (count > 0)
+    cells_out_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(acc, count, take_log, t);
   return cudaGetLastError();
 }
 

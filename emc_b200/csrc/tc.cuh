@@ -215,6 +215,11 @@ struct RespArgs {
   int2* list_rp;
   float* list_P;
   float list_min;
+  // rotation chunks: the sweep covers Y rows of rotations list_r0 .. list_r0
+  // + R - 1 (R, rowstat and Y are the chunk's), appends (list_r0 + r, p, y)
+  // with the stored y instead of P, and writes no Tpart (nullptr)
+  int64_t list_r0;
+  int list_store_y;
 };
 cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st);
 // The pass in two parts: combine + row sums (partials of T_r), then the
@@ -236,6 +241,32 @@ cudaError_t launch_list_rowscan(const int64_t* rowtot, int64_t R, int64_t* rowof
 cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int64_t* rowtot,
                                      int64_t* cursor, int64_t* rowoff, int32_t* pat, float* xv,
                                      cudaStream_t st);
+// After a maximize over rotation chunks (launch_resp_rowsums per chunk with
+// the running lse and list_store_y): P = exp(LL - lse_p) of the n candidates
+// into Pv (their y stay in a.list_P), T_r = sum of P over each rotation's
+// candidates (T64 [R] scratch; a.T), then the lists as launch_list_from_compact
+// forms them from (a.list_rp, Pv).  a.R, a.rowstat: every rotation.
+cudaError_t launch_list_from_candidates(RespArgs& a, int64_t n, float rel_min, float* Pv,
+                                        double* T64, int64_t* rowtot, int64_t* cursor,
+                                        int64_t* rowoff, int32_t* pat, float* xv, cudaStream_t st);
+// Exports of a chunked iteration from its candidates (rp, Pv; n of them):
+// dense P [R][N] (zeroed by the caller) ...
+cudaError_t launch_cand_scatter(const int2* rp, const float* Pv, int64_t n, int64_t N, float* P,
+                                cudaStream_t st);
+// ... columns out[r][a] of patterns cols[a] (zeroed by the caller) ...
+cudaError_t launch_cand_columns(const int2* rp, const float* Pv, int64_t n, const int64_t* cols,
+                                int64_t ncols, float* out, cudaStream_t st);
+// ... most probable rotation per pattern (largest LL from the stored y;
+// ties to the lower rotation) and its P (key [N] scratch) ...
+cudaError_t launch_cand_argmax(const RespArgs& a, int64_t n, unsigned long long* key,
+                               int32_t* best, float* bestp, cudaStream_t st);
+// ... and the responsibility mass per (pattern, cell) in FP64 (acc [N][C],
+// zeroed by the caller), then t = acc or t = log(acc) (-inf where 0).
+cudaError_t launch_cand_cells(const int2* rp, const float* Pv, int64_t n, const int32_t* cell,
+                              int C, double* acc, cudaStream_t st);
+cudaError_t launch_cells_out(const double* acc, int64_t count, int take_log, float* t,
+                             cudaStream_t st);
+
 // Compress from the lists with the counts' photon lists (kptr [N+1], kidx =
 // active pixel, kval = count): one block per rotation accumulates its slice
 // in shared memory (npa floats) and inserts it as the contraction's epilogue

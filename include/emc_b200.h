@@ -149,6 +149,30 @@ emc_status emc_stage_times(emc_context *ctx, float ms[5]);
  * held.  emc_memory_used: device bytes the context holds. */
 emc_status emc_set_memory_limit(emc_context *ctx, size_t bytes);
 size_t emc_memory_used(const emc_context *ctx);
+/* Rotation chunks (mixed contexts).  The log-likelihood Y of a dense
+ * iteration takes R x N x 4 bytes; with chunks of `rows` rotations (a
+ * multiple of 256) Y holds one chunk at a time: per chunk the contraction,
+ * an online log-sum-exp over the tile partials of the chunks so far, and a
+ * sweep that keeps every entry whose responsibility under that running
+ * log-sum-exp is at least 1e-30 (it can only fall later).  The last chunk's
+ * log-sum-exp is final; lse, scaling and sum P log P are those of the
+ * unchunked iteration, and the compress reads the responsibility lists
+ * formed from the kept entries (the dense compress operand P' is not
+ * allocated).  The last chunk holds the remainder (uneven).
+ * rows: 0 = one chunk of every rotation; -1 = the most rotations whose Y
+ * fits in half of what the memory limit and the free device memory leave.
+ * capacity: entries the kept-entry arrays start with (0: max(64 N, 2^20));
+ * an iteration that keeps more grows them and runs its chunks again.
+ * emc_set_geometry already chooses chunks (rows -1) when Y and P' of every
+ * rotation do not fit.  EMC_ERR_UNSUPPORTED for FP32 contexts and above
+ * 51,200 active pixels (the responsibility lists' limit); EMC_ERR_STATE
+ * inside an iteration or a batch (a batch takes unchunked contexts only).
+ * After a chunked iteration the responsibilities are read as usual
+ * (emc_get_buffer EMC_BUF_RESP, emc_get_resp_columns, emc_orientation_stats,
+ * emc_cell_targets, emc_cell_log_mass) from the kept entries, 0 elsewhere.
+ * emc_rotation_chunk: the rotations Y holds (R when unchunked). */
+emc_status emc_set_rotation_chunk(emc_context *ctx, int64_t rows, int64_t capacity);
+int64_t emc_rotation_chunk(const emc_context *ctx);
 /* Checkpoint (emc.c:715-716 resumes from a model file at start_iteration;
  * this keeps the whole state): model, weight grid and per-pattern scaling
  * with the iteration number, in a raw little-endian file.  The model and the

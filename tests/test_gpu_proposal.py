@@ -340,6 +340,41 @@ def test_topk_iteration_matches_restricted_oracle(prec, use_probs, use_keep, tol
         assert np.abs(lm[big] - np.log(t_ref[big])).max() <= 1e-2
 
 
+@pytest.mark.parametrize("coarse_n", [1, 2])
+def test_grouped_forms_agree(coarse_n):
+    """The grouped maximize on SM pairs and on one SM, each with the compress
+    from responsibility lists and with the grouped tensor-core compress, give
+    the same scaling and model; 60 or 420 uneven cells, ragged slot counts
+    (301 patterns)."""
+    import torch
+
+    from emc_b200 import workloads as W
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    d = W.make("tiny16", n_patterns=301)
+    q, w, cell, n_cells = sorted_rotations(d["q"], d["w"], coarse_n=coarse_n)
+    d = dict(d, q=q, w=w)
+    N = d["counts"].shape[0]
+    rng = np.random.default_rng(11)
+    z = rng.standard_normal((N, n_cells)) * 2.0
+    probs = np.exp(z - z.max(1, keepdims=True))
+    probs = torch.from_numpy((probs / probs.sum(1, keepdims=True)).astype(np.float32)).cuda()
+    out = {}
+    for pair in (1, 0):
+        for lists in (True, False):
+            with make_ctx(d, "poisson", "nearest", "mixed") as ctx:
+                ctx.set_tuning(1, 6, pair, 0)
+                ctx.set_sparse_compress(lists)
+                lp = LearnedProposal(ctx, cell, n_cells)
+                st = lp.iterate_topk(probs, None, top_k=1, max_cells=9, mass_target=0.8)
+                assert st["fallback"] == 0
+                out[pair, lists] = (ctx.get_model(), ctx.get_scaling(), st["pairs"])
+    ref = out[1, True]
+    for key, (m, phi, pairs) in out.items():
+        assert pairs == ref[2]
+        assert rel(phi, ref[1]) <= 1e-6, (key, rel(phi, ref[1]))
+        assert rel(m, ref[0]) <= 1e-5, (key, rel(m, ref[0]))
+
+
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])
 def test_log_mass_of_a_dense_iteration(prec):
     """emc_cell_log_mass after a dense maximize: log of the oracle's per-cell
