@@ -61,6 +61,10 @@ def parse():
     ap.add_argument("--likelihood", default="poisson", choices=["poisson", "gauss"])
     ap.add_argument("--interp", default="nearest", choices=["nearest", "trilinear"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
+    ap.add_argument("--rotation-chunk", type=int, default=0,
+                    help="rotations the log-likelihood buffer holds at a time (0: all)")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="order-independent insertion sums (bitwise reproducible)")
     ap.add_argument("--fp32-steps", type=int, default=3, help="steps of the plain FP32 comparison")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -294,7 +298,9 @@ def config_desc(a, d):
                         f"(beamstop r={w.beamstop:g}, {npa} active px), {R} rotations, {N} patterns, "
                         f"{a.likelihood} likelihood, {a.interp} interpolation",
             "precision": a.precision, "patterns": N, "rotations": R, "active_pixels": npa,
-            "l2": "inputs larger than L2"}
+            "l2": "inputs larger than L2"} | (
+        {"rotation_chunk": a.rotation_chunk} if getattr(a, "rotation_chunk", 0) else {}) | (
+        {"insertion": "deterministic"} if getattr(a, "deterministic", False) else {})
 
 
 # ------------------------------------------------------- learned proposal --
@@ -621,6 +627,10 @@ def main():
         c.set_patterns(d["counts"])
         c.set_model(d["model0"])
         c.set_scaling(d["scaling0"])
+        if a.rotation_chunk and precision == "mixed":
+            c.set_rotation_chunk(a.rotation_chunk)
+        if a.deterministic:
+            c.set_deterministic(True)
         return c
 
     from emc_b200.parallel import ShardedIteration

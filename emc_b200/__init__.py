@@ -112,6 +112,7 @@ def lib():
             ("emc_memory_used", [P], C.c_size_t),
             ("emc_set_rotation_chunk", [P, C.c_int64, C.c_int64], C.c_int),
             ("emc_rotation_chunk", [P], C.c_int64),
+            ("emc_set_deterministic", [P, C.c_int], C.c_int),
             ("emc_save_state", [P, C.c_char_p, I64], C.c_int),
             ("emc_load_state", [P, C.c_char_p, P], C.c_int),
         ]:
@@ -473,6 +474,11 @@ class Context:
         rotations at a time (a multiple of 256; 0 = all, -1 = what fits the
         memory limit); capacity = initial kept-entry capacity (0: default)."""
         self._c(lib().emc_set_rotation_chunk(self._h, int(rows), int(capacity)))
+
+    def set_deterministic(self, on=True):
+        """emc_set_deterministic: order-independent (bitwise reproducible)
+        insertion sums and responsibility lists."""
+        self._c(lib().emc_set_deterministic(self._h, int(bool(on))))
 
     @property
     def rotation_chunk(self):

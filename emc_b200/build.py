@@ -16,7 +16,7 @@ OUT = os.path.join(HERE, "libemc_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
 SOURCES = ["host.cpp", "kernels_fp32.cu", "kernels_tc.cu", "context.cu", "legacy.cu", "noalloc.cu",
            "net.cu", "proposal.cu"]
-HEADERS = ["voxel.h", "kernels.cuh", "tc.cuh", "tile.cuh", "proposal.cuh"]
+HEADERS = ["voxel.h", "kernels.cuh", "tc.cuh", "tile.cuh", "proposal.cuh", "fixed.cuh"]
 PUBLIC = [os.path.join(REPO, "include", h) for h in ("emc.h", "emc_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST = ["-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off,-O3"]

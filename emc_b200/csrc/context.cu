@@ -186,6 +186,14 @@ struct emc_context {
   // y) and their final P (d_cand_P) until the next maximize
   int64_t y_rows = 0, cand_n = 0, cand_cap_min = 0, cand_P_cap = 0;
   bool batched = false;  // a member of an emc_batch
+  // deterministic insertion: fixed-point limbs [M][8] (fixed.cuh) and the
+  // scratch of the (rotation, pattern) sort of the responsibility lists
+  bool det = false;
+  unsigned long long* d_acc64 = nullptr;
+  int2* d_sort_rp = nullptr;
+  float* d_sort_v = nullptr;
+  int64_t *d_sort_hist = nullptr, *d_sort_flag = nullptr;
+  int64_t sort_cap = 0, sort_cap2 = 0, sort_hist_cap = 0, sort_flag_cap = 0;
   float* d_cand_P = nullptr;
   double* d_T64 = nullptr;
   unsigned long long* d_cand_key = nullptr;
@@ -490,6 +498,15 @@ emc_status emc_set_rotation_chunk(emc_context* c, int64_t rows, int64_t capacity
 
 int64_t emc_rotation_chunk(const emc_context* c) { return c ? c->y_rows : 0; }
 
+emc_status emc_set_deterministic(emc_context* c, int on) {
+  if (!c || (on != 0 && on != 1)) return EMC_ERR_ARG;
+  if (c->stage != 0 || c->batched)
+    return c->fail(EMC_ERR_STATE, "the insertion mode changes between iterations, outside a batch");
+  if (on && !c->d_acc64) TRY(c->alloc(&c->d_acc64, 8 * c->M));
+  c->det = on != 0;
+  return EMC_OK;
+}
+
 emc_status emc_set_profiling(emc_context* c, int on) {
   if (!c) return EMC_ERR_ARG;
   if (on && !c->ev[0][0])
@@ -593,6 +610,9 @@ static emc_status alloc_work(emc_context* c) {
   c->Rpad = round_up(R, 256);
   c->nrt = c->Rpad / 256;
   TRY(c->alloc(&c->d_acc, c->M, true));
+  // the nearest expansion's voxel table (here rather than at the first
+  // expansion, so an iteration can be captured into a graph before any ran)
+  if (c->cfg.interp == EMC_INTERP_NEAREST) TRY(c->alloc(&c->d_vtab, c->M + 1));
   TRY(c->alloc(&c->d_Kh, c->Npad * c->Ppad, true));
   TRY(c->alloc(&c->d_Kt, c->Ppad * c->Npad, true));
   TRY(c->alloc(&c->d_Bhi, c->Rpad * c->Ppad, true));
@@ -987,6 +1007,15 @@ static emc_status compact_capacity(emc_context* c, int64_t n) {
   return EMC_OK;
 }
 
+// Scratch of the deterministic (rotation, pattern) sort of n entries.
+static emc_status sort_scratch(emc_context* c, int64_t n) {
+  TRY(grow(c, &c->d_sort_rp, c->sort_cap, n + 1));
+  TRY(grow(c, &c->d_sort_v, c->sort_cap2, n + 1));
+  TRY(grow(c, &c->d_sort_hist, c->sort_hist_cap, sort_hist_size(n)));
+  TRY(grow(c, &c->d_sort_flag, c->sort_flag_cap, 2 * n + 2));
+  return EMC_OK;
+}
+
 static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
   const int64_t N = c->N;
   RespArgs a = resp_args(c);
@@ -1015,8 +1044,20 @@ static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
       int64_t cap = c->lcap_x;
       TRY(grow(c, &c->d_lx, cap, c->list_nnz + 1));
       c->lcap_x = cap;
-      CK(c, launch_list_from_compact(a, c->list_nnz, kListRel, c->d_lrowtot, c->d_lcursor,
-                                     c->d_lrowoff, c->d_lpat, c->d_lx, c->st));
+      if (c->det) {
+        // the entries in (rotation, pattern) order, so the lists do not
+        // depend on the order the sweep appended them
+        TRY(sort_scratch(c, c->list_nnz));
+        CK(c, launch_finish_T(c->d_Tpart, N, c->R, c->d_T, c->st));
+        CK(c, launch_sort_entries(c->d_lcomp_rp, c->d_lcomp_P, c->list_nnz, N, c->R,
+                                  c->d_sort_rp, c->d_sort_v, c->d_sort_hist, c->st));
+        CK(c, launch_list_from_sorted(c->d_lcomp_rp, c->d_lcomp_P, c->list_nnz, c->R, c->d_T,
+                                      c->d_scaling, kListRel, c->d_lrowtot, c->d_lrowoff,
+                                      c->d_sort_flag, c->d_lpat, c->d_lx, c->st));
+      } else {
+        CK(c, launch_list_from_compact(a, c->list_nnz, kListRel, c->d_lrowtot, c->d_lcursor,
+                                       c->d_lrowoff, c->d_lpat, c->d_lx, c->st));
+      }
       c->list_mode = true;
       c->launches += 6;  // combine, row sums, T, count, scan, fill
     } else {
@@ -1110,8 +1151,23 @@ static emc_status chunked_maximize(emc_context* c) {
   a.R = R;
   a.rowstat = c->d_rowstat;
   a.list_r0 = 0;
-  CK(c, launch_list_from_candidates(a, c->cand_n, kListRel, c->d_cand_P, c->d_T64, c->d_lrowtot,
-                                    c->d_lcursor, c->d_lrowoff, c->d_lpat, c->d_lx, c->st));
+  if (c->det) {
+    // candidates in (rotation, pattern) order, then P, T_r summed in that
+    // order and the lists in it
+    TRY(sort_scratch(c, c->cand_n));
+    CK(c, launch_sort_entries(c->d_lcomp_rp, c->d_lcomp_P, c->cand_n, N, R, c->d_sort_rp,
+                              c->d_sort_v, c->d_sort_hist, c->st));
+    CK(c, launch_cand_probs(a, c->cand_n, c->d_cand_P, c->d_T64, c->st));
+    CK(c, launch_T_from_sorted(c->d_lcomp_rp, c->d_cand_P, c->cand_n, R, c->d_lrowtot,
+                               c->d_lrowoff, c->d_T, c->st));
+    CK(c, launch_list_from_sorted(c->d_lcomp_rp, c->d_cand_P, c->cand_n, R, c->d_T, c->d_scaling,
+                                  kListRel, c->d_lrowtot, c->d_lrowoff, c->d_sort_flag, c->d_lpat,
+                                  c->d_lx, c->st));
+  } else {
+    CK(c, launch_list_from_candidates(a, c->cand_n, kListRel, c->d_cand_P, c->d_T64,
+                                      c->d_lrowtot, c->d_lcursor, c->d_lrowoff, c->d_lpat,
+                                      c->d_lx, c->st));
+  }
   c->list_mode = true;
   CK(c, launch_sum_f64(c->d_plogp, N, c->d_stats + 2, c->st));
   CK(c, launch_sum_f64(c->d_lse, N, c->d_stats + 3, c->st));
@@ -1298,7 +1354,9 @@ emc_status emc_compress_insert(emc_context* c) {
   if (!c) return EMC_ERR_ARG;
   if (c->stage != 2) return c->fail(EMC_ERR_STATE, "compress called before maximize");
   // emc.c:1025-1026 reset, then emc_cuda.cu:292-362 insert, :414-433 normalise
-  if (!c->mixed) {
+  if (c->det) {
+    CK(c, cudaMemsetAsync(c->d_acc64, 0, sizeof(unsigned long long) * 8 * c->M, c->st));
+  } else if (!c->mixed) {
     CK(c, cudaMemsetAsync(c->d_model, 0, sizeof(float) * c->M, c->st));
     CK(c, cudaMemsetAsync(c->d_weight, 0, sizeof(float) * c->M, c->st));
   } else {
@@ -1338,10 +1396,12 @@ emc_status emc_compress_insert(emc_context* c) {
     in.interp = c->cfg.interp;
     in.model = c->d_model;
     in.weight = c->d_weight;
+    in.acc64 = c->det ? c->d_acc64 : nullptr;
     CK(c, launch_insert(in, c->st));
     c->launches += 2;
   } else {
     CmpEpiArgs e = cmp_args(c);
+    e.acc64 = c->det ? c->d_acc64 : nullptr;
     if (c->list_mode) {
       // responsibility lists x the counts' photon lists (built once per upload)
       if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
@@ -1353,6 +1413,7 @@ emc_status emc_compress_insert(emc_context* c) {
       la.kidx = c->csr.idx;
       la.kval = c->csr.val;
       la.e = e;
+      la.ordered = c->det ? 1 : 0;
       CK(c, launch_list_compress(la, c->st));
     } else if (c->tune.compress_pair) {
       CK(c, launch_compress_pair_tc(c->tmPhi, c->tmPlo, c->tmKt128, c->Rpad, c->Ppad, c->Npad, e,
@@ -1361,6 +1422,16 @@ emc_status emc_compress_insert(emc_context* c) {
       CK(c, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
                                c->d_status, c->num_sms, c->st, c->tune.compress_raster));
     }
+    c->launches += 1;
+  }
+  if (c->det) {
+    // the exact sums as the FP32 accumulators the normalisation (and a
+    // pattern-sharded caller's all-reduce) read
+    if (c->mixed)
+      CK(c, launch_fixed_to_pairs(c->d_acc64, c->M, reinterpret_cast<float*>(c->d_acc),
+                                  reinterpret_cast<float*>(c->d_acc) + 1, 2, c->st));
+    else
+      CK(c, launch_fixed_to_pairs(c->d_acc64, c->M, c->d_model, c->d_weight, 1, c->st));
     c->launches += 1;
   }
   c->mark(4);
@@ -2200,15 +2271,16 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
   const int64_t MM = tc ? 256 : c->max_members;
   TRY(grow(c, &c->d_gpair, c->slots_cap, S));
   TRY(grow(c, &c->d_Yc, c->yc_cap, S * MM));
-  TRY(grow(c, &c->d_Pt, c->pt_cap, evals));
+  // compress from responsibility lists (as the dense mixed iteration does);
+  // the grouped compresses read the per-cell operand Pt instead
+  const bool lists = tc && c->tune.compress_sparse && c->npa <= kListMaxPixels;
+  if (!lists) TRY(grow(c, &c->d_Pt, c->pt_cap, evals));
   std::vector<int4> mt, ct;
   int64_t n_gmt = 0, n_gct = 0;
   TileDesc *gmt = nullptr, *gct = nullptr;
   // the grouped maximize on SM pairs (256-slot tiles) where the dense one is
   const bool gpair_form = tc && c->tune.maximize_pair;
   const int32_t gm_rows = gpair_form ? 256 : 128;
-  // compress from responsibility lists (as the dense mixed iteration does)
-  const bool lists = c->tune.compress_sparse && c->npa <= kListMaxPixels;
   if (tc) {
     const int64_t ptiles = (c->npa + 255) / 256;
     for (int32_t k = 0; k < n_cells; ++k)
@@ -2300,7 +2372,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
   g.patsum = c->d_patsum;
   g.gauss_inv = gauss_inv(c);
   g.Y = c->d_Yc;
-  g.Pt = c->d_Pt;
+  g.Pt = lists ? nullptr : c->d_Pt;
   g.T = c->d_T;
   g.lse = c->d_lse_c;
   g.plogp = c->d_plogp_c;
@@ -2325,7 +2397,14 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     CUtensorMap tmKg, tmKg64, tmAhi, tmAlo;
     if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, gpair_form ? kPairBoxK : kMaximizeBK))
       return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
-    CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->st));
+    if (slot_rows_fit(c->Ppad)) {
+      // the slot rows from the photon lists (writes the rows, reads the lists)
+      if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
+      CK(c, launch_slot_rows(c->csr.ptr, c->csr.idx, c->csr.val, c->Ppad, c->d_gpair, S, c->d_Kg,
+                             c->st));
+    } else {
+      CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->st));
+    }
     if (!lists &&
         (!tc_encode_2d(&tmKg64, c->d_Kg, c->Ppad, S, kCompressBK, 64) ||
          !tc_encode_2d_strided(&tmAhi, c->d_Ahi, c->a_ld, R, c->a_ld, 128, kCompressBK) ||
@@ -2445,6 +2524,7 @@ emc_status emc_iterate_proposed(emc_context* c, const float* probs, const float*
   if (!c || !probs || m < 1 || min_m < 1 || min_m > m) return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
   if (m > c->n_cells) return c->fail(EMC_ERR_ARG, "more cells per pattern than cells");
+  if (c->det) return c->fail(EMC_ERR_UNSUPPORTED, "deterministic insertion is a dense-iteration mode");
   ProposedPlan pl;
   pl.m = m;
   pl.threshold = threshold;
@@ -2461,6 +2541,7 @@ emc_status emc_iterate_topk(emc_context* c, const float* probs, const float* log
       !(cfg->keep_tail >= 0.0f && cfg->keep_tail < 1.0f))
     return EMC_ERR_ARG;
   if (!c->n_cells) return c->fail(EMC_ERR_STATE, "emc_set_cells first");
+  if (c->det) return c->fail(EMC_ERR_UNSUPPORTED, "deterministic insertion is a dense-iteration mode");
   const int32_t m = std::min<int32_t>(cfg->max_cells, c->n_cells);
   ProposedPlan pl;
   pl.m = m;
@@ -2583,8 +2664,9 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
     if (!c->have_geom || !c->have_rot || !c->have_pat || !c->have_model || c->stage != 0 ||
         c->batched)
       return EMC_ERR_STATE;
-    // the batched contractions read every rotation's Y and P'
-    if (c->y_rows < c->R) return EMC_ERR_UNSUPPORTED;
+    // the batched contractions read every rotation's Y and P' and insert
+    // with FP32 atomics
+    if (c->y_rows < c->R || c->det) return EMC_ERR_UNSUPPORTED;
     for (int32_t k = 0; k < i; ++k)
       if (ctxs[k] == c) return EMC_ERR_ARG;
   }

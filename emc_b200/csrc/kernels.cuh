@@ -168,8 +168,14 @@ struct InsertArgs {
   int side, interp;
   float* model;
   float* weight;
+  // deterministic insertion: fixed-point limbs [M][8] (fixed.cuh) instead of
+  // FP32 atomics into model and weight
+  unsigned long long* acc64;
 };
 cudaError_t launch_insert(const InsertArgs& a, cudaStream_t st);
+// The fixed-point sums (fixed.cuh) as FP32 pairs a[i stride], b[i stride].
+cudaError_t launch_fixed_to_pairs(const unsigned long long* acc64, int64_t M, float* a, float* b,
+                                  int64_t stride, cudaStream_t st);
 
 // model = weight > 0 ? model / weight : 0; then model /= mean; stats[0] = mean,
 // stats[1] = max after normalisation.  fp64 selects the FP64 division.

@@ -5,6 +5,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "fixed.cuh"
 #include "kernels.cuh"
 #include "tile.cuh"
 #include "voxel.h"
@@ -489,25 +490,45 @@ __global__ void __launch_bounds__(kBlock) insert_kernel(const InsertArgs a) {
     float u[3];
     emc_voxel::position(m, a.side, a.cx[i], a.cy[i], a.cz[i], u);
     const float s = a.U[r * a.ldU + i];
+    // FP32 atomics, or the order-independent fixed-point limbs
+    auto add = [&](int64_t v, float x, float y) {
+      if (a.acc64) {
+        add_fixed(a.acc64 + 8 * v, x);
+        add_fixed(a.acc64 + 8 * v + 4, y);
+      } else {
+        atomicAdd(a.model + v, x);
+        atomicAdd(a.weight + v, y);
+      }
+    };
     if (a.interp == 0) {
       int64_t v;
       if (!emc_voxel::nearest(u, a.side, 0, &v)) continue;
-      atomicAdd(a.model + v, w * s);
-      atomicAdd(a.weight + v, w);
+      add(v, w * s, w);
     } else {
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         int64_t v;
         float wc;
         if (!emc_voxel::trilinear_corner(u, a.side, c, &v, &wc) || wc == 0.0f) continue;
-        atomicAdd(a.model + v, wc * w * s);
-        atomicAdd(a.weight + v, wc * w);
+        add(v, wc * w * s, wc * w);
       }
     }
   }
 }
 
 // ------------------------------------------------------------- normalise --
+// Fixed-point accumulators -> FP32 (value, weight) pairs: a[i*stride],
+// b[i*stride] (the FP32 path's model and weight, or the mixed path's
+// interleaved accumulators), each sum rounded once.
+__global__ void fixed_to_pairs_kernel(const unsigned long long* acc64, int64_t M, float* a,
+                                      float* b, int64_t stride) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    a[i * stride] = (float)fixed_value(acc64 + 8 * i);
+    b[i * stride] = (float)fixed_value(acc64 + 8 * i + 4);
+  }
+}
+
 __global__ void divide_kernel(float* model, const float* weight, int64_t M, int fp64,
                               double* part) {
   __shared__ double red[32];
@@ -935,6 +956,12 @@ cudaError_t launch_normalize_model(float* model, const float* weight, int64_t M,
   sum_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, scratch + kReduceBlocks);
   scale_max_kernel<<<g, kBlock, 0, st>>>(model, M, scratch + kReduceBlocks, fp64, stats, scratch);
   max_f64_kernel<<<1, kBlock, 0, st>>>(scratch, g, stats + 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fixed_to_pairs(const unsigned long long* acc64, int64_t M, float* a, float* b,
+                                  int64_t stride, cudaStream_t st) {
+  fixed_to_pairs_kernel<<<grid_for(M), kBlock, 0, st>>>(acc64, M, a, b, stride);
   return cudaGetLastError();
 }
 

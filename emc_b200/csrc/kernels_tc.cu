@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <type_traits>
 
+#include "fixed.cuh"
 #include "tc.cuh"
 #include "voxel.h"
 
@@ -141,6 +142,14 @@ template <class E, class = void>
 struct b_major_mn : std::false_type {};
 template <class E>
 struct b_major_mn<E, std::void_t<decltype(E::kBMajorMN)>> : std::bool_constant<E::kBMajorMN> {};
+
+// Listed pair epilogues with kCellN = true narrow each tile's MMA to its
+// cell's members rounded up to 16 (epi.a.mcnt[cell]); each CTA of the pair
+// then holds half of that many B rows.
+template <class E, class = void>
+struct cell_n : std::false_type {};
+template <class E>
+struct cell_n<E, std::void_t<decltype(E::kCellN)>> : std::bool_constant<E::kCellN> {};
 
 struct Ctl {
   volatile int* abort;
@@ -588,6 +597,16 @@ using EpiMax = EpiMaxT<4>;
 __device__ __forceinline__ void red_add_v2(float2* p, float x, float y) {
   asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(x), "f"(y) : "memory");
 }
+// The same into the context's accumulators: FP32, or the order-independent
+// fixed-point limbs of the deterministic mode.
+__device__ __forceinline__ void insert_add(const CmpEpiArgs& e, int64_t vox, float x, float y) {
+  if (e.acc64) {
+    add_fixed(e.acc64 + 8 * vox, x);
+    add_fixed(e.acc64 + 8 * vox + 4, y);
+  } else {
+    red_add_v2(e.acc + vox, x, y);
+  }
+}
 
 // compress: row = rotation, column = active pixel; inserts into model/weight.
 struct EpiCmp {
@@ -642,7 +661,7 @@ struct EpiCmp {
         emc_voxel::position(m, a.side, q.x, q.y, q.z, u);
         int64_t vox;
         if (!emc_voxel::nearest(u, a.side, 0, &vox)) continue;
-        red_add_v2(a.acc + vox, __uint_as_float(v[k]) * wU, wT);
+        insert_add(a, vox, __uint_as_float(v[k]) * wU, wT);
       }
     } else {
 #pragma unroll
@@ -657,7 +676,7 @@ struct EpiCmp {
           int64_t vox;
           float wc;
           if (!emc_voxel::trilinear_corner(u, a.side, cc, &vox, &wc) || wc == 0.0f) continue;
-          red_add_v2(a.acc + vox, wc * val, wc * wT);
+          insert_add(a, vox, wc * val, wc * wT);
         }
       }
     }
@@ -734,6 +753,7 @@ struct EpiGMax {
 // pair tile's first slot), this CTA's accumulator holds slots 128 rank ..
 // 128 rank + 127 of it against all the tile's member columns.
 struct EpiGMaxPair : EpiGMax {
+  static constexpr bool kCellN = true;  // MMAs as wide as the cell (rounded up to 16)
   __device__ void tile_begin(int64_t t, int64_t x, int tid, uint8_t* smem) {
     EpiGMax::tile_begin(t, x, tid, smem);
     uint32_t rank;
@@ -1108,6 +1128,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
           const TileDesc d = epi.a.tiles[t];
           ar = d.a_row + (int)rank * 128;
           br = d.b_row + (int)rank * 128;
+          if constexpr (cell_n<Epi>::value)
+            br = d.b_row + (int)rank * (((epi.a.mcnt[d.cell] + 15) & ~15) / 2);
           kbs = d.k_blocks;
           set = d.set;
         } else {
@@ -1184,7 +1206,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
         int64_t kbs = k_blocks;
-        if constexpr (Epi::kListed) kbs = epi.a.tiles[t].k_blocks;
+        uint32_t idesc = kIdescPair;
+        if constexpr (Epi::kListed) {
+          const TileDesc td = epi.a.tiles[t];
+          kbs = td.k_blocks;
+          if constexpr (cell_n<Epi>::value) {
+            // N = the cell's members rounded up to 16 (bits 17..22: N >> 3)
+            const uint32_t n16 = (uint32_t)((epi.a.mcnt[td.cell] + 15) & ~15);
+            idesc = (kIdescPair & ~(0x3Fu << 17)) | ((n16 >> 3) << 17);
+          }
+        }
         for (int64_t kb = 0; kb < kbs; ++kb) {
           if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3)) {
             ok = false;
@@ -1200,7 +1231,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
             for (int q = 0; q < 2; ++q)
               mma_f16_pair(d, sdesc<kPairBK>(base + (NA == 2 ? q : 0) * A_BYTES + k * 32),
                            sdesc<kPairBK>(bbase + (NB == 2 ? q : 0) * B_BYTES + k * 32),
-                           kIdescPair, (kb | k | q) != 0);
+                           idesc, (kb | k | q) != 0);
           }
           // release this stage in both CTAs once its MMAs are done
           const uint32_t eb = smem_u32(&empty_bar[s]);
@@ -1724,6 +1755,101 @@ __global__ void cells_out_kernel(const double* acc, int64_t count, int take_log,
   t[i] = take_log ? (v > 0.0 ? (float)log(v) : -INFINITY) : (float)v;
 }
 
+// --------------------------------------------- deterministic list order --
+// The compaction appends entries in the order warps reach it.  For the
+// deterministic mode they are sorted by (rotation, pattern) with a stable
+// LSD radix sort, 8 bits per pass (pattern bits first): per tile of
+// kSortTile entries the digit counts hist[digit][tile], one exclusive scan
+// over them digit-major, then one warp per tile writes its entries in order
+// (ranks within a warp's 32 entries by __match_any_sync).
+constexpr int kSortTile = 1024;
+
+__device__ __forceinline__ uint32_t sort_digit(int2 v, int field, int shift) {
+  return ((uint32_t)(field ? v.x : v.y) >> shift) & 0xffu;
+}
+
+__global__ void radix_hist_kernel(const int2* rp, int64_t n, int field, int shift,
+                                  int64_t ntiles, int64_t* hist) {
+  __shared__ int cnt[256];
+  const int64_t tile = blockIdx.x;
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) cnt[d] = 0;
+  __syncthreads();
+  const int64_t e0 = tile * kSortTile;
+  for (int64_t e = e0 + threadIdx.x; e < n && e < e0 + kSortTile; e += blockDim.x)
+    atomicAdd(&cnt[sort_digit(rp[e], field, shift)], 1);
+  __syncthreads();
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(int64_t)d * ntiles + tile] = cnt[d];
+}
+
+__global__ void radix_scatter_kernel(const int2* rp, const float* v, int64_t n, int field,
+                                     int shift, int64_t ntiles, const int64_t* off, int2* rp2,
+                                     float* v2) {
+  __shared__ int64_t base[256];
+  const int64_t tile = blockIdx.x;
+  const int lane = threadIdx.x;
+  for (int d = lane; d < 256; d += 32) base[d] = off[(int64_t)d * ntiles + tile];
+  __syncwarp();
+  const int64_t e0 = tile * kSortTile;
+  const int64_t e1 = e0 + kSortTile < n ? e0 + kSortTile : n;
+  for (int64_t c = e0; c < e1; c += 32) {
+    const int64_t e = c + lane;
+    const unsigned active = __ballot_sync(0xffffffffu, e < e1);
+    if (e < e1) {
+      const int2 x = rp[e];
+      const uint32_t d = sort_digit(x, field, shift);
+      const unsigned peers = __match_any_sync(active, d);
+      const int rank = __popc(peers & ((1u << lane) - 1u));
+      const int64_t pos = base[d] + rank;
+      rp2[pos] = x;
+      v2[pos] = v[e];
+      __syncwarp(active);
+      // the group's last lane moves the digit's offset past the group
+      if ((peers >> lane) == 1u) base[d] += __popc(peers);
+    }
+    __syncwarp();
+  }
+}
+
+// Entries sorted by rotation: rowtot[r] = entries of row r (all, or those
+// kept by the list filter P >= rel_min T_r, T_r > 0), flag[e] = kept.
+__global__ void sorted_count_kernel(const int2* rp, const float* Pv, int64_t n, const float* T,
+                                    float rel_min, int filter, unsigned long long* rowtot,
+                                    int64_t* flag) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int2 v = rp[e];
+    bool keep = true;
+    if (filter) {
+      const float Tr = T[v.x];
+      keep = Tr > 0.0f && Pv[e] >= rel_min * Tr;
+    }
+    if (flag) flag[e] = keep ? 1 : 0;
+    if (keep) atomicAdd(rowtot + v.x, 1ull);
+  }
+}
+
+// T_r = sum of the row's sorted entries in order (FP64).
+__global__ void sorted_T_kernel(const float* Pv, const int64_t* rowoff, int64_t R, float* T) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  double t = 0.0;
+  for (int64_t e = rowoff[r]; e < rowoff[r + 1]; ++e) t += Pv[e];
+  T[r] = (float)t;
+}
+
+// Kept entries to their list positions (the exclusive scan of flag).
+__global__ void sorted_place_kernel(const int2* rp, const float* Pv, int64_t n, const float* T,
+                                    const float* new_scaling, const int64_t* flag,
+                                    const int64_t* pos, int32_t* pat, float* xv) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    if (!flag[e]) continue;
+    const int2 v = rp[e];
+    pat[pos[e]] = v.y;
+    xv[pos[e]] = Pv[e] / T[v.x] / new_scaling[v.y];
+  }
+}
+
 // Compress from the lists: one block per rotation.  U_r / T_r over the active
 // pixels is accumulated in shared memory from the listed patterns' photon
 // lists (x times each non-zero count), then inserted exactly as the dense
@@ -1737,11 +1863,24 @@ __global__ void __launch_bounds__(256) list_compress_kernel(const ListCmpArgs a)
   for (int64_t j = threadIdx.x; j < e.npa; j += blockDim.x) Us[j] = 0.0f;
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int64_t q = a.rowoff[r] + w; q < a.rowoff[r + 1]; q += blockDim.x >> 5) {
-    const int64_t p = a.pat[q];
-    const float x = a.xv[q];
-    for (int64_t t = a.kptr[p] + lane; t < a.kptr[p + 1]; t += 32)
-      atomicAdd(&Us[a.kidx[t]], x * a.kval[t]);
+  if (a.ordered) {
+    // the listed patterns in list order by one warp: a pattern's photons lie
+    // on distinct pixels, so each pixel sums its terms in that order
+    if (w == 0)
+      for (int64_t q = a.rowoff[r]; q < a.rowoff[r + 1]; ++q) {
+        const int64_t p = a.pat[q];
+        const float x = a.xv[q];
+        for (int64_t t = a.kptr[p] + lane; t < a.kptr[p + 1]; t += 32)
+          Us[a.kidx[t]] += x * a.kval[t];
+        __syncwarp();
+      }
+  } else {
+    for (int64_t q = a.rowoff[r] + w; q < a.rowoff[r + 1]; q += blockDim.x >> 5) {
+      const int64_t p = a.pat[q];
+      const float x = a.xv[q];
+      for (int64_t t = a.kptr[p] + lane; t < a.kptr[p + 1]; t += 32)
+        atomicAdd(&Us[a.kidx[t]], x * a.kval[t]);
+    }
   }
   __syncthreads();
   const float wT = e.rotw[r] * T;
@@ -1754,14 +1893,14 @@ __global__ void __launch_bounds__(256) list_compress_kernel(const ListCmpArgs a)
     const float val = Us[j] * wT;
     if (e.interp == 0) {
       int64_t vox;
-      if (emc_voxel::nearest(u, e.side, 0, &vox)) red_add_v2(e.acc + vox, val, wT);
+      if (emc_voxel::nearest(u, e.side, 0, &vox)) insert_add(e, vox, val, wT);
     } else {
 #pragma unroll
       for (int cc = 0; cc < 8; ++cc) {
         int64_t vox;
         float wc;
         if (!emc_voxel::trilinear_corner(u, e.side, cc, &vox, &wc) || wc == 0.0f) continue;
-        red_add_v2(e.acc + vox, wc * val, wc * wT);
+        insert_add(e, vox, wc * val, wc * wT);
       }
     }
   }
@@ -2049,15 +2188,22 @@ static unsigned grid_for(int64_t n) {
   return (unsigned)std::min<int64_t>((n + 255) / 256 + 1, 4096);
 }
 
+cudaError_t launch_cand_probs(const RespArgs& a, int64_t n, float* Pv, double* T64,
+                              cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(T64, 0, sizeof(double) * a.R, st);
+  if (e != cudaSuccess) return e;
+  if (n > 0) cand_finish_kernel<<<grid_for(n), 256, 0, st>>>(a, n, Pv, T64);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_list_from_candidates(RespArgs& a, int64_t n, float rel_min, float* Pv,
                                         double* T64, int64_t* rowtot, int64_t* cursor,
                                         int64_t* rowoff, int32_t* pat, float* xv, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(T64, 0, sizeof(double) * a.R, st);
+  cudaError_t e = launch_cand_probs(a, n, Pv, T64, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(rowtot, 0, sizeof(int64_t) * a.R, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, sizeof(int64_t) * a.R, st);
   if (e != cudaSuccess) return e;
   const unsigned g = grid_for(n);
-  cand_finish_kernel<<<g, 256, 0, st>>>(a, n, Pv, T64);
   T_from64_kernel<<<(unsigned)((a.R + 255) / 256), 256, 0, st>>>(T64, a.R, a.T);
   compact_sort_kernel<0><<<g, 256, 0, st>>>(a.list_rp, Pv, n, a.T, a.new_scaling, rel_min,
                                             reinterpret_cast<unsigned long long*>(rowtot),
@@ -2066,6 +2212,78 @@ cudaError_t launch_list_from_candidates(RespArgs& a, int64_t n, float rel_min, f
   compact_sort_kernel<1><<<g, 256, 0, st>>>(a.list_rp, Pv, n, a.T, a.new_scaling, rel_min,
                                             reinterpret_cast<unsigned long long*>(cursor), rowoff,
                                             pat, xv);
+  return cudaGetLastError();
+}
+
+int64_t sort_hist_size(int64_t n) { return 2 * 256 * ((n + kSortTile - 1) / kSortTile) + 1; }
+
+cudaError_t launch_sort_entries(int2* rp, float* v, int64_t n, int64_t N, int64_t R, int2* rp2,
+                                float* v2, int64_t* hist, cudaStream_t st) {
+  if (n <= 1) return cudaSuccess;
+  const int64_t ntiles = (n + kSortTile - 1) / kSortTile;
+  const int64_t hn = 256 * ntiles;
+  auto bits = [](int64_t m) {
+    int b = 1;
+    while (b < 31 && (int64_t(1) << b) < m) ++b;
+    return b;
+  };
+  int2 *src = rp, *dst = rp2;
+  float *vs = v, *vd = v2;
+  for (int field = 0; field < 2; ++field) {
+    const int nb = bits(field ? R : N);
+    for (int shift = 0; shift < nb; shift += 8) {
+      // counts in hist[0 .. hn), their exclusive offsets in hist[hn .. 2 hn]
+      radix_hist_kernel<<<(unsigned)ntiles, 256, 0, st>>>(src, n, field, shift, ntiles, hist);
+      list_rowscan_kernel<<<1, 1024, 0, st>>>(hist, hn, hist + hn);
+      radix_scatter_kernel<<<(unsigned)ntiles, 32, 0, st>>>(src, vs, n, field, shift, ntiles,
+                                                            hist + hn, dst, vd);
+      std::swap(src, dst);
+      std::swap(vs, vd);
+    }
+  }
+  if (src != rp) {
+    cudaError_t e = cudaMemcpyAsync(rp, src, sizeof(int2) * n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v, vs, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_T_from_sorted(const int2* rp, const float* Pv, int64_t n, int64_t R,
+                                 int64_t* rowtot, int64_t* rowoff, float* T, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(rowtot, 0, sizeof(int64_t) * R, st);
+  if (e != cudaSuccess) return e;
+  if (n > 0)
+    sorted_count_kernel<<<grid_for(n), 256, 0, st>>>(rp, Pv, n, nullptr, 0.0f, 0,
+                                                     reinterpret_cast<unsigned long long*>(rowtot),
+                                                     nullptr);
+  list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, R, rowoff);
+  sorted_T_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(Pv, rowoff, R, T);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_list_from_sorted(const int2* rp, const float* Pv, int64_t n, int64_t R,
+                                    const float* T, const float* new_scaling, float rel_min,
+                                    int64_t* rowtot, int64_t* rowoff, int64_t* flag,
+                                    int32_t* pat, float* xv, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(rowtot, 0, sizeof(int64_t) * R, st);
+  if (e != cudaSuccess) return e;
+  if (n > 0)
+    sorted_count_kernel<<<grid_for(n), 256, 0, st>>>(rp, Pv, n, T, rel_min, 1,
+                                                     reinterpret_cast<unsigned long long*>(rowtot),
+                                                     flag);
+  list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, R, rowoff);
+  if (n > 0) {
+    // positions: the exclusive scan of the flags, in flag[n + 1 ..]
+    list_rowscan_kernel<<<1, 1024, 0, st>>>(flag, n, flag + n + 1);
+    sorted_place_kernel<<<grid_for(n), 256, 0, st>>>(rp, Pv, n, T, new_scaling, flag,
+                                                     flag + n + 1, pat, xv);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finish_T(const float* Tpart, int64_t N, int64_t R, float* T, cudaStream_t st) {
+  finish_T_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(Tpart, resp_list_blocks(N), R, T);
   return cudaGetLastError();
 }
 

@@ -66,8 +66,22 @@ __global__ void __launch_bounds__(256) targets_kernel(const TargetArgs a) {
   const int64_t p = (int64_t)blockIdx.x * 32 + lane;
   for (int i = threadIdx.x; i < a.n_cells * 32; i += blockDim.x) tc[i] = 0.0f;
   __syncthreads();
-  if (p < a.N)
-    for (int64_t r = w; r < a.R; r += 8) atomicAdd(&tc[a.cell[r] * 32 + lane], resp_of(a, r, p));
+  if (p < a.N) {
+    // sums over runs of one cell in registers (the rotations are sorted by
+    // cell), one shared-memory atomic per run
+    int cur = -1;
+    float sum = 0.0f;
+    for (int64_t r = w; r < a.R; r += 8) {
+      const int c = a.cell[r];
+      if (c != cur) {
+        if (cur >= 0) atomicAdd(&tc[cur * 32 + lane], sum);
+        cur = c;
+        sum = 0.0f;
+      }
+      sum += resp_of(a, r, p);
+    }
+    if (cur >= 0) atomicAdd(&tc[cur * 32 + lane], sum);
+  }
   __syncthreads();
   if (p < a.N)
     for (int c = w; c < a.n_cells; c += 8) a.t[p * a.n_cells + c] = tc[c * 32 + lane];
@@ -107,14 +121,42 @@ __global__ void __launch_bounds__(256) log_targets_kernel(const TargetArgs a) {
     return ((double)y * 2.0 / phi - a.rowstat[r] - a.patstat[p] / (phi * phi)) * a.gauss_inv;
   };
   const double lse = a.P ? 0.0 : a.lse[p < a.N ? p : 0];
-  if (p < a.N)
-    for (int64_t r = rl; r < a.R; r += 16) atomic_max_f32(&tcm[a.cell[r] * 16 + pl], (float)ll_of(r));
-  __syncthreads();
-  if (p < a.N)
+  // The rotations are sorted by cell, so a thread's rotations r, r + 16, ...
+  // stay in one cell for many steps: it keeps the running maximum (then sum)
+  // of its current cell in registers and folds it into shared memory when the
+  // cell changes, one shared-memory atomic per run instead of per rotation.
+  if (p < a.N) {
+    int cur = -1;
+    float m = -INFINITY;
     for (int64_t r = rl; r < a.R; r += 16) {
-      const int k = a.cell[r] * 16 + pl;
-      atomicAdd(&tcd[k], exp(ll_of(r) - (double)tcm[k]));
+      const int c = a.cell[r];
+      const float v = (float)ll_of(r);
+      if (c != cur) {
+        if (cur >= 0) atomic_max_f32(&tcm[cur * 16 + pl], m);
+        cur = c;
+        m = v;
+      } else {
+        m = fmaxf(m, v);
+      }
     }
+    if (cur >= 0) atomic_max_f32(&tcm[cur * 16 + pl], m);
+  }
+  __syncthreads();
+  if (p < a.N) {
+    int cur = -1;
+    double sum = 0.0, mx = 0.0;
+    for (int64_t r = rl; r < a.R; r += 16) {
+      const int c = a.cell[r];
+      if (c != cur) {
+        if (cur >= 0) atomicAdd(&tcd[cur * 16 + pl], sum);
+        cur = c;
+        sum = 0.0;
+        mx = (double)tcm[c * 16 + pl];
+      }
+      sum += exp(ll_of(r) - mx);
+    }
+    if (cur >= 0) atomicAdd(&tcd[cur * 16 + pl], sum);
+  }
   __syncthreads();
   if (p < a.N)
     for (int c = rl; c < a.n_cells; c += 16) {
@@ -377,7 +419,7 @@ struct OpGroupLL {
 
 // Per pattern (one warp): log-sum-exp over its candidate rotations (FP64), new
 // scaling, sum P log P; writes P / phi_new into the per-cell compress operand
-// Pt and adds P into T_r.
+// Pt (when the grouped compress reads it) and adds P into T_r.
 __global__ void group_softmax_kernel(const GroupArgs g) {
   const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -458,8 +500,9 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
     for (int k = lane; k < g.mcnt[c]; k += 32) {
       const double l = ll_of(c, q, k);
       const float P = (float)exp(l - lse);
-      g.Pt[g.goff[c] + (int64_t)k * g.gcnt[c] + col] = (float)(P / phi_new);
-      atomicAdd(g.T + g.mbeg[c] + k, P);
+      if (g.Pt) g.Pt[g.goff[c] + (int64_t)k * g.gcnt[c] + col] = (float)(P / phi_new);
+      // most candidates of a sharp posterior underflow: no atomic for those
+      if (P != 0.0f) atomicAdd(g.T + g.mbeg[c] + k, P);
       cm += P;
       if (g.lcmass) crel += exp(l - cmx);
     }
@@ -616,6 +659,30 @@ __global__ void gather_rows_kernel(const __half* Kh, int64_t Ppad, const int32_t
     dst[i] = p < 0 ? make_uint4(0, 0, 0, 0) : src[i];
 }
 
+// The same rows built from the counts' photon lists (kptr [N+1], kidx =
+// active pixel, kval = count): the row is zeroed in shared memory, the
+// pattern's photons scattered into it as FP16 (exact: integers <= 2048), and
+// written out whole, so only the rows are written and only the photon lists
+// read (the dense gather reads every row of Kh as well).
+__global__ void slot_rows_kernel(const int64_t* kptr, const int32_t* kidx, const float* kval,
+                                 int64_t Ppad, const int32_t* slot_pat, int64_t S, __half* Kg) {
+  extern __shared__ uint4 srow[];  // [Ppad / 8]
+  const int64_t s = blockIdx.x;  // one block per slot
+  if (s >= S) return;
+  const int p = slot_pat[s];
+  const int64_t n16 = Ppad / 8;
+  for (int64_t i = threadIdx.x; i < n16; i += blockDim.x) srow[i] = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  if (p >= 0) {
+    __half* h = reinterpret_cast<__half*>(srow);
+    for (int64_t t = kptr[p] + threadIdx.x; t < kptr[p + 1]; t += blockDim.x)
+      h[kidx[t]] = __float2half_rn(kval[t]);
+  }
+  __syncthreads();
+  uint4* dst = reinterpret_cast<uint4*>(Kg + s * Ppad);
+  for (int64_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = srow[i];
+}
+
 // The grouped compress operand: A[r][q] = P / (T_r phi) of rotation r and the
 // q-th slot of its cell as FP16 hi + lo, zero from the cell's slot count up to
 // the next multiple of 64 (the contraction's k-blocks), and zero rows for
@@ -766,6 +833,19 @@ cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* s
                                 __half* Kg, cudaStream_t st) {
   if (S == 0) return cudaSuccess;
   gather_rows_kernel<<<(unsigned)S, 256, 0, st>>>(Kh, Ppad, slot_pat, S, Kg);
+  return cudaGetLastError();
+}
+
+bool slot_rows_fit(int64_t Ppad) { return Ppad * 2 <= 200 * 1024; }
+
+cudaError_t launch_slot_rows(const int64_t* kptr, const int32_t* kidx, const float* kval,
+                             int64_t Ppad, const int32_t* slot_pat, int64_t S, __half* Kg,
+                             cudaStream_t st) {
+  const size_t smem = (size_t)Ppad * sizeof(__half);
+  cudaError_t e = cudaFuncSetAttribute(slot_rows_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (S > 0) slot_rows_kernel<<<(unsigned)S, 256, smem, st>>>(kptr, kidx, kval, Ppad, slot_pat, S, Kg);
   return cudaGetLastError();
 }
 

@@ -70,7 +70,7 @@ struct GroupArgs {
   const double* patsum;    // sum K
   double gauss_inv;
   float* Y;                // [pairs][MM]
-  float* Pt;               // per cell [mcnt][gcnt]: P / phi_new
+  float* Pt;               // per cell [mcnt][gcnt]: P / phi_new (nullptr: not needed)
   float* T;                // [R] (zeroed by the caller)
   double* lse;             // [N]
   double* plogp;           // [N]
@@ -99,6 +99,12 @@ cudaError_t launch_group_softmax(const GroupArgs& g, cudaStream_t st);
 // slot_pat[slot] = pattern, -1 for padding (zero).
 cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* slot_pat, int64_t S,
                                 __half* Kg, cudaStream_t st);
+// The same rows from the counts' photon lists (kptr [N+1], kidx, kval), each
+// row built in shared memory: Ppad FP16 must fit (slot_rows_fit).
+bool slot_rows_fit(int64_t Ppad);
+cudaError_t launch_slot_rows(const int64_t* kptr, const int32_t* kidx, const float* kval,
+                             int64_t Ppad, const int32_t* slot_pat, int64_t S, __half* Kg,
+                             cudaStream_t st);
 // A[r][q] = P / (T_r phi) of the grouped compress as FP16 hi + lo ([R][ldA]).
 cudaError_t launch_p_split(const GroupArgs& g, const int32_t* cell_of, int64_t R, const float* T,
                            int64_t ldA, __half* Ahi, __half* Alo, cudaStream_t st);

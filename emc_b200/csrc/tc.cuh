@@ -77,6 +77,7 @@ struct CmpEpiArgs {
   const float* cz;
   const int32_t* ins;      // [npa] insert flag (mask == 1)
   float2* acc;             // [side^3] interleaved (model, weight) accumulators
+  unsigned long long* acc64;  // or, when set, fixed-point limbs [side^3][8] (fixed.cuh)
 };
 // raster: rotation tiles per band of the tile order.
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
@@ -246,9 +247,31 @@ cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int6
 // into Pv (their y stay in a.list_P), T_r = sum of P over each rotation's
 // candidates (T64 [R] scratch; a.T), then the lists as launch_list_from_compact
 // forms them from (a.list_rp, Pv).  a.R, a.rowstat: every rotation.
+// Only the first step: Pv and the FP64 row sums T64 (atomics).
+cudaError_t launch_cand_probs(const RespArgs& a, int64_t n, float* Pv, double* T64,
+                              cudaStream_t st);
 cudaError_t launch_list_from_candidates(RespArgs& a, int64_t n, float rel_min, float* Pv,
                                         double* T64, int64_t* rowtot, int64_t* cursor,
                                         int64_t* rowoff, int32_t* pat, float* xv, cudaStream_t st);
+// Deterministic list order: the n entries (rp, v) sorted by (rotation,
+// pattern) in place (stable radix sort; rp2, v2 [n] and hist
+// [sort_hist_size(n)] scratch; N, R bound the fields) ...
+int64_t sort_hist_size(int64_t n);
+cudaError_t launch_sort_entries(int2* rp, float* v, int64_t n, int64_t N, int64_t R, int2* rp2,
+                                float* v2, int64_t* hist, cudaStream_t st);
+// ... T_r as the FP64 sum of each rotation's sorted entries in order
+// (rowtot [R], rowoff [R+1] scratch) ...
+cudaError_t launch_T_from_sorted(const int2* rp, const float* Pv, int64_t n, int64_t R,
+                                 int64_t* rowtot, int64_t* rowoff, float* T, cudaStream_t st);
+// ... and the lists of the entries with P >= rel_min T_r in sorted order,
+// x = P / (T_r phi_new) (rowoff [R+1] of the lists; flag [2n + 2] scratch).
+cudaError_t launch_list_from_sorted(const int2* rp, const float* Pv, int64_t n, int64_t R,
+                                    const float* T, const float* new_scaling, float rel_min,
+                                    int64_t* rowtot, int64_t* rowoff, int64_t* flag,
+                                    int32_t* pat, float* xv, cudaStream_t st);
+// T_r from the row-sum partials (FP64, pattern-block order).
+cudaError_t launch_finish_T(const float* Tpart, int64_t N, int64_t R, float* T, cudaStream_t st);
+
 // Exports of a chunked iteration from its candidates (rp, Pv; n of them):
 // dense P [R][N] (zeroed by the caller) ...
 cudaError_t launch_cand_scatter(const int2* rp, const float* Pv, int64_t n, int64_t N, float* P,
@@ -279,6 +302,7 @@ struct ListCmpArgs {
   const int32_t* kidx;
   const float* kval;
   CmpEpiArgs e;
+  int ordered;  // sum each pixel's terms in list order (deterministic mode)
 };
 cudaError_t launch_list_compress(const ListCmpArgs& a, cudaStream_t st);
 // FP32 responsibilities [R][N] from Y and lse (readback / tests).

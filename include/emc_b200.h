@@ -173,6 +173,16 @@ size_t emc_memory_used(const emc_context *ctx);
  * emc_rotation_chunk: the rotations Y holds (R when unchunked). */
 emc_status emc_set_rotation_chunk(emc_context *ctx, int64_t rows, int64_t capacity);
 int64_t emc_rotation_chunk(const emc_context *ctx);
+/* Deterministic insertion (on = 1): every insertion sum (model and weight per
+ * voxel) is formed exactly as a fixed-point integer (64 fraction bits, 32-bit
+ * pieces added to 64-bit limbs; integer addition does not depend on order)
+ * and rounded once; the responsibility lists are sorted by (rotation,
+ * pattern) and each rotation's slice sums its patterns in that order.  Two
+ * runs of the same iterations then give bitwise the same model, weight and
+ * scaling, chunked or not, in either precision.  Costs 64 bytes of device
+ * memory per voxel.  EMC_ERR_UNSUPPORTED for the proposed iterations; a
+ * batch takes contexts without it. */
+emc_status emc_set_deterministic(emc_context *ctx, int on);
 /* Checkpoint (emc.c:715-716 resumes from a model file at start_iteration;
  * this keeps the whole state): model, weight grid and per-pattern scaling
  * with the iteration number, in a raw little-endian file.  The model and the

@@ -109,3 +109,24 @@ def test_batched_pair_maximize_matches_separate_iterations():
     finally:
         for c in ctxs:
             c.close()
+
+
+def test_single_dataset_iteration_as_a_graph():
+    """The iteration of one dataset captured as one CUDA graph (a batch of
+    one context) and replayed three times, against three eager iterations
+    with the same (dense) compress."""
+    import emc_b200 as E
+    from emc_b200 import workloads as W
+    d = W.make("small32")
+    with make_ctx(d, "poisson", "nearest", "mixed") as c:
+        c.set_sparse_compress(False)
+        for _ in range(3):
+            c.iterate()
+        ref_m, ref_s = c.get_model(), c.get_scaling()
+    with make_ctx(d, "poisson", "nearest", "mixed") as c:
+        with E.Batch([c]) as b:
+            b.capture()
+            b.launch(3)
+            b.synchronize()
+            assert rel(c.get_model(), ref_m) < 1e-5, rel(c.get_model(), ref_m)
+            assert rel(c.get_scaling(), ref_s) < 1e-5
