@@ -29,8 +29,14 @@ struct ExpandArgs {
   // optional, nearest + EXP_F16_SPLIT: per-voxel table from launch_expand_table
   // ([side^3 + 1], the last entry for pixels that fall outside the grid)
   const uint2* tab;
+  // optional, trilinear: the stencil table of launch_tri_table
+  const float4* tri;
 };
 cudaError_t launch_expand(const ExpandArgs& a, cudaStream_t st);
+// Trilinear stencil table: per base voxel of [-1, side)^3 the model at its 8
+// corners (0 outside the grid), tri_table_entries(side) float4.
+int64_t tri_table_entries(int side);
+cudaError_t launch_tri_table(const float* model, int side, float4* tri, cudaStream_t st);
 // tab[v] = (bits of model[v], FP16 hi | lo << 16 of the split operand value:
 // log(max(model[v], floor)) when log_split, else model[v]) for v < M, and
 // tab[M] the same for a pixel outside the grid (value 0).

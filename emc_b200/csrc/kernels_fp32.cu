@@ -72,6 +72,50 @@ __device__ __forceinline__ float gather(const float* __restrict__ model, const f
   return acc;
 }
 
+// Trilinear through the stencil table (launch_tri_table): the 8 corner values
+// of base voxel floor(u) in one aligned 32-byte load, 0 for corners outside
+// the grid.  The same FMAs in the same corner order as gather<1>: a corner
+// that gather<1> skips (outside, or weight 0) adds w * 0 or 0 * value here,
+// which leaves the sum unchanged, so the result is bit for bit the same.
+__device__ __forceinline__ float gather_tri(const float4* __restrict__ tri, const float* u,
+                                            int side) {
+  const float fx = floorf(u[0]), fy = floorf(u[1]), fz = floorf(u[2]);
+  const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+  if (x0 < -1 || x0 >= side || y0 < -1 || y0 >= side || z0 < -1 || z0 >= side) return 0.0f;
+  const int64_t s1 = side + 1;
+  const int64_t e = ((int64_t)(z0 + 1) * s1 + (y0 + 1)) * s1 + (x0 + 1);
+  const float4 lo = __ldg(tri + 2 * e), hi = __ldg(tri + 2 * e + 1);
+  const float val[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+  const float ax = u[0] - fx, ay = u[1] - fy, az = u[2] - fz;
+  float acc = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int bx = c & 1, by = (c >> 1) & 1, bz = (c >> 2) & 1;
+    const float w = (bx ? ax : 1.0f - ax) * (by ? ay : 1.0f - ay) * (bz ? az : 1.0f - az);
+    acc = fmaf(w, val[c], acc);
+  }
+  return acc;
+}
+
+// tri[2e], tri[2e + 1] = the model at the 8 corners (bit 0: x + 1, bit 1:
+// y + 1, bit 2: z + 1; 0 outside the grid) of base voxel e = (z0 + 1, y0 + 1,
+// x0 + 1) over [-1, side)^3.
+__global__ void tri_table_kernel(const float* __restrict__ model, int side, float4* tri) {
+  const int64_t s1 = side + 1;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= s1 * s1 * s1) return;
+  const int x0 = (int)(e % s1) - 1, y0 = (int)((e / s1) % s1) - 1, z0 = (int)(e / (s1 * s1)) - 1;
+  float v[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int kx = x0 + (c & 1), ky = y0 + ((c >> 1) & 1), kz = z0 + ((c >> 2) & 1);
+    const bool in = kx >= 0 && kx < side && ky >= 0 && ky < side && kz >= 0 && kz < side;
+    v[c] = in ? model[((int64_t)kz * side + ky) * side + kx] : 0.0f;
+  }
+  tri[2 * e] = make_float4(v[0], v[1], v[2], v[3]);
+  tri[2 * e + 1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+
 // Four pixels per thread and iteration: their gathers are independent, so
 // four L2 round trips are in flight per thread.
 constexpr int kExpandUnroll = 4;
@@ -92,7 +136,8 @@ __global__ void __launch_bounds__(kBlock) expand_kernel(const ExpandArgs a) {
       if (i < a.npix) {
         float pos[3];
         emc_voxel::position(m, a.side, __ldg(a.cx + i), __ldg(a.cy + i), __ldg(a.cz + i), pos);
-        w[u] = gather<INTERP>(a.model, pos, a.side);
+        w[u] = (INTERP == 1 && a.tri) ? gather_tri(a.tri, pos, a.side)
+                                      : gather<INTERP>(a.model, pos, a.side);
       }
     }
 #pragma unroll
@@ -642,6 +687,14 @@ cudaError_t launch_expand(const ExpandArgs& a, cudaStream_t st) {
     expand_dispatch<0>(a, st);
   else
     expand_dispatch<1>(a, st);
+  return cudaGetLastError();
+}
+
+int64_t tri_table_entries(int side) { return 2 * (int64_t)(side + 1) * (side + 1) * (side + 1); }
+
+cudaError_t launch_tri_table(const float* model, int side, float4* tri, cudaStream_t st) {
+  const int64_t n = (int64_t)(side + 1) * (side + 1) * (side + 1);
+  tri_table_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(model, side, tri);
   return cudaGetLastError();
 }
 

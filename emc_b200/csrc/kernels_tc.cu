@@ -143,6 +143,18 @@ struct b_major_mn : std::false_type {};
 template <class E>
 struct b_major_mn<E, std::void_t<decltype(E::kBMajorMN)>> : std::bool_constant<E::kBMajorMN> {};
 
+// Listed pair epilogues with kBuildA = true have their A tiles written into
+// shared memory by builder warps (from the counts' photon lists) instead of
+// loaded by TMA; see the builder branch of tc_pair_kernel.
+template <class E, class = void>
+struct build_a : std::false_type {};
+template <class E>
+struct build_a<E, std::void_t<decltype(E::kBuildA)>> : std::bool_constant<E::kBuildA> {};
+template <class Epi>
+constexpr int pair_threads() {
+  return 64 + 32 * Epi::kEpiWarps + (build_a<Epi>::value ? 32 * 8 : 0);
+}
+
 // Listed pair epilogues with kCellN = true narrow each tile's MMA to its
 // cell's members rounded up to 16 (epi.a.mcnt[cell]); each CTA of the pair
 // then holds half of that many B rows.
@@ -156,12 +168,27 @@ struct Ctl {
   TcStatus* st;
 };
 
+// The same wait with cluster-scope acquire: the phase's arrivals include the
+// peer CTA's, whose shared-memory writes before them must be visible.
+__device__ __forceinline__ bool mbar_test_cluster(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int site,
-                             uint64_t limit_ns = kWaitLimitNs) {
-  if (mbar_test(bar, parity)) return true;
+                             uint64_t limit_ns = kWaitLimitNs, bool cluster = false) {
+  auto test = [&]() { return cluster ? mbar_test_cluster(bar, parity) : mbar_test(bar, parity); };
+  if (test()) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
-    if (mbar_test(bar, parity)) return true;
+    if (test()) return true;
     if ((it & 31) == 0) {
       if (*c.abort) return false;
       if (globaltimer() - t0 > limit_ns) {
@@ -763,6 +790,12 @@ struct EpiGMaxPair : EpiGMax {
   }
 };
 
+// The same with the A tiles built from the counts' photon lists in shared
+// memory (no gathered copy of the counts).
+struct EpiGMaxBuild : EpiGMaxPair {
+  static constexpr bool kBuildA = true;
+};
+
 // Grouped compress: row = member rotation r of the tile's cell, column =
 // active pixel; acc = U_r (the operand rows are P / (T_r phi)), inserted with
 // weight rotw T_r as in EpiCmp.
@@ -964,7 +997,7 @@ cudaError_t run_gemm(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n
   const int64_t tiles = m_tiles * n_tiles;
   if (tiles == 0) return cudaSuccess;
   const int grid = (int)(tiles < num_sms ? tiles : num_sms);
-  kern<<<grid, 64 + 32 * Epi::kEpiWarps, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks, raster,
+  kern<<<grid, pair_threads<Epi>(), dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks, raster,
                                                        epi, st);
   return cudaGetLastError();
 }
@@ -1035,7 +1068,7 @@ constexpr int kPairStages = 4;
 // pair (a_row, b_row: the CTA adds 128 x rank), k-block count and tensor-map
 // set; its row_begin then receives the row inside this CTA's 128 rows.
 template <int NA, int NB, bool M_INNER, class Epi>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(pair_threads<Epi>(), 1)
     tc_pair_kernel(const __grid_constant__ TmapSet<Epi::kSets> maps, const int64_t m_tiles,
                    const int64_t n_tiles, const int64_t k_blocks, const int raster,
                    const Epi epi, TcStatus* status) {
@@ -1065,9 +1098,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
     asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(pa), "r"(1) : "memory");
   };
 
+  constexpr bool kBuild = build_a<Epi>::value;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      mbar_init(smem_u32(&full_bar[s]), 1);
+      // built A tiles: the leader's producer and four builder warps per CTA
+      mbar_init(smem_u32(&full_bar[s]), kBuild ? 1 + 2 * 4 : 1);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -1148,12 +1183,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
             break;
           }
           const uint32_t fb = smem_u32(&full_bar[s]);
-          if (leader) mbar_expect_tx(fb, 2 * STAGE_BYTES);  // both CTAs' bytes
+          // both CTAs' bytes (only B's when builder warps write A)
+          if (leader) mbar_expect_tx(fb, kBuild ? 2 * NB * B_BYTES : 2 * STAGE_BYTES);
           const uint32_t fb_leader = peer_addr(fb, 0);
           const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
           const int kc = (int)(kb * kPairBK);
-          tma_load_2d_pair(base, tA0, kc, ar, fb_leader);
-          if (NA == 2) tma_load_2d_pair(base + A_BYTES, tA1, kc, ar, fb_leader);
+          if constexpr (!kBuild) {
+            tma_load_2d_pair(base, tA0, kc, ar, fb_leader);
+            if (NA == 2) tma_load_2d_pair(base + A_BYTES, tA1, kc, ar, fb_leader);
+          }
           const uint32_t bbase = base + NA * A_BYTES;
           tma_load_2d_pair(bbase, tB0, kc, br, fb_leader);
           if (NB == 2) tma_load_2d_pair(bbase + B_BYTES, tB1, kc, br, fb_leader);
@@ -1217,7 +1255,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
           }
         }
         for (int64_t kb = 0; kb < kbs; ++kb) {
-          if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3)) {
+          if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3, kWaitLimitNs, kBuild)) {
             ok = false;
             abort_pair();
             break;
@@ -1252,6 +1290,60 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
       const uint64_t t0 = globaltimer();
       while (!mbar_test(smem_u32(&drain_bar), 0) && globaltimer() - t0 < kWaitLimitNs) {
       }
+    }
+  } else if (warp >= 2 + Epi::kEpiWarps) {
+    // -------------------------------------------------- A-tile builders (both CTAs)
+    // Eight warps: warp pair b (of four) owns rows 32 b .. 32 b + 31 of this
+    // CTA's 128, one row (slot) per lane, and its two warps take the even and
+    // the odd k-blocks.  Per k-block a lane zeroes its 128-byte row of the
+    // stage and writes the row's counts from its pattern's photon lists (the
+    // entries of k-block kb are koff[p][kb] .. koff[p][kb + 1] - 1) at their
+    // 128-byte-swizzle positions, then the warp makes the writes visible to
+    // the tensor core (proxy fence) and arrives on the leader's full barrier.
+    if constexpr (kBuild) {
+      const int bw = warp - 2 - Epi::kEpiWarps;
+      const int par = bw & 1, row = (bw >> 1) * 32 + lane;
+      int s = 0;
+      uint32_t ph = 0;
+      int64_t g = 0;
+      bool ok = true;
+      for (int64_t t = cid; t < num_tiles && ok; t += ncl) {
+        const TileDesc d = epi.a.tiles[t];
+        const int64_t slot = (int64_t)d.a_row + rank * 128 + row;
+        const int p = slot < epi.a.n_slots ? epi.a.gpair[slot] : -1;
+        const int32_t* koff = p >= 0 ? epi.a.koff + (int64_t)p * epi.a.kb_stride : nullptr;
+        for (int64_t kb = 0; kb < d.k_blocks; ++kb, ++g) {
+          const int cs = s;
+          const uint32_t cph = ph;
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1;
+          }
+          if ((int)(g & 1) != par) continue;
+          bool free_stage = lane == 0 ? bounded_wait(smem_u32(&empty_bar[cs]), cph ^ 1, ctl, 6) : true;
+          free_stage = __shfl_sync(0xffffffffu, free_stage, 0);
+          if (!free_stage) {
+            ok = false;
+            break;
+          }
+          uint8_t* rowp = smem + (size_t)cs * STAGE_BYTES + row * 128;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) reinterpret_cast<uint4*>(rowp)[q] = make_uint4(0u, 0u, 0u, 0u);
+          if (koff) {
+            const int32_t e0 = koff[kb], e1 = koff[kb + 1];
+            const int kc = (int)(kb * kPairBK);
+            for (int32_t e = e0; e < e1; ++e) {
+              const int col = epi.a.kidx[e] - kc;
+              *reinterpret_cast<__half*>(rowp + ((((col >> 3) ^ (row & 7)) << 4) + ((col & 7) << 1))) =
+                  __float2half_rn(epi.a.kval[e]);
+            }
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive_cluster(peer_addr(smem_u32(&full_bar[cs]), 0));
+        }
+      }
+      if (!ok && lane == 0) abort_pair();
     }
   } else {
     // -------------------------------------------------- epilogue warps (both CTAs)
@@ -1614,6 +1706,58 @@ __global__ void __launch_bounds__(1024) list_rowscan_kernel(const int64_t* rowto
     run += rowtot[r];
   }
   if (t == 1023) rowoff[R] = part[1023];
+}
+
+// Exclusive prefix sums of long arrays in three launches: per block of
+// kScanBlock elements its total, one block scanning the totals
+// (list_rowscan_kernel), then each block's elements from its offset.
+constexpr int kScanPer = 8;
+constexpr int kScanBlock = 1024 * kScanPer;
+
+__global__ void __launch_bounds__(1024) scan_totals_kernel(const int64_t* in, int64_t n,
+                                                           int64_t* tot) {
+  __shared__ int64_t red[32];
+  const int64_t b0 = (int64_t)blockIdx.x * kScanBlock + (int64_t)threadIdx.x * kScanPer;
+  int64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k)
+    if (b0 + k < n) s += in[b0 + k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int64_t v = red[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) tot[blockIdx.x] = v;
+  }
+}
+
+__global__ void __launch_bounds__(1024) scan_apply_kernel(const int64_t* in, int64_t n,
+                                                          const int64_t* boff, int64_t* out) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t b0 = (int64_t)blockIdx.x * kScanBlock + (int64_t)t * kScanPer;
+  int64_t v[kScanPer], s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    v[k] = b0 + k < n ? in[b0 + k] : 0;
+    s += v[k];
+  }
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int64_t x = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += x;
+    __syncthreads();
+  }
+  int64_t run = boff[blockIdx.x] + part[t] - s;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    if (b0 + k < n) out[b0 + k] = run;
+    run += v[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && t == 0) out[n] = boff[gridDim.x];  // the total
 }
 
 // T_r from the row-sum partials (FP64 sum in pattern-block order, as
@@ -2088,6 +2232,16 @@ cudaError_t launch_group_maximize_pair_tc(const CUtensorMap& tmKg, const CUtenso
                               num_sms, st, 1);
 }
 
+cudaError_t launch_group_maximize_build_tc(const CUtensorMap& tmBhi, const CUtensorMap& tmBlo,
+                                           int64_t n_tiles, const GMaxEpiArgs& e,
+                                           TcStatus* status, int num_sms, cudaStream_t st) {
+  EpiGMaxBuild epi;
+  epi.a = e;
+  // the A maps are not read (builder warps write A)
+  return run_pair<1, 2, true>(one_set(tmBhi, tmBhi, tmBhi, tmBlo), n_tiles, 1, 0, epi, status,
+                              num_sms, st, 1);
+}
+
 cudaError_t launch_group_compress_tc(const CUtensorMap& tmAhi, const CUtensorMap& tmAlo,
                                      const CUtensorMap& tmKg64, int64_t n_tiles,
                                      const GCmpEpiArgs& e, TcStatus* status, int num_sms,
@@ -2215,7 +2369,24 @@ cudaError_t launch_list_from_candidates(RespArgs& a, int64_t n, float rel_min, f
   return cudaGetLastError();
 }
 
-int64_t sort_hist_size(int64_t n) { return 2 * 256 * ((n + kSortTile - 1) / kSortTile) + 1; }
+int64_t scan_scratch(int64_t n) { return 2 * ((n + kScanBlock - 1) / kScanBlock) + 2; }
+
+// out[0..n] = exclusive prefix sums of in[0..n) (out[n] = total); scratch
+// [scan_scratch(n)].
+static cudaError_t scan_i64(const int64_t* in, int64_t n, int64_t* out, int64_t* scratch,
+                            cudaStream_t st) {
+  const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  if (nb == 0) return cudaMemsetAsync(out, 0, sizeof(int64_t), st);
+  scan_totals_kernel<<<(unsigned)nb, 1024, 0, st>>>(in, n, scratch);
+  list_rowscan_kernel<<<1, 1024, 0, st>>>(scratch, nb, scratch + nb);
+  scan_apply_kernel<<<(unsigned)nb, 1024, 0, st>>>(in, n, scratch + nb, out);
+  return cudaGetLastError();
+}
+
+int64_t sort_hist_size(int64_t n) {
+  const int64_t hn = 256 * ((n + kSortTile - 1) / kSortTile);
+  return 2 * hn + 1 + scan_scratch(hn);
+}
 
 cudaError_t launch_sort_entries(int2* rp, float* v, int64_t n, int64_t N, int64_t R, int2* rp2,
                                 float* v2, int64_t* hist, cudaStream_t st) {
@@ -2234,7 +2405,8 @@ cudaError_t launch_sort_entries(int2* rp, float* v, int64_t n, int64_t N, int64_
     for (int shift = 0; shift < nb; shift += 8) {
       // counts in hist[0 .. hn), their exclusive offsets in hist[hn .. 2 hn]
       radix_hist_kernel<<<(unsigned)ntiles, 256, 0, st>>>(src, n, field, shift, ntiles, hist);
-      list_rowscan_kernel<<<1, 1024, 0, st>>>(hist, hn, hist + hn);
+      cudaError_t e = scan_i64(hist, hn, hist + hn, hist + 2 * hn + 1, st);
+      if (e != cudaSuccess) return e;
       radix_scatter_kernel<<<(unsigned)ntiles, 32, 0, st>>>(src, vs, n, field, shift, ntiles,
                                                             hist + hn, dst, vd);
       std::swap(src, dst);
@@ -2275,7 +2447,8 @@ cudaError_t launch_list_from_sorted(const int2* rp, const float* Pv, int64_t n, 
   list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, R, rowoff);
   if (n > 0) {
     // positions: the exclusive scan of the flags, in flag[n + 1 ..]
-    list_rowscan_kernel<<<1, 1024, 0, st>>>(flag, n, flag + n + 1);
+    e = scan_i64(flag, n, flag + n + 1, flag + 2 * n + 2, st);
+    if (e != cudaSuccess) return e;
     sorted_place_kernel<<<grid_for(n), 256, 0, st>>>(rp, Pv, n, T, new_scaling, flag,
                                                      flag + n + 1, pat, xv);
   }

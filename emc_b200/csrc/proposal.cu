@@ -58,33 +58,28 @@ __device__ __forceinline__ float resp_of(const TargetArgs& a, int64_t r, int64_t
   return expf((float)(ll - a.lse[p]));
 }
 
-// t[p][c] = sum over the fine rotations r of cell c of P_rp; 32 patterns per
-// block (lane = pattern), the 8 warps share the rotations, shared-memory sums.
+// The cell sums read Y (or P / LL64) once, 32 patterns per block (lane =
+// pattern, 128-byte rows) and one cell per warp: the rotations are sorted by
+// cell, so a cell is the row range mbeg .. mbeg + mcnt - 1 and each (pattern,
+// cell) sum has one owner (no atomics).  Rows are loaded four at a time so
+// each warp keeps four loads in flight.
+constexpr int kCellWarps = 8;
+
+// t[p][c] = sum over the fine rotations r of cell c of P_rp.
 __global__ void __launch_bounds__(256) targets_kernel(const TargetArgs a) {
-  extern __shared__ float tc[];  // [n_cells][32]
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.y * kCellWarps + (threadIdx.x >> 5);
   const int64_t p = (int64_t)blockIdx.x * 32 + lane;
-  for (int i = threadIdx.x; i < a.n_cells * 32; i += blockDim.x) tc[i] = 0.0f;
-  __syncthreads();
-  if (p < a.N) {
-    // sums over runs of one cell in registers (the rotations are sorted by
-    // cell), one shared-memory atomic per run
-    int cur = -1;
-    float sum = 0.0f;
-    for (int64_t r = w; r < a.R; r += 8) {
-      const int c = a.cell[r];
-      if (c != cur) {
-        if (cur >= 0) atomicAdd(&tc[cur * 32 + lane], sum);
-        cur = c;
-        sum = 0.0f;
-      }
-      sum += resp_of(a, r, p);
-    }
-    if (cur >= 0) atomicAdd(&tc[cur * 32 + lane], sum);
+  if (c >= a.n_cells || p >= a.N) return;
+  const int64_t r0 = a.mbeg[c], r1 = r0 + a.mcnt[c];
+  float sum = 0.0f;
+  for (int64_t r = r0; r < r1; r += 4) {
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = r + u < r1 ? resp_of(a, r + u, p) : 0.0f;
+    sum += (v[0] + v[1]) + (v[2] + v[3]);
   }
-  __syncthreads();
-  if (p < a.N)
-    for (int c = w; c < a.n_cells; c += 8) a.t[p * a.n_cells + c] = tc[c * 32 + lane];
+  a.t[p * a.n_cells + c] = sum;
 }
 
 // Largest of *addr and v for floats (ordered through their bit patterns:
@@ -97,21 +92,15 @@ __device__ __forceinline__ void atomic_max_f32(float* addr, float v) {
     atomicMin(reinterpret_cast<unsigned int*>(addr), __float_as_uint(v));
 }
 
-// lt[p][c] = natural log of the responsibility mass of cell c, in the log
-// domain (cell maximum, then a FP64 sum of exponentials relative to it), so
-// every cell is ranked however far down the tail it lies.  16 patterns per
-// block (tid & 15), 16 rotation lanes (tid >> 4); two passes over the
-// rotations (maximum, then sums) through shared memory.
+// lt[p][c] = natural log of the responsibility mass of cell c in the log
+// domain (an online maximum with a rescaled FP64 sum of exponentials), so
+// every cell is ranked however far down the tail it lies.  Layout as
+// targets_kernel.
 __global__ void __launch_bounds__(256) log_targets_kernel(const TargetArgs a) {
-  extern __shared__ double tcd[];  // [n_cells][16] sums, then [n_cells][16] float maxima
-  float* tcm = reinterpret_cast<float*>(tcd + a.n_cells * 16);
-  const int pl = threadIdx.x & 15, rl = threadIdx.x >> 4;
-  const int64_t p = (int64_t)blockIdx.x * 16 + pl;
-  for (int i = threadIdx.x; i < a.n_cells * 16; i += blockDim.x) {
-    tcd[i] = 0.0;
-    tcm[i] = -INFINITY;
-  }
-  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.y * kCellWarps + (threadIdx.x >> 5);
+  const int64_t p = (int64_t)blockIdx.x * 32 + lane;
+  if (c >= a.n_cells || p >= a.N) return;
   auto ll_of = [&](int64_t r) -> double {  // log-likelihood (FP32 path: minus lse)
     if (a.L64) return a.L64[r * a.ldP + p];
     if (a.P) return log((double)a.P[r * a.ldP + p]);
@@ -120,51 +109,25 @@ __global__ void __launch_bounds__(256) log_targets_kernel(const TargetArgs a) {
     const double phi = a.scaling[p];
     return ((double)y * 2.0 / phi - a.rowstat[r] - a.patstat[p] / (phi * phi)) * a.gauss_inv;
   };
-  const double lse = a.P ? 0.0 : a.lse[p < a.N ? p : 0];
-  // The rotations are sorted by cell, so a thread's rotations r, r + 16, ...
-  // stay in one cell for many steps: it keeps the running maximum (then sum)
-  // of its current cell in registers and folds it into shared memory when the
-  // cell changes, one shared-memory atomic per run instead of per rotation.
-  if (p < a.N) {
-    int cur = -1;
-    float m = -INFINITY;
-    for (int64_t r = rl; r < a.R; r += 16) {
-      const int c = a.cell[r];
-      const float v = (float)ll_of(r);
-      if (c != cur) {
-        if (cur >= 0) atomic_max_f32(&tcm[cur * 16 + pl], m);
-        cur = c;
-        m = v;
+  const double lse = a.P ? 0.0 : a.lse[p];
+  const int64_t r0 = a.mbeg[c], r1 = r0 + a.mcnt[c];
+  double mx = -INFINITY, sum = 0.0;
+  for (int64_t r = r0; r < r1; r += 4) {
+    double l[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) l[u] = r + u < r1 ? ll_of(r + u) : -INFINITY;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (!(l[u] > -INFINITY)) continue;
+      if (l[u] > mx) {
+        sum = sum * exp(mx - l[u]) + 1.0;
+        mx = l[u];
       } else {
-        m = fmaxf(m, v);
+        sum += exp(l[u] - mx);
       }
     }
-    if (cur >= 0) atomic_max_f32(&tcm[cur * 16 + pl], m);
   }
-  __syncthreads();
-  if (p < a.N) {
-    int cur = -1;
-    double sum = 0.0, mx = 0.0;
-    for (int64_t r = rl; r < a.R; r += 16) {
-      const int c = a.cell[r];
-      if (c != cur) {
-        if (cur >= 0) atomicAdd(&tcd[cur * 16 + pl], sum);
-        cur = c;
-        sum = 0.0;
-        mx = (double)tcm[c * 16 + pl];
-      }
-      sum += exp(ll_of(r) - mx);
-    }
-    if (cur >= 0) atomicAdd(&tcd[cur * 16 + pl], sum);
-  }
-  __syncthreads();
-  if (p < a.N)
-    for (int c = rl; c < a.n_cells; c += 16) {
-      const double sum = tcd[c * 16 + pl];
-      const float mx = tcm[c * 16 + pl];
-      a.t[p * a.n_cells + c] =
-          (sum > 0.0 && mx > -INFINITY) ? (float)((double)mx + log(sum) - lse) : -INFINITY;
-    }
+  a.t[p * a.n_cells + c] = (sum > 0.0 && mx > -INFINITY) ? (float)(mx + log(sum) - lse) : -INFINITY;
 }
 
 // Most probable cell of a row among those not yet taken (lane owns cells
@@ -723,11 +686,8 @@ cudaError_t launch_features(const float* K, const int32_t* pix, int64_t N, int64
 }
 
 cudaError_t launch_targets(const TargetArgs& a, cudaStream_t st) {
-  const size_t smem = sizeof(float) * 32 * a.n_cells;
-  cudaError_t e = cudaFuncSetAttribute(targets_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  targets_kernel<<<(unsigned)((a.N + 31) / 32), 256, smem, st>>>(a);
+  const dim3 grid((unsigned)((a.N + 31) / 32), (unsigned)((a.n_cells + kCellWarps - 1) / kCellWarps));
+  targets_kernel<<<grid, 32 * kCellWarps, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -746,11 +706,8 @@ __global__ void fill_f32_kernel(float* x, int64_t n, float v) {
 }
 
 cudaError_t launch_log_targets(const TargetArgs& a, cudaStream_t st) {
-  const size_t smem = (sizeof(double) + sizeof(float)) * 16 * a.n_cells;
-  cudaError_t e = cudaFuncSetAttribute(log_targets_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  log_targets_kernel<<<(unsigned)((a.N + 15) / 16), 256, smem, st>>>(a);
+  const dim3 grid((unsigned)((a.N + 31) / 32), (unsigned)((a.n_cells + kCellWarps - 1) / kCellWarps));
+  log_targets_kernel<<<grid, 32 * kCellWarps, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -833,6 +790,32 @@ cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* s
                                 __half* Kg, cudaStream_t st) {
   if (S == 0) return cudaSuccess;
   gather_rows_kernel<<<(unsigned)S, 256, 0, st>>>(Kh, Ppad, slot_pat, S, Kg);
+  return cudaGetLastError();
+}
+
+// koff[p][kb] = the first entry of pattern p's photon list (kptr, kidx
+// ascending within a pattern) at pixel >= 64 kb, kb = 0 .. KB.
+__global__ void koff_kernel(const int64_t* kptr, const int32_t* kidx, int64_t N, int KB,
+                            int32_t* koff) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * (KB + 1)) return;
+  const int64_t p = i / (KB + 1);
+  const int32_t key = (int32_t)(i % (KB + 1)) * 64;
+  int64_t lo = kptr[p], hi = kptr[p + 1];
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (kidx[mid] < key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  koff[i] = (int32_t)lo;
+}
+
+cudaError_t launch_koff(const int64_t* kptr, const int32_t* kidx, int64_t N, int KB, int32_t* koff,
+                        cudaStream_t st) {
+  const int64_t n = N * (KB + 1);
+  koff_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(kptr, kidx, N, KB, koff);
   return cudaGetLastError();
 }
 

@@ -15,6 +15,8 @@ struct TargetArgs {
   int64_t N, R;
   int n_cells;
   const int32_t* cell;     // [R] cell of every fine rotation
+  const int64_t* mbeg;     // [n_cells] first rotation of each cell (rotations sorted by cell)
+  const int32_t* mcnt;     // [n_cells] its rotation count
   const float* P;          // FP32 responsibilities [R][ldP] (FP32 path) or nullptr
   const double* L64;       // log targets of FP32 contexts: the FP64 log-likelihood [R][ldP]
   int64_t ldP;
@@ -99,6 +101,10 @@ cudaError_t launch_group_softmax(const GroupArgs& g, cudaStream_t st);
 // slot_pat[slot] = pattern, -1 for padding (zero).
 cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* slot_pat, int64_t S,
                                 __half* Kg, cudaStream_t st);
+// Per pattern and 64-pixel k-block the first entry of its photon list in the
+// block: koff [N][KB + 1] (int32 entry indices).
+cudaError_t launch_koff(const int64_t* kptr, const int32_t* kidx, int64_t N, int KB, int32_t* koff,
+                        cudaStream_t st);
 // The same rows from the counts' photon lists (kptr [N+1], kidx, kval), each
 // row built in shared memory: Ppad FP16 must fit (slot_rows_fit).
 bool slot_rows_fit(int64_t Ppad);

@@ -120,6 +120,15 @@ struct GMaxEpiArgs {
   const double* rowstat;   // [R] poisson: sum W_r
   float* Y;                // [slots][ldY]
   int64_t ldY;
+  // A tiles built from photon lists (launch_group_maximize_build_tc): the
+  // entries of pattern p in k-block kb (64 pixels) are koff[p * kb_stride +
+  // kb] .. koff[p * kb_stride + kb + 1] - 1 of (kidx = active pixel, kval =
+  // count); slots from n_slots on are zero rows
+  const int32_t* koff;
+  const int32_t* kidx;
+  const float* kval;
+  int64_t n_slots;
+  int32_t kb_stride;
 };
 cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap& tmBhi,
                                      const CUtensorMap& tmBlo, int64_t n_tiles,
@@ -133,6 +142,13 @@ cudaError_t launch_group_maximize_pair_tc(const CUtensorMap& tmKg, const CUtenso
                                           const CUtensorMap& tmBlo, int64_t n_tiles,
                                           const GMaxEpiArgs& e, TcStatus* status, int num_sms,
                                           cudaStream_t st);
+
+// The same with each tile's A rows (one slot each) written into shared
+// memory by builder warps from the counts' photon lists (GMaxEpiArgs.koff
+// ...): no gathered copy Kg is read or written.
+cudaError_t launch_group_maximize_build_tc(const CUtensorMap& tmBhi, const CUtensorMap& tmBlo,
+                                           int64_t n_tiles, const GMaxEpiArgs& e,
+                                           TcStatus* status, int num_sms, cudaStream_t st);
 
 // Grouped compress: acc[member][j] = sum_q A[mbeg_c + member][q] Kg[slot0_c + q][j]
 // with A = P / (T_r phi) as FP16 hi + lo (zero beyond the cell's slots);
@@ -264,7 +280,9 @@ cudaError_t launch_sort_entries(int2* rp, float* v, int64_t n, int64_t N, int64_
 cudaError_t launch_T_from_sorted(const int2* rp, const float* Pv, int64_t n, int64_t R,
                                  int64_t* rowtot, int64_t* rowoff, float* T, cudaStream_t st);
 // ... and the lists of the entries with P >= rel_min T_r in sorted order,
-// x = P / (T_r phi_new) (rowoff [R+1] of the lists; flag [2n + 2] scratch).
+// x = P / (T_r phi_new) (rowoff [R+1] of the lists; flag [2n + 2 +
+// scan_scratch(n)] scratch).
+int64_t scan_scratch(int64_t n);
 cudaError_t launch_list_from_sorted(const int2* rp, const float* Pv, int64_t n, int64_t R,
                                     const float* T, const float* new_scaling, float rel_min,
                                     int64_t* rowtot, int64_t* rowoff, int64_t* flag,
