@@ -168,8 +168,6 @@ struct emc_context {
   double* d_rowstat = nullptr;
   uint2* d_vtab = nullptr;  // mixed + nearest: per-voxel (W, split operand) table of the expand
   float4* d_tri = nullptr;  // trilinear: the expansion's stencil table (8 corners per base voxel)
-  int32_t* d_koff = nullptr;  // first photon-list entry per pattern and 64-pixel k-block
-  bool koff_valid = false;
   double* d_scratch = nullptr;  // reductions
   double* d_stats = nullptr;    // [0] mean [1] max [2] plogp [3] loglik
   // FP32 path
@@ -780,7 +778,6 @@ static emc_status finish_patterns(emc_context* c) {
   c->have_pat = true;
   c->csr.valid = false;
   c->csc.valid = false;
-  c->koff_valid = false;
   return EMC_OK;
 }
 
@@ -2288,18 +2285,6 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
   // the grouped compresses read the per-cell operand Pt instead
   const bool lists = tc && c->tune.compress_sparse && c->npa <= kListMaxPixels;
   if (!lists) TRY(grow(c, &c->d_Pt, c->pt_cap, evals));
-  // the grouped maximize on SM pairs builds its A tiles from the photon lists
-  // when nothing else reads the gathered counts Kg
-  const bool build_a = tc && c->tune.maximize_pair && lists;
-  if (build_a && !c->koff_valid) {
-    if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
-    if (c->csr.nnz >= ((int64_t)1 << 31))
-      return c->fail(EMC_ERR_UNSUPPORTED, "more than 2^31 photon-list entries");
-    const int KB = (int)(c->Ppad / kPairBoxK);
-    if (!c->d_koff) TRY(c->alloc(&c->d_koff, c->N * (KB + 1)));
-    CK(c, launch_koff(c->csr.ptr, c->csr.idx, c->N, KB, c->d_koff, c->st));
-    c->koff_valid = true;
-  }
   std::vector<int4> mt, ct;
   int64_t n_gmt = 0, n_gct = 0;
   TileDesc *gmt = nullptr, *gct = nullptr;
@@ -2330,7 +2315,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     }
     TRY(grow(c, &c->d_gmt, c->gmt_cap, n_gmt));
     TRY(grow(c, &c->d_gct, c->gct_cap, n_gct));
-    if (!build_a) TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
+    TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
     if (!lists && kw > c->a_ld) {
       for (__half** q : {&c->d_Ahi, &c->d_Alo})
         if (*q) {
@@ -2420,12 +2405,9 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
   int launches = 0;
   if (tc) {
     CUtensorMap tmKg, tmKg64, tmAhi, tmAlo;
-    if (!build_a &&
-        !tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, gpair_form ? kPairBoxK : kMaximizeBK))
+    if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, gpair_form ? kPairBoxK : kMaximizeBK))
       return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
-    if (build_a) {
-      // no Kg: the maximize writes its A tiles itself
-    } else if (slot_rows_fit(c->Ppad)) {
+    if (slot_rows_fit(c->Ppad)) {
       // the slot rows from the photon lists (writes the rows, reads the lists)
       if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
       CK(c, launch_slot_rows(c->csr.ptr, c->csr.idx, c->csr.val, c->Ppad, c->d_gpair, S, c->d_Kg,
@@ -2449,15 +2431,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     ge.rowstat = c->d_rowstat;
     ge.Y = c->d_Yc;
     ge.ldY = MM;
-    if (build_a) {
-      ge.koff = c->d_koff;
-      ge.kidx = c->csr.idx;
-      ge.kval = c->csr.val;
-      ge.n_slots = S;
-      ge.kb_stride = (int32_t)(c->Ppad / kPairBoxK) + 1;
-      CK(c, launch_group_maximize_build_tc(c->tmBhi64, c->tmBlo64, n_gmt, ge, c->d_status,
-                                           c->num_sms, c->st));
-    } else if (gpair_form)
+    if (gpair_form)
       CK(c, launch_group_maximize_pair_tc(tmKg, c->tmBhi64, c->tmBlo64, n_gmt, ge, c->d_status,
                                           c->num_sms, c->st));
     else
@@ -2497,8 +2471,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
       la.e = cmp_args(c);
       la.e.Tskip = nullptr;  // the proposed iteration's own T_r
       CK(c, launch_list_compress(la, c->st));
-      // (row build,) contraction, softmax, count + scan, fill, compress
-      launches = build_a ? 6 : 7;
+      launches = 7;  // row build, contraction, softmax, count + scan, fill, compress
     } else {
     CK(c, launch_p_split(g, c->d_cell, R, c->d_T, c->a_ld, c->d_Ahi, c->d_Alo, c->st));
     c->mark(3);

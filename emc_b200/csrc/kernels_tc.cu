@@ -143,18 +143,6 @@ struct b_major_mn : std::false_type {};
 template <class E>
 struct b_major_mn<E, std::void_t<decltype(E::kBMajorMN)>> : std::bool_constant<E::kBMajorMN> {};
 
-// Listed pair epilogues with kBuildA = true have their A tiles written into
-// shared memory by builder warps (from the counts' photon lists) instead of
-// loaded by TMA; see the builder branch of tc_pair_kernel.
-template <class E, class = void>
-struct build_a : std::false_type {};
-template <class E>
-struct build_a<E, std::void_t<decltype(E::kBuildA)>> : std::bool_constant<E::kBuildA> {};
-template <class Epi>
-constexpr int pair_threads() {
-  return 64 + 32 * Epi::kEpiWarps + (build_a<Epi>::value ? 32 * 8 : 0);
-}
-
 // Listed pair epilogues with kCellN = true narrow each tile's MMA to its
 // cell's members rounded up to 16 (epi.a.mcnt[cell]); each CTA of the pair
 // then holds half of that many B rows.
@@ -168,27 +156,12 @@ struct Ctl {
   TcStatus* st;
 };
 
-// The same wait with cluster-scope acquire: the phase's arrivals include the
-// peer CTA's, whose shared-memory writes before them must be visible.
-__device__ __forceinline__ bool mbar_test_cluster(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
 __device__ bool bounded_wait(uint32_t bar, uint32_t parity, const Ctl& c, int site,
-                             uint64_t limit_ns = kWaitLimitNs, bool cluster = false) {
-  auto test = [&]() { return cluster ? mbar_test_cluster(bar, parity) : mbar_test(bar, parity); };
-  if (test()) return true;
+                             uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_test(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
-    if (test()) return true;
+    if (mbar_test(bar, parity)) return true;
     if ((it & 31) == 0) {
       if (*c.abort) return false;
       if (globaltimer() - t0 > limit_ns) {
@@ -790,12 +763,6 @@ struct EpiGMaxPair : EpiGMax {
   }
 };
 
-// The same with the A tiles built from the counts' photon lists in shared
-// memory (no gathered copy of the counts).
-struct EpiGMaxBuild : EpiGMaxPair {
-  static constexpr bool kBuildA = true;
-};
-
 // Grouped compress: row = member rotation r of the tile's cell, column =
 // active pixel; acc = U_r (the operand rows are P / (T_r phi)), inserted with
 // weight rotw T_r as in EpiCmp.
@@ -997,7 +964,7 @@ cudaError_t run_gemm(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n
   const int64_t tiles = m_tiles * n_tiles;
   if (tiles == 0) return cudaSuccess;
   const int grid = (int)(tiles < num_sms ? tiles : num_sms);
-  kern<<<grid, pair_threads<Epi>(), dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks, raster,
+  kern<<<grid, 64 + 32 * Epi::kEpiWarps, dyn, stream>>>(maps, m_tiles, n_tiles, k_blocks, raster,
                                                        epi, st);
   return cudaGetLastError();
 }
@@ -1068,7 +1035,7 @@ constexpr int kPairStages = 4;
 // pair (a_row, b_row: the CTA adds 128 x rank), k-block count and tensor-map
 // set; its row_begin then receives the row inside this CTA's 128 rows.
 template <int NA, int NB, bool M_INNER, class Epi>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(pair_threads<Epi>(), 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
     tc_pair_kernel(const __grid_constant__ TmapSet<Epi::kSets> maps, const int64_t m_tiles,
                    const int64_t n_tiles, const int64_t k_blocks, const int raster,
                    const Epi epi, TcStatus* status) {
@@ -1098,11 +1065,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(pair_threads<Epi>(),
     asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(pa), "r"(1) : "memory");
   };
 
-  constexpr bool kBuild = build_a<Epi>::value;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      // built A tiles: the leader's producer and four builder warps per CTA
-      mbar_init(smem_u32(&full_bar[s]), kBuild ? 1 + 2 * 4 : 1);
+      mbar_init(smem_u32(&full_bar[s]), 1);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -1183,15 +1148,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(pair_threads<Epi>(),
             break;
           }
           const uint32_t fb = smem_u32(&full_bar[s]);
-          // both CTAs' bytes (only B's when builder warps write A)
-          if (leader) mbar_expect_tx(fb, kBuild ? 2 * NB * B_BYTES : 2 * STAGE_BYTES);
+          if (leader) mbar_expect_tx(fb, 2 * STAGE_BYTES);  // both CTAs' bytes
           const uint32_t fb_leader = peer_addr(fb, 0);
           const uint32_t base = smem_u32(smem + (size_t)s * STAGE_BYTES);
           const int kc = (int)(kb * kPairBK);
-          if constexpr (!kBuild) {
-            tma_load_2d_pair(base, tA0, kc, ar, fb_leader);
-            if (NA == 2) tma_load_2d_pair(base + A_BYTES, tA1, kc, ar, fb_leader);
-          }
+          tma_load_2d_pair(base, tA0, kc, ar, fb_leader);
+          if (NA == 2) tma_load_2d_pair(base + A_BYTES, tA1, kc, ar, fb_leader);
           const uint32_t bbase = base + NA * A_BYTES;
           tma_load_2d_pair(bbase, tB0, kc, br, fb_leader);
           if (NB == 2) tma_load_2d_pair(bbase + B_BYTES, tB1, kc, br, fb_leader);
@@ -1255,7 +1217,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(pair_threads<Epi>(),
           }
         }
         for (int64_t kb = 0; kb < kbs; ++kb) {
-          if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3, kWaitLimitNs, kBuild)) {
+          if (!bounded_wait(smem_u32(&full_bar[s]), ph, ctl, 3)) {
             ok = false;
             abort_pair();
             break;
@@ -1290,60 +1252,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(pair_threads<Epi>(),
       const uint64_t t0 = globaltimer();
       while (!mbar_test(smem_u32(&drain_bar), 0) && globaltimer() - t0 < kWaitLimitNs) {
       }
-    }
-  } else if (warp >= 2 + Epi::kEpiWarps) {
-    // -------------------------------------------------- A-tile builders (both CTAs)
-    // Eight warps: warp pair b (of four) owns rows 32 b .. 32 b + 31 of this
-    // CTA's 128, one row (slot) per lane, and its two warps take the even and
-    // the odd k-blocks.  Per k-block a lane zeroes its 128-byte row of the
-    // stage and writes the row's counts from its pattern's photon lists (the
-    // entries of k-block kb are koff[p][kb] .. koff[p][kb + 1] - 1) at their
-    // 128-byte-swizzle positions, then the warp makes the writes visible to
-    // the tensor core (proxy fence) and arrives on the leader's full barrier.
-    if constexpr (kBuild) {
-      const int bw = warp - 2 - Epi::kEpiWarps;
-      const int par = bw & 1, row = (bw >> 1) * 32 + lane;
-      int s = 0;
-      uint32_t ph = 0;
-      int64_t g = 0;
-      bool ok = true;
-      for (int64_t t = cid; t < num_tiles && ok; t += ncl) {
-        const TileDesc d = epi.a.tiles[t];
-        const int64_t slot = (int64_t)d.a_row + rank * 128 + row;
-        const int p = slot < epi.a.n_slots ? epi.a.gpair[slot] : -1;
-        const int32_t* koff = p >= 0 ? epi.a.koff + (int64_t)p * epi.a.kb_stride : nullptr;
-        for (int64_t kb = 0; kb < d.k_blocks; ++kb, ++g) {
-          const int cs = s;
-          const uint32_t cph = ph;
-          if (++s == STAGES) {
-            s = 0;
-            ph ^= 1;
-          }
-          if ((int)(g & 1) != par) continue;
-          bool free_stage = lane == 0 ? bounded_wait(smem_u32(&empty_bar[cs]), cph ^ 1, ctl, 6) : true;
-          free_stage = __shfl_sync(0xffffffffu, free_stage, 0);
-          if (!free_stage) {
-            ok = false;
-            break;
-          }
-          uint8_t* rowp = smem + (size_t)cs * STAGE_BYTES + row * 128;
-#pragma unroll
-          for (int q = 0; q < 8; ++q) reinterpret_cast<uint4*>(rowp)[q] = make_uint4(0u, 0u, 0u, 0u);
-          if (koff) {
-            const int32_t e0 = koff[kb], e1 = koff[kb + 1];
-            const int kc = (int)(kb * kPairBK);
-            for (int32_t e = e0; e < e1; ++e) {
-              const int col = epi.a.kidx[e] - kc;
-              *reinterpret_cast<__half*>(rowp + ((((col >> 3) ^ (row & 7)) << 4) + ((col & 7) << 1))) =
-                  __float2half_rn(epi.a.kval[e]);
-            }
-          }
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          __syncwarp();
-          if (lane == 0) mbar_arrive_cluster(peer_addr(smem_u32(&full_bar[cs]), 0));
-        }
-      }
-      if (!ok && lane == 0) abort_pair();
     }
   } else {
     // -------------------------------------------------- epilogue warps (both CTAs)
@@ -2229,16 +2137,6 @@ cudaError_t launch_group_maximize_pair_tc(const CUtensorMap& tmKg, const CUtenso
   EpiGMaxPair epi;
   epi.a = e;
   return run_pair<1, 2, true>(one_set(tmKg, tmKg, tmBhi, tmBlo), n_tiles, 1, 0, epi, status,
-                              num_sms, st, 1);
-}
-
-cudaError_t launch_group_maximize_build_tc(const CUtensorMap& tmBhi, const CUtensorMap& tmBlo,
-                                           int64_t n_tiles, const GMaxEpiArgs& e,
-                                           TcStatus* status, int num_sms, cudaStream_t st) {
-  EpiGMaxBuild epi;
-  epi.a = e;
-  // the A maps are not read (builder warps write A)
-  return run_pair<1, 2, true>(one_set(tmBhi, tmBhi, tmBhi, tmBlo), n_tiles, 1, 0, epi, status,
                               num_sms, st, 1);
 }
 

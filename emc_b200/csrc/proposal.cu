@@ -793,32 +793,6 @@ cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* s
   return cudaGetLastError();
 }
 
-// koff[p][kb] = the first entry of pattern p's photon list (kptr, kidx
-// ascending within a pattern) at pixel >= 64 kb, kb = 0 .. KB.
-__global__ void koff_kernel(const int64_t* kptr, const int32_t* kidx, int64_t N, int KB,
-                            int32_t* koff) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N * (KB + 1)) return;
-  const int64_t p = i / (KB + 1);
-  const int32_t key = (int32_t)(i % (KB + 1)) * 64;
-  int64_t lo = kptr[p], hi = kptr[p + 1];
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (kidx[mid] < key)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  koff[i] = (int32_t)lo;
-}
-
-cudaError_t launch_koff(const int64_t* kptr, const int32_t* kidx, int64_t N, int KB, int32_t* koff,
-                        cudaStream_t st) {
-  const int64_t n = N * (KB + 1);
-  koff_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(kptr, kidx, N, KB, koff);
-  return cudaGetLastError();
-}
-
 bool slot_rows_fit(int64_t Ppad) { return Ppad * 2 <= 200 * 1024; }
 
 cudaError_t launch_slot_rows(const int64_t* kptr, const int32_t* kidx, const float* kval,

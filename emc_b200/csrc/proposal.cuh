@@ -101,10 +101,6 @@ cudaError_t launch_group_softmax(const GroupArgs& g, cudaStream_t st);
 // slot_pat[slot] = pattern, -1 for padding (zero).
 cudaError_t launch_gather_slots(const __half* Kh, int64_t Ppad, const int32_t* slot_pat, int64_t S,
                                 __half* Kg, cudaStream_t st);
-// Per pattern and 64-pixel k-block the first entry of its photon list in the
-// block: koff [N][KB + 1] (int32 entry indices).
-cudaError_t launch_koff(const int64_t* kptr, const int32_t* kidx, int64_t N, int KB, int32_t* koff,
-                        cudaStream_t st);
 // The same rows from the counts' photon lists (kptr [N+1], kidx, kval), each
 // row built in shared memory: Ppad FP16 must fit (slot_rows_fit).
 bool slot_rows_fit(int64_t Ppad);

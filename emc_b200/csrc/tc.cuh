@@ -120,15 +120,6 @@ struct GMaxEpiArgs {
   const double* rowstat;   // [R] poisson: sum W_r
   float* Y;                // [slots][ldY]
   int64_t ldY;
-  // A tiles built from photon lists (launch_group_maximize_build_tc): the
-  // entries of pattern p in k-block kb (64 pixels) are koff[p * kb_stride +
-  // kb] .. koff[p * kb_stride + kb + 1] - 1 of (kidx = active pixel, kval =
-  // count); slots from n_slots on are zero rows
-  const int32_t* koff;
-  const int32_t* kidx;
-  const float* kval;
-  int64_t n_slots;
-  int32_t kb_stride;
 };
 cudaError_t launch_group_maximize_tc(const CUtensorMap& tmKg, const CUtensorMap& tmBhi,
                                      const CUtensorMap& tmBlo, int64_t n_tiles,
@@ -142,13 +133,6 @@ cudaError_t launch_group_maximize_pair_tc(const CUtensorMap& tmKg, const CUtenso
                                           const CUtensorMap& tmBlo, int64_t n_tiles,
                                           const GMaxEpiArgs& e, TcStatus* status, int num_sms,
                                           cudaStream_t st);
-
-// The same with each tile's A rows (one slot each) written into shared
-// memory by builder warps from the counts' photon lists (GMaxEpiArgs.koff
-// ...): no gathered copy Kg is read or written.
-cudaError_t launch_group_maximize_build_tc(const CUtensorMap& tmBhi, const CUtensorMap& tmBlo,
-                                           int64_t n_tiles, const GMaxEpiArgs& e,
-                                           TcStatus* status, int num_sms, cudaStream_t st);
 
 // Grouped compress: acc[member][j] = sum_q A[mbeg_c + member][q] Kg[slot0_c + q][j]
 // with A = P / (T_r phi) as FP16 hi + lo (zero beyond the cell's slots);
