@@ -152,3 +152,24 @@ def test_chunk_arguments_are_checked(small):
         with pytest.raises(E.EmcError) as ei:
             ctx.set_rotation_chunk(512)
         assert ei.value.status == 7
+
+
+def test_chunked_cell_masses_match_unchunked(small):
+    """Cell masses and log masses after a chunked iteration (from the kept
+    entries) against the unchunked iteration's (from Y): equal where the
+    mass is above the kept entries' 1e-30 floor."""
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    q, w, cell, n_cells = sorted_rotations(small["q"], small["w"], coarse_n=1)
+    d = dict(small, q=q, w=w)
+    out = {}
+    for rows in (0, 512):
+        with make_ctx(d, "poisson", "nearest", "mixed") as ctx:
+            ctx.set_rotation_chunk(rows)
+            lp = LearnedProposal(ctx, cell, n_cells)
+            ctx.iterate()
+            out[rows] = (lp.targets().cpu().numpy(), lp.log_mass().cpu().numpy())
+    (t0, l0), (t1, l1) = out[0], out[512]
+    np.testing.assert_allclose(t1, t0, rtol=1e-5, atol=1e-7)
+    big = l0 > np.log(1e-25)
+    assert big.any()
+    assert np.abs(l1[big] - l0[big]).max() <= 1e-4

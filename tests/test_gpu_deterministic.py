@@ -2,9 +2,8 @@
 same model, weight and scaling (fixed-point insertion sums, responsibility
 lists in (rotation, pattern) order, slices summed in list order), in both
 precisions, with the compress from lists, the dense tensor-core compress and
-rotation chunks.  After three iterations the exact sums stay within 1e-5 of
-the FP32 atomic ones (whose own rounding the iterations carry forward), and
-they hold the oracle bars."""
+rotation chunks.  After one iteration the exact sums are within 1e-6 of the
+FP32 atomic ones, and over three they hold the oracle bars."""
 import numpy as np
 import pytest
 
@@ -50,11 +49,13 @@ def test_two_runs_are_bitwise_equal(small, lik, interp, prec, lists, chunk):
     b = _run(small, lik, interp, prec, lists=lists, chunk=chunk)
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
-    # the exact sums against the FP32 atomics of the default mode
-    c = _run(small, lik, interp, prec, det=False, lists=lists, chunk=chunk)
-    assert rel(a[0], c[0]) <= 1e-5, rel(a[0], c[0])
-    assert rel(a[1], c[1]) <= 1e-5, rel(a[1], c[1])
-    assert rel(a[2], c[2]) <= 1e-5, rel(a[2], c[2])
+    # the exact sums against the FP32 atomics of the default mode, one
+    # iteration (later iterations carry the atomics' own rounding forward)
+    e = _run(small, lik, interp, prec, lists=lists, chunk=chunk, iters=1)
+    c = _run(small, lik, interp, prec, det=False, lists=lists, chunk=chunk, iters=1)
+    assert rel(e[0], c[0]) <= 1e-6, rel(e[0], c[0])
+    assert rel(e[1], c[1]) <= 1e-6, rel(e[1], c[1])
+    assert rel(e[2], c[2]) <= 1e-6, rel(e[2], c[2])
 
 
 @pytest.mark.parametrize("prec,tol", [("mixed", 1e-4), ("fp32", 1e-5)])
