@@ -82,16 +82,6 @@ __global__ void __launch_bounds__(256) targets_kernel(const TargetArgs a) {
   a.t[p * a.n_cells + c] = sum;
 }
 
-// Largest of *addr and v for floats (ordered through their bit patterns:
-// atomicMax on the signed bits of non-negative values, atomicMin on the
-// unsigned bits of negative ones).
-__device__ __forceinline__ void atomic_max_f32(float* addr, float v) {
-  if (__float_as_int(v) >= 0)
-    atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
-  else
-    atomicMin(reinterpret_cast<unsigned int*>(addr), __float_as_uint(v));
-}
-
 // lt[p][c] = natural log of the responsibility mass of cell c in the log
 // domain (an online maximum with a rescaled FP64 sum of exponentials), so
 // every cell is ranked however far down the tail it lies.  Layout as
