@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=12)
     ap.add_argument("--top-k", type=int, default=2048,
                     help="fine rotations per pattern covered by the cells of its previous posterior")
+    ap.add_argument("--keep-tail", type=float, default=0.0,
+                    help="also keep the cells holding all but this share of the previous posterior")
     ap.add_argument("--spec-top-k", type=int, default=512,
                     help="the smaller top-k reported beside the timed one (one step and 12 chained)")
     ap.add_argument("--oracle-patterns", type=int, default=16,
@@ -395,7 +397,7 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
     def one_step(pr, keep):
         ctx.set_model(m0)
         ctx.set_scaling(s0)
-        st = lp.iterate_topk(pr, keep, top_k, max_cells, target, audit, min_cap)
+        st = lp.iterate_topk(pr, keep, top_k, max_cells, target, audit, min_cap, a.keep_tail)
         cand = torch.isfinite(lp.log_mass())
         cap = (t_next * cand).sum(1)
         return st, ctx.get_model(), {
@@ -428,7 +430,8 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
         ctx.set_scaling(s0)
         keep, fb = lk, 0
         for _ in range(12):
-            fb += lp.iterate_topk(probs, keep, k, max_cells, target, audit, min_cap)["fallback"]
+            fb += lp.iterate_topk(probs, keep, k, max_cells, target, audit, min_cap,
+                                  a.keep_tail)["fallback"]
             keep = lp.log_mass()
         return rel_err(ctx.get_model(), m_d12), fb
 
@@ -436,7 +439,7 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
     # the configuration's own top-k (512 fine rotations): one step and 12 chained
     ctx.set_model(m0)
     ctx.set_scaling(s0)
-    st512 = lp.iterate_topk(probs, lk, a.spec_top_k, max_cells, target, audit, min_cap)
+    st512 = lp.iterate_topk(probs, lk, a.spec_top_k, max_cells, target, audit, min_cap, a.keep_tail)
     cap512 = (t_next * torch.isfinite(lp.log_mass())).sum(1)
     spec = {"top_k": a.spec_top_k, "cells": st512["pairs"] / N,
             "captured_min": float(cap512.min()),
@@ -448,7 +451,7 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
     ctx.set_scaling(s0)
     keep = lk
     for _ in range(2):
-        lp.iterate_topk(probs, keep, top_k, max_cells, target, audit, min_cap)
+        lp.iterate_topk(probs, keep, top_k, max_cells, target, audit, min_cap, a.keep_tail)
         keep = lp.log_mass()
     ext = torch.cuda.ExternalStream(ctx.stream)
     torch.cuda.synchronize()
@@ -457,7 +460,7 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
         e0.record()
     evals = fallbacks = pairs = 0
     for _ in range(a.learned_steps):
-        st = lp.iterate_topk(probs, keep, top_k, max_cells, target, audit, min_cap)
+        st = lp.iterate_topk(probs, keep, top_k, max_cells, target, audit, min_cap, a.keep_tail)
         keep = lp.log_mass()
         evals += st["evaluations"]
         pairs += st["pairs"]
@@ -469,7 +472,7 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
     ctx.set_profiling(True)
     stage = np.zeros(5)
     for i in range(3):
-        lp.iterate_topk(probs, keep, top_k, max_cells, target, audit, min_cap)
+        lp.iterate_topk(probs, keep, top_k, max_cells, target, audit, min_cap, a.keep_tail)
         keep = lp.log_mass()
         if i >= 1:
             stage += ctx.stage_times()
@@ -478,6 +481,7 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
     lp.net.close()
     return {
         "ms_per_step": ms, "top_k": top_k, "audit_patterns": audit, "min_captured": min_cap,
+        **({"keep_tail": a.keep_tail} if a.keep_tail else {}),
         "fallback_iterations": fallbacks, "forced_fallback_iterations": st_f["fallback"],
         "cells_per_pattern": round(pairs / a.learned_steps / N, 2),
         "evaluated_fraction": evals / a.learned_steps / (N * R),
