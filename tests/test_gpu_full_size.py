@@ -60,8 +60,8 @@ def test_full_size_properties(workload, n_patterns):
 
 
 # Bars of the benchmark geometry against the FP64 oracle: the mixed path must
-# hold the north-star bar (responsibility L1 <= 1e-2 per pattern, model <= 1e-3
-# relative); the FP32 path the FP32 bars of the parity tests.
+# hold responsibility L1 <= 1e-2 per pattern and model <= 1e-3 relative; the
+# FP32 path the FP32 bars of the parity tests.
 LARGE_BARS = {"mixed": (1e-2, 1e-3), "fp32": (1e-4, 1e-5)}
 
 
