@@ -173,3 +173,34 @@ def test_chunked_cell_masses_match_unchunked(small):
     big = l0 > np.log(1e-25)
     assert big.any()
     assert np.abs(l1[big] - l0[big]).max() <= 1e-4
+
+
+def test_proposed_iterations_on_a_chunked_context(small):
+    """The learned-proposal iteration on a chunked context: the dense
+    iteration before it runs in chunks (its log cell masses come from the
+    kept entries), and the proposed iteration, over the same candidates,
+    gives the model and scaling of the unchunked context's."""
+    import torch
+
+    from emc_b200.proposal import LearnedProposal, sorted_rotations
+    q, w, cell, n_cells = sorted_rotations(small["q"], small["w"], coarse_n=1)
+    d = dict(small, q=q, w=w)
+    N = d["counts"].shape[0]
+    rng = np.random.default_rng(3)
+    z = rng.standard_normal((N, n_cells)) * 2.0
+    probs = np.exp(z - z.max(1, keepdims=True))
+    probs = torch.from_numpy((probs / probs.sum(1, keepdims=True)).astype(np.float32)).cuda()
+    out = {}
+    for rows in (0, 512):
+        with make_ctx(d, "poisson", "nearest", "mixed") as ctx:
+            ctx.set_rotation_chunk(rows)
+            lp = LearnedProposal(ctx, cell, n_cells)
+            ctx.iterate()
+            assert np.isfinite(lp.log_mass().cpu().numpy().max(axis=1)).all()
+            # the same candidates for both contexts: from the fixed probabilities
+            st = lp.iterate_topk(probs, None, top_k=1, max_cells=8, mass_target=0.9)
+            assert st["fallback"] == 0
+            out[rows] = (ctx.get_model(), ctx.get_scaling(), st["pairs"])
+    assert out[512][2] == out[0][2]
+    assert rel(out[512][1], out[0][1]) <= 1e-5
+    assert rel(out[512][0], out[0][0]) <= 1e-5
