@@ -502,8 +502,9 @@ def learned_proposal(a, E, W, d, device, dense_ms, dense_err):
 def batched_datasets(a, E, W, device, workloads):
     """Six independent datasets (48 ... 128 px detectors) iterated (1) one
     after the other, each with its own launches, and (2) together: one
-    persistent launch per contraction over all datasets' tiles, the whole
-    iteration captured in a CUDA graph and replayed."""
+    persistent launch per contraction over the datasets' tiles (a dataset
+    that fills the GPU alone keeps its own), the whole iteration captured in
+    a CUDA graph and replayed."""
     import torch
     data = [W.make(w) for w in workloads]
     ctxs = []

@@ -120,6 +120,9 @@ constexpr float kListRel = 1e-12f;
 constexpr float kListMinP = 1e-30f;
 // Shared memory of the list compress: one FP32 per active pixel.
 constexpr int64_t kListMaxPixels = 51200;
+// A batched dataset keeps its own contraction launches when its maximize
+// alone fills the persistent grid this many times over.
+constexpr int64_t kAloneWaves = 8;
 
 // Non-zero entries of a dense matrix as compressed rows (see build_rows).
 struct SparseRows {
@@ -2619,6 +2622,7 @@ struct emc_batch {
   int64_t n_mt = 0, n_ct = 0;
   bool pair = false;      // the batched maximize on SM pairs
   bool cmp_pair = false;  // the batched compress on SM pairs
+  std::vector<char> alone;  // datasets that keep their own contraction launches
   MaxEpiArgs* d_max = nullptr;  // per-dataset epilogue arguments (fixed per context)
   CmpEpiArgs* d_cmp = nullptr;
   cudaGraph_t graph = nullptr;
@@ -2695,11 +2699,23 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
     ctxs[i]->st = b->st;  // every stage of every dataset on the batch's stream
     ctxs[i]->batched = true;
   }
+  // A dataset whose own maximize fills the persistent grid for
+  // kAloneWaves waves gains nothing from sharing it: it keeps its own
+  // contraction launches (its tuned form and tile order) inside the batch's
+  // iteration and graph, and the batched launches cover the others.
+  std::vector<int32_t> order;
+  for (int32_t i = 0; i < n; ++i) {
+    const emc_context* c = ctxs[i];
+    const bool pr = c->tune.maximize_pair;
+    const int64_t tiles = pr ? ((c->Npad + 255) / 256) * (c->Rpad / 256)
+                             : (c->Npad / 128) * (c->Rpad / 256);
+    const int64_t wave = pr ? c->num_sms / 2 : c->num_sms;
+    b->alone.push_back(tiles >= kAloneWaves * wave ? 1 : 0);
+    if (!b->alone.back()) order.push_back(i);
+  }
   // Tile lists, the costliest tiles first (a tile's time grows with its K
   // extent), each dataset's tiles in the order of its own launch.
-  std::vector<int32_t> order(n);
   std::vector<TileDesc> mt, ct;
-  for (int32_t i = 0; i < n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(),
                    [&](int32_t x, int32_t y) { return ctxs[x]->Ppad > ctxs[y]->Ppad; });
   // the order of the single-dataset launch (tile_mn in kernels_tc.cu): the
@@ -2714,7 +2730,7 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
   // one form for the batched maximize: SM pairs when the datasets that chose
   // them on their own hold most of the work
   double work = 0.0, work_pair = 0.0;
-  for (int32_t i = 0; i < n; ++i) {
+  for (int32_t i : order) {
     const double w = (double)ctxs[i]->Npad * ctxs[i]->Rpad * ctxs[i]->Ppad;
     work += w;
     if (ctxs[i]->tune.maximize_pair) work_pair += w;
@@ -2737,7 +2753,7 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
   std::stable_sort(order.begin(), order.end(),
                    [&](int32_t x, int32_t y) { return ctxs[x]->Npad > ctxs[y]->Npad; });
   double cwork_pair = 0.0;
-  for (int32_t i = 0; i < n; ++i)
+  for (int32_t i : order)
     if (ctxs[i]->tune.compress_pair)
       cwork_pair += (double)ctxs[i]->Npad * ctxs[i]->Rpad * ctxs[i]->Ppad;
   b->cmp_pair = cwork_pair * 2.0 >= work;
@@ -2756,6 +2772,8 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
   }
   b->n_mt = (int64_t)mt.size();
   b->n_ct = (int64_t)ct.size();
+  mt.resize(std::max<size_t>(mt.size(), 1));  // no merged dataset: a list never read
+  ct.resize(std::max<size_t>(ct.size(), 1));
   std::vector<MaxEpiArgs> me(n);
   std::vector<CmpEpiArgs> ce(n);
   for (int32_t i = 0; i < n; ++i) {
@@ -2810,10 +2828,22 @@ emc_status emc_batch_iterate(emc_batch* b) {
     maps.b0[i] = maps.b0[0];
     maps.b1[i] = maps.b1[0];
   }
-  if (b->pair)
+  if (b->n_mt && b->pair)
     BCK(b, launch_batch_maximize_pair_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
-  else
+  else if (b->n_mt)
     BCK(b, launch_batch_maximize_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
+  for (int i = 0; i < n; ++i) {
+    if (!b->alone[i]) continue;
+    emc_context* c = b->ctx[i];
+    const MaxEpiArgs e = max_args(c);
+    if (c->tune.maximize_pair)
+      BCK(b, launch_maximize_pair_tc(c->tmKh64, c->tmBhi64, c->tmBlo64, c->Npad, c->Rpad, c->Ppad,
+                                     e, c->d_status, c->num_sms, b->st, c->tune.maximize_raster));
+    else
+      BCK(b, launch_maximize_tc(c->tmKh, c->tmBhi, c->tmBlo, c->Npad, c->Rpad, c->Ppad, e,
+                                c->d_status, c->num_sms, b->st, c->tune.maximize_raster));
+    c->launches += 1;
+  }
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];
     BTRY(b, c, mixed_resp_pass(c, false));
@@ -2832,11 +2862,23 @@ emc_status emc_batch_iterate(emc_batch* b) {
     maps.b0[i] = maps.b0[0];
     maps.b1[i] = maps.b1[0];
   }
-  if (b->cmp_pair)
+  if (b->n_ct && b->cmp_pair)
     BCK(b, launch_batch_compress_pair_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
-  else
+  else if (b->n_ct)
     BCK(b, launch_batch_compress_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
-  c0->launches += 2;
+  for (int i = 0; i < n; ++i) {
+    if (!b->alone[i]) continue;
+    emc_context* c = b->ctx[i];
+    const CmpEpiArgs e = cmp_args(c);
+    if (c->tune.compress_pair)
+      BCK(b, launch_compress_pair_tc(c->tmPhi, c->tmPlo, c->tmKt128, c->Rpad, c->Ppad, c->Npad, e,
+                                     c->d_status, c->num_sms, b->st, c->tune.compress_raster));
+    else
+      BCK(b, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
+                                c->d_status, c->num_sms, b->st, c->tune.compress_raster));
+    c->launches += 1;
+  }
+  c0->launches += (b->n_mt ? 1 : 0) + (b->n_ct ? 1 : 0);
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];
     c->stage = 3;
@@ -2887,13 +2929,15 @@ emc_status emc_batch_launch(emc_batch* b, int32_t iterations) {
   if (!b || iterations < 0) return EMC_ERR_ARG;
   if (!b->exec) return b->fail(EMC_ERR_STATE, "emc_batch_capture first");
   for (int32_t k = 0; k < iterations; ++k) BCK(b, cudaGraphLaunch(b->exec, b->st));
-  // per dataset: expand, resp pass (5), normalise (4); two batched contractions
-  for (emc_context* c : b->ctx) {
-    c->launches += 10LL * iterations;
+  // per dataset: expand, resp pass (5), normalise (4), and its own two
+  // contractions if it keeps them; the batched contractions
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    emc_context* c = b->ctx[i];
+    c->launches += (b->alone[i] ? 12LL : 10LL) * iterations;
     c->resp_source = 1;
     c->stage = 0;
   }
-  b->ctx[0]->launches += 2LL * iterations;
+  b->ctx[0]->launches += ((b->n_mt ? 1LL : 0LL) + (b->n_ct ? 1LL : 0LL)) * iterations;
   return EMC_OK;
 }
 

@@ -212,8 +212,10 @@ emc_status emc_orientation_stats(emc_context *ctx, int32_t *best_rot, float *bes
  * Up to 8 mixed-precision contexts on one device (each set up with its own
  * geometry, rotations, patterns and model; detector sizes may differ) iterate
  * together: both contractions run as one persistent launch over a tile list
- * spanning every dataset (costliest tiles first), the per-dataset stages
- * between them on one shared stream.  The contexts keep that stream until
+ * spanning the datasets (costliest tiles first), the per-dataset stages
+ * between them on one shared stream.  A dataset whose maximize alone fills
+ * the GPU for eight waves of tiles keeps its own contraction launches in the
+ * same stream and graph.  The contexts keep that stream until
  * emc_batch_destroy; their own calls (get_model, ...) stay ordered with the
  * batch.  emc_batch_capture records one batched iteration into a CUDA graph;
  * emc_batch_launch replays it.  Destroy a batch before its contexts. */

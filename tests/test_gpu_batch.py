@@ -76,6 +76,42 @@ def test_graph_replay_matches_batched_iterations():
             c.close()
 
 
+def test_a_dataset_that_fills_the_gpu_keeps_its_own_launches():
+    """A dataset whose maximize alone fills the persistent grid for eight
+    waves (2,048 patterns x 25,680 rotations: 16 x 101 tiles) runs its own
+    contraction launches inside the batch's graph, the other dataset the
+    batched ones; both end where their separate iterations do."""
+    import emc_b200 as E
+    from emc_b200 import workloads as W
+    ds = [W.make(W.Workload("b32r", 32, 8, 2048, 1000.0, 0.3, 2.0, 1, seed=4)),
+          W.make(W.Workload("b16", 16, 2, 64, 400.0, 0.3, 1.5, 1, seed=1))]
+    solo = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
+    for c in solo:
+        c.set_sparse_compress(False)
+        c.iterate()
+        c.iterate()
+    refs = [(c.get_model(), c.get_scaling()) for c in solo]
+    for c in solo:
+        c.close()
+    ctxs = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
+    try:
+        with E.Batch(ctxs) as b:
+            b.capture()
+            l0, l1 = ctxs[0].launch_count, ctxs[1].launch_count
+            b.launch(2)
+            b.synchronize()
+            # its own two contractions besides its ten stage launches, and
+            # the two batched ones counted on the first context
+            assert ctxs[0].launch_count == l0 + 2 * 14
+            assert ctxs[1].launch_count == l1 + 2 * 10
+            for c, (m, s) in zip(ctxs, refs):
+                assert rel(c.get_model(), m) < 1e-5, rel(c.get_model(), m)
+                assert rel(c.get_scaling(), s) < 1e-5
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_batch_rejects_fp32_contexts():
     import emc_b200 as E
     from emc_b200 import workloads as W
