@@ -517,7 +517,6 @@ def batched_datasets(a, E, W, device, workloads):
         c.set_patterns_sparse(*E.photon_lists(d["counts"]))
         c.set_model(d["model0"])
         c.set_scaling(d["scaling0"])
-        c.set_sparse_compress(False)  # the batched graph runs the dense compress: compare like
         ctxs.append(c)
     evals = sum(c.N * c.R for c in ctxs)
     K = a.batch_steps

@@ -1088,6 +1088,48 @@ static emc_status mixed_resp_pass(emc_context* c, bool allow_lists = true) {
   return EMC_OK;
 }
 
+// The responsibility pass of a batched dataset with lists, in a form a CUDA
+// graph can hold: the count of compacted entries stays on the device, the
+// lists are built from it when it fits the compaction's capacity, and the
+// dense compress operand is written only when it does not (write_kernel
+// gated on the count), so the compress then runs from the lists or, gated
+// the other way, as the dense contraction.  No host wait and no allocation:
+// batch_lists_ready sized every buffer when the batch was made.
+static emc_status gated_list_pass(emc_context* c) {
+  RespArgs a = resp_args(c);
+  c->list_mode = false;
+  CK(c, cudaMemsetAsync(c->d_lcount, 0, sizeof(unsigned long long), c->st));
+  a.list_count = c->d_lcount;
+  a.list_cap = c->lcomp_cap;
+  a.list_rp = c->d_lcomp_rp;
+  a.list_P = c->d_lcomp_P;
+  a.list_min = kListMinP;
+  CK(c, launch_resp_rowsums(a, c->st));
+  CK(c, launch_list_from_compact(a, c->lcomp_cap, kListRel, c->d_lrowtot, c->d_lcursor,
+                                 c->d_lrowoff, c->d_lpat, c->d_lx, c->st, c->d_lcount));
+  a.gate_count = c->d_lcount;
+  a.gate_cap = c->lcomp_cap;
+  CK(c, launch_resp_write(a, c->st));
+  CK(c, launch_sum_f64(c->d_plogp, c->N, c->d_stats + 2, c->st));
+  CK(c, launch_sum_f64(c->d_lse, c->N, c->d_stats + 3, c->st));
+  c->launches += 9;  // combine, row sums, T, count, scan, fill, write, 2 sums
+  return EMC_OK;
+}
+
+// The buffers of gated_list_pass and of the list compress: the compaction
+// (room for at least `entries`), the lists at its capacity and the counts'
+// photon lists.
+static emc_status batch_lists_ready(emc_context* c, int64_t entries) {
+  TRY(list_buffers(c));
+  TRY(compact_capacity(c, entries));
+  TRY(grow(c, &c->d_lpat, c->lcap, c->lcomp_cap + 1));
+  int64_t cap = c->lcap_x;
+  TRY(grow(c, &c->d_lx, cap, c->lcomp_cap + 1));
+  c->lcap_x = cap;
+  if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
+  return EMC_OK;
+}
+
 // The maximize over rotation chunks of y_rows rotations, Y holding one chunk
 // at a time.  Per chunk: the contraction into Y and the chunk's tile
 // partials; the combine over the partials of the chunks so far (the running
@@ -2623,6 +2665,8 @@ struct emc_batch {
   bool pair = false;      // the batched maximize on SM pairs
   bool cmp_pair = false;  // the batched compress on SM pairs
   std::vector<char> alone;  // datasets that keep their own contraction launches
+  std::vector<char> lists;  // datasets whose compress reads responsibility lists
+  std::vector<int64_t> per_iter;  // each dataset's launches in one captured iteration
   MaxEpiArgs* d_max = nullptr;  // per-dataset epilogue arguments (fixed per context)
   CmpEpiArgs* d_cmp = nullptr;
   cudaGraph_t graph = nullptr;
@@ -2703,6 +2747,22 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
   // kAloneWaves waves gains nothing from sharing it: it keeps its own
   // contraction launches (its tuned form and tile order) inside the batch's
   // iteration and graph, and the batched launches cover the others.
+  // Datasets with responsibility lists compress from them (gated_list_pass),
+  // with the dense contraction of their own as the gated fallback; the
+  // batched compress takes the others.
+  for (int32_t i = 0; i < n; ++i) {
+    emc_context* c = ctxs[i];
+    b->lists.push_back(c->tune.compress_sparse && c->npa <= kListMaxPixels ? 1 : 0);
+    if (b->lists.back()) {
+      const emc_status ls = batch_lists_ready(
+          c, c->cand_cap_min > 0 ? c->cand_cap_min : std::max<int64_t>(64 * c->N, 1 << 20));
+      if (ls != EMC_OK) {
+        b->err = c->err;
+        emc_batch_destroy(b);
+        return ls;
+      }
+    }
+  }
   std::vector<int32_t> order;
   for (int32_t i = 0; i < n; ++i) {
     const emc_context* c = ctxs[i];
@@ -2759,6 +2819,7 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
   b->cmp_pair = cwork_pair * 2.0 >= work;
   for (int32_t i : order) {
     const emc_context* c = ctxs[i];
+    if (b->lists[i]) continue;
     if (b->cmp_pair)
       banded(c->Ppad / 256, c->Rpad / 256, c->tune.compress_raster, [&](int64_t nt, int64_t m) {
         ct.push_back(TileDesc{(int32_t)(m * 256), 0, (int32_t)(nt * 256), 0,
@@ -2846,7 +2907,7 @@ emc_status emc_batch_iterate(emc_batch* b) {
   }
   for (int i = 0; i < n; ++i) {
     emc_context* c = b->ctx[i];
-    BTRY(b, c, mixed_resp_pass(c, false));
+    BTRY(b, c, b->lists[i] ? gated_list_pass(c) : mixed_resp_pass(c, false));
     BCK(b, cudaMemcpyAsync(c->d_Tskip, c->d_T, sizeof(float) * c->R, cudaMemcpyDeviceToDevice, b->st));
     c->resp_source = 1;
     c->stage = 2;
@@ -2867,9 +2928,27 @@ emc_status emc_batch_iterate(emc_batch* b) {
   else if (b->n_ct)
     BCK(b, launch_batch_compress_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
   for (int i = 0; i < n; ++i) {
-    if (!b->alone[i]) continue;
+    if (!b->alone[i] && !b->lists[i]) continue;
     emc_context* c = b->ctx[i];
-    const CmpEpiArgs e = cmp_args(c);
+    CmpEpiArgs e = cmp_args(c);
+    if (b->lists[i]) {
+      // from the lists when they fit, else (gated) the dense contraction
+      if (!c->csr.valid) BTRY(b, c, build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
+      ListCmpArgs la{};
+      la.rowoff = c->d_lrowoff;
+      la.pat = c->d_lpat;
+      la.xv = c->d_lx;
+      la.kptr = c->csr.ptr;
+      la.kidx = c->csr.idx;
+      la.kval = c->csr.val;
+      la.e = e;
+      la.gate_count = c->d_lcount;
+      la.gate_cap = c->lcomp_cap;
+      BCK(b, launch_list_compress(la, b->st));
+      e.gate_count = c->d_lcount;
+      e.gate_cap = c->lcomp_cap;
+      c->launches += 1;
+    }
     if (c->tune.compress_pair)
       BCK(b, launch_compress_pair_tc(c->tmPhi, c->tmPlo, c->tmKt128, c->Rpad, c->Ppad, c->Npad, e,
                                      c->d_status, c->num_sms, b->st, c->tune.compress_raster));
@@ -2909,9 +2988,11 @@ emc_status emc_batch_capture(emc_batch* b) {
   const emc_status s = emc_batch_iterate(b);
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(b->st, &g);
+  b->per_iter.assign(b->ctx.size(), 0);
   for (size_t i = 0; i < b->ctx.size(); ++i) {
     b->ctx[i]->prof = prof[i];
-    b->ctx[i]->launches = l0[i];  // captured, not launched
+    b->per_iter[i] = b->ctx[i]->launches - l0[i];  // counted per replay instead
+    b->ctx[i]->launches = l0[i];                    // captured, not launched
   }
   if (s != EMC_OK) {
     if (g) cudaGraphDestroy(g);
@@ -2929,15 +3010,12 @@ emc_status emc_batch_launch(emc_batch* b, int32_t iterations) {
   if (!b || iterations < 0) return EMC_ERR_ARG;
   if (!b->exec) return b->fail(EMC_ERR_STATE, "emc_batch_capture first");
   for (int32_t k = 0; k < iterations; ++k) BCK(b, cudaGraphLaunch(b->exec, b->st));
-  // per dataset: expand, resp pass (5), normalise (4), and its own two
-  // contractions if it keeps them; the batched contractions
   for (size_t i = 0; i < b->ctx.size(); ++i) {
     emc_context* c = b->ctx[i];
-    c->launches += (b->alone[i] ? 12LL : 10LL) * iterations;
+    c->launches += b->per_iter[i] * iterations;
     c->resp_source = 1;
     c->stage = 0;
   }
-  b->ctx[0]->launches += ((b->n_mt ? 1LL : 0LL) + (b->n_ct ? 1LL : 0LL)) * iterations;
   return EMC_OK;
 }
 
@@ -2945,6 +3023,21 @@ emc_status emc_batch_synchronize(emc_batch* b) {
   if (!b) return EMC_ERR_ARG;
   BCK(b, cudaStreamSynchronize(b->st));
   for (emc_context* c : b->ctx) BTRY(b, c, check_status(c));
+  // a dataset whose compacted entries passed the capacity ran the dense
+  // compress (correct, slower): room for them from the next iteration on,
+  // and a recorded graph is recorded again with the new buffers
+  bool grew = false;
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    emc_context* c = b->ctx[i];
+    if (!b->lists[i]) continue;
+    unsigned long long n = 0;
+    BCK(b, cudaMemcpy(&n, c->d_lcount, sizeof(n), cudaMemcpyDeviceToHost));
+    if ((int64_t)n > c->lcomp_cap) {
+      BTRY(b, c, batch_lists_ready(c, (int64_t)n));
+      grew = true;
+    }
+  }
+  if (grew && b->exec) return emc_batch_capture(b);
   return EMC_OK;
 }
 

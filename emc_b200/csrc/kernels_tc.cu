@@ -151,6 +151,21 @@ struct cell_n : std::false_type {};
 template <class E>
 struct cell_n<E, std::void_t<decltype(E::kCellN)>> : std::bool_constant<E::kCellN> {};
 
+// Epilogues whose arguments carry gate_count / gate_cap (CmpEpiArgs) return
+// from the whole launch unless *gate_count > gate_cap; checked before any
+// barrier, TMEM allocation or cluster exchange, so every CTA leaves alike.
+template <class E, class = void>
+struct has_gate : std::false_type {};
+template <class E>
+struct has_gate<E, std::void_t<decltype(std::declval<E>().a.gate_count)>> : std::true_type {};
+template <class Epi>
+__device__ __forceinline__ bool gated_off(const Epi& e) {
+  if constexpr (has_gate<Epi>::value)
+    return e.a.gate_count && *e.a.gate_count <= (unsigned long long)e.a.gate_cap;
+  else
+    return false;
+}
+
 struct Ctl {
   volatile int* abort;
   TcStatus* st;
@@ -197,6 +212,7 @@ __global__ void __launch_bounds__(64 + 32 * Epi::kEpiWarps, 1)
                    const int64_t m_tiles, const int64_t n_tiles, const int64_t k_blocks,
                    const int raster, const Epi epi, TcStatus* status) {
   static_assert(NA * NB == 2, "one hi/lo split per contraction");
+  if (gated_off(epi)) return;
   constexpr bool BMN = b_major_mn<Epi>::value;
   static_assert(!BMN || (NB == 1 && BK == 64 && BN % 64 == 0), "MN-major B: one 64-row operand");
   constexpr uint32_t A_BYTES = BM * BK * 2;
@@ -1040,6 +1056,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * Epi::kEpiW
                    const int64_t n_tiles, const int64_t k_blocks, const int raster,
                    const Epi epi, TcStatus* status) {
   static_assert(NA * NB == 2, "one hi/lo split per contraction");
+  if (gated_off(epi)) return;
   constexpr uint32_t A_BYTES = 128 * kPairBK * 2;   // this CTA's 128 rows of A
   constexpr uint32_t B_BYTES = 128 * kPairBK * 2;   // this CTA's 128 rows (half) of B
   constexpr uint32_t STAGE_BYTES = NA * A_BYTES + NB * B_BYTES;
@@ -1545,6 +1562,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) rowsum_kernel(const RespArgs
 // relative precision instead of underflowing FP16.
 template <bool POISSON>
 __global__ void __launch_bounds__(kSweepThreads, 4) write_kernel(const RespArgs a, int64_t nblk) {
+  if (a.gate_count && *a.gate_count <= (unsigned long long)a.gate_cap) return;
   __shared__ float invT[kSweepRows];
   const int64_t p0 = (int64_t)blockIdx.x * kSweepPatterns + 4 * threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.y * kSweepRows;
@@ -1709,7 +1727,12 @@ template <int STEP>
 __global__ void compact_sort_kernel(const int2* rp, const float* Pv, int64_t n, const float* T,
                                     const float* new_scaling, float rel_min,
                                     unsigned long long* cnt, const int64_t* rowoff, int32_t* pat,
-                                    float* xv) {
+                                    float* xv, const unsigned long long* n_dev) {
+  if (n_dev) {  // the count on the device; above the capacity n the lists stay empty
+    const unsigned long long c = *n_dev;
+    if (c > (unsigned long long)n) return;
+    n = (int64_t)c;
+  }
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int2 v = rp[e];
@@ -1933,6 +1956,7 @@ __global__ void __launch_bounds__(256) list_compress_kernel(const ListCmpArgs a)
   extern __shared__ float Us[];  // [npa]
   const int64_t r = blockIdx.x;
   const CmpEpiArgs& e = a.e;
+  if (a.gate_count && *a.gate_count > (unsigned long long)a.gate_cap) return;
   const float T = e.T[r];
   if (!((e.Tskip ? e.Tskip[r] : T) > 1e-10f) || !(T > 0.0f)) return;  // emc_atomic.cu:128
   for (int64_t j = threadIdx.x; j < e.npa; j += blockDim.x) Us[j] = 0.0f;
@@ -2242,7 +2266,7 @@ cudaError_t launch_list_rowscan(const int64_t* rowtot, int64_t R, int64_t* rowof
 
 cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int64_t* rowtot,
                                      int64_t* cursor, int64_t* rowoff, int32_t* pat, float* xv,
-                                     cudaStream_t st) {
+                                     cudaStream_t st, const unsigned long long* n_dev) {
   const int64_t nblk = resp_list_blocks(a.N);
   finish_T_kernel<<<(unsigned)((a.R + 255) / 256), 256, 0, st>>>(a.Tpart, nblk, a.R, a.T);
   cudaError_t e = cudaMemsetAsync(rowtot, 0, sizeof(int64_t) * a.R, st);
@@ -2251,11 +2275,11 @@ cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int6
   const unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256 + 1, 4096);
   compact_sort_kernel<0><<<g, 256, 0, st>>>(a.list_rp, a.list_P, n, a.T, a.new_scaling, rel_min,
                                             reinterpret_cast<unsigned long long*>(rowtot),
-                                            nullptr, nullptr, nullptr);
+                                            nullptr, nullptr, nullptr, n_dev);
   list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, a.R, rowoff);
   compact_sort_kernel<1><<<g, 256, 0, st>>>(a.list_rp, a.list_P, n, a.T, a.new_scaling, rel_min,
                                             reinterpret_cast<unsigned long long*>(cursor), rowoff,
-                                            pat, xv);
+                                            pat, xv, n_dev);
   return cudaGetLastError();
 }
 
@@ -2282,11 +2306,11 @@ cudaError_t launch_list_from_candidates(RespArgs& a, int64_t n, float rel_min, f
   T_from64_kernel<<<(unsigned)((a.R + 255) / 256), 256, 0, st>>>(T64, a.R, a.T);
   compact_sort_kernel<0><<<g, 256, 0, st>>>(a.list_rp, Pv, n, a.T, a.new_scaling, rel_min,
                                             reinterpret_cast<unsigned long long*>(rowtot),
-                                            nullptr, nullptr, nullptr);
+                                            nullptr, nullptr, nullptr, nullptr);
   list_rowscan_kernel<<<1, 1024, 0, st>>>(rowtot, a.R, rowoff);
   compact_sort_kernel<1><<<g, 256, 0, st>>>(a.list_rp, Pv, n, a.T, a.new_scaling, rel_min,
                                             reinterpret_cast<unsigned long long*>(cursor), rowoff,
-                                            pat, xv);
+                                            pat, xv, nullptr);
   return cudaGetLastError();
 }
 

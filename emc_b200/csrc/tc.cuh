@@ -78,6 +78,10 @@ struct CmpEpiArgs {
   const int32_t* ins;      // [npa] insert flag (mask == 1)
   float2* acc;             // [side^3] interleaved (model, weight) accumulators
   unsigned long long* acc64;  // or, when set, fixed-point limbs [side^3][8] (fixed.cuh)
+  // optional: the launch returns at once unless *gate_count > gate_cap (the
+  // dense form as the fallback of responsibility lists that overflowed)
+  const unsigned long long* gate_count;
+  int64_t gate_cap;
 };
 // raster: rotation tiles per band of the tile order.
 cudaError_t launch_compress_tc(const CUtensorMap& tmPhi, const CUtensorMap& tmPlo,
@@ -221,6 +225,9 @@ struct RespArgs {
   // with the stored y instead of P, and writes no Tpart (nullptr)
   int64_t list_r0;
   int list_store_y;
+  // optional: write_kernel returns at once unless *gate_count > gate_cap
+  const unsigned long long* gate_count;
+  int64_t gate_cap;
 };
 cudaError_t launch_resp_pass(RespArgs& a, cudaStream_t st);
 // The pass in two parts: combine + row sums (partials of T_r), then the
@@ -238,10 +245,13 @@ cudaError_t launch_list_rowscan(const int64_t* rowtot, int64_t R, int64_t* rowof
 // From the entries compacted by launch_resp_rowsums (n of them): T_r, then
 // the lists sorted by rotation with x = P / (T_r phi_new), keeping entries
 // with P >= rel_min T_r (rowtot, cursor: [R] scratch; rowoff [R+1]).  Order
-// within a row is not fixed.
+// within a row is not fixed.  With n_dev the count is read on the device (n
+// is then the capacity; a count above it leaves every list empty), so no host
+// wait is needed, as in a captured graph.
 cudaError_t launch_list_from_compact(RespArgs& a, int64_t n, float rel_min, int64_t* rowtot,
                                      int64_t* cursor, int64_t* rowoff, int32_t* pat, float* xv,
-                                     cudaStream_t st);
+                                     cudaStream_t st,
+                                     const unsigned long long* n_dev = nullptr);
 // After a maximize over rotation chunks (launch_resp_rowsums per chunk with
 // the running lse and list_store_y): P = exp(LL - lse_p) of the n candidates
 // into Pv (their y stay in a.list_P), T_r = sum of P over each rotation's
@@ -305,6 +315,10 @@ struct ListCmpArgs {
   const float* kval;
   CmpEpiArgs e;
   int ordered;  // sum each pixel's terms in list order (deterministic mode)
+  // optional: the launch returns at once if *gate_count > gate_cap (lists
+  // that overflowed their capacity are incomplete)
+  const unsigned long long* gate_count;
+  int64_t gate_cap;
 };
 cudaError_t launch_list_compress(const ListCmpArgs& a, cudaStream_t st);
 // FP32 responsibilities [R][N] from Y and lse (readback / tests).

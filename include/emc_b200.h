@@ -162,7 +162,8 @@ size_t emc_memory_used(const emc_context *ctx);
  * rows: 0 = one chunk of every rotation; -1 = the most rotations whose Y
  * fits in half of what the memory limit and the free device memory leave.
  * capacity: entries the kept-entry arrays start with (0: max(64 N, 2^20));
- * an iteration that keeps more grows them and runs its chunks again.
+ * an iteration that keeps more grows them and runs its chunks again.  In a
+ * batch (rows 0) it is the first capacity of the responsibility lists.
  * emc_set_geometry already chooses chunks (rows -1) when Y and P' of every
  * rotation do not fit.  EMC_ERR_UNSUPPORTED for FP32 contexts and above
  * 51,200 active pixels (the responsibility lists' limit); EMC_ERR_STATE
@@ -215,7 +216,11 @@ emc_status emc_orientation_stats(emc_context *ctx, int32_t *best_rot, float *bes
  * spanning the datasets (costliest tiles first), the per-dataset stages
  * between them on one shared stream.  A dataset whose maximize alone fills
  * the GPU for eight waves of tiles keeps its own contraction launches in the
- * same stream and graph.  The contexts keep that stream until
+ * same stream and graph.  A dataset with responsibility lists
+ * (emc_set_tuning compress_sparse) compresses from them with their count kept
+ * on the device: past their capacity that iteration runs its dense compress
+ * instead, and emc_batch_synchronize gives the lists room (recording a
+ * captured graph again).  The contexts keep that stream until
  * emc_batch_destroy; their own calls (get_model, ...) stay ordered with the
  * batch.  emc_batch_capture records one batched iteration into a CUDA graph;
  * emc_batch_launch replays it.  Destroy a batch before its contexts. */
@@ -226,7 +231,8 @@ emc_status emc_batch_destroy(emc_batch *batch);
 emc_status emc_batch_iterate(emc_batch *batch);
 emc_status emc_batch_capture(emc_batch *batch);
 emc_status emc_batch_launch(emc_batch *batch, int32_t iterations);
-/* Wait for the batch's stream; reports device wait timeouts of its kernels. */
+/* Wait for the batch's stream; reports device wait timeouts of its kernels;
+ * grows the lists of a dataset that overflowed them (see above). */
 emc_status emc_batch_synchronize(emc_batch *batch);
 void *emc_batch_stream(emc_batch *batch);
 const char *emc_batch_last_error(const emc_batch *batch);

@@ -17,14 +17,16 @@ def _datasets():
     return [W.make(w) for w in ws]
 
 
-def test_batched_iteration_matches_separate_iterations():
+@pytest.mark.parametrize("lists", [True, False])
+def test_batched_iteration_matches_separate_iterations(lists):
+    """With responsibility lists each dataset compresses from its own lists
+    (their count kept on the device); without, the batched dense compress
+    contraction covers them all."""
     import emc_b200 as E
     ds = _datasets()
     solo = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
     for c in solo:
-        # a batch runs the dense compress contraction (its iteration is one
-        # graph, which cannot wait for the responsibility lists' size)
-        c.set_sparse_compress(False)
+        c.set_sparse_compress(lists)
         c.iterate()
         c.iterate()
     refs = [(c.get_model(), c.get_scaling()) for c in solo]
@@ -32,6 +34,8 @@ def test_batched_iteration_matches_separate_iterations():
         c.close()
     ctxs = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
     try:
+        for c in ctxs:
+            c.set_sparse_compress(lists)
         with E.Batch(ctxs) as b:
             b.iterate()
             b.iterate()
@@ -47,14 +51,55 @@ def test_batched_iteration_matches_separate_iterations():
             c.close()
 
 
+def test_overflowing_lists_fall_back_and_grow():
+    """Lists started with room for 16 entries overflow in the first
+    iteration: the gated dense compress runs instead, synchronize gives the
+    lists room and records the graph again, and every iteration ends where
+    the separate iterations do."""
+    import emc_b200 as E
+    ds = _datasets()
+    # the same sequence one by one: the dense compress, then lists
+    solo = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
+    refs = []
+    for c in solo:
+        ms = []
+        for k in range(3):
+            c.set_sparse_compress(k > 0)
+            c.iterate()
+            ms.append(c.get_model())
+        refs.append(ms)
+        c.close()
+    ctxs = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
+    try:
+        for c in ctxs:
+            c.set_rotation_chunk(0, 16)
+        with E.Batch(ctxs) as b:
+            b.capture()
+            b.launch(1)      # overflows: the dense compress
+            b.synchronize()  # grows the lists, records the graph again
+            for c, ms in zip(ctxs, refs):
+                assert rel(c.get_model(), ms[0]) < 1e-5, rel(c.get_model(), ms[0])
+            b.launch(1)
+            b.synchronize()
+            b.iterate()
+            b.synchronize()
+            for c, ms in zip(ctxs, refs):
+                assert rel(c.get_model(), ms[2]) < 1e-5, rel(c.get_model(), ms[2])
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_graph_replay_matches_batched_iterations():
     import emc_b200 as E
     ds = _datasets()
     ctxs = [make_ctx(d, "gauss", "nearest", "mixed") for d in ds]
     try:
         with E.Batch(ctxs) as b:
+            l_eager = [c.launch_count for c in ctxs]
             b.iterate()
             b.synchronize()
+            l_eager = [c.launch_count - l for c, l in zip(ctxs, l_eager)]
             after1 = [c.get_model() for c in ctxs]
             for c, d in zip(ctxs, ds):
                 c.set_model(d["model0"])
@@ -64,10 +109,11 @@ def test_graph_replay_matches_batched_iterations():
             b.synchronize()
             for c, m in zip(ctxs, after1):
                 assert rel(c.get_model(), m) < 1e-5
-            l0 = ctxs[0].launch_count
+            l0 = [c.launch_count for c in ctxs]
             b.launch(3)
             b.synchronize()
-            assert ctxs[0].launch_count == l0 + 3 * 12
+            # a replay counts the launches of an eager batched iteration
+            assert [c.launch_count - l for c, l in zip(ctxs, l0)] == [3 * d for d in l_eager]
             for c in ctxs:
                 m = c.get_model()
                 assert np.isfinite(m).all() and abs(m.astype(np.float64).mean() - 1.0) < 1e-4
@@ -87,7 +133,6 @@ def test_a_dataset_that_fills_the_gpu_keeps_its_own_launches():
           W.make(W.Workload("b16", 16, 2, 64, 400.0, 0.3, 1.5, 1, seed=1))]
     solo = [make_ctx(d, "poisson", "nearest", "mixed") for d in ds]
     for c in solo:
-        c.set_sparse_compress(False)
         c.iterate()
         c.iterate()
     refs = [(c.get_model(), c.get_scaling()) for c in solo]
@@ -100,10 +145,10 @@ def test_a_dataset_that_fills_the_gpu_keeps_its_own_launches():
             l0, l1 = ctxs[0].launch_count, ctxs[1].launch_count
             b.launch(2)
             b.synchronize()
-            # its own two contractions besides its ten stage launches, and
-            # the two batched ones counted on the first context
-            assert ctxs[0].launch_count == l0 + 2 * 14
-            assert ctxs[1].launch_count == l1 + 2 * 10
+            # the same launches but for its own maximize and dense compress
+            # (the other dataset's dense compress is its own too: lists), and
+            # the batched maximize counted on the first context
+            assert (ctxs[0].launch_count - l0) - (ctxs[1].launch_count - l1) == 2 * 2
             for c, (m, s) in zip(ctxs, refs):
                 assert rel(c.get_model(), m) < 1e-5, rel(c.get_model(), m)
                 assert rel(c.get_scaling(), s) < 1e-5
@@ -149,13 +194,13 @@ def test_batched_pair_maximize_matches_separate_iterations():
 
 def test_single_dataset_iteration_as_a_graph():
     """The iteration of one dataset captured as one CUDA graph (a batch of
-    one context) and replayed three times, against three eager iterations
-    with the same (dense) compress."""
+    one context) and replayed three times, against three eager iterations;
+    both compress from responsibility lists, the graph's with their count
+    read on the device."""
     import emc_b200 as E
     from emc_b200 import workloads as W
     d = W.make("small32")
     with make_ctx(d, "poisson", "nearest", "mixed") as c:
-        c.set_sparse_compress(False)
         for _ in range(3):
             c.iterate()
         ref_m, ref_s = c.get_model(), c.get_scaling()
