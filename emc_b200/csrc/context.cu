@@ -2694,6 +2694,67 @@ struct emc_batch {
     if (_s != EMC_OK) return (b)->fail(_s, (c)->err); \
   } while (0)
 
+// Dataset i's stages of a batched iteration that are not shared launches.
+// The maximize contraction of a dataset with its own launches.
+static emc_status batch_own_maximize(emc_batch* b, int i) {
+  emc_context* c = b->ctx[i];
+  const MaxEpiArgs e = max_args(c);
+  if (c->tune.maximize_pair)
+    BCK(b, launch_maximize_pair_tc(c->tmKh64, c->tmBhi64, c->tmBlo64, c->Npad, c->Rpad, c->Ppad, e,
+                                   c->d_status, c->num_sms, b->st, c->tune.maximize_raster));
+  else
+    BCK(b, launch_maximize_tc(c->tmKh, c->tmBhi, c->tmBlo, c->Npad, c->Rpad, c->Ppad, e,
+                              c->d_status, c->num_sms, b->st, c->tune.maximize_raster));
+  c->launches += 1;
+  return EMC_OK;
+}
+
+// The responsibility pass (lists gated on their device-side count, or the
+// dense compress operand) and the compress's starting state.
+static emc_status batch_resp(emc_batch* b, int i) {
+  emc_context* c = b->ctx[i];
+  BTRY(b, c, b->lists[i] ? gated_list_pass(c) : mixed_resp_pass(c, false));
+  BCK(b, cudaMemcpyAsync(c->d_Tskip, c->d_T, sizeof(float) * c->R, cudaMemcpyDeviceToDevice,
+                         b->st));
+  c->resp_source = 1;
+  c->stage = 2;
+  BCK(b, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, b->st));
+  return EMC_OK;
+}
+
+// The compress of a dataset outside the batched compress: from its lists
+// when they fit, else (gated on the same count) its dense contraction; or,
+// without lists, its dense contraction.
+static emc_status batch_own_compress(emc_batch* b, int i) {
+  emc_context* c = b->ctx[i];
+  CmpEpiArgs e = cmp_args(c);
+  if (b->lists[i]) {
+    if (!c->csr.valid) BTRY(b, c, build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
+    ListCmpArgs la{};
+    la.rowoff = c->d_lrowoff;
+    la.pat = c->d_lpat;
+    la.xv = c->d_lx;
+    la.kptr = c->csr.ptr;
+    la.kidx = c->csr.idx;
+    la.kval = c->csr.val;
+    la.e = e;
+    la.gate_count = c->d_lcount;
+    la.gate_cap = c->lcomp_cap;
+    BCK(b, launch_list_compress(la, b->st));
+    e.gate_count = c->d_lcount;
+    e.gate_cap = c->lcomp_cap;
+    c->launches += 1;
+  }
+  if (c->tune.compress_pair)
+    BCK(b, launch_compress_pair_tc(c->tmPhi, c->tmPlo, c->tmKt128, c->Rpad, c->Ppad, c->Npad, e,
+                                   c->d_status, c->num_sms, b->st, c->tune.compress_raster));
+  else
+    BCK(b, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
+                              c->d_status, c->num_sms, b->st, c->tune.compress_raster));
+  c->launches += 1;
+  return EMC_OK;
+}
+
 extern "C" {
 
 emc_status emc_batch_destroy(emc_batch* b) {
@@ -2865,6 +2926,28 @@ emc_status emc_batch_iterate(emc_batch* b) {
   if (!b) return EMC_ERR_ARG;
   const int n = (int)b->ctx.size();
   emc_context* c0 = b->ctx[0];
+  for (int i = 0; i < n; ++i)
+    if (b->ctx[i]->stage != 0) return b->fail(EMC_ERR_STATE, "a dataset is between stages");
+  // datasets with their own launches: one whole iteration each, in the order
+  // a dataset iterated alone runs its stages
+  for (int i = 0; i < n; ++i) {
+    if (!b->alone[i]) continue;
+    emc_context* c = b->ctx[i];
+    BTRY(b, c, emc_expand(c));
+    BCK(b, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * c->N,
+                           cudaMemcpyDeviceToDevice, b->st));
+    emc_status s = batch_own_maximize(b, i);
+    if (s == EMC_OK) s = batch_resp(b, i);
+    if (s == EMC_OK) s = batch_own_compress(b, i);
+    if (s != EMC_OK) return s;
+    c->stage = 3;
+    BTRY(b, c, emc_normalize(c));
+  }
+  if (b->n_mt == 0) return EMC_OK;  // no dataset shares the batched launches
+  // the others through the batched launches (unused sets of the tensor-map
+  // parameter repeat the first shared dataset's; no tile indexes them)
+  int first = 0;
+  while (b->alone[first]) ++first;
   TmapSet<kMaxBatch> maps;
   BatchMaxArgs me{};
   BatchCmpArgs ce{};
@@ -2873,92 +2956,50 @@ emc_status emc_batch_iterate(emc_batch* b) {
   ce.tiles = b->d_ct;
   ce.set = b->d_cmp;
   for (int i = 0; i < n; ++i) {
+    if (b->alone[i]) continue;
     emc_context* c = b->ctx[i];
-    if (c->stage != 0) return b->fail(EMC_ERR_STATE, "a dataset is between stages");
     BTRY(b, c, emc_expand(c));
     BCK(b, cudaMemcpyAsync(c->d_scaling_prev, c->d_scaling, sizeof(float) * c->N,
                            cudaMemcpyDeviceToDevice, b->st));
+  }
+  for (int i = 0; i < kMaxBatch; ++i) {
+    const emc_context* c = b->ctx[i < n && !b->alone[i] ? i : first];
     maps.a0[i] = b->pair ? c->tmKh64 : c->tmKh;
     maps.a1[i] = maps.a0[i];
     maps.b0[i] = b->pair ? c->tmBhi64 : c->tmBhi;
     maps.b1[i] = b->pair ? c->tmBlo64 : c->tmBlo;
   }
-  for (int i = n; i < kMaxBatch; ++i) {  // unused sets repeat the first (never indexed)
-    maps.a0[i] = maps.a0[0];
-    maps.a1[i] = maps.a1[0];
-    maps.b0[i] = maps.b0[0];
-    maps.b1[i] = maps.b1[0];
-  }
-  if (b->n_mt && b->pair)
+  if (b->pair)
     BCK(b, launch_batch_maximize_pair_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
-  else if (b->n_mt)
+  else
     BCK(b, launch_batch_maximize_tc(maps, b->n_mt, me, c0->d_status, c0->num_sms, b->st));
+  c0->launches += 1;
   for (int i = 0; i < n; ++i) {
-    if (!b->alone[i]) continue;
-    emc_context* c = b->ctx[i];
-    const MaxEpiArgs e = max_args(c);
-    if (c->tune.maximize_pair)
-      BCK(b, launch_maximize_pair_tc(c->tmKh64, c->tmBhi64, c->tmBlo64, c->Npad, c->Rpad, c->Ppad,
-                                     e, c->d_status, c->num_sms, b->st, c->tune.maximize_raster));
-    else
-      BCK(b, launch_maximize_tc(c->tmKh, c->tmBhi, c->tmBlo, c->Npad, c->Rpad, c->Ppad, e,
-                                c->d_status, c->num_sms, b->st, c->tune.maximize_raster));
-    c->launches += 1;
+    if (b->alone[i]) continue;
+    const emc_status s = batch_resp(b, i);
+    if (s != EMC_OK) return s;
   }
-  for (int i = 0; i < n; ++i) {
-    emc_context* c = b->ctx[i];
-    BTRY(b, c, b->lists[i] ? gated_list_pass(c) : mixed_resp_pass(c, false));
-    BCK(b, cudaMemcpyAsync(c->d_Tskip, c->d_T, sizeof(float) * c->R, cudaMemcpyDeviceToDevice, b->st));
-    c->resp_source = 1;
-    c->stage = 2;
-    BCK(b, cudaMemsetAsync(c->d_acc, 0, sizeof(float2) * c->M, b->st));
-    maps.a0[i] = c->tmPhi;
-    maps.a1[i] = c->tmPlo;
-    maps.b0[i] = b->cmp_pair ? c->tmKt128 : c->tmKt;
-    maps.b1[i] = maps.b0[i];
-  }
-  for (int i = n; i < kMaxBatch; ++i) {
-    maps.a0[i] = maps.a0[0];
-    maps.a1[i] = maps.a1[0];
-    maps.b0[i] = maps.b0[0];
-    maps.b1[i] = maps.b1[0];
-  }
-  if (b->n_ct && b->cmp_pair)
-    BCK(b, launch_batch_compress_pair_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
-  else if (b->n_ct)
-    BCK(b, launch_batch_compress_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
-  for (int i = 0; i < n; ++i) {
-    if (!b->alone[i] && !b->lists[i]) continue;
-    emc_context* c = b->ctx[i];
-    CmpEpiArgs e = cmp_args(c);
-    if (b->lists[i]) {
-      // from the lists when they fit, else (gated) the dense contraction
-      if (!c->csr.valid) BTRY(b, c, build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
-      ListCmpArgs la{};
-      la.rowoff = c->d_lrowoff;
-      la.pat = c->d_lpat;
-      la.xv = c->d_lx;
-      la.kptr = c->csr.ptr;
-      la.kidx = c->csr.idx;
-      la.kval = c->csr.val;
-      la.e = e;
-      la.gate_count = c->d_lcount;
-      la.gate_cap = c->lcomp_cap;
-      BCK(b, launch_list_compress(la, b->st));
-      e.gate_count = c->d_lcount;
-      e.gate_cap = c->lcomp_cap;
-      c->launches += 1;
+  if (b->n_ct) {
+    for (int i = 0; i < kMaxBatch; ++i) {
+      const emc_context* c = b->ctx[i < n && !b->alone[i] ? i : first];
+      maps.a0[i] = c->tmPhi;
+      maps.a1[i] = c->tmPlo;
+      maps.b0[i] = b->cmp_pair ? c->tmKt128 : c->tmKt;
+      maps.b1[i] = maps.b0[i];
     }
-    if (c->tune.compress_pair)
-      BCK(b, launch_compress_pair_tc(c->tmPhi, c->tmPlo, c->tmKt128, c->Rpad, c->Ppad, c->Npad, e,
-                                     c->d_status, c->num_sms, b->st, c->tune.compress_raster));
+    if (b->cmp_pair)
+      BCK(b, launch_batch_compress_pair_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
     else
-      BCK(b, launch_compress_tc(c->tmPhi, c->tmPlo, c->tmKt, c->Rpad, c->Ppad, c->Npad, e,
-                                c->d_status, c->num_sms, b->st, c->tune.compress_raster));
-    c->launches += 1;
+      BCK(b, launch_batch_compress_tc(maps, b->n_ct, ce, c0->d_status, c0->num_sms, b->st));
+    c0->launches += 1;
   }
-  c0->launches += (b->n_mt ? 1 : 0) + (b->n_ct ? 1 : 0);
   for (int i = 0; i < n; ++i) {
+    if (b->alone[i] || !b->lists[i]) continue;
+    const emc_status s = batch_own_compress(b, i);
+    if (s != EMC_OK) return s;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (b->alone[i]) continue;
     emc_context* c = b->ctx[i];
     c->stage = 3;
     BTRY(b, c, emc_normalize(c));

@@ -1561,17 +1561,17 @@ __global__ void __launch_bounds__(kSweepThreads, 4) rowsum_kernel(const RespArgs
 // keeps every entry in [0, c0/phi_p], so rotations with a tiny T_r keep their
 // relative precision instead of underflowing FP16.
 template <bool POISSON>
-__global__ void __launch_bounds__(kSweepThreads, 4) write_kernel(const RespArgs a, int64_t nblk) {
-  if (a.gate_count && *a.gate_count <= (unsigned long long)a.gate_cap) return;
-  __shared__ float invT[kSweepRows];
-  const int64_t p0 = (int64_t)blockIdx.x * kSweepPatterns + 4 * threadIdx.x;
-  const int64_t r0 = (int64_t)blockIdx.y * kSweepRows;
+__device__ __forceinline__ void write_tile(const RespArgs& a, int64_t nblk, int64_t bx,
+                                           int64_t by, float* invT) {
+  const int64_t p0 = bx * kSweepPatterns + 4 * threadIdx.x;
+  const int64_t r0 = by * kSweepRows;
+  __syncthreads();  // the previous tile's invT is read
   if (threadIdx.x < kSweepRows) {
     const int64_t r = r0 + threadIdx.x;
     double T = 0.0;
     if (r < a.R) {
       for (int64_t b = 0; b < nblk; ++b) T += a.Tpart[b * a.R + r];
-      if (blockIdx.x == 0) a.T[r] = (float)T;
+      if (bx == 0) a.T[r] = (float)T;
     }
     // P <= T, so P / T stays finite; the insertion decides which rows count
     invT[threadIdx.x] = T > 1e-30 ? (float)(1.0 / T) : 0.0f;
@@ -1622,6 +1622,21 @@ __global__ void __launch_bounds__(kSweepThreads, 4) write_kernel(const RespArgs 
         if (k.ok[j]) a.P32[r * a.N + p0 + j] = P[j];
     }
     }
+  }
+}
+
+// Tiles of kSweepPatterns columns x kSweepRows rows, tile t = (t % wblk, t /
+// wblk); a block takes tiles blockIdx.x, + gridDim.x, ...  Launched one tile
+// per block, or, gated, on a small grid (a launch whose gate stays closed
+// then costs a few thousand empty blocks, not one per tile).
+template <bool POISSON>
+__global__ void __launch_bounds__(kSweepThreads, 4) write_kernel(const RespArgs a, int64_t nblk,
+                                                                 int64_t wblk, int64_t ntiles) {
+  if (a.gate_count && *a.gate_count <= (unsigned long long)a.gate_cap) return;
+  __shared__ float invT[kSweepRows];
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t bx = t % wblk, by = t / wblk;
+    write_tile<POISSON>(a, nblk, bx, by, invT);
   }
 }
 
@@ -2244,10 +2259,12 @@ cudaError_t launch_resp_write(RespArgs& a, cudaStream_t st) {
   const int64_t nblk = (a.N + kSweepPatterns - 1) / kSweepPatterns;
   const int64_t rblk = (a.R + kSweepRows - 1) / kSweepRows;
   const int64_t wblk = (a.ldP + kSweepPatterns - 1) / kSweepPatterns;
+  const int64_t ntiles = wblk * rblk;
+  const unsigned grid = (unsigned)(a.gate_count ? std::min<int64_t>(ntiles, 2048) : ntiles);
   if (a.poisson)
-    write_kernel<true><<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
+    write_kernel<true><<<grid, kSweepThreads, 0, st>>>(a, nblk, wblk, ntiles);
   else
-    write_kernel<false><<<dim3((unsigned)wblk, (unsigned)rblk), kSweepThreads, 0, st>>>(a, nblk);
+    write_kernel<false><<<grid, kSweepThreads, 0, st>>>(a, nblk, wblk, ntiles);
   return cudaGetLastError();
 }
 
