@@ -2307,6 +2307,23 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
       gpair[q] = (int32_t)p;
       ppos[p * m + i] = q;
     }
+  // tcgen05 grouped contractions: mixed precision, cells of at most 256 rotations
+  const bool tc = c->mixed && c->max_members <= 256 && S > 0 && (S + 31) / 32 <= 65535;
+  TRY(grow(c, &c->d_gpair, c->slots_cap, S));
+  CK(c, cudaMemcpyAsync(c->d_gpair, gpair, sizeof(int32_t) * S, cudaMemcpyHostToDevice, c->st));
+  if (tc) {
+    // the slot rows change no state, so they go ahead of the audit's verdict
+    // and keep the GPU busy while the host waits for it
+    TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
+    if (slot_rows_fit(c->Ppad)) {
+      // the slot rows from the photon lists (writes the rows, reads the lists)
+      if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
+      CK(c, launch_slot_rows(c->csr.ptr, c->csr.idx, c->csr.val, c->Ppad, c->d_gpair, S, c->d_Kg,
+                             c->st));
+    } else {
+      CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->st));
+    }
+  }
   // the audited patterns' captured responsibility decides between the
   // grouped stages and the dense iteration
   if (n_aud > 0) {
@@ -2321,10 +2338,7 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     st.audit_min_captured = cmin;
     if (cmin < pl.min_captured) return dense_instead();
   }
-  // tcgen05 grouped contractions: mixed precision, cells of at most 256 rotations
-  const bool tc = c->mixed && c->max_members <= 256 && S > 0 && (S + 31) / 32 <= 65535;
   const int64_t MM = tc ? 256 : c->max_members;
-  TRY(grow(c, &c->d_gpair, c->slots_cap, S));
   TRY(grow(c, &c->d_Yc, c->yc_cap, S * MM));
   // compress from responsibility lists (as the dense mixed iteration does);
   // the grouped compresses read the per-cell operand Pt instead
@@ -2360,7 +2374,6 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     }
     TRY(grow(c, &c->d_gmt, c->gmt_cap, n_gmt));
     TRY(grow(c, &c->d_gct, c->gct_cap, n_gct));
-    TRY(grow(c, &c->d_Kg, c->kg_cap, S * c->Ppad));
     if (!lists && kw > c->a_ld) {
       for (__half** q : {&c->d_Ahi, &c->d_Alo})
         if (*q) {
@@ -2389,7 +2402,6 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     CK(c, cudaMemcpyAsync(c->d_mtiles, mt.data(), sizeof(int4) * mt.size(), cudaMemcpyHostToDevice, c->st));
     CK(c, cudaMemcpyAsync(c->d_ctiles, ct.data(), sizeof(int4) * ct.size(), cudaMemcpyHostToDevice, c->st));
   }
-  CK(c, cudaMemcpyAsync(c->d_gpair, gpair, sizeof(int32_t) * S, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_ppos, ppos, sizeof(int64_t) * pairs, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_gbeg, gbeg.data(), sizeof(int64_t) * n_cells, cudaMemcpyHostToDevice, c->st));
   CK(c, cudaMemcpyAsync(c->d_gcnt, gcnt.data(), sizeof(int32_t) * n_cells, cudaMemcpyHostToDevice, c->st));
@@ -2452,14 +2464,6 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
     CUtensorMap tmKg, tmKg64, tmAhi, tmAlo;
     if (!tc_encode_2d(&tmKg, c->d_Kg, c->Ppad, S, 128, gpair_form ? kPairBoxK : kMaximizeBK))
       return c->fail(EMC_ERR_CUDA, "tensor map encoding failed");
-    if (slot_rows_fit(c->Ppad)) {
-      // the slot rows from the photon lists (writes the rows, reads the lists)
-      if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
-      CK(c, launch_slot_rows(c->csr.ptr, c->csr.idx, c->csr.val, c->Ppad, c->d_gpair, S, c->d_Kg,
-                             c->st));
-    } else {
-      CK(c, launch_gather_slots(c->d_Kh, c->Ppad, c->d_gpair, S, c->d_Kg, c->st));
-    }
     if (!lists &&
         (!tc_encode_2d(&tmKg64, c->d_Kg, c->Ppad, S, kCompressBK, 64) ||
          !tc_encode_2d_strided(&tmAhi, c->d_Ahi, c->a_ld, R, c->a_ld, 128, kCompressBK) ||
@@ -2490,17 +2494,14 @@ static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select se
         TRY(c->alloc(&c->d_lrowoff, R + 1));
       }
       if (!c->d_lcursor) TRY(c->alloc(&c->d_lcursor, R));
+      // a list entry is an evaluated (rotation, pattern) pair: `evals` bounds
+      // their number, so the lists need no count from the device
+      TRY(grow(c, &c->d_lpat, c->lcap, evals + 1));
+      int64_t cap = c->lcap_x;
+      TRY(grow(c, &c->d_lx, cap, evals + 1));
+      c->lcap_x = cap;
       CK(c, launch_group_list_count(g, kListRel, c->d_lrowtot, c->st));
       CK(c, launch_list_rowscan(c->d_lrowtot, R, c->d_lrowoff, c->st));
-      int64_t* hn = c->pinned<int64_t>(7, 1);
-      if (!hn) return c->fail(EMC_ERR_OOM, "pinned host staging");
-      CK(c, cudaMemcpyAsync(hn, c->d_lrowoff + R, sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
-      CK(c, cudaStreamSynchronize(c->st));
-      c->list_nnz = *hn;
-      TRY(grow(c, &c->d_lpat, c->lcap, c->list_nnz + 1));
-      int64_t cap = c->lcap_x;
-      TRY(grow(c, &c->d_lx, cap, c->list_nnz + 1));
-      c->lcap_x = cap;
       CK(c, launch_group_list_fill(g, kListRel, c->d_lcursor, c->d_lrowoff, c->d_lpat, c->d_lx,
                                    c->st));
       if (!c->csr.valid) TRY(build_rows(c, c->d_K, c->N, c->npa, c->csr, false));
