@@ -299,8 +299,7 @@ def config_desc(a, d):
     return {"workload": f"{w.name}: {w.side}^3 model, {w.side}x{w.side} detector "
                         f"(beamstop r={w.beamstop:g}, {npa} active px), {R} rotations, {N} patterns, "
                         f"{a.likelihood} likelihood, {a.interp} interpolation",
-            "precision": a.precision, "patterns": N, "rotations": R, "active_pixels": npa,
-            "l2": "inputs larger than L2"} | (
+            "precision": a.precision, "l2": "inputs larger than L2"} | (
         {"rotation_chunk": a.rotation_chunk} if getattr(a, "rotation_chunk", 0) else {}) | (
         {"insertion": "deterministic"} if getattr(a, "deterministic", False) else {})
 
