@@ -1424,6 +1424,7 @@ constexpr int kSweepPatterns = 4 * kSweepThreads;
 template <bool POISSON>
 struct PatConst {
   double lse[4];
+  float lse_hi[4], lse_lo[4];  // poisson: lse = hi + lo, hi = lse rounded to FP32
   double c1[4], c0[4];  // gaussian only
   bool ok[4];
 };
@@ -1435,6 +1436,8 @@ __device__ __forceinline__ void load_consts(const RespArgs& a, int64_t p0, PatCo
     const int64_t p = p0 + i;
     k.ok[i] = p < a.N;
     k.lse[i] = k.ok[i] ? a.lse[p] : 0.0;
+    k.lse_hi[i] = (float)k.lse[i];
+    k.lse_lo[i] = (float)(k.lse[i] - (double)k.lse_hi[i]);
     if constexpr (!POISSON) {
       const LLFromY f = make_llf(a, p);
       k.c1[i] = f.c1;
@@ -1443,19 +1446,24 @@ __device__ __forceinline__ void load_consts(const RespArgs& a, int64_t p0, PatCo
   }
 }
 
-// P = exp(LL - lse): the difference in FP64 (LL and lse are ~1e4), exp in FP32.
+// P = exp(LL - lse), exp in FP32.  LL and lse are ~1e4, so the difference
+// needs more than FP32: gaussian, in FP64; poisson (LL = y, an FP32 value),
+// as (y - hi) - lo with lse = hi + lo split into FP32 parts: y - hi is exact
+// whenever y lies within a factor of two of hi (Sterbenz), which holds for
+// every entry that does not underflow, and the one rounding left is the
+// one the FP64 difference gets when it is rounded to FP32.
 template <bool POISSON>
 __device__ __forceinline__ void probs_from(const PatConst<POISSON>& k, float4 y, double rs,
                                            float (&P)[4]) {
   const float yy[4] = {y.x, y.y, y.z, y.w};
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    double ll;
+    float d;
     if constexpr (POISSON)
-      ll = (double)yy[i];
+      d = __fsub_rn(__fsub_rn(yy[i], k.lse_hi[i]), k.lse_lo[i]);
     else
-      ll = fma((double)yy[i], k.c1[i], k.c0[i] - rs);
-    P[i] = k.ok[i] ? expf((float)(ll - k.lse[i])) : 0.0f;
+      d = (float)(fma((double)yy[i], k.c1[i], k.c0[i] - rs) - k.lse[i]);
+    P[i] = k.ok[i] ? expf(d) : 0.0f;
   }
 }
 
