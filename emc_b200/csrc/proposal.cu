@@ -415,7 +415,8 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
     const int64_t q = g.ppos[p * g.m + i];
     for (int k = lane; k < g.mcnt[c]; k += 32) {
       const double l = ll_of(c, q, k);
-      const double e = exp(l - mx);
+      // the difference in FP64, exp in FP32 (relative error ~1e-7), sums in FP64
+      const double e = (double)expf((float)(l - mx));
       s += e;
       d += e * (g.poisson ? g.rowstat[g.mbeg[c] + k] : (double)g.Y[q * g.MM + k]);
       pl += e * (l - mx);
@@ -454,12 +455,12 @@ __global__ void group_softmax_kernel(const GroupArgs g) {
     double crel = 0.0;
     for (int k = lane; k < g.mcnt[c]; k += 32) {
       const double l = ll_of(c, q, k);
-      const float P = (float)exp(l - lse);
+      const float P = expf((float)(l - lse));
       if (g.Pt) g.Pt[g.goff[c] + (int64_t)k * g.gcnt[c] + col] = (float)(P / phi_new);
       // most candidates of a sharp posterior underflow: no atomic for those
       if (P != 0.0f) atomicAdd(g.T + g.mbeg[c] + k, P);
       cm += P;
-      if (g.lcmass) crel += exp(l - cmx);
+      if (g.lcmass) crel += (double)expf((float)(l - cmx));
     }
     for (int o = 16; o > 0; o >>= 1) {
       cm += __shfl_xor_sync(0xffffffffu, cm, o);
