@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256) audit_kernel(const AuditArgs a) {
   __syncthreads();
   double s = 0.0, in = 0.0;
   for (int64_t r = t; r < a.R; r += blockDim.x) {
-    const double e = exp(ll_of(r) - mx);
+    const double e = (double)expf((float)(ll_of(r) - mx));
     s += e;
     const int c = a.cell[r];
     if ((mask[c >> 5] >> (c & 31)) & 1u) in += e;
@@ -502,7 +502,7 @@ __global__ void group_list_kernel(const GroupArgs g, float theta, unsigned long 
       if (!(T > 0.0f)) continue;
       const double y = (double)g.Y[q * g.MM + k];
       const double l = g.poisson ? y : fma(y, c1, c0 - g.rowstat[r] * g.gauss_inv);
-      const float P = (float)exp(l - lse);
+      const float P = expf((float)(l - lse));  // as group_softmax_kernel forms it
       if (!(P >= theta * T)) continue;
       const float x = P / T * inv_phi;
       if (FILL == 0) {
