@@ -816,9 +816,17 @@ def main():
 
     batch = None
     if rank == 0 and world == 1 and not a.no_batch and a.precision == "mixed":
-        batch = {"large": batched_datasets(a, E, W, local, W.BATCH6),
-                 "large_with_headline": batched_datasets(a, E, W, local, W.BATCH6, extra=d),
-                 "small": batched_datasets(a, E, W, local, W.BATCH6_SMALL)}
+        def batch_case(*args, **kw):
+            # a side measurement: its failure (say, device memory taken by
+            # another process) is reported in its place, not the whole line lost
+            try:
+                return batched_datasets(a, E, W, local, *args, **kw)
+            except (E.EmcError, RuntimeError, MemoryError) as ex:
+                torch.cuda.synchronize()
+                return {"unavailable": str(ex)[:120]}
+        batch = {"large": batch_case(W.BATCH6),
+                 "large_with_headline": batch_case(W.BATCH6, extra=d),
+                 "small": batch_case(W.BATCH6_SMALL)}
 
     fp32 = None
     if rank == 0 and world == 1 and not a.no_fp32 and a.precision == "mixed":
