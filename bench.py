@@ -507,54 +507,56 @@ def batched_datasets(a, E, W, device, workloads, extra=None):
     a CUDA graph and replayed."""
     import torch
     data = [W.make(w) for w in workloads] + ([extra] if extra is not None else [])
-    ctxs = []
-    for d in data:
-        w = d["workload"]
-        c = E.Context(w.side, d["counts"].shape[0], d["q"].shape[0], likelihood=a.likelihood,
-                      interp=a.interp, precision="mixed", device=device)
-        c.set_geometry(d["x"], d["y"], d["z"], d["mask"])
-        c.set_rotations(d["q"], d["w"])
-        c.set_patterns_sparse(*E.photon_lists(d["counts"]))
-        c.set_model(d["model0"])
-        c.set_scaling(d["scaling0"])
-        ctxs.append(c)
-    evals = sum(c.N * c.R for c in ctxs)
-    K = a.batch_steps
+    ctxs, b = [], None
+    try:
+        for d in data:
+            w = d["workload"]
+            c = E.Context(w.side, d["counts"].shape[0], d["q"].shape[0], likelihood=a.likelihood,
+                          interp=a.interp, precision="mixed", device=device)
+            ctxs.append(c)
+            c.set_geometry(d["x"], d["y"], d["z"], d["mask"])
+            c.set_rotations(d["q"], d["w"])
+            c.set_patterns_sparse(*E.photon_lists(d["counts"]))
+            c.set_model(d["model0"])
+            c.set_scaling(d["scaling0"])
+        K = a.batch_steps
 
-    def device_ms(stream, fn):
-        ext = torch.cuda.ExternalStream(stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        with torch.cuda.stream(ext):
-            e0.record()
-        fn()
-        with torch.cuda.stream(ext):
-            e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
+        def device_ms(stream, fn):
+            ext = torch.cuda.ExternalStream(stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(ext):
+                e0.record()
+            fn()
+            with torch.cuda.stream(ext):
+                e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1)
 
-    # (1) one after the other (each context on its own stream, serialised),
-    # after the three warm-up iterations the graph below also gets (an early
-    # iteration whose responsibility lists outgrow their first capacity runs
-    # the dense compress once and is not the steady state)
-    for c in ctxs:
-        for _ in range(3):
-            c.iterate(stats=False)
-    sep = 0.0
-    for c in ctxs:
-        sep += device_ms(c.stream, lambda c=c: [c.iterate(stats=False) for _ in range(K)]) / K
-    # (2) one batch, CUDA graph
-    b = E.Batch(ctxs)
-    b.iterate()
-    b.capture()
-    b.launch(2)
-    b.synchronize()
-    ms = device_ms(b.stream, lambda: b.launch(K)) / K
-    b.synchronize()
-    ok = all(np.isfinite(c.get_model()).all() for c in ctxs)
-    b.close()
-    for c in ctxs:
-        c.close()
+        # (1) one after the other (each context on its own stream, serialised),
+        # after the three warm-up iterations the graph below also gets (an early
+        # iteration whose responsibility lists outgrow their first capacity runs
+        # the dense compress once and is not the steady state)
+        for c in ctxs:
+            for _ in range(3):
+                c.iterate(stats=False)
+        sep = 0.0
+        for c in ctxs:
+            sep += device_ms(c.stream, lambda c=c: [c.iterate(stats=False) for _ in range(K)]) / K
+        # (2) one batch, CUDA graph
+        b = E.Batch(ctxs)
+        b.iterate()
+        b.capture()
+        b.launch(2)
+        b.synchronize()
+        ms = device_ms(b.stream, lambda: b.launch(K)) / K
+        b.synchronize()
+        ok = all(np.isfinite(c.get_model()).all() for c in ctxs)
+    finally:
+        if b is not None:
+            b.close()
+        for c in ctxs:
+            c.close()
     assert ok, "batched iteration gave a non-finite model"
     return {"separate_ms": round(sep, 2), "graph_ms": round(ms, 2), "speedup": round(sep / ms, 3)}
 
