@@ -2,6 +2,7 @@
 // in the order of the reference's main loop (emc.c:989-1084).
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -16,6 +17,18 @@
 #include "proposal.cuh"
 #include "tc.cuh"
 #include "tile.cuh"
+
+namespace {
+// An NVTX range over one stage of an iteration (nsys and ncu show the stages
+// by name; without a profiler attached the calls do nothing), closed on every
+// return path.
+struct StageRange {
+  explicit StageRange(const char* name) { nvtxRangePushA(name); }
+  ~StageRange() { nvtxRangePop(); }
+  StageRange(const StageRange&) = delete;
+  StageRange& operator=(const StageRange&) = delete;
+};
+}  // namespace
 
 using namespace emc;
 
@@ -862,6 +875,7 @@ static double gauss_inv(const emc_context* c) {
 }
 
 emc_status emc_expand(emc_context* c) {
+  StageRange range("emc expand");
   if (!c) return EMC_ERR_ARG;
   if (!c->have_geom || !c->have_rot || !c->have_pat || !c->have_model)
     return c->fail(EMC_ERR_STATE, "geometry, rotations, patterns and model must be set first");
@@ -1327,6 +1341,7 @@ static emc_status sparse_slicesums(emc_context* c) {
 extern "C" {
 
 emc_status emc_maximize(emc_context* c) {
+  StageRange range("emc maximize");
   if (!c) return EMC_ERR_ARG;
   if (c->stage != 1) return c->fail(EMC_ERR_STATE, "maximize called before expand");
   const int64_t R = c->R, N = c->N;
@@ -1404,6 +1419,7 @@ emc_status emc_maximize(emc_context* c) {
 }
 
 emc_status emc_compress_insert(emc_context* c) {
+  StageRange range("emc compress");
   if (!c) return EMC_ERR_ARG;
   if (c->stage != 2) return c->fail(EMC_ERR_STATE, "compress called before maximize");
   // emc.c:1025-1026 reset, then emc_cuda.cu:292-362 insert, :414-433 normalise
@@ -1493,6 +1509,7 @@ emc_status emc_compress_insert(emc_context* c) {
 }
 
 emc_status emc_normalize(emc_context* c) {
+  StageRange range("emc normalize");
   if (!c) return EMC_ERR_ARG;
   if (c->stage != 3) return c->fail(EMC_ERR_STATE, "normalize called before compress_insert");
   if (!c->mixed)
@@ -2204,6 +2221,7 @@ static emc_status run_audit(emc_context* c, int32_t n_aud, int32_t m, float** ho
 template <class Select>
 static emc_status run_proposed(emc_context* c, const ProposedPlan& pl, Select select,
                                emc_proposal_stats* stats) {
+  StageRange range("emc proposed iteration");
   const int32_t m = pl.m;
   const int64_t N = c->N, R = c->R, pairs = N * m;
   if (!c->d_mass) {
@@ -2924,6 +2942,7 @@ emc_status emc_batch_create(emc_context* const* ctxs, int32_t n, emc_batch** out
 }
 
 emc_status emc_batch_iterate(emc_batch* b) {
+  StageRange range("emc batch iteration");
   if (!b) return EMC_ERR_ARG;
   const int n = (int)b->ctx.size();
   emc_context* c0 = b->ctx[0];

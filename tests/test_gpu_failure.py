@@ -137,3 +137,28 @@ def test_checkpoint_resume_continues_the_run(tiny, tmp_path, prec):
         with pytest.raises(E.EmcError) as ei:
             c.load_state(path)
         assert ei.value.status == ERR_RANGE
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_checkpoint_resume_is_bitwise_in_deterministic_mode(tiny, tmp_path, prec):
+    """With the order-independent insertion sums, a run resumed from its
+    checkpoint ends bitwise where the uninterrupted run does."""
+    import emc_b200 as E
+    d = tiny
+    path = os.path.join(tmp_path, "state_det.bin")
+    with make_ctx(d, "poisson", precision=prec) as a:
+        a.set_deterministic(True)
+        a.iterate()
+        a.iterate()
+        a.save_state(path, iteration=2)
+        a.iterate()
+        a.iterate()
+        m4, s4, w4 = a.get_model(), a.get_scaling(), a.get_buffer(E.BUF_WEIGHT)
+    with make_ctx(d, "poisson", precision=prec) as b:
+        b.set_deterministic(True)
+        assert b.load_state(path) == 2
+        b.iterate()
+        b.iterate()
+        np.testing.assert_array_equal(b.get_model(), m4)
+        np.testing.assert_array_equal(b.get_scaling(), s4)
+        np.testing.assert_array_equal(b.get_buffer(E.BUF_WEIGHT), w4)
