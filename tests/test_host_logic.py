@@ -54,3 +54,30 @@ def test_pattern_shards_cut_one_seeded_sequence():
     for k in ("mask", "q", "w", "model0", "true_model"):
         np.testing.assert_array_equal(a[k], whole[k])
         np.testing.assert_array_equal(b[k], whole[k])
+
+
+def test_metrics_log_appends_one_record_per_iteration(tmp_path):
+    import json
+
+    from emc_b200.diagnostics import MetricsLog
+
+    class FakeContext:  # what MetricsLog reads of a context
+        N, R = 4, 10
+
+        def get_scaling(self):
+            return np.array([0.5, 1.0, 1.5, 2.0], np.float32)
+
+    log = MetricsLog(str(tmp_path))
+    stats = {"sum_plogp": -12.5, "total_loglik": -1.25e4, "model_max": 3.0, "total_resp": 4.0}
+    log.record(1, FakeContext(), stats, seconds=0.5, stages_ms=[1, 2, 3, 4, 5],
+               errors={"model_rel_err": 1e-5})
+    log.record(2, FakeContext(), stats)
+    lines = open(tmp_path / "metrics.jsonl").read().splitlines()
+    assert len(lines) == 2
+    a, b = (json.loads(x) for x in lines)
+    assert a["iteration"] == 1 and b["iteration"] == 2
+    assert a["total_loglik"] == -1.25e4 and a["sum_plogp"] == -12.5
+    assert a["scaling"] == {"mean": 1.25, "min": 0.5, "max": 2.0}
+    assert a["evals_per_s"] == 80.0 and a["stages_ms"] == [1, 2, 3, 4, 5]
+    assert a["errors"] == {"model_rel_err": 1e-5}
+    assert "evals_per_s" not in b and "stages_ms" not in b
