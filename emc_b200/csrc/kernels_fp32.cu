@@ -252,7 +252,7 @@ struct OpLL {
     const float k = __ldg(p.K + n * p.ldK + col_of(p.pix, j));
     return p.poisson ? k : k / __ldg(p.scaling + n);  // gaussian: image / scaling (emc_cuda.cu:121)
   }
-  static __device__ __forceinline__ float inner(float acc, float a, float b);
+  // inner(acc, a, b): each likelihood's own term, in OpLLGauss / OpLLPoisson
   __device__ void epilogue(double (&acc)[8][4], int64_t r0, int64_t n0, float*) const {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {

@@ -1349,12 +1349,6 @@ cudaError_t run_pair(const TmapSet<Epi::kSets>& maps, int64_t m_tiles, int64_t n
 
 // ------------------------------------------------------ responsibility pass --
 
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
 // Per pattern: lse_p, the new scaling and sum P log P from the tile partials.
 //   lse = M + log sum_k s_k e^(m_k - M)
 //   D   = sum_k d_k e^(m_k - lse)                       (= sum_r P_rp X_rp)
